@@ -1,0 +1,172 @@
+/*
+ * rgpu.h -- C ABI of the B200 Godunov level step (librgpu.so).
+ *
+ * The library replaces the CPU hydro hot path of RAMSES-CPP,
+ * HydroSolver::godunov_fine(ilevel, dt, dx) and the calls around it in
+ * Simulation::amr_step, for a host application that keeps owning its AmrGrid.
+ * Every entry point takes plain pointers and sizes; no C++ or torch type
+ * crosses the boundary.  Every function that can fail returns an int status
+ * (RG_OK == 0, negative on error) and never throws or aborts; the message of
+ * the last failure is returned by rg_last_error().
+ *
+ * Reference interfaces replaced (paths relative to the RAMSES-CPP tree):
+ *   include/ramses/solvers/hydro/HydroSolver.hpp:19   godunov_fine
+ *   include/ramses/solvers/hydro/HydroSolver.hpp:20   set_uold
+ *   include/ramses/solvers/hydro/HydroSolver.hpp:21   set_unew
+ *   include/ramses/solvers/hydro/HydroSolver.hpp:22   compute_courant_step
+ *   include/ramses/core/AmrGrid.hpp:26-31,104-107     grid arrays and uold layout
+ *
+ * Data layout is the reference's own (AmrGrid.hpp:104-107): the state is
+ * [nvar][ncell] doubles, variable-major; cell ids are 1-based,
+ * icell = ncoarse + (ic-1)*ngridmax + igrid (AmrGrid.cpp:279).
+ *
+ * Threading: one host thread per rg_ctx; calls are not re-entrant.  All device
+ * work is queued on the context's own stream; rg_download_state and
+ * rg_synchronize are the synchronisation points.
+ */
+#ifndef RGPU_H
+#define RGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RG_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+    RG_OK = 0,
+    RG_ERR_ARG = -1,         /* invalid argument (null pointer, bad size, bad level)   */
+    RG_ERR_CUDA = -2,        /* a CUDA runtime call failed (message has the CUDA error) */
+    RG_ERR_UNSUPPORTED = -3, /* configuration outside what the GPU path implements      */
+    RG_ERR_TOPOLOGY = -4,    /* inconsistent tree arrays (list cycle, bad index)        */
+    RG_ERR_STATE = -5,       /* call made before the data it needs was provided         */
+    RG_ERR_TIMEOUT = -6,     /* a bounded device-side wait gave up                      */
+    RG_ERR_DEVICE = -7,      /* a device-side check set the error word (see message)    */
+    RG_ERR_NOMEM = -8        /* device allocation failed                                */
+};
+
+/* ---- Riemann solver selection (hydro_params/riemann) -------------------- */
+/* The reference resolves the string at HydroSolver.cpp:456-461; any string it
+ * does not know falls back to LLF, and rg_riemann_from_string does the same. */
+enum {
+    RG_RIEMANN_LLF = 0,
+    RG_RIEMANN_HLL = 1,
+    RG_RIEMANN_HLLC = 2,
+    RG_RIEMANN_EXACT = 3,
+    RG_RIEMANN_ACOUSTIC = 4
+};
+
+/* Exact-solver Newton initial guess. */
+enum {
+    RG_GUESS_TWO_SHOCK = 0, /* RiemannSolver.cpp:215 (the reference's guess)          */
+    RG_GUESS_LEARNED = 1    /* MLP prediction (rg_mlp_*), two-shock as the fallback   */
+};
+
+/* Solver knobs, read once per call instead of per interface
+ * (HydroSolver.cpp:55,62,216-217,456 look them up by string inside the loop). */
+typedef struct rg_params {
+    int ndim;            /* 1 or 3 (compile-time NDIM of the host build)              */
+    int nvar;            /* ndim+2 plus passive scalars; non-thermal energies unsupported */
+    int slope_type;      /* hydro_params/slope_type, 0..8 (SlopeLimiter.cpp:7-60)     */
+    int riemann;         /* RG_RIEMANN_*                                               */
+    int interpol_type;   /* refine_params/interpol_type (ghost-cell slopes)            */
+    int interpol_var;    /* refine_params/interpol_var                                 */
+    double gamma;        /* AmrGrid::gamma                                             */
+    double courant_factor;
+    int exact_niter;     /* Newton iteration cap; reference value 10 (RiemannSolver.cpp:198) */
+    double exact_tol;    /* stop when |dp/(p+1e-10)| < tol; reference 1e-6 (:234)      */
+    int exact_guess;     /* RG_GUESS_*                                                 */
+    double boxlen;       /* amr_params/boxlen; only sets the CFL start value (HydroSolver.cpp:880) */
+    int flags;           /* reserved, must be 0                                        */
+} rg_params;
+
+/* Borrowed view of the host AmrGrid arrays (AmrGrid.hpp:15-31).  The library
+ * copies what it needs during rg_sync_topology and keeps no host pointer. */
+typedef struct rg_grid_view {
+    int ncoarse, ngridmax, ncell, nvar;
+    int nx, ny, nz;
+    int ncpu, nboundary, nlevelmax;
+    const int* son;        /* [ncell]                                   */
+    const int* father;     /* [ngridmax]                                */
+    const int* nbor;       /* [6*ngridmax]: father cell of each neighbour oct */
+    const int* next;       /* [ngridmax]: level / free linked lists     */
+    const int* headl;      /* [(ncpu+nboundary)*(nlevelmax+1)] (headl_vec) */
+    const int* bound_type; /* [nbound_type] or NULL                     */
+    int nbound_type;
+} rg_grid_view;
+
+typedef struct rg_ctx rg_ctx;
+
+/* ---- lifecycle ----------------------------------------------------------- */
+/* Replaces HydroSolver::HydroSolver (HydroSolver.hpp:16).  device < 0 picks the
+ * current CUDA device.  Returns NULL only when allocation of the host-side
+ * context itself fails; a context whose set-up failed reports it through
+ * rg_last_error and returns errors from every later call. */
+rg_ctx* rg_create(const rg_params* params, int device);
+void rg_destroy(rg_ctx* ctx);
+const char* rg_last_error(const rg_ctx* ctx);
+int rg_set_params(rg_ctx* ctx, const rg_params* params);
+int rg_riemann_from_string(const char* name);
+const char* rg_version(void);
+
+/* ---- grid mirror ---------------------------------------------------------- */
+/* Upload the tree arrays.  Must be called after every host change of the tree
+ * (TreeUpdater) or of ngridmax (AmrGrid::resize_grids, AmrGrid.cpp:118-238);
+ * it invalidates every cached level plan and CUDA graph. */
+int rg_sync_topology(rg_ctx* ctx, const rg_grid_view* grid);
+/* Copy host state [nvar][ncell] to the device; either pointer may be NULL. */
+int rg_upload_state(rg_ctx* ctx, const double* uold, const double* unew);
+/* Copy device state back to host [nvar][ncell]; either pointer may be NULL.
+ * Synchronises the context stream. */
+int rg_download_state(rg_ctx* ctx, double* uold, double* unew);
+/* Device addresses of the resident state (for callers that keep data on the
+ * GPU between steps).  Valid until the next rg_sync_topology. */
+int rg_device_state(rg_ctx* ctx, double** uold_dev, double** unew_dev);
+
+/* ---- the level step ------------------------------------------------------- */
+/* HydroSolver::set_unew (HydroSolver.cpp:575-590): unew <- uold on level. */
+int rg_set_unew(rg_ctx* ctx, int ilevel);
+/* HydroSolver::set_uold (HydroSolver.cpp:592-611): uold <- unew, son==0 only. */
+int rg_set_uold(rg_ctx* ctx, int ilevel);
+/* HydroSolver::godunov_fine (HydroSolver.cpp:18-573), including the reflux
+ * into coarser and same-level neighbour cells in the reference's order. */
+int rg_godunov_level(rg_ctx* ctx, int ilevel, double dt, double dx);
+/* HydroSolver::compute_courant_step (HydroSolver.cpp:878-977).  With
+ * pressure_cap != 0 the reference formula is used as is (p <= 100 rho);
+ * with 0 the cap is left out (the stable variant for strong blasts).
+ * Synchronises and writes the minimum to *dt_out. */
+int rg_courant_step(rg_ctx* ctx, int ilevel, double dx, double courant_factor,
+                    int pressure_cap, double* dt_out);
+/* One device-resident level substep: dt from the on-device CFL reduction
+ * (rg_courant_step semantics, no host round trip), then set_unew,
+ * godunov_fine and set_uold.  With use_graph != 0 the sequence is captured in
+ * a CUDA graph on first use and replayed afterwards.  *dt_used (may be NULL)
+ * receives the dt of this substep after an implicit synchronisation only when
+ * dt_used is non-NULL. */
+int rg_level_substep(rg_ctx* ctx, int ilevel, double dx, int pressure_cap,
+                     int use_graph, double* dt_used);
+int rg_synchronize(rg_ctx* ctx);
+
+/* ---- introspection (integer parity checks, profiling) ---------------------- */
+/* Oct ids (1-based) of level ilevel in linked-list order.  *n_out gets the
+ * count; at most cap entries are written. */
+int rg_level_octs(rg_ctx* ctx, int ilevel, int* octs_out, int cap, int* n_out);
+/* Neighbour cell ids per level cell, the result of AmrGrid::get_nbor_cells
+ * (AmrGrid.cpp:402-444): out[(k*2^ndim + ic-1)*6 + j], j = 2*idim+side. */
+int rg_level_nbor_cells(rg_ctx* ctx, int ilevel, int* out, int cap);
+/* Number of cell updates (son==0 cells) the last rg_godunov_level or
+ * rg_level_substep of this level processed. */
+int64_t rg_level_cell_updates(rg_ctx* ctx, int ilevel);
+/* Milliseconds of device time of the last godunov kernels (CUDA events on the
+ * context stream); per-kernel breakdown in out[0..n) (prim, face, fold). */
+int rg_last_kernel_ms(rg_ctx* ctx, float* out, int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RGPU_H */

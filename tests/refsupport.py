@@ -1,0 +1,296 @@
+"""ctypes bindings to the parity checkers (test infrastructure only).
+
+- ``RefHarness``: the RAMSES-CPP reference compiled from its own sources into
+  ``oracle/_ref/libref_harness{1,3}d.so`` (see ``oracle/Makefile``), driven
+  through its AmrGrid / TreeUpdater / HydroSolver API.
+- ``Oracle``: the C restatement ``oracle/rg_oracle.c`` built into
+  ``oracle/_build/liboracle.so``.
+
+Both operate on the reference data layout: state ``[nvar][ncell]`` doubles,
+1-based cell ids (``AmrGrid.hpp:104-107``).
+"""
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[1]
+ORACLE_DIR = ROOT / "oracle"
+REF_SRC = Path(os.environ.get("RG_REFERENCE_DIR", "/root/reference"))
+
+I32P = C.POINTER(C.c_int)
+F64P = C.POINTER(C.c_double)
+
+
+class rg_params(C.Structure):
+    _fields_ = [("ndim", C.c_int), ("nvar", C.c_int), ("slope_type", C.c_int), ("riemann", C.c_int),
+                ("interpol_type", C.c_int), ("interpol_var", C.c_int), ("gamma", C.c_double),
+                ("courant_factor", C.c_double), ("exact_niter", C.c_int), ("exact_tol", C.c_double),
+                ("exact_guess", C.c_int), ("boxlen", C.c_double), ("flags", C.c_int)]
+
+
+class rg_grid_view(C.Structure):
+    _fields_ = [("ncoarse", C.c_int), ("ngridmax", C.c_int), ("ncell", C.c_int), ("nvar", C.c_int),
+                ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("ncpu", C.c_int),
+                ("nboundary", C.c_int), ("nlevelmax", C.c_int),
+                ("son", I32P), ("father", I32P), ("nbor", I32P), ("next", I32P), ("headl", I32P),
+                ("bound_type", I32P), ("nbound_type", C.c_int)]
+
+
+RIEMANN = {"llf": 0, "hll": 1, "hllc": 2, "exact": 3, "acoustic": 4}
+
+
+def make_params(ndim, nvar=None, slope_type=1, riemann="hllc", interpol_type=1, interpol_var=0,
+                gamma=1.4, courant_factor=0.8, exact_niter=10, exact_tol=1e-6, exact_guess=0, boxlen=1.0):
+    return rg_params(ndim, nvar if nvar else ndim + 2, slope_type, RIEMANN.get(riemann, 0), interpol_type,
+                     interpol_var, gamma, courant_factor, exact_niter, exact_tol, exact_guess, boxlen, 0)
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(t)
+
+
+def ensure_built(target):
+    """Build oracle targets on demand (``oracle`` always; ``ref`` needs the reference tree)."""
+    lib = {"oracle": ORACLE_DIR / "_build" / "liboracle.so",
+           "ref": ORACLE_DIR / "_ref" / "libref_harness3d.so"}[target]
+    if lib.exists():
+        return True
+    if target == "ref" and not REF_SRC.exists():
+        return False
+    subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), target, f"REF={REF_SRC}", "-j8"], check=True)
+    return lib.exists()
+
+
+class GridArrays:
+    """numpy copies of the tree arrays + a matching ``rg_grid_view``."""
+
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+        self._keep = []
+        v = rg_grid_view()
+        for k in ("ncoarse", "ngridmax", "ncell", "nvar", "nx", "ny", "nz", "ncpu", "nboundary", "nlevelmax"):
+            setattr(v, k, int(kw[k]))
+        for k in ("son", "father", "nbor", "next", "headl"):
+            a = np.ascontiguousarray(kw[k], dtype=np.int32)
+            setattr(self, k, a)
+            setattr(v, k, _ptr(a, I32P))
+        v.bound_type = None
+        v.nbound_type = 0
+        self.view = v
+
+    def level_octs(self, ilevel):
+        octs = []
+        ig = int(self.headl[ilevel * (self.ncpu + self.nboundary)]) if 0 <= ilevel <= self.nlevelmax else 0
+        while ig > 0:
+            octs.append(ig)
+            ig = int(self.next[ig - 1])
+        return np.array(octs, dtype=np.int32)
+
+    def cell_ids(self, ilevel, ndim):
+        octs = self.level_octs(ilevel)
+        ttd = 1 << ndim
+        ic = np.arange(1, ttd + 1)
+        return (self.ncoarse + (ic[None, :] - 1) * self.ngridmax + octs[:, None]).reshape(-1)
+
+
+class RefHarness:
+    def __init__(self, ndim):
+        assert ensure_built("ref"), "reference sources unavailable"
+        self.ndim = ndim
+        self.lib = C.CDLL(str(ORACLE_DIR / "_ref" / f"libref_harness{ndim}d.so"))
+        L = self.lib
+        L.rh_create.restype = C.c_void_p
+        L.rh_create.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                C.c_double, C.c_double]
+        L.rh_destroy.argtypes = [C.c_void_p]
+        L.rh_get.restype = C.c_longlong
+        L.rh_get.argtypes = [C.c_void_p, C.c_char_p]
+        L.rh_ptr.restype = C.c_void_p
+        L.rh_ptr.argtypes = [C.c_void_p, C.c_char_p]
+        L.rh_count_grids.argtypes = [C.c_void_p, C.c_int]
+        L.rh_cell_center.argtypes = [C.c_void_p, C.c_int, F64P]
+        L.rh_flag_fine.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                   C.c_int, C.c_int, C.c_int]
+        for n in ("rh_make_grid_fine", "rh_remove_grid_fine", "rh_restrict_fine", "rh_set_unew", "rh_set_uold"):
+            getattr(L, n).argtypes = [C.c_void_p, C.c_int]
+        L.rh_godunov_fine.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double]
+        L.rh_courant.restype = C.c_double
+        L.rh_courant.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double]
+        L.rh_riemann.argtypes = [C.c_char_p, F64P, F64P, F64P, C.c_double]
+        L.rh_slope.restype = C.c_double
+        L.rh_slope.argtypes = [C.c_double] * 3 + [C.c_int, C.c_double, C.c_double]
+        L.rh_interpol_hydro.argtypes = [C.c_void_p, F64P, F64P]
+        self.h = None
+
+    # -- construction -----------------------------------------------------------
+    def create(self, nml, nx=1, ny=1, nz=1, ngridmax=1000, nvar=None, levelmin=1, nlevelmax=1,
+               gamma=1.4, boxlen=1.0):
+        nvar = nvar or self.ndim + 2
+        self.h = self.lib.rh_create(nml.encode(), nx, ny, nz, ngridmax, nvar, levelmin, nlevelmax, gamma, boxlen)
+        assert self.h, "rh_create failed"
+        self.nvar = nvar
+        self.levelmin, self.nlevelmax = levelmin, nlevelmax
+        return self
+
+    def close(self):
+        if self.h:
+            self.lib.rh_destroy(self.h)
+            self.h = None
+
+    def get(self, name):
+        return int(self.lib.rh_get(self.h, name.encode()))
+
+    def _arr(self, name, n, dtype):
+        p = self.lib.rh_ptr(self.h, name.encode())
+        ct = C.c_double if dtype == np.float64 else C.c_int
+        return np.ctypeslib.as_array(C.cast(p, C.POINTER(ct)), shape=(n,))
+
+    def arrays(self):
+        """Live numpy views of the reference's vectors (invalid after a resize)."""
+        ncell, ngm, nvar = self.get("ncell"), self.get("ngridmax"), self.nvar
+        return dict(uold=self._arr("uold", nvar * ncell, np.float64), unew=self._arr("unew", nvar * ncell, np.float64),
+                    son=self._arr("son", ncell, np.int32), father=self._arr("father", ngm, np.int32),
+                    nbor=self._arr("nbor", 6 * ngm, np.int32), next=self._arr("next", ngm, np.int32),
+                    headl=self._arr("headl", self.get("headl_size"), np.int32),
+                    xg=self._arr("xg", 3 * ngm, np.float64), flag1=self._arr("flag1", ncell, np.int32))
+
+    def grid(self):
+        a = self.arrays()
+        return GridArrays(ncoarse=self.get("ncoarse"), ngridmax=self.get("ngridmax"), ncell=self.get("ncell"),
+                          nvar=self.nvar, nx=self.get("nx"), ny=self.get("ny"), nz=self.get("nz"),
+                          ncpu=self.get("ncpu"), nboundary=self.get("nboundary"), nlevelmax=self.get("nlevelmax"),
+                          son=a["son"].copy(), father=a["father"].copy(), nbor=a["nbor"].copy(),
+                          next=a["next"].copy(), headl=a["headl"].copy())
+
+    def cell_centers(self, ids):
+        out = np.zeros((len(ids), 3))
+        buf = (C.c_double * 3)()
+        for i, c in enumerate(ids):
+            self.lib.rh_cell_center(self.h, int(c), buf)
+            out[i] = buf[:]
+        return out
+
+    def count_grids(self, il):
+        return self.lib.rh_count_grids(self.h, il)
+
+    # -- tree operations (reference TreeUpdater) ------------------------------------
+    def flag_fine(self, il, ed=-1.0, ep=-1.0, ev=-1.0, eb2=-1.0, nexp=1, icount=1, nsub=2):
+        self.lib.rh_flag_fine(self.h, il, ed, ep, ev, eb2, nexp, icount, nsub)
+
+    def make_grid_fine(self, il):
+        self.lib.rh_make_grid_fine(self.h, il)
+
+    def remove_grid_fine(self, il):
+        self.lib.rh_remove_grid_fine(self.h, il)
+
+    def restrict_fine(self, il):
+        self.lib.rh_restrict_fine(self.h, il)
+
+    def refine_uniform(self, levelmin, nexpand=1):
+        """Base refinement loop of Simulation::initialize (Simulation.cpp:226-234)."""
+        for _ in range(1, levelmin + 1):
+            for il in range(1, self.nlevelmax + 1):
+                self.flag_fine(il, -1, -1, -1, -1, nexpand, 1)
+                self.make_grid_fine(il)
+
+    # -- hydro ------------------------------------------------------------------------
+    def set_unew(self, il):
+        self.lib.rh_set_unew(self.h, il)
+
+    def set_uold(self, il):
+        self.lib.rh_set_uold(self.h, il)
+
+    def godunov_fine(self, il, dt, dx):
+        self.lib.rh_godunov_fine(self.h, il, dt, dx)
+
+    def courant(self, il, dx, gamma, cfl):
+        return self.lib.rh_courant(self.h, il, dx, gamma, cfl)
+
+    def riemann(self, name, ql, qr, gamma):
+        ql = np.ascontiguousarray(ql, dtype=np.float64)
+        qr = np.ascontiguousarray(qr, dtype=np.float64)
+        f = np.zeros(20)
+        self.lib.rh_riemann(name.encode(), _ptr(ql, F64P), _ptr(qr, F64P), _ptr(f, F64P), gamma)
+        return f
+
+    def slope(self, ql, qc, qr, t, theta=1.5, nu=0.0):
+        return self.lib.rh_slope(ql, qc, qr, t, theta, nu)
+
+
+def namelist(slope_type=2, riemann="hllc", interpol_type=1, interpol_var=0, levelmin=1, levelmax=1,
+             err_grad_d=-1.0, err_grad_p=-1.0, nexpand=1, extra=""):
+    return (f"&AMR_PARAMS\nlevelmin={levelmin}\nlevelmax={levelmax}\nnexpand={nexpand}\n/\n"
+            f"&HYDRO_PARAMS\nslope_type={slope_type}\nriemann='{riemann}'\n/\n"
+            f"&REFINE_PARAMS\ninterpol_type={interpol_type}\ninterpol_var={interpol_var}\n"
+            f"err_grad_d={err_grad_d}\nerr_grad_p={err_grad_p}\n/\n{extra}")
+
+
+class Oracle:
+    def __init__(self):
+        ensure_built("oracle")
+        self.lib = L = C.CDLL(str(ORACLE_DIR / "_build" / "liboracle.so"))
+        GV = C.POINTER(rg_grid_view)
+        PP = C.POINTER(rg_params)
+        L.orc_godunov_fine.argtypes = [GV, PP, C.c_int, C.c_double, C.c_double, F64P, F64P,
+                                       C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+        L.orc_set_unew.argtypes = [GV, C.c_int, C.c_int, C.c_int, F64P, F64P]
+        L.orc_set_uold.argtypes = [GV, C.c_int, C.c_int, C.c_int, F64P, F64P]
+        L.orc_courant_step.restype = C.c_double
+        L.orc_courant_step.argtypes = [GV, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                       C.c_double, C.c_int, F64P]
+        L.orc_level_cell_updates.restype = C.c_longlong
+        L.orc_level_cell_updates.argtypes = [GV, C.c_int, C.c_int]
+        L.orc_get_nbor_cells.argtypes = [GV, C.c_int, I32P, C.c_int, I32P, C.c_int]
+        L.orc_get_nbor_grids.argtypes = [GV, C.c_int, I32P]
+        for n in ("orc_solve_llf", "orc_solve_hll", "orc_solve_hllc", "orc_solve_acoustic"):
+            getattr(L, n).argtypes = [F64P, F64P, F64P, C.c_double, C.c_int]
+        L.orc_solve_exact.argtypes = [F64P, F64P, F64P, C.c_double, C.c_int, C.c_int, C.c_double, C.c_double,
+                                      I32P, F64P]
+        L.orc_compute_slope.restype = C.c_double
+        L.orc_compute_slope.argtypes = [C.c_double] * 3 + [C.c_int, C.c_double, C.c_double]
+
+    def godunov_fine(self, grid, params, il, dt, dx, uold, unew):
+        it, calls = C.c_longlong(0), C.c_longlong(0)
+        rc = self.lib.orc_godunov_fine(C.byref(grid.view), C.byref(params), il, dt, dx, _ptr(uold, F64P),
+                                       _ptr(unew, F64P), C.byref(it), C.byref(calls))
+        assert rc == 0, f"orc_godunov_fine rc={rc}"
+        return it.value, calls.value
+
+    def set_unew(self, grid, ndim, nvar, il, uold, unew):
+        assert self.lib.orc_set_unew(C.byref(grid.view), ndim, nvar, il, _ptr(uold, F64P), _ptr(unew, F64P)) == 0
+
+    def set_uold(self, grid, ndim, nvar, il, uold, unew):
+        assert self.lib.orc_set_uold(C.byref(grid.view), ndim, nvar, il, _ptr(uold, F64P), _ptr(unew, F64P)) == 0
+
+    def courant(self, grid, ndim, nvar, il, dx, gamma, cfl, uold, pressure_cap=True, boxlen=1.0):
+        return self.lib.orc_courant_step(C.byref(grid.view), ndim, nvar, il, dx, gamma, cfl, boxlen,
+                                         1 if pressure_cap else 0, _ptr(uold, F64P))
+
+    def cell_updates(self, grid, ndim, il):
+        return self.lib.orc_level_cell_updates(C.byref(grid.view), ndim, il)
+
+    def nbor_cells(self, grid, ndim, igrid, ic):
+        ign = (C.c_int * 7)()
+        self.lib.orc_get_nbor_grids(C.byref(grid.view), igrid, ign)
+        icn = (C.c_int * 6)()
+        self.lib.orc_get_nbor_cells(C.byref(grid.view), ndim, ign, ic, icn, igrid)
+        return list(icn)
+
+    def riemann(self, name, ql, qr, gamma, ndim, niter=10, tol=1e-6, p0=-1.0):
+        ql = np.ascontiguousarray(ql, dtype=np.float64)
+        qr = np.ascontiguousarray(qr, dtype=np.float64)
+        f = np.zeros(20)
+        if name == "exact":
+            it = C.c_int(0)
+            ps = C.c_double(0)
+            self.lib.orc_solve_exact(_ptr(ql, F64P), _ptr(qr, F64P), _ptr(f, F64P), gamma, ndim, niter, tol, p0,
+                                     C.byref(it), C.byref(ps))
+            return f
+        getattr(self.lib, f"orc_solve_{name}")(_ptr(ql, F64P), _ptr(qr, F64P), _ptr(f, F64P), gamma, ndim)
+        return f
+
+    def slope(self, ql, qc, qr, t, theta=1.5, nu=0.0):
+        return self.lib.orc_compute_slope(ql, qc, qr, t, theta, nu)
