@@ -1,0 +1,497 @@
+// rg_api.cu -- the extern "C" boundary of librgpu.so (declared in include/rgpu.h).
+//
+// Mirrors the HydroSolver entry points that Simulation::amr_step calls
+// (RAMSES-CPP src/core/Simulation.cpp:550,564,589,614): every call takes the
+// same arguments as its HydroSolver counterpart plus the context, returns an
+// int status and never throws across the boundary.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "rg_internal.cuh"
+
+namespace rg {
+
+int set_error(rg_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int check_cuda(rg_ctx* c, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return RG_OK;
+    std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    // errors that poison the context (faults) make every later call fail fast
+    if (e == cudaErrorIllegalAddress || e == cudaErrorLaunchFailure || e == cudaErrorIllegalInstruction ||
+        e == cudaErrorMisalignedAddress || e == cudaErrorHardwareStackError || e == cudaErrorAssert)
+        c->broken = true;
+    if (e == cudaErrorMemoryAllocation) return set_error(c, RG_ERR_NOMEM, m);
+    return set_error(c, RG_ERR_CUDA, m);
+}
+
+static const char* dev_err_name(int e) {
+    switch (e) {
+        case DE_TOPO_CYCLE: return "cyclic linked list or father chain";
+        case DE_LIST: return "level linked list inconsistent with next[]";
+        case DE_SAME_OUTSIDE:
+            return "same-level branch names a cell outside the level (the reference would read stale traces)";
+        case DE_NBOR_DEPTH: return "neighbour lookup deeper than 64 father levels";
+        case DE_EVENT_OVERFLOW: return "event list overflow";
+        case DE_BAD_INDEX: return "neighbour index beyond ncell";
+        default: return "unknown device error";
+    }
+}
+
+int check_device_status(rg_ctx* c) {
+    if (int rc = check_cuda(c, cudaMemcpyAsync(c->h_status, c->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                                               c->stream),
+                            "status copy"))
+        return rc;
+    if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "stream sync")) return rc;
+    if (c->h_status->err != DE_NONE) {
+        int e = c->h_status->err, info = c->h_status->info;
+        cudaMemsetAsync(c->d_status, 0, 2 * sizeof(int), c->stream);
+        cudaStreamSynchronize(c->stream);
+        int code = (e == DE_SAME_OUTSIDE) ? RG_ERR_UNSUPPORTED : RG_ERR_TOPOLOGY;
+        return set_error(c, code, std::string("device check: ") + dev_err_name(e) + " (index " + std::to_string(info) + ")");
+    }
+    return RG_OK;
+}
+
+}  // namespace rg
+
+using namespace rg;
+
+namespace {
+
+template <typename T>
+int grow(rg_ctx* c, T** p, size_t* cap, size_t n, const char* what) {
+    if (*cap >= n && *p) return RG_OK;
+    cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    if (cudaMalloc((void**)p, sizeof(T) * (n ? n : 1)) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(c, RG_ERR_NOMEM, std::string("cudaMalloc failed: ") + what);
+    }
+    *cap = n;
+    return RG_OK;
+}
+
+int validate_params(rg_ctx* c, const rg_params* p) {
+    if (!p) return set_error(c, RG_ERR_ARG, "params is NULL");
+    if (p->ndim != 1 && p->ndim != 3) return set_error(c, RG_ERR_UNSUPPORTED, "ndim must be 1 or 3");
+    if (p->nvar != p->ndim + 2)
+        return set_error(c, RG_ERR_UNSUPPORTED, "nvar must be ndim+2 (passive scalars and non-thermal energies are not implemented on the GPU path)");
+    if (p->slope_type < 0 || p->slope_type > 8) return set_error(c, RG_ERR_ARG, "slope_type out of 0..8");
+    if (p->riemann < 0 || p->riemann > 4) return set_error(c, RG_ERR_ARG, "riemann out of range");
+    if (!(p->gamma > 1.0)) return set_error(c, RG_ERR_ARG, "gamma must be > 1");
+    if (p->flags != 0) return set_error(c, RG_ERR_ARG, "flags must be 0");
+    return RG_OK;
+}
+
+#define CTX_GUARD(c)                                                              \
+    do {                                                                          \
+        if (!(c)) return RG_ERR_ARG;                                              \
+        if ((c)->broken) return set_error((c), RG_ERR_CUDA, (c)->err.empty() ? "context unusable after a device fault" : (c)->err); \
+        cudaSetDevice((c)->device);                                               \
+    } while (0)
+
+void invalidate_plans(rg_ctx* c) {
+    for (auto& p : c->plans) free_plan(p);
+}
+
+int get_plan(rg_ctx* c, int ilevel, Plan** out) {
+    if (!c->have_topology) return set_error(c, RG_ERR_STATE, "rg_sync_topology has not been called");
+    if (ilevel < 0 || ilevel > c->nlevelmax) return set_error(c, RG_ERR_ARG, "ilevel outside 0..nlevelmax");
+    if ((int)c->plans.size() < c->nlevelmax + 1) c->plans.resize(c->nlevelmax + 1);
+    Plan& p = c->plans[ilevel];
+    if (!p.valid) {
+        if (int rc = build_plan(c, ilevel, p)) {
+            free_plan(p);
+            return rc;
+        }
+    }
+    *out = &p;
+    return RG_OK;
+}
+
+// The flux scratch is shared by all levels and baked into captured graphs:
+// growing it invalidates every graph.
+int ensure_flux(rg_ctx* c, const Plan& P) {
+    size_t need = (size_t)(2 * c->params.ndim) * (c->params.ndim + 2) * (size_t)P.ncells;
+    if (c->cap_flux >= need && c->d_flux) return RG_OK;
+    cudaStreamSynchronize(c->stream);
+    for (auto& p : c->plans)
+        if (p.graph) {
+            cudaGraphExecDestroy(p.graph);
+            p.graph = nullptr;
+        }
+    return grow(c, &c->d_flux, &c->cap_flux, need, "flux scratch");
+}
+
+void record_updates(rg_ctx* c, int ilevel, const Plan& P) {
+    if ((int)c->cell_updates.size() < c->nlevelmax + 1) c->cell_updates.resize(c->nlevelmax + 1, 0);
+    c->cell_updates[ilevel] = P.nactive;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* rg_version(void) { return "rgpu 1 (sm_100a, FP64 Godunov level step)"; }
+
+int rg_riemann_from_string(const char* name) {
+    // HydroSolver.cpp:456-461: exact, case-sensitive comparisons; LLF otherwise.
+    if (!name) return RG_RIEMANN_LLF;
+    if (!strcmp(name, "hllc")) return RG_RIEMANN_HLLC;
+    if (!strcmp(name, "hll")) return RG_RIEMANN_HLL;
+    if (!strcmp(name, "exact")) return RG_RIEMANN_EXACT;
+    if (!strcmp(name, "acoustic")) return RG_RIEMANN_ACOUSTIC;
+    return RG_RIEMANN_LLF;
+}
+
+rg_ctx* rg_create(const rg_params* params, int device) {
+    rg_ctx* c = new (std::nothrow) rg_ctx();
+    if (!c) return nullptr;
+    if (validate_params(c, params)) {
+        c->broken = true;
+        return c;
+    }
+    c->params = *params;
+    if (c->params.boxlen <= 0) c->params.boxlen = 1.0;
+    if (device < 0) {
+        if (cudaGetDevice(&device) != cudaSuccess) device = 0;
+    }
+    c->device = device;
+    if (check_cuda(c, cudaSetDevice(device), "cudaSetDevice") ||
+        check_cuda(c, cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device), "SM count") ||
+        check_cuda(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream") ||
+        check_cuda(c, cudaMalloc(&c->d_status, sizeof(DevStatus)), "status") ||
+        check_cuda(c, cudaMallocHost(&c->h_status, sizeof(DevStatus)), "pinned status") ||
+        check_cuda(c, cudaMemset(c->d_status, 0, sizeof(DevStatus)), "status init")) {
+        c->broken = true;
+        return c;
+    }
+    for (auto& e : c->ev) cudaEventCreate(&e);
+    const char* t = getenv("RG_TIMING");
+    c->timing = t && t[0] == '1';
+    return c;
+}
+
+void rg_destroy(rg_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    invalidate_plans(c);
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    int* ip[] = {c->d_son, c->d_father, c->d_nbor, c->d_next, c->d_bound, c->d_jump, c->d_dist, c->d_jump2,
+                 c->d_dist2, c->d_cell_level, c->d_cpos, c->d_tmap, c->d_pmark, c->d_scan};
+    for (int* p : ip) cudaFree(p);
+    cudaFree(c->d_uold);
+    cudaFree(c->d_unew);
+    cudaFree(c->d_prim);
+    cudaFree(c->d_flux);
+    cudaFree(c->d_status);
+    if (c->h_status) cudaFreeHost(c->h_status);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char* rg_last_error(const rg_ctx* c) {
+    if (!c) return "null context";
+    return c->err.c_str();
+}
+
+int rg_set_params(rg_ctx* c, const rg_params* params) {
+    CTX_GUARD(c);
+    if (int rc = validate_params(c, params)) return rc;
+    if (params->ndim != c->params.ndim && c->have_topology)
+        return set_error(c, RG_ERR_ARG, "ndim cannot change after rg_sync_topology");
+    c->params = *params;
+    if (c->params.boxlen <= 0) c->params.boxlen = 1.0;
+    // graphs bake the solver choice and constants in: drop them, keep the plans
+    for (auto& p : c->plans)
+        if (p.graph) {
+            cudaGraphExecDestroy(p.graph);
+            p.graph = nullptr;
+        }
+    return RG_OK;
+}
+
+int rg_sync_topology(rg_ctx* c, const rg_grid_view* g) {
+    CTX_GUARD(c);
+    if (!g || !g->son || !g->father || !g->nbor || !g->next || !g->headl) return set_error(c, RG_ERR_ARG, "null grid array");
+    if (g->ngridmax < 1 || g->ncoarse < 1 || g->nx < 1 || g->ny < 1 || g->nz < 1 || g->ncpu < 1 || g->nlevelmax < 1)
+        return set_error(c, RG_ERR_ARG, "bad grid sizes");
+    int ttd = 1 << c->params.ndim;
+    if ((long long)g->ncell != (long long)g->ncoarse + (long long)ttd * g->ngridmax)
+        return set_error(c, RG_ERR_ARG, "ncell != ncoarse + 2^ndim * ngridmax");
+    if ((long long)g->nx * g->ny * g->nz != g->ncoarse) return set_error(c, RG_ERR_ARG, "ncoarse != nx*ny*nz");
+    if (g->nvar != c->params.nvar) return set_error(c, RG_ERR_ARG, "grid nvar differs from params.nvar");
+    if (g->nboundary != 0)
+        return set_error(c, RG_ERR_UNSUPPORTED, "nboundary != 0 (boundary patches are not read by the reference either)");
+    if (g->ncpu != 1) return set_error(c, RG_ERR_UNSUPPORTED, "ncpu must be 1 (the hydro path has no halo exchange)");
+    cudaStreamSynchronize(c->stream);
+    invalidate_plans(c);
+    bool resized = g->ncell != c->ncell;
+    c->ncoarse = g->ncoarse;
+    c->ngridmax = g->ngridmax;
+    c->ncell = g->ncell;
+    c->nvar = g->nvar;
+    c->nx = g->nx;
+    c->ny = g->ny;
+    c->nz = g->nz;
+    c->ncpu = g->ncpu;
+    c->nboundary = g->nboundary;
+    c->nlevelmax = g->nlevelmax;
+    c->nbound_type = (g->bound_type && g->nbound_type > 0) ? g->nbound_type : 0;
+    size_t ncell1 = (size_t)c->ncell + 1, ngm = (size_t)c->ngridmax;
+    size_t cap;
+    cap = c->cap_cell;
+    if (int rc = grow(c, &c->d_son, &cap, ncell1, "son")) return rc;
+    cap = c->cap_cell;
+    if (int rc = grow(c, &c->d_cell_level, &cap, ncell1, "cell_level")) return rc;
+    cap = c->cap_cell;
+    if (int rc = grow(c, &c->d_cpos, &cap, ncell1, "cpos")) return rc;
+    cap = c->cap_cell;
+    if (int rc = grow(c, &c->d_tmap, &cap, ncell1, "tmap")) return rc;
+    cap = c->cap_cell;
+    if (int rc = grow(c, &c->d_pmark, &cap, ncell1, "pmark")) return rc;
+    c->cap_cell = std::max(c->cap_cell, ncell1);
+    cap = c->cap_grid;
+    if (int rc = grow(c, &c->d_father, &cap, ngm, "father")) return rc;
+    cap = c->cap_grid;
+    if (int rc = grow(c, &c->d_next, &cap, ngm, "next")) return rc;
+    cap = c->cap_grid;
+    if (int rc = grow(c, &c->d_jump, &cap, ngm, "jump")) return rc;
+    cap = c->cap_grid;
+    if (int rc = grow(c, &c->d_dist, &cap, ngm, "dist")) return rc;
+    cap = c->cap_grid;
+    if (int rc = grow(c, &c->d_jump2, &cap, ngm, "jump2")) return rc;
+    cap = c->cap_grid;
+    if (int rc = grow(c, &c->d_dist2, &cap, ngm, "dist2")) return rc;
+    cap = c->cap_grid * 6;
+    if (int rc = grow(c, &c->d_nbor, &cap, 6 * ngm, "nbor")) return rc;
+    c->cap_grid = std::max(c->cap_grid, ngm);
+    cudaFree(c->d_bound);
+    c->d_bound = nullptr;
+    if (c->nbound_type) {
+        if (check_cuda(c, cudaMalloc(&c->d_bound, sizeof(int) * c->nbound_type), "bound_type")) return RG_ERR_NOMEM;
+        cudaMemcpyAsync(c->d_bound, g->bound_type, sizeof(int) * c->nbound_type, cudaMemcpyHostToDevice, c->stream);
+    }
+    size_t nheadl = (size_t)(c->ncpu + c->nboundary) * (c->nlevelmax + 1);
+    c->h_headl.assign(g->headl, g->headl + nheadl);
+    cudaStream_t s = c->stream;
+    if (int rc = check_cuda(c, cudaMemcpyAsync(c->d_son, g->son, sizeof(int) * c->ncell, cudaMemcpyHostToDevice, s), "son upload")) return rc;
+    cudaMemsetAsync(c->d_son + c->ncell, 0, sizeof(int), s);
+    cudaMemcpyAsync(c->d_father, g->father, sizeof(int) * ngm, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(c->d_nbor, g->nbor, sizeof(int) * 6 * ngm, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(c->d_next, g->next, sizeof(int) * ngm, cudaMemcpyHostToDevice, s);
+    if (int rc = check_cuda(c, cudaStreamSynchronize(s), "topology upload")) return rc;
+    if (resized) {
+        size_t ns = (size_t)c->nvar * c->ncell;
+        cap = c->cap_state;
+        if (int rc = grow(c, &c->d_uold, &cap, ns, "uold")) return rc;
+        cap = c->cap_state;
+        if (int rc = grow(c, &c->d_unew, &cap, ns, "unew")) return rc;
+        cap = c->cap_state;
+        if (int rc = grow(c, &c->d_prim, &cap, ns, "prim")) return rc;
+        c->cap_state = std::max(c->cap_state, ns);
+        c->have_state = false;
+    }
+    c->have_topology = true;
+    c->topo_version++;
+    if (int rc = rank_lists(c)) return rc;
+    if (int rc = compute_cell_levels(c)) return rc;
+    return check_device_status(c);
+}
+
+int rg_upload_state(rg_ctx* c, const double* uold, const double* unew) {
+    CTX_GUARD(c);
+    if (!c->have_topology) return set_error(c, RG_ERR_STATE, "rg_sync_topology has not been called");
+    size_t bytes = sizeof(double) * (size_t)c->nvar * c->ncell;
+    if (uold && check_cuda(c, cudaMemcpyAsync(c->d_uold, uold, bytes, cudaMemcpyHostToDevice, c->stream), "uold upload"))
+        return RG_ERR_CUDA;
+    if (unew && check_cuda(c, cudaMemcpyAsync(c->d_unew, unew, bytes, cudaMemcpyHostToDevice, c->stream), "unew upload"))
+        return RG_ERR_CUDA;
+    if (uold || unew) c->have_state = true;
+    return RG_OK;
+}
+
+int rg_download_state(rg_ctx* c, double* uold, double* unew) {
+    CTX_GUARD(c);
+    if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state on the device");
+    size_t bytes = sizeof(double) * (size_t)c->nvar * c->ncell;
+    if (uold && check_cuda(c, cudaMemcpyAsync(uold, c->d_uold, bytes, cudaMemcpyDeviceToHost, c->stream), "uold download"))
+        return RG_ERR_CUDA;
+    if (unew && check_cuda(c, cudaMemcpyAsync(unew, c->d_unew, bytes, cudaMemcpyDeviceToHost, c->stream), "unew download"))
+        return RG_ERR_CUDA;
+    return check_cuda(c, cudaStreamSynchronize(c->stream), "download sync");
+}
+
+int rg_device_state(rg_ctx* c, double** uold_dev, double** unew_dev) {
+    CTX_GUARD(c);
+    if (!c->have_topology) return set_error(c, RG_ERR_STATE, "rg_sync_topology has not been called");
+    if (uold_dev) *uold_dev = c->d_uold;
+    if (unew_dev) *unew_dev = c->d_unew;
+    c->have_state = true;
+    return RG_OK;
+}
+
+int rg_set_unew(rg_ctx* c, int ilevel) {
+    CTX_GUARD(c);
+    Plan* P;
+    if (int rc = get_plan(c, ilevel, &P)) return rc;
+    return launch_set_unew(c, *P);
+}
+
+int rg_set_uold(rg_ctx* c, int ilevel) {
+    CTX_GUARD(c);
+    Plan* P;
+    if (int rc = get_plan(c, ilevel, &P)) return rc;
+    return launch_set_uold(c, *P);
+}
+
+int rg_godunov_level(rg_ctx* c, int ilevel, double dt, double dx) {
+    CTX_GUARD(c);
+    if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state uploaded");
+    Plan* P;
+    if (int rc = get_plan(c, ilevel, &P)) return rc;
+    record_updates(c, ilevel, *P);
+    if (P->ncells == 0) return RG_OK;
+    if (int rc = ensure_flux(c, *P)) return rc;
+    if (int rc = launch_set_dt_host(c, dt, dx)) return rc;
+    return launch_godunov(c, *P);
+}
+
+int rg_courant_step(rg_ctx* c, int ilevel, double dx, double courant_factor, int pressure_cap, double* dt_out) {
+    CTX_GUARD(c);
+    if (!dt_out) return set_error(c, RG_ERR_ARG, "dt_out is NULL");
+    if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state uploaded");
+    Plan* P;
+    if (int rc = get_plan(c, ilevel, &P)) return rc;
+    if (int rc = launch_courant(c, *P, dx, pressure_cap, courant_factor)) return rc;
+    if (int rc = check_cuda(c, cudaMemcpyAsync(c->h_status, c->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                                               c->stream),
+                            "dt copy"))
+        return rc;
+    if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "courant sync")) return rc;
+    unsigned long long b = c->h_status->dtmin_bits;
+    double dt;
+    memcpy(&dt, &b, sizeof(dt));
+    *dt_out = dt;
+    return RG_OK;
+}
+
+int rg_level_substep(rg_ctx* c, int ilevel, double dx, int pressure_cap, int use_graph, double* dt_used) {
+    CTX_GUARD(c);
+    if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state uploaded");
+    Plan* P;
+    if (int rc = get_plan(c, ilevel, &P)) return rc;
+    record_updates(c, ilevel, *P);
+    if (int rc = ensure_flux(c, *P)) return rc;
+    auto enqueue = [&]() -> int {
+        if (int rc = launch_courant(c, *P, dx, pressure_cap, c->params.courant_factor)) return rc;
+        if (int rc = launch_finalize_dt(c, dx)) return rc;
+        if (int rc = launch_set_unew(c, *P)) return rc;
+        if (int rc = launch_godunov(c, *P)) return rc;
+        return launch_set_uold(c, *P);
+    };
+    if (use_graph) {
+        int cap_key = pressure_cap ? 1 : 0;
+        if (!P->graph || P->graph_cap != cap_key ) {
+            if (P->graph) {
+                cudaGraphExecDestroy(P->graph);
+                P->graph = nullptr;
+            }
+            bool timing = c->timing;
+            c->timing = false;
+            cudaGraph_t g = nullptr;
+            if (int rc = check_cuda(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture")) {
+                c->timing = timing;
+                return rc;
+            }
+            int rc_enq = enqueue();
+            cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+            c->timing = timing;
+            if (rc_enq) {
+                if (g) cudaGraphDestroy(g);
+                return rc_enq;
+            }
+            if (int rc = check_cuda(c, e, "end capture")) return rc;
+            cudaError_t ei = cudaGraphInstantiate(&P->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (int rc = check_cuda(c, ei, "graph instantiate")) return rc;
+            P->graph_cap = cap_key;
+        }
+        if (int rc = check_cuda(c, cudaGraphLaunch(P->graph, c->stream), "graph launch")) return rc;
+    } else {
+        if (int rc = enqueue()) return rc;
+    }
+    if (dt_used) {
+        if (int rc = check_cuda(c, cudaMemcpyAsync(c->h_status, c->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                                                   c->stream),
+                                "dt copy"))
+            return rc;
+        if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "substep sync")) return rc;
+        *dt_used = c->h_status->dt;
+    }
+    return RG_OK;
+}
+
+int rg_synchronize(rg_ctx* c) {
+    CTX_GUARD(c);
+    if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "synchronize")) return rc;
+    if (c->timing) {
+        for (int i = 0; i < 3; ++i) cudaEventElapsedTime(&c->last_ms[i], c->ev[i], c->ev[i + 1]);
+        cudaGetLastError();
+    }
+    return check_device_status(c);
+}
+
+int rg_level_octs(rg_ctx* c, int ilevel, int* octs_out, int cap, int* n_out) {
+    CTX_GUARD(c);
+    Plan* P;
+    if (int rc = get_plan(c, ilevel, &P)) return rc;
+    if (n_out) *n_out = P->noct;
+    int n = std::min(cap, P->noct);
+    if (n > 0 && octs_out) {
+        if (int rc = check_cuda(c, cudaMemcpyAsync(octs_out, P->octs, sizeof(int) * n, cudaMemcpyDeviceToHost, c->stream), "octs copy")) return rc;
+        return check_cuda(c, cudaStreamSynchronize(c->stream), "octs sync");
+    }
+    return RG_OK;
+}
+
+int rg_level_nbor_cells(rg_ctx* c, int ilevel, int* out, int cap) {
+    CTX_GUARD(c);
+    Plan* P;
+    if (int rc = get_plan(c, ilevel, &P)) return rc;
+    int ns = 2 * c->params.ndim, ttd = 1 << c->params.ndim;
+    if ((long long)cap < (long long)P->ncells * 6) return set_error(c, RG_ERR_ARG, "output too small (need ncells*6)");
+    std::vector<int> h((size_t)ns * P->ncells);
+    if (P->ncells) {
+        if (int rc = check_cuda(c, cudaMemcpyAsync(h.data(), P->icn, sizeof(int) * h.size(), cudaMemcpyDeviceToHost, c->stream), "icn copy")) return rc;
+        if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "icn sync")) return rc;
+    }
+    for (int p = 0; p < P->ncells; ++p) {
+        int cpu = P->level0 ? p : (p % P->noct) * ttd + p / P->noct;
+        for (int j = 0; j < 6; ++j) out[(size_t)cpu * 6 + j] = (j < ns) ? h[(size_t)j * P->ncells + p] : 0;
+    }
+    return RG_OK;
+}
+
+int64_t rg_level_cell_updates(rg_ctx* c, int ilevel) {
+    if (!c || ilevel < 0 || ilevel >= (int)c->cell_updates.size()) return 0;
+    return c->cell_updates[ilevel];
+}
+
+int rg_last_kernel_ms(rg_ctx* c, float* out, int n) {
+    CTX_GUARD(c);
+    for (int i = 0; i < n && i < 3; ++i) out[i] = c->last_ms[i];
+    return c->timing ? RG_OK : set_error(c, RG_ERR_STATE, "timing disabled (set RG_TIMING=1)");
+}
+
+}  // extern "C"

@@ -1,0 +1,158 @@
+// rg_internal.cuh -- device data model of the B200 Godunov level step.
+//
+// The host application owns the AmrGrid (RAMSES-CPP include/ramses/core/
+// AmrGrid.hpp); the library mirrors the tree and the state in HBM and keeps,
+// per refinement level, a "level plan": the integer work of
+// HydroSolver::godunov_fine (src/solvers/hydro/HydroSolver.cpp:18-115) done
+// once per topology instead of once per call:
+//   - the level's oct list in linked-list order (HydroSolver.cpp:43-47),
+//     from a pointer-jumping list ranking of next[];
+//   - the six neighbour cells of every level cell (AmrGrid::get_nbor_cells,
+//     AmrGrid.cpp:402-444) and, per interface, the two neighbours of that
+//     neighbour along the interface normal (the ghost-branch stencil,
+//     HydroSolver.cpp:179-191);
+//   - the interface kind (refined -> zero flux, ghost, same-level, boundary)
+//     and whether it refluxes into its neighbour (HydroSolver.cpp:125-162,476);
+//   - per target cell, the ordered list of updates it receives (refluxes from
+//     neighbours and its own flux-sum update), sorted by the CPU loop key
+//     (oct position, ic, idim, side), so the GPU fold applies them in the
+//     reference's order without atomics.
+// Cell storage index inside a plan: p = (ic-1)*noct + k (k = oct position);
+// for fixed ic consecutive k touch consecutive octs, which keeps the state
+// reads of a warp coalesced when octs are allocated in list order.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/rgpu.h"
+
+namespace rg {
+
+enum Kind : int8_t { K_NONE = 0, K_ZERO = 1, K_GHOST = 2, K_SAME = 3, K_BOUND = 4 };
+constexpr int KIND_MASK = 7;
+constexpr int KIND_REFLUX = 8;   // interface refluxes into its neighbour
+constexpr int KIND_REFLECT = 16; // boundary branch with btype == 1 (velocity flip)
+constexpr int OWN_SLOT = 7;      // event slot of a cell's own update
+
+// device error word: first error wins; info carries an index for the message
+enum DevErr : int { DE_NONE = 0, DE_TOPO_CYCLE = 1, DE_LIST = 2, DE_SAME_OUTSIDE = 3, DE_NBOR_DEPTH = 4,
+                    DE_EVENT_OVERFLOW = 5, DE_BAD_INDEX = 6 };
+
+struct DevStatus {
+    int err;
+    int info;
+    unsigned long long dtmin_bits;  // CFL min-reduction scratch
+    double dt, dx, dtdx;            // values of the current step (read by kernels)
+    unsigned long long cell_updates;
+};
+
+// Read-only view of the mirrored tree handed to kernels.
+struct TreeView {
+    int ncoarse, ngridmax, ncell, nx, ny, nz;
+    int nbound_type;
+    const int* son;
+    const int* father;
+    const int* nbor;
+    const int* bound_type;
+    const int* cell_level;  // [ncell+1] HydroSolver.cpp:22-38
+};
+
+// Per-level plan arrays (device).  NS = 2*ndim interface slots.
+struct PlanView {
+    int ilevel, level0, noct, ncells, ntarg, nextra_prim;
+    const int* octs;       // [noct] (level > 0)
+    const int* icn;        // [NS][ncells]
+    const int* stc;        // [NS][2][ncells]
+    const int8_t* kind;    // [NS][ncells]
+    const int* toff;       // [ntarg+1]
+    const int* tev;        // [toff[ntarg]] event keys: (cpu_pos*8 + slot)
+    const int* textra;     // [ntarg-ncells] cell ids of extra (coarser) targets
+    const int* xprim;      // [nextra_prim] cells outside the level needing primitives
+};
+
+struct Plan {
+    bool valid = false;
+    int ilevel = -1, level0 = 0, noct = 0, ncells = 0, ntarg = 0, nextra_prim = 0, nevents = 0;
+    long long nactive = 0;
+    int *octs = nullptr, *icn = nullptr, *stc = nullptr, *toff = nullptr, *tev = nullptr, *textra = nullptr,
+        *xprim = nullptr;
+    int8_t* kind = nullptr;
+    cudaGraphExec_t graph = nullptr;  // substep graph (set_unew..set_uold)
+    int graph_cap = -1;
+    PlanView view() const {
+        return PlanView{ilevel, level0, noct, ncells, ntarg, nextra_prim, octs, icn, stc, kind, toff, tev, textra, xprim};
+    }
+};
+
+struct Tuning {
+    int face_block = 128;
+    int face_blocks_per_sm = 0;  // 0 = plain grid covering all work
+    int fold_block = 256;
+};
+
+}  // namespace rg
+
+struct rg_ctx {
+    rg_params params{};
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    bool broken = false;
+
+    // mirrored tree
+    int ncoarse = 0, ngridmax = 0, ncell = 0, nvar = 0, nx = 1, ny = 1, nz = 1, ncpu = 1, nboundary = 0,
+        nlevelmax = 0, nbound_type = 0;
+    size_t cap_cell = 0, cap_grid = 0, cap_headl = 0;
+    int *d_son = nullptr, *d_father = nullptr, *d_nbor = nullptr, *d_next = nullptr, *d_bound = nullptr;
+    int *d_jump = nullptr, *d_dist = nullptr, *d_jump2 = nullptr, *d_dist2 = nullptr;
+    int* d_cell_level = nullptr;
+    int *d_cpos = nullptr, *d_tmap = nullptr, *d_pmark = nullptr;  // [ncell+1] plan-build scratch
+    std::vector<int> h_headl;
+    bool have_topology = false, ranked = false;
+    long long topo_version = 0;
+
+    // state
+    size_t cap_state = 0;
+    double *d_uold = nullptr, *d_unew = nullptr, *d_prim = nullptr;
+    bool have_state = false;
+
+    // scratch shared by all levels (levels run one after another on the stream)
+    size_t cap_flux = 0;
+    double* d_flux = nullptr;
+    size_t cap_scan = 0;
+    int* d_scan = nullptr;
+
+    rg::DevStatus* d_status = nullptr;
+    rg::DevStatus* h_status = nullptr;  // pinned mirror
+
+    std::vector<rg::Plan> plans;
+    rg::Tuning tuning;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    float last_ms[3] = {0, 0, 0};
+    bool timing = false;
+    std::vector<long long> cell_updates;
+};
+
+namespace rg {
+// host-side helpers shared by the translation units
+int set_error(rg_ctx* c, int code, const std::string& msg);
+int check_cuda(rg_ctx* c, cudaError_t e, const char* what);
+int check_device_status(rg_ctx* c);  // synchronises
+int build_plan(rg_ctx* c, int ilevel, Plan& plan);
+void free_plan(Plan& plan);
+int rank_lists(rg_ctx* c);
+int compute_cell_levels(rg_ctx* c);
+// step launchers (enqueue only)
+int launch_set_unew(rg_ctx* c, const Plan& p);
+int launch_set_uold(rg_ctx* c, const Plan& p);
+int launch_courant(rg_ctx* c, const Plan& p, double dx, int pressure_cap, double courant_factor);
+int launch_set_dt_host(rg_ctx* c, double dt, double dx);
+int launch_finalize_dt(rg_ctx* c, double dx);
+int launch_godunov(rg_ctx* c, const Plan& p);
+TreeView tree_view(const rg_ctx* c);
+}  // namespace rg

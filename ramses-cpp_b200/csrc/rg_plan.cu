@@ -1,0 +1,544 @@
+// rg_plan.cu -- integer work of the level step, built once per topology.
+//
+// Reference behaviour reproduced bit-exactly (paths relative to RAMSES-CPP):
+//   level list order         HydroSolver.cpp:43-47 (walk of headl/next)
+//   cell_levels              HydroSolver.cpp:22-38
+//   get_nbor_grids/cells     AmrGrid.cpp:389-444 (iii/jjj of Constants.cpp:8-43)
+//   get_nbor_cells_coarse    AmrGrid.cpp:513-550 (periodic; nboundary == 0)
+//   interface branches       HydroSolver.cpp:118-162, reflux test :476
+//   CPU update order         HydroSolver.cpp:565-572 (octs, ic, idim, side)
+#include <algorithm>
+#include <cstdio>
+
+#include "rg_internal.cuh"
+
+namespace rg {
+
+namespace {
+
+constexpr int TPB = 256;
+inline int nblk(long long n, int tpb = TPB) { return (int)std::max(1LL, std::min((n + tpb - 1) / tpb, 1LL << 30)); }
+
+__device__ __forceinline__ void raise_err(DevStatus* st, int code, int info) {
+    if (atomicCAS(&st->err, 0, code) == 0) st->info = info;
+}
+
+__device__ __forceinline__ int coarse_nbor(const TreeView& T, int icell, int idim, int side) {
+    if (icell <= 0 || icell > T.ncoarse) return 0;
+    int nx = T.nx, ny = T.ny, nz = T.nz;
+    int idx = icell - 1;
+    int iz = idx / (nx * ny), rem = idx % (nx * ny);
+    int iy = rem / nx, ix = rem % nx;
+    int c0 = ix, c1 = iy, c2 = iz;
+    int d = (side == 0) ? -1 : 1;
+    if (idim == 0) c0 = (c0 + d + nx) % nx;
+    else if (idim == 1) c1 = (c1 + d + ny) % ny;
+    else c2 = (c2 + d + nz) % nz;
+    return c2 * nx * ny + c1 * nx + c0 + 1;
+}
+
+// AmrGrid::get_nbor_cells for one direction; the recursion through the father
+// oct (AmrGrid.cpp:429-440) becomes a bounded loop.
+__device__ int nbor_cell_dir(const TreeView& T, int igrid, int ic, int idim, int side, DevStatus* st) {
+    for (int depth = 0; depth < 64; ++depth) {
+        int bit = ((ic - 1) >> idim) & 1;
+        int ig_idx = (side == 0) ? (bit ? 0 : 2 * idim + 1) : (bit ? 2 * idim + 2 : 0);
+        int ic_pos = ((ic - 1) ^ (1 << idim)) + 1;
+        int ig;
+        if (ig_idx == 0) {
+            ig = igrid;
+        } else {
+            int v = T.nbor[(size_t)(ig_idx - 1) * T.ngridmax + igrid - 1];
+            ig = (v > T.ncell) ? 0 : v;
+        }
+        if (ig > 0) {
+            if (ig_idx == 0) return T.ncoarse + (ic_pos - 1) * T.ngridmax + ig;
+            int ch = (ig <= T.ncell) ? T.son[ig - 1] : 0;
+            return (ch > 0) ? T.ncoarse + (ic_pos - 1) * T.ngridmax + ch : ig;
+        }
+        if (ig < 0) return ig;
+        int ifather = T.father[igrid - 1];
+        if (ifather <= T.ncoarse) return coarse_nbor(T, ifather, idim, side);
+        igrid = ((ifather - T.ncoarse - 1) % T.ngridmax) + 1;
+        ic = ((ifather - T.ncoarse - 1) / T.ngridmax) + 1;
+    }
+    raise_err(st, DE_NBOR_DEPTH, igrid);
+    return 0;
+}
+
+// Neighbour of an arbitrary cell id, as the ghost branch looks it up
+// (HydroSolver.cpp:179-187).
+__device__ __forceinline__ int nbor_of_cell(const TreeView& T, int id, int idim, int side, DevStatus* st) {
+    if (id <= T.ncoarse) return coarse_nbor(T, id, idim, side);
+    int ig = ((id - T.ncoarse - 1) % T.ngridmax) + 1;
+    int ic = ((id - T.ncoarse - 1) / T.ngridmax) + 1;
+    return nbor_cell_dir(T, ig, ic, idim, side, st);
+}
+
+// ---------------------------------------------------------------- list ranking
+__global__ void k_rank_init(const int* __restrict__ next, int n, int* jump, int* dist) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int nx = next[i];
+        bool ok = nx >= 1 && nx <= n;
+        jump[i] = ok ? nx - 1 : i;
+        dist[i] = ok ? 1 : 0;
+    }
+}
+__global__ void k_rank_step(int n, const int* __restrict__ j0, const int* __restrict__ d0, int* j1, int* d1) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int j = j0[i];
+        j1[i] = j0[j];
+        d1[i] = d0[i] + d0[j];
+    }
+}
+__global__ void k_rank_check(int n, const int* __restrict__ jump, const int* __restrict__ dist, DevStatus* st) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int j = jump[i];
+        if (jump[j] != j || dist[j] != 0) raise_err(st, DE_TOPO_CYCLE, i + 1);
+    }
+}
+
+__global__ void k_cell_levels(TreeView T, int* cell_level, int ttd, DevStatus* st) {
+    for (int ig = blockIdx.x * blockDim.x + threadIdx.x + 1; ig <= T.ngridmax; ig += gridDim.x * blockDim.x) {
+        if (T.father[ig - 1] <= 0) continue;
+        int level = 1, curr = ig, guard = 0;
+        while (curr > 0) {
+            int fc = T.father[curr - 1];
+            if (fc <= T.ncoarse) break;
+            curr = ((fc - T.ncoarse - 1) % T.ngridmax) + 1;
+            level++;
+            if (++guard > 4096) {
+                raise_err(st, DE_TOPO_CYCLE, ig);
+                break;
+            }
+        }
+        for (int ic = 1; ic <= ttd; ++ic) cell_level[T.ncoarse + (ic - 1) * T.ngridmax + ig] = level;
+    }
+}
+
+__global__ void k_level_octs(int n, const int* __restrict__ jump, const int* __restrict__ dist, int head0, int noct,
+                             int* octs, int* count, DevStatus* st) {
+    int tail = jump[head0];
+    int dh = dist[head0];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (jump[i] != tail) continue;
+        int pos = dh - dist[i];
+        if (pos < 0 || pos >= noct) {
+            raise_err(st, DE_LIST, i + 1);
+            continue;
+        }
+        octs[pos] = i + 1;
+        atomicAdd(count, 1);
+    }
+}
+
+// ---------------------------------------------------------------- plan cells
+__device__ __forceinline__ int plan_cell_id(const TreeView& T, const int* octs, int level0, int noct, int p) {
+    if (level0) return p + 1;
+    int icx = p / noct, k = p - icx * noct;
+    return T.ncoarse + icx * T.ngridmax + octs[k];
+}
+
+__global__ void k_plan_cpos(TreeView T, const int* __restrict__ octs, int level0, int noct, int ncells, int* cpos) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < ncells; p += gridDim.x * blockDim.x)
+        cpos[plan_cell_id(T, octs, level0, noct, p)] = p;
+}
+
+template <int NDIM>
+__global__ void k_plan_cells(TreeView T, const int* __restrict__ octs, int level0, int ilevel, int noct, int ncells,
+                             const int* __restrict__ cpos, int* icn, int* stc, int8_t* kind,
+                             unsigned long long* nactive, DevStatus* st) {
+    constexpr int NS = 2 * NDIM;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < ncells; p += gridDim.x * blockDim.x) {
+        int c = plan_cell_id(T, octs, level0, noct, p);
+        int icx = level0 ? 0 : p / noct;
+        int ig = level0 ? 0 : octs[p - icx * noct];
+        bool active = T.son[c - 1] == 0;
+        if (active) atomicAdd(nactive, 1ULL);
+        for (int s = 0; s < NS; ++s) {
+            int idim = s >> 1, side = s & 1;
+            int n = level0 ? coarse_nbor(T, c, idim, side) : nbor_cell_dir(T, ig, icx + 1, idim, side, st);
+            icn[(size_t)s * ncells + p] = n;
+            int kd = K_NONE, nl = 0, nr = 0;
+            if (active) {
+                if (n > T.ncell) {
+                    raise_err(st, DE_BAD_INDEX, c);
+                    n = 0;
+                }
+                int nlev = (n > 0) ? T.cell_level[n] : 0;
+                if (n > 0 && (T.son[n - 1] > 0 || nlev > ilevel)) {
+                    kd = K_ZERO;
+                } else if (n <= 0) {
+                    int ib = -n;
+                    int btype = 1;
+                    if (ib > 0 && ib <= T.nbound_type && T.bound_type) btype = T.bound_type[ib - 1];
+                    kd = K_BOUND | (btype == 1 ? KIND_REFLECT : 0);
+                } else if (nlev == ilevel) {  // son[n-1] == 0 here
+                    if (cpos[n] < 0) raise_err(st, DE_SAME_OUTSIDE, n);
+                    kd = K_SAME;
+                } else {
+                    kd = K_GHOST;
+                }
+                if ((kd & KIND_MASK) == K_SAME || (kd & KIND_MASK) == K_GHOST) {
+                    if (!level0) {
+                        nl = nbor_of_cell(T, n, idim, 0, st);
+                        nr = nbor_of_cell(T, n, idim, 1, st);
+                    }
+                    if (nlev < ilevel) kd |= KIND_REFLUX;
+                }
+            }
+            kind[(size_t)s * ncells + p] = (int8_t)kd;
+            stc[((size_t)s * 2 + 0) * ncells + p] = nl;
+            stc[((size_t)s * 2 + 1) * ncells + p] = nr;
+        }
+    }
+}
+
+// Cells outside the level whose primitives the step reads.
+template <int NDIM>
+__global__ void k_plan_xprim(int ncells, const int* __restrict__ cpos, const int* __restrict__ icn,
+                             const int* __restrict__ stc, const int8_t* __restrict__ kind, int* pmark, int* xprim,
+                             int* nx) {
+    constexpr int NS = 2 * NDIM;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < ncells; p += gridDim.x * blockDim.x) {
+        if (kind[p] == K_NONE) continue;  // inactive cell (slot 0 is NONE iff inactive)
+        for (int s = 0; s < NS; ++s) {
+            int refs[3] = {icn[(size_t)s * ncells + p], stc[((size_t)s * 2) * ncells + p],
+                           stc[((size_t)s * 2 + 1) * ncells + p]};
+            for (int r = 0; r < 3; ++r) {
+                int id = refs[r];
+                if (id <= 0 || cpos[id] >= 0) continue;
+                if (atomicCAS(&pmark[id], 0, 1) == 0) xprim[atomicAdd(nx, 1)] = id;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- events
+__device__ __forceinline__ int cpu_key(int level0, int ttd, int noct, int p, int slot) {
+    if (level0) return p * 8 + slot;
+    int icx = p / noct, k = p - icx * noct;
+    return (k * ttd + icx) * 8 + slot;
+}
+
+template <int NDIM>
+__global__ void k_ev_claim(int ncells, const int* __restrict__ cpos, const int* __restrict__ icn,
+                           const int8_t* __restrict__ kind, int* tmap, int* textra, int* nextra) {
+    constexpr int NS = 2 * NDIM;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < ncells; p += gridDim.x * blockDim.x) {
+        for (int s = 0; s < NS; ++s) {
+            if (!(kind[(size_t)s * ncells + p] & KIND_REFLUX)) continue;
+            int n = icn[(size_t)s * ncells + p];
+            if (cpos[n] >= 0) continue;
+            if (atomicCAS(&tmap[n], -1, -2) == -1) {
+                int j = atomicAdd(nextra, 1);
+                textra[j] = n;
+                tmap[n] = ncells + j;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ int target_of(const int* cpos, const int* tmap, int n) {
+    int t = cpos[n];
+    return t >= 0 ? t : tmap[n];
+}
+
+template <int NDIM>
+__global__ void k_ev_count(int ncells, const int* __restrict__ cpos, const int* __restrict__ tmap,
+                           const int* __restrict__ icn, const int8_t* __restrict__ kind, int* cnt) {
+    constexpr int NS = 2 * NDIM;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < ncells; p += gridDim.x * blockDim.x) {
+        if (kind[p] == K_NONE) continue;
+        atomicAdd(&cnt[p], 1);  // own update
+        for (int s = 0; s < NS; ++s) {
+            if (!(kind[(size_t)s * ncells + p] & KIND_REFLUX)) continue;
+            atomicAdd(&cnt[target_of(cpos, tmap, icn[(size_t)s * ncells + p])], 1);
+        }
+    }
+}
+
+template <int NDIM>
+__global__ void k_ev_fill(int ncells, int level0, int noct, const int* __restrict__ cpos, const int* __restrict__ tmap,
+                          const int* __restrict__ icn, const int8_t* __restrict__ kind, const int* __restrict__ off,
+                          int* fillc, int* ev) {
+    constexpr int NS = 2 * NDIM, TTD = 1 << NDIM;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < ncells; p += gridDim.x * blockDim.x) {
+        if (kind[p] == K_NONE) continue;
+        ev[off[p] + atomicAdd(&fillc[p], 1)] = cpu_key(level0, TTD, noct, p, OWN_SLOT);
+        for (int s = 0; s < NS; ++s) {
+            if (!(kind[(size_t)s * ncells + p] & KIND_REFLUX)) continue;
+            int t = target_of(cpos, tmap, icn[(size_t)s * ncells + p]);
+            ev[off[t] + atomicAdd(&fillc[t], 1)] = cpu_key(level0, TTD, noct, p, s);
+        }
+    }
+}
+
+__global__ void k_ev_sort(int ntarg, const int* __restrict__ off, int* ev) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntarg; t += gridDim.x * blockDim.x) {
+        int a = off[t], b = off[t + 1];
+        for (int i = a + 1; i < b; ++i) {
+            int v = ev[i], j = i - 1;
+            while (j >= a && ev[j] > v) {
+                ev[j + 1] = ev[j];
+                --j;
+            }
+            ev[j + 1] = v;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- exclusive scan
+constexpr int SCAN_TPB = 512;
+constexpr int SCAN_ITEMS = SCAN_TPB * 2;
+
+__device__ __forceinline__ int block_scan_excl(int v, int* sh, int* total) {
+    int tid = threadIdx.x;
+    sh[tid] = v;
+    __syncthreads();
+    for (int off = 1; off < blockDim.x; off <<= 1) {
+        int t = (tid >= off) ? sh[tid - off] : 0;
+        __syncthreads();
+        sh[tid] += t;
+        __syncthreads();
+    }
+    int incl = sh[tid];
+    if (total) *total = sh[blockDim.x - 1];
+    __syncthreads();
+    return incl - v;
+}
+
+// Each block scans SCAN_ITEMS entries (2 per thread) and writes its total.
+__global__ void k_scan_blocks(const int* __restrict__ in, int* out, int n, int* sums) {
+    __shared__ int sh[SCAN_TPB];
+    long long base = (long long)blockIdx.x * SCAN_ITEMS;
+    long long i0 = base + 2 * threadIdx.x;
+    int a = (i0 < n) ? in[i0] : 0, b = (i0 + 1 < n) ? in[i0 + 1] : 0;
+    int tot;
+    int e = block_scan_excl(a + b, sh, &tot);
+    if (i0 < n) out[i0] = e;
+    if (i0 + 1 < n) out[i0 + 1] = e + a;
+    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+// Single block: exclusive scan of the block totals, sequential over chunks.
+__global__ void k_scan_sums(int* sums, int nb, int* grand) {
+    __shared__ int sh[SCAN_TPB];
+    int carry = 0;
+    for (int base = 0; base < nb; base += SCAN_TPB) {
+        int i = base + threadIdx.x;
+        int v = (i < nb) ? sums[i] : 0;
+        int tot;
+        int e = block_scan_excl(v, sh, &tot);
+        if (i < nb) sums[i] = e + carry;
+        carry += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *grand = carry;
+}
+__global__ void k_scan_add(int* out, int n, const int* __restrict__ sums) {
+    long long i = (long long)blockIdx.x * SCAN_ITEMS + threadIdx.x;
+    int add = sums[blockIdx.x];
+    if (i < n) out[i] += add;
+    if (i + SCAN_TPB < n) out[i + SCAN_TPB] += add;
+}
+
+template <int NDIM>
+int build_plan_t(rg_ctx* c, int ilevel, Plan& P);
+
+}  // namespace
+
+TreeView tree_view(const rg_ctx* c) {
+    return TreeView{c->ncoarse, c->ngridmax, c->ncell, c->nx, c->ny, c->nz, c->nbound_type,
+                    c->d_son, c->d_father, c->d_nbor, c->d_bound, c->d_cell_level};
+}
+
+void free_plan(Plan& p) {
+    if (p.graph) cudaGraphExecDestroy(p.graph);
+    cudaFree(p.octs);
+    cudaFree(p.icn);
+    cudaFree(p.stc);
+    cudaFree(p.kind);
+    cudaFree(p.toff);
+    cudaFree(p.tev);
+    cudaFree(p.textra);
+    cudaFree(p.xprim);
+    p = Plan();
+}
+
+int rank_lists(rg_ctx* c) {
+    int n = c->ngridmax;
+    cudaStream_t s = c->stream;
+    k_rank_init<<<nblk(n), TPB, 0, s>>>(c->d_next, n, c->d_jump, c->d_dist);
+    int rounds = 1;
+    while ((1LL << rounds) < (long long)n) ++rounds;
+    rounds += 1;
+    for (int r = 0; r < rounds; ++r) {
+        k_rank_step<<<nblk(n), TPB, 0, s>>>(n, c->d_jump, c->d_dist, c->d_jump2, c->d_dist2);
+        std::swap(c->d_jump, c->d_jump2);
+        std::swap(c->d_dist, c->d_dist2);
+    }
+    k_rank_check<<<nblk(n), TPB, 0, s>>>(n, c->d_jump, c->d_dist, c->d_status);
+    if (int rc = check_cuda(c, cudaGetLastError(), "list ranking")) return rc;
+    c->ranked = true;
+    return RG_OK;
+}
+
+int compute_cell_levels(rg_ctx* c) {
+    cudaStream_t s = c->stream;
+    if (int rc = check_cuda(c, cudaMemsetAsync(c->d_cell_level, 0, sizeof(int) * ((size_t)c->ncell + 1), s),
+                            "memset cell_level"))
+        return rc;
+    k_cell_levels<<<nblk(c->ngridmax), TPB, 0, s>>>(tree_view(c), c->d_cell_level, 1 << c->params.ndim, c->d_status);
+    return check_cuda(c, cudaGetLastError(), "cell levels");
+}
+
+namespace {
+
+// Exclusive scan of n ints on the context stream; returns the grand total.
+int exclusive_scan(rg_ctx* c, const int* in, int* out, int n, int* total) {
+    int nb = (n + SCAN_ITEMS - 1) / SCAN_ITEMS;
+    if (nb < 1) nb = 1;
+    size_t need = (size_t)nb + 1;
+    if (c->cap_scan < need) {
+        cudaFree(c->d_scan);
+        c->d_scan = nullptr;
+        if (cudaMalloc(&c->d_scan, sizeof(int) * need) != cudaSuccess) return set_error(c, RG_ERR_NOMEM, "scan scratch");
+        c->cap_scan = need;
+    }
+    k_scan_blocks<<<nb, SCAN_TPB, 0, c->stream>>>(in, out, n, c->d_scan);
+    k_scan_sums<<<1, SCAN_TPB, 0, c->stream>>>(c->d_scan, nb, c->d_scan + nb);
+    k_scan_add<<<nb, SCAN_TPB, 0, c->stream>>>(out, n, c->d_scan);
+    if (int rc = check_cuda(c, cudaGetLastError(), "scan")) return rc;
+    if (int rc = check_cuda(c, cudaMemcpyAsync(total, c->d_scan + nb, sizeof(int), cudaMemcpyDeviceToHost, c->stream),
+                            "scan total"))
+        return rc;
+    return check_cuda(c, cudaStreamSynchronize(c->stream), "scan sync");
+}
+
+template <typename T>
+int dalloc(rg_ctx* c, T** p, size_t n, const char* what) {
+    if (cudaMalloc((void**)p, sizeof(T) * (n ? n : 1)) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(c, RG_ERR_NOMEM, std::string("cudaMalloc failed: ") + what);
+    }
+    return RG_OK;
+}
+
+template <int NDIM>
+int build_plan_t(rg_ctx* c, int ilevel, Plan& P) {
+    constexpr int NS = 2 * NDIM, TTD = 1 << NDIM;
+    cudaStream_t s = c->stream;
+    TreeView T = tree_view(c);
+    free_plan(P);
+    P.ilevel = ilevel;
+    P.level0 = (ilevel == 0);
+    int hv[4] = {0, 0, 0, 0};
+
+    // ---- oct list in linked-list order
+    if (!P.level0) {
+        int head = 0;
+        if (ilevel >= 0 && ilevel <= c->nlevelmax) head = c->h_headl[(size_t)ilevel * (c->ncpu + c->nboundary)];
+        if (head > c->ngridmax || head < 0) return set_error(c, RG_ERR_TOPOLOGY, "headl entry out of range");
+        if (head > 0) {
+            int dh = 0;
+            if (int rc = check_cuda(c, cudaMemcpyAsync(&dh, c->d_dist + head - 1, sizeof(int), cudaMemcpyDeviceToHost, s),
+                                    "list length"))
+                return rc;
+            if (int rc = check_cuda(c, cudaStreamSynchronize(s), "list length sync")) return rc;
+            P.noct = dh + 1;
+        }
+        if (P.noct == 0) {
+            P.valid = true;
+            return RG_OK;
+        }
+        if (int rc = dalloc(c, &P.octs, P.noct, "octs")) return rc;
+        int* d_count = c->d_scan;  // reuse scan scratch as a counter
+        if (c->cap_scan < 4) {
+            cudaFree(c->d_scan);
+            if (int rc = dalloc(c, &c->d_scan, 1024, "scan scratch")) return rc;
+            c->cap_scan = 1024;
+            d_count = c->d_scan;
+        }
+        cudaMemsetAsync(d_count, 0, sizeof(int), s);
+        k_level_octs<<<nblk(c->ngridmax), TPB, 0, s>>>(c->ngridmax, c->d_jump, c->d_dist, head - 1, P.noct, P.octs,
+                                                       d_count, c->d_status);
+        cudaMemcpyAsync(&hv[0], d_count, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (int rc = check_cuda(c, cudaStreamSynchronize(s), "level octs")) return rc;
+        if (hv[0] != P.noct) return set_error(c, RG_ERR_TOPOLOGY, "level linked list merges with another chain");
+        P.ncells = P.noct * TTD;
+    } else {
+        P.ncells = c->ncoarse;
+    }
+    int nc = P.ncells;
+
+    // ---- per-cell neighbours and interface kinds
+    if (int rc = dalloc(c, &P.icn, (size_t)NS * nc, "icn")) return rc;
+    if (int rc = dalloc(c, &P.stc, (size_t)NS * 2 * nc, "stencil")) return rc;
+    if (int rc = dalloc(c, &P.kind, (size_t)NS * nc, "kind")) return rc;
+    cudaMemsetAsync(c->d_cpos, 0xff, sizeof(int) * ((size_t)c->ncell + 1), s);
+    cudaMemsetAsync(c->d_tmap, 0xff, sizeof(int) * ((size_t)c->ncell + 1), s);
+    cudaMemsetAsync(c->d_pmark, 0, sizeof(int) * ((size_t)c->ncell + 1), s);
+    k_plan_cpos<<<nblk(nc), TPB, 0, s>>>(T, P.octs, P.level0, P.noct, nc, c->d_cpos);
+    unsigned long long* d_nact = (unsigned long long*)&c->d_status->cell_updates;
+    cudaMemsetAsync(d_nact, 0, sizeof(unsigned long long), s);
+    k_plan_cells<NDIM><<<nblk(nc), TPB, 0, s>>>(T, P.octs, P.level0, ilevel, P.noct, nc, c->d_cpos, P.icn, P.stc,
+                                                P.kind, d_nact, c->d_status);
+    if (int rc = check_cuda(c, cudaGetLastError(), "plan cells")) return rc;
+
+    // ---- extra primitives (coarser cells read by ghost stencils) and extra
+    //      targets (coarser cells receiving reflux); both lists are bounded by ncell
+    int* d_nx = nullptr;  // [0] extra-prim count, [1] extra-target count
+    int* d_xp = nullptr;
+    int* d_textra = nullptr;
+    auto cleanup = [&]() { cudaFree(d_nx); cudaFree(d_xp); cudaFree(d_textra); };
+    if (int rc = dalloc(c, &d_nx, 8, "plan counters")) return rc;
+    if (int rc = dalloc(c, &d_xp, (size_t)c->ncell + 1, "xprim")) { cleanup(); return rc; }
+    if (int rc = dalloc(c, &d_textra, (size_t)c->ncell + 1, "textra")) { cleanup(); return rc; }
+    cudaMemsetAsync(d_nx, 0, sizeof(int) * 8, s);
+    k_plan_xprim<NDIM><<<nblk(nc), TPB, 0, s>>>(nc, c->d_cpos, P.icn, P.stc, P.kind, c->d_pmark, d_xp, d_nx);
+    k_ev_claim<NDIM><<<nblk(nc), TPB, 0, s>>>(nc, c->d_cpos, P.icn, P.kind, c->d_tmap, d_textra, d_nx + 1);
+    cudaMemcpyAsync(hv, d_nx, 2 * sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&P.nactive, d_nact, sizeof(long long), cudaMemcpyDeviceToHost, s);
+    if (int rc = check_cuda(c, cudaStreamSynchronize(s), "plan extras")) { cleanup(); return rc; }
+    P.nextra_prim = hv[0];
+    int nextra = hv[1];
+    P.ntarg = nc + nextra;
+    if (int rc = dalloc(c, &P.xprim, (size_t)P.nextra_prim, "xprim")) { cleanup(); return rc; }
+    if (int rc = dalloc(c, &P.textra, (size_t)nextra, "textra")) { cleanup(); return rc; }
+    if (P.nextra_prim) cudaMemcpyAsync(P.xprim, d_xp, sizeof(int) * P.nextra_prim, cudaMemcpyDeviceToDevice, s);
+    if (nextra) cudaMemcpyAsync(P.textra, d_textra, sizeof(int) * nextra, cudaMemcpyDeviceToDevice, s);
+
+    // ---- ordered event lists (CSR over targets)
+    // targets are distinct cells, so ntarg + 1 <= ncell + 1 and d_xp can hold the counts
+    int* cnt = d_xp;
+    if ((size_t)P.ntarg + 1 > (size_t)c->ncell + 1) { cleanup(); return set_error(c, RG_ERR_TOPOLOGY, "too many targets"); }
+    cudaMemsetAsync(cnt, 0, sizeof(int) * ((size_t)P.ntarg + 1), s);
+    k_ev_count<NDIM><<<nblk(nc), TPB, 0, s>>>(nc, c->d_cpos, c->d_tmap, P.icn, P.kind, cnt);
+    if (int rc = dalloc(c, &P.toff, (size_t)P.ntarg + 1, "toff")) { cleanup(); return rc; }
+    int total = 0;
+    if (int rc = exclusive_scan(c, cnt, P.toff, P.ntarg + 1, &total)) { cleanup(); return rc; }
+    P.nevents = total;
+    if (int rc = dalloc(c, &P.tev, (size_t)total, "events")) { cleanup(); return rc; }
+    cudaMemsetAsync(cnt, 0, sizeof(int) * ((size_t)P.ntarg + 1), s);
+    k_ev_fill<NDIM><<<nblk(nc), TPB, 0, s>>>(nc, P.level0, P.noct, c->d_cpos, c->d_tmap, P.icn, P.kind, P.toff, cnt,
+                                             P.tev);
+    k_ev_sort<<<nblk(P.ntarg), TPB, 0, s>>>(P.ntarg, P.toff, P.tev);
+    int rc_ev = check_cuda(c, cudaStreamSynchronize(s), "plan events");
+    cleanup();
+    if (rc_ev) return rc_ev;
+    if (int rc = check_device_status(c)) return rc;
+    P.valid = true;
+    return RG_OK;
+}
+
+}  // namespace
+
+int build_plan(rg_ctx* c, int ilevel, Plan& plan) {
+    switch (c->params.ndim) {
+        case 1: return build_plan_t<1>(c, ilevel, plan);
+        case 3: return build_plan_t<3>(c, ilevel, plan);
+        default: return set_error(c, RG_ERR_UNSUPPORTED, "ndim must be 1 or 3");
+    }
+}
+
+}  // namespace rg

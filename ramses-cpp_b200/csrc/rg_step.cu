@@ -1,0 +1,582 @@
+// rg_step.cu -- the per-substep kernels of the Godunov level step.
+//
+// One level substep (Simulation.cpp:548-614 of RAMSES-CPP) is, on the device:
+//   k_courant   per-cell CFL candidate + exact min-reduction
+//               (HydroSolver::compute_courant_step, HydroSolver.cpp:878-977)
+//   k_set_unew  unew <- uold on the level           (HydroSolver.cpp:575-590)
+//   k_prim      conservative -> primitive, once per cell the level reads
+//               (the reference recomputes it ~34x per cell update)
+//   k_face      per (cell, dimension): the cell's own MUSCL-Hancock trace,
+//               the neighbours' face states (ghost / same-level / boundary
+//               branches) and the two Riemann fluxes of the cell's faces
+//               (HydroSolver.cpp:93-115,118-474)
+//   k_fold      per target cell: its updates applied in the CPU order --
+//               refluxes from neighbours processed earlier, its own flux sum
+//               and clamps, refluxes from later neighbours
+//               (HydroSolver.cpp:476-547)
+//   k_set_uold  uold <- unew where son == 0          (HydroSolver.cpp:592-611)
+// All FP64; compiled with -fmad=false so every result is bit-identical to the
+// reference's x86-64 build for the HLLC/HLL/LLF/acoustic solvers.
+#include <algorithm>
+
+#include "rg_internal.cuh"
+#include "rg_physics.cuh"
+
+namespace rg {
+
+namespace {
+
+__device__ __forceinline__ int cell_of(const TreeView& T, const PlanView& P, int p) {
+    if (P.level0) return p + 1;
+    int icx = p / P.noct, k = p - icx * P.noct;
+    return T.ncoarse + icx * T.ngridmax + P.octs[k];
+}
+
+// Primitive state of cell id, rotated so the velocity along idim sits at 1.
+template <int NDIM>
+__device__ __forceinline__ void load_rot(const double* __restrict__ prim, size_t ncell, int id, int idim, double* q) {
+    constexpr int NV = Dims<NDIM>::NV;
+    const double* b = prim + (size_t)(id - 1);
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) q[iv] = __ldg(b + iv * ncell);
+    rot_swap<NDIM>(q, idim);
+}
+
+// Neighbour primitive for a slope stencil: the cell's own state when the
+// neighbour id is <= 0, with the normal velocity flipped for a reflecting
+// boundary entry (HydroSolver.cpp:661-664, 194-204).
+template <int NDIM>
+__device__ __forceinline__ void load_nb_rot(const TreeView& T, const double* __restrict__ prim, size_t ncell, int id,
+                                            int idim, const double* qself, double* q) {
+    constexpr int NV = Dims<NDIM>::NV;
+    if (id > 0) {
+        load_rot<NDIM>(prim, ncell, id, idim, q);
+        return;
+    }
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) q[iv] = qself[iv];
+    int ib = -id;
+    if (ib > 0 && ib <= T.nbound_type && T.bound_type[ib - 1] == 1) q[1] *= -1.0;
+}
+
+struct StepK {
+    double gamma, smalle;
+    int slope_type, interpol_type, interpol_var, exact_niter;
+    double exact_tol;
+};
+
+// Own trace (compute_slopes + trace, HydroSolver.cpp:653-732) on rotated data.
+template <int NDIM>
+__device__ __forceinline__ void own_trace(const double* qc, const double* ql, const double* qr, double dt, double dx,
+                                          const StepK& K, double* qm, double* qp) {
+    constexpr int NV = Dims<NDIM>::NV;
+    double dq[NV];
+    double nu = qc[1] * dt / dx;
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) {
+        if (K.slope_type == 0) dq[iv] = 0.0;
+        else if ((K.slope_type == 5 || K.slope_type == 6) && iv != 0) dq[iv] = 0.0;
+        else dq[iv] = compute_slope(ql[iv], qc[iv], qr[iv], K.slope_type, 1.5, nu) / dx;
+    }
+    trace<NDIM>(qc, dq, dt, dx, qm, qp, K.gamma);
+}
+
+// Ghost trace of a coarser (or same-level) neighbour, 2D/3D form
+// (HydroSolver.cpp:357-440): interpolation slopes over 2dx.
+template <int NDIM>
+__device__ __forceinline__ void ghost_trace(const double* qc, const double* ql, const double* qr, double dt,
+                                            double dx, const StepK& K, double* qm, double* qp) {
+    constexpr int NV = Dims<NDIM>::NV;
+    double dq[NV];
+    double dxc = 2.0 * dx;
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) {
+        double dlft = qc[iv] - ql[iv];
+        double drgt = qr[iv] - qc[iv];
+        double slope = 0.0;
+        if (K.interpol_type > 0 && dlft * drgt > 0.0) slope = interp_slope(dlft, drgt, K.interpol_type);
+        dq[iv] = slope / dxc;
+    }
+    trace<NDIM>(qc, dq, dt, dxc, qm, qp, K.gamma);
+}
+
+// Ghost face state of the 1D build (HydroSolver.cpp:219-356): the coarse
+// neighbour's child states, then a slope_type slope against the active cell.
+__device__ void ghost_1d(const double* __restrict__ uold, size_t ncell, const TreeView& T, int n, int nl, int nr,
+                         int side, const double* q_act, double dt, double dx, const StepK& K, double* qm,
+                         double* qp) {
+    constexpr int NV = 3;
+    double uc[NV], ul[NV], ur[NV];
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) uc[iv] = uold[(size_t)iv * ncell + n - 1];
+    for (int k = 0; k < 2; ++k) {
+        int id = k ? nr : nl;
+        double* uo = k ? ur : ul;
+        if (id > 0) {
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) uo[iv] = uold[(size_t)iv * ncell + id - 1];
+        } else {
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) uo[iv] = uc[iv];
+            int ib = -id;
+            if (ib > 0 && ib <= T.nbound_type && T.bound_type[ib - 1] == 1) uo[1] *= -1.0;
+        }
+    }
+    const double gamma = K.gamma;
+    const int ivar = K.interpol_var, itp = K.interpol_type;
+    double q1[3][NV];
+    const double* us[3] = {ul, uc, ur};
+    for (int k = 0; k < 3; ++k) {
+        const double* u = us[k];
+        double* q = q1[k];
+        if (ivar == 0) {
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) q[iv] = u[iv];
+        } else if (ivar == 1) {
+            double d = smax(u[0], 1e-10);
+            q[0] = u[0];
+            q[1] = 0.0;
+            double e_kin = 0.5 * u[1] * u[1] / d;
+            q[2] = u[2] - e_kin - 0.0;
+        } else {
+            ctoprim<1>(u, q, gamma, K.smalle);
+        }
+    }
+    double slopes[NV];
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) {
+        slopes[iv] = 0.0;
+        double dlft = q1[1][iv] - q1[0][iv];
+        double drgt = q1[2][iv] - q1[1][iv];
+        if (dlft * drgt > 0.0) {
+            int itype = itp;
+            if (itp == 4) itype = (ivar == 2 && iv == 1) ? 3 : 2;
+            if (itype >= 1 && itype <= 3) slopes[iv] = interp_slope(dlft, drgt, itype);
+        }
+    }
+    double uch[2][NV];
+    for (int k = 0; k < 2; ++k) {
+        double q2[NV];
+#pragma unroll
+        for (int iv = 0; iv < NV; ++iv) q2[iv] = k ? q1[1][iv] + 0.5 * slopes[iv] : q1[1][iv] - 0.5 * slopes[iv];
+        double* u = uch[k];
+        if (ivar == 0) {
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) u[iv] = q2[iv];
+        } else if (ivar == 1) {
+            double d = smax(q2[0], 1e-10);
+            u[0] = d;
+            u[1] = 0.0;
+            double e_kin = 0.5 * q2[1] * q2[1] / d;
+            u[2] = q2[2] + e_kin + 0.0;
+        } else {
+            double d = smax(q2[0], 1e-10);
+            u[0] = d;
+            u[1] = 0.0;
+            double e_kin = 0.5 * d * q2[1] * q2[1];
+            u[2] = q2[2] / (gamma - 1.0) + e_kin + 0.0;
+        }
+    }
+    double qg2[NV], qg[NV];
+    ctoprim<1>(uch[side == 0 ? 0 : 1], qg2, gamma, K.smalle);
+    ctoprim<1>(uch[side == 0 ? 1 : 0], qg, gamma, K.smalle);
+    double dq[NV];
+    double nu = qg[1] * dt / dx;
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) {
+        double dlft, drgt;
+        if (side == 0) {
+            dlft = qg[iv] - qg2[iv];
+            drgt = q_act[iv] - qg[iv];
+        } else {
+            dlft = qg[iv] - q_act[iv];
+            drgt = qg2[iv] - qg[iv];
+        }
+        if ((K.slope_type == 5 || K.slope_type == 6) && iv != 0) dq[iv] = 0.0;
+        else dq[iv] = compute_slope(qg[iv] - dlft, qg[iv], qg[iv] + drgt, K.slope_type, 1.5, nu) / dx;
+    }
+    trace<1>(qg, dq, dt, dx, qm, qp, gamma);
+}
+
+template <int NDIM, int RS>
+__device__ __forceinline__ int riemann(const double* ql, const double* qr, double* f, const StepK& K) {
+    if constexpr (RS == RG_RIEMANN_HLLC) solve_hllc<NDIM>(ql, qr, f, K.gamma);
+    else if constexpr (RS == RG_RIEMANN_HLL) solve_hll<NDIM>(ql, qr, f, K.gamma);
+    else if constexpr (RS == RG_RIEMANN_ACOUSTIC) solve_acoustic<NDIM>(ql, qr, f, K.gamma);
+    else if constexpr (RS == RG_RIEMANN_EXACT) return solve_exact<NDIM>(ql, qr, f, K.gamma, K.exact_niter, K.exact_tol, -1.0);
+    else solve_llf<NDIM>(ql, qr, f, K.gamma);
+    return 0;
+}
+
+// Face state of the neighbour across slot (idim, side), rotated.  Writes the
+// state the Riemann problem needs: the neighbour's right-face state (qm) for
+// side 0, its left-face state (qp) for side 1.
+template <int NDIM>
+__device__ __forceinline__ void neighbour_face(const TreeView& T, const PlanView& P, const double* __restrict__ prim,
+                                               const double* __restrict__ uold, size_t ncell, int p, int c, int idim,
+                                               int side, int kd, int n, const double* qc, double dt, double dx,
+                                               const StepK& K, double* qf) {
+    constexpr int NV = Dims<NDIM>::NV;
+    double qm[NV], qp[NV];
+    int kind = kd & KIND_MASK;
+    int s = 2 * idim + side;
+    if (kind == K_BOUND) {
+        double qb[NV], dq0[NV];
+#pragma unroll
+        for (int iv = 0; iv < NV; ++iv) {
+            qb[iv] = qc[iv];
+            dq0[iv] = 0.0;
+        }
+        if (kd & KIND_REFLECT) qb[1] *= -1.0;
+        trace<NDIM>(qb, dq0, dt, dx, qm, qp, K.gamma);
+    } else {
+        if (P.level0) {
+            // level 0 traces are unrotated first-order states (HydroSolver.cpp:77-91)
+            double qn[NV], dq0[NV], qmn[NV], qpn[NV];
+            load_rot<NDIM>(prim, ncell, n, 0, qn);
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) dq0[iv] = 0.0;
+            trace<NDIM>(qn, dq0, dt, dx, qmn, qpn, K.gamma);
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) {
+                qm[iv] = qmn[iv];
+                qp[iv] = qpn[iv];
+            }
+            rot_swap<NDIM>(qm, idim);
+            rot_swap<NDIM>(qp, idim);
+        } else {
+            int nl = P.stc[((size_t)s * 2 + 0) * P.ncells + p];
+            int nr = P.stc[((size_t)s * 2 + 1) * P.ncells + p];
+            if constexpr (NDIM == 1) {
+                if (kind == K_GHOST) {
+                    ghost_1d(uold, ncell, T, n, nl, nr, side, qc, dt, dx, K, qm, qp);
+                    goto have_face;
+                }
+            }
+            {
+                double qn[NV], qnl[NV], qnr[NV];
+                load_rot<NDIM>(prim, ncell, n, idim, qn);
+                load_nb_rot<NDIM>(T, prim, ncell, nl, idim, qn, qnl);
+                load_nb_rot<NDIM>(T, prim, ncell, nr, idim, qn, qnr);
+                if (kind == K_GHOST) ghost_trace<NDIM>(qn, qnl, qnr, dt, dx, K, qm, qp);
+                else own_trace<NDIM>(qn, qnl, qnr, dt, dx, K, qm, qp);
+            }
+        have_face:;
+        }
+    }
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) qf[iv] = side == 0 ? qm[iv] : qp[iv];
+}
+
+template <int NDIM, int RS>
+__global__ void __launch_bounds__(128) k_face(TreeView T, PlanView P, const double* __restrict__ prim,
+                                              const double* __restrict__ uold, double* __restrict__ flux,
+                                              const DevStatus* __restrict__ st, StepK K,
+                                              unsigned long long* __restrict__ exact_iters) {
+    constexpr int NV = Dims<NDIM>::NV;
+    const size_t ncell = (size_t)T.ncell;
+    const int nc = P.ncells;
+    const double dt = st->dt, dx = st->dx;
+    const long long total = (long long)nc * NDIM;
+    unsigned long long iters = 0;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int idim = (int)(t / nc), p = (int)(t - (long long)idim * nc);
+        int s0 = 2 * idim;
+        int kd0 = P.kind[(size_t)s0 * nc + p];
+        if (kd0 == K_NONE) continue;
+        int kd1 = P.kind[(size_t)(s0 + 1) * nc + p];
+        int c = cell_of(T, P, p);
+        double qc[NV], qmo[NV], qpo[NV];
+        load_rot<NDIM>(prim, ncell, c, idim, qc);
+        if (P.level0) {
+            double qn[NV], dq0[NV];
+            load_rot<NDIM>(prim, ncell, c, 0, qn);
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) dq0[iv] = 0.0;
+            trace<NDIM>(qn, dq0, dt, dx, qmo, qpo, K.gamma);
+            rot_swap<NDIM>(qmo, idim);
+            rot_swap<NDIM>(qpo, idim);
+        } else {
+            int l = P.icn[(size_t)s0 * nc + p], r = P.icn[(size_t)(s0 + 1) * nc + p];
+            double ql[NV], qr[NV];
+            load_nb_rot<NDIM>(T, prim, ncell, l, idim, qc, ql);
+            load_nb_rot<NDIM>(T, prim, ncell, r, idim, qc, qr);
+            own_trace<NDIM>(qc, ql, qr, dt, dx, K, qmo, qpo);
+        }
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            int kd = side ? kd1 : kd0;
+            int s = s0 + side;
+            double f[NV];
+            if ((kd & KIND_MASK) == K_ZERO) {
+#pragma unroll
+                for (int iv = 0; iv < NV; ++iv) f[iv] = 0.0;
+            } else {
+                int n = P.icn[(size_t)s * nc + p];
+                double qf[NV];
+                neighbour_face<NDIM>(T, P, prim, uold, ncell, p, c, idim, side, kd, n, qc, dt, dx, K, qf);
+                if (side == 0) iters += riemann<NDIM, RS>(qf, qpo, f, K);
+                else iters += riemann<NDIM, RS>(qmo, qf, f, K);
+                rot_swap<NDIM>(f, idim);
+            }
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) flux[((size_t)s * NV + iv) * nc + p] = f[iv];
+        }
+    }
+    if (RS == RG_RIEMANN_EXACT && exact_iters && iters) atomicAdd(exact_iters, iters);
+}
+
+template <int NDIM>
+__global__ void k_prim(TreeView T, PlanView P, const double* __restrict__ uold, double* __restrict__ prim,
+                       double gamma, double smalle) {
+    constexpr int NV = Dims<NDIM>::NV;
+    const size_t ncell = (size_t)T.ncell;
+    const int total = P.ncells + P.nextra_prim;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        int c = (t < P.ncells) ? cell_of(T, P, t) : P.xprim[t - P.ncells];
+        double u[NV], q[NV];
+#pragma unroll
+        for (int iv = 0; iv < NV; ++iv) u[iv] = uold[(size_t)iv * ncell + c - 1];
+        ctoprim<NDIM>(u, q, gamma, smalle);
+#pragma unroll
+        for (int iv = 0; iv < NV; ++iv) prim[(size_t)iv * ncell + c - 1] = q[iv];
+    }
+}
+
+template <int NDIM>
+__global__ void k_fold(TreeView T, PlanView P, const double* __restrict__ flux, double* __restrict__ unew,
+                       const DevStatus* __restrict__ st, double gamma) {
+    constexpr int NV = Dims<NDIM>::NV, NS = Dims<NDIM>::NS, TTD = Dims<NDIM>::TTD;
+    const size_t ncell = (size_t)T.ncell;
+    const int nc = P.ncells;
+    const double dtdx = st->dtdx;
+    const double factor = 1.0 / (1 << NDIM);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < P.ntarg; t += gridDim.x * blockDim.x) {
+        int a = P.toff[t], b = P.toff[t + 1];
+        if (a == b) continue;
+        int cell = (t < nc) ? cell_of(T, P, t) : P.textra[t - nc];
+        double u[NV];
+#pragma unroll
+        for (int iv = 0; iv < NV; ++iv) u[iv] = unew[(size_t)iv * ncell + cell - 1];
+        for (int e = a; e < b; ++e) {
+            int key = P.tev[e];
+            int slot = key & 7, cp = key >> 3;
+            int ps = P.level0 ? cp : (cp % TTD) * P.noct + cp / TTD;
+            if (slot == OWN_SLOT) {
+                double fs[NV];
+#pragma unroll
+                for (int iv = 0; iv < NV; ++iv) fs[iv] = 0.0;
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    double sign = (s & 1) ? -1.0 : 1.0;
+#pragma unroll
+                    for (int iv = 0; iv < NV; ++iv) fs[iv] = fs[iv] + sign * flux[((size_t)s * NV + iv) * nc + ps];
+                }
+#pragma unroll
+                for (int iv = 0; iv < NV; ++iv) u[iv] = u[iv] + dtdx * fs[iv];
+                // clamps (HydroSolver.cpp:534-547)
+                double d = sclamp(u[0], 1e-10, 1e6);
+                u[0] = d;
+#pragma unroll
+                for (int i = 1; i <= NDIM; ++i) u[i] = sclamp(u[i], -d * 10.0, d * 10.0);
+                double v2 = 0.0;
+#pragma unroll
+                for (int i = 1; i <= NDIM; ++i) {
+                    double v = u[i] / d;
+                    v2 = v2 + v * v;
+                }
+                constexpr int IE = NDIM + 1;
+                double ei = u[IE] - 0.5 * d * v2;
+                if (ei < d * 1e-10 / (gamma - 1.0)) {
+                    double e_non = 0;
+                    u[IE] = d * 1e-10 / (gamma - 1.0) + 0.5 * d * v2 + e_non;
+                }
+                u[IE] = smin(u[IE], d * 1e8);
+            } else {
+                double sign = (slot & 1) ? -1.0 : 1.0;
+#pragma unroll
+                for (int iv = 0; iv < NV; ++iv)
+                    u[iv] = u[iv] - dtdx * sign * flux[((size_t)slot * NV + iv) * nc + ps] * factor;
+            }
+        }
+#pragma unroll
+        for (int iv = 0; iv < NV; ++iv) unew[(size_t)iv * ncell + cell - 1] = u[iv];
+    }
+}
+
+__global__ void k_copy_level(TreeView T, PlanView P, int nvar, const double* __restrict__ src, double* __restrict__ dst,
+                             int only_leaf) {
+    const size_t ncell = (size_t)T.ncell;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P.ncells; p += gridDim.x * blockDim.x) {
+        int c = cell_of(T, P, p);
+        if (only_leaf && T.son[c - 1] != 0) continue;
+        for (int iv = 0; iv < nvar; ++iv) dst[(size_t)iv * ncell + c - 1] = src[(size_t)iv * ncell + c - 1];
+    }
+}
+
+template <int NDIM>
+__global__ void k_courant(TreeView T, PlanView P, const double* __restrict__ uold, DevStatus* st, double dx,
+                          double gamma, double cfl, int pressure_cap) {
+    const size_t ncell = (size_t)T.ncell;
+    unsigned long long best = ~0ULL;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P.ncells; p += gridDim.x * blockDim.x) {
+        int id = cell_of(T, P, p);
+        if (T.son[id - 1] > 0) continue;
+        const double* u = uold + (id - 1);
+        double d = smax(u[0], 1e-10), v2 = 0.0;
+#pragma unroll
+        for (int i = 1; i <= NDIM; ++i) {
+            double v = u[i * ncell] / d;
+            v2 = v2 + v * v;
+        }
+        double e_non = 0.0, sum_gamma_p = 0.0;
+        double pr = smax((u[(NDIM + 1) * ncell] - 0.5 * d * v2 - e_non) * (gamma - 1.0), d * 1e-10);
+        if (pressure_cap) pr = smin(pr, d * 1e2);
+        double cs2 = cs2_of(d, pr, gamma);
+        cs2 = cs2 + sum_gamma_p / d;
+        double cs = sqrt(smax(cs2, 1e-10));
+        double u_wave = NDIM * cs;
+#pragma unroll
+        for (int i = 1; i <= NDIM; ++i) u_wave = u_wave + fabs(u[i * ncell] / d);
+        double a_grav = 0.0;
+#pragma unroll
+        for (int i = 1; i <= NDIM; ++i) a_grav = a_grav + fabs(0.0);
+        double alpha = a_grav * dx / (u_wave * u_wave);
+        alpha = smax(alpha, 0.0001);
+        double dtc = (dx / u_wave) * (sqrt(1.0 + 2.0 * cfl * alpha) - 1.0) / alpha;
+        // positive doubles order like their bit patterns; NaN patterns sort
+        // above every finite value, matching std::min's NaN fall-through.
+        unsigned long long b = (unsigned long long)__double_as_longlong(dtc);
+        if (dtc >= 0.0 && b < best) best = b;
+    }
+    // warp reduction then one atomic per warp
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
+        best = other < best ? other : best;
+    }
+    if ((threadIdx.x & 31) == 0 && best != ~0ULL) atomicMin(&st->dtmin_bits, best);
+}
+
+__global__ void k_courant_init(DevStatus* st, double dt_start) {
+    st->dtmin_bits = (unsigned long long)__double_as_longlong(dt_start);
+}
+__global__ void k_dt_finalize(DevStatus* st, double dx) {
+    double dt = __longlong_as_double((long long)st->dtmin_bits);
+    st->dt = dt;
+    st->dx = dx;
+    st->dtdx = dt / dx;
+}
+__global__ void k_dt_set(DevStatus* st, double dt, double dx) {
+    st->dt = dt;
+    st->dx = dx;
+    st->dtdx = dt / dx;
+}
+
+inline int grid_for(rg_ctx* c, long long work, int block) {
+    long long b = (work + block - 1) / block;
+    long long cap = (long long)c->sm_count * 32;
+    if (b > cap) b = cap;
+    return (int)std::max(1LL, b);
+}
+
+StepK step_consts(const rg_ctx* c) {
+    const rg_params& p = c->params;
+    StepK K;
+    K.gamma = p.gamma;
+    K.smalle = 1e-10 * 1e-10 / p.gamma / (p.gamma - 1.0);
+    K.slope_type = p.slope_type;
+    K.interpol_type = p.interpol_type;
+    K.interpol_var = p.interpol_var;
+    K.exact_niter = p.exact_niter > 0 ? p.exact_niter : 10;
+    K.exact_tol = p.exact_tol > 0 ? p.exact_tol : 1e-6;
+    return K;
+}
+
+template <int NDIM, int RS>
+void launch_face_t(rg_ctx* c, const Plan& P, const StepK& K) {
+    long long work = (long long)P.ncells * NDIM;
+    int block = 128;
+    k_face<NDIM, RS><<<grid_for(c, work, block), block, 0, c->stream>>>(
+        tree_view(c), P.view(), c->d_prim, c->d_uold, c->d_flux, c->d_status, K, nullptr);
+}
+
+template <int NDIM>
+void launch_face_n(rg_ctx* c, const Plan& P, const StepK& K) {
+    switch (c->params.riemann) {
+        case RG_RIEMANN_HLLC: launch_face_t<NDIM, RG_RIEMANN_HLLC>(c, P, K); break;
+        case RG_RIEMANN_HLL: launch_face_t<NDIM, RG_RIEMANN_HLL>(c, P, K); break;
+        case RG_RIEMANN_EXACT: launch_face_t<NDIM, RG_RIEMANN_EXACT>(c, P, K); break;
+        case RG_RIEMANN_ACOUSTIC: launch_face_t<NDIM, RG_RIEMANN_ACOUSTIC>(c, P, K); break;
+        default: launch_face_t<NDIM, RG_RIEMANN_LLF>(c, P, K); break;
+    }
+}
+
+template <int NDIM>
+int launch_godunov_t(rg_ctx* c, const Plan& P) {
+    constexpr int NV = NDIM + 2, NS = 2 * NDIM;
+    if (P.ncells == 0) return RG_OK;
+    // the caller sized the shared flux scratch (ensure_flux) outside any capture
+    if (c->cap_flux < (size_t)NS * NV * P.ncells) return set_error(c, RG_ERR_STATE, "flux scratch not sized");
+    StepK K = step_consts(c);
+    TreeView T = tree_view(c);
+    PlanView V = P.view();
+    if (c->timing) cudaEventRecord(c->ev[0], c->stream);
+    int nprim = P.ncells + P.nextra_prim;
+    k_prim<NDIM><<<grid_for(c, nprim, 256), 256, 0, c->stream>>>(T, V, c->d_uold, c->d_prim, K.gamma, K.smalle);
+    if (c->timing) cudaEventRecord(c->ev[1], c->stream);
+    launch_face_n<NDIM>(c, P, K);
+    if (c->timing) cudaEventRecord(c->ev[2], c->stream);
+    k_fold<NDIM><<<grid_for(c, P.ntarg, 256), 256, 0, c->stream>>>(T, V, c->d_flux, c->d_unew, c->d_status, K.gamma);
+    if (c->timing) cudaEventRecord(c->ev[3], c->stream);
+    return check_cuda(c, cudaGetLastError(), "godunov kernels");
+}
+
+}  // namespace
+
+int launch_godunov(rg_ctx* c, const Plan& P) {
+    if (c->params.ndim == 1) return launch_godunov_t<1>(c, P);
+    return launch_godunov_t<3>(c, P);
+}
+
+int launch_set_unew(rg_ctx* c, const Plan& P) {
+    if (P.ncells == 0) return RG_OK;
+    k_copy_level<<<grid_for(c, P.ncells, 256), 256, 0, c->stream>>>(tree_view(c), P.view(), c->nvar, c->d_uold,
+                                                                     c->d_unew, 0);
+    return check_cuda(c, cudaGetLastError(), "set_unew");
+}
+
+int launch_set_uold(rg_ctx* c, const Plan& P) {
+    if (P.ncells == 0) return RG_OK;
+    k_copy_level<<<grid_for(c, P.ncells, 256), 256, 0, c->stream>>>(tree_view(c), P.view(), c->nvar, c->d_unew,
+                                                                     c->d_uold, 1);
+    return check_cuda(c, cudaGetLastError(), "set_uold");
+}
+
+int launch_courant(rg_ctx* c, const Plan& P, double dx, int pressure_cap, double cfl) {
+    double start = c->params.boxlen / 1e-10;
+    k_courant_init<<<1, 1, 0, c->stream>>>(c->d_status, start);
+    if (P.ncells > 0) {
+        if (c->params.ndim == 1)
+            k_courant<1><<<grid_for(c, P.ncells, 256), 256, 0, c->stream>>>(tree_view(c), P.view(), c->d_uold,
+                                                                             c->d_status, dx, c->params.gamma, cfl,
+                                                                             pressure_cap);
+        else
+            k_courant<3><<<grid_for(c, P.ncells, 256), 256, 0, c->stream>>>(tree_view(c), P.view(), c->d_uold,
+                                                                             c->d_status, dx, c->params.gamma, cfl,
+                                                                             pressure_cap);
+    }
+    return check_cuda(c, cudaGetLastError(), "courant");
+}
+
+int launch_finalize_dt(rg_ctx* c, double dx) {
+    k_dt_finalize<<<1, 1, 0, c->stream>>>(c->d_status, dx);
+    return check_cuda(c, cudaGetLastError(), "dt finalize");
+}
+
+int launch_set_dt_host(rg_ctx* c, double dt, double dx) {
+    k_dt_set<<<1, 1, 0, c->stream>>>(c->d_status, dt, dx);
+    return check_cuda(c, cudaGetLastError(), "dt set");
+}
+
+}  // namespace rg

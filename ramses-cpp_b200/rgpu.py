@@ -1,0 +1,202 @@
+"""ctypes binding of librgpu.so (the C ABI declared in include/rgpu.h).
+
+This is the Python face of the same extern "C" boundary a C++ host (the
+GpuHydroSolver patch) calls; tests and bench.py use it.  It loads the
+in-tree library and fails loudly when it is missing: there is no CPU
+fallback on this path.
+"""
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "librgpu.so"
+
+I32P = C.POINTER(C.c_int)
+F64P = C.POINTER(C.c_double)
+
+RG_OK, RG_ERR_ARG, RG_ERR_CUDA, RG_ERR_UNSUPPORTED, RG_ERR_TOPOLOGY, RG_ERR_STATE, RG_ERR_TIMEOUT, RG_ERR_DEVICE, \
+    RG_ERR_NOMEM = 0, -1, -2, -3, -4, -5, -6, -7, -8
+RIEMANN = {"llf": 0, "hll": 1, "hllc": 2, "exact": 3, "acoustic": 4}
+
+
+class rg_params(C.Structure):
+    _fields_ = [("ndim", C.c_int), ("nvar", C.c_int), ("slope_type", C.c_int), ("riemann", C.c_int),
+                ("interpol_type", C.c_int), ("interpol_var", C.c_int), ("gamma", C.c_double),
+                ("courant_factor", C.c_double), ("exact_niter", C.c_int), ("exact_tol", C.c_double),
+                ("exact_guess", C.c_int), ("boxlen", C.c_double), ("flags", C.c_int)]
+
+
+class rg_grid_view(C.Structure):
+    _fields_ = [("ncoarse", C.c_int), ("ngridmax", C.c_int), ("ncell", C.c_int), ("nvar", C.c_int),
+                ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("ncpu", C.c_int),
+                ("nboundary", C.c_int), ("nlevelmax", C.c_int),
+                ("son", I32P), ("father", I32P), ("nbor", I32P), ("next", I32P), ("headl", I32P),
+                ("bound_type", I32P), ("nbound_type", C.c_int)]
+
+
+def make_params(ndim, nvar=None, slope_type=1, riemann="hllc", interpol_type=1, interpol_var=0, gamma=1.4,
+                courant_factor=0.8, exact_niter=10, exact_tol=1e-6, exact_guess=0, boxlen=1.0):
+    r = RIEMANN.get(riemann, 0) if isinstance(riemann, str) else int(riemann)
+    return rg_params(ndim, nvar if nvar else ndim + 2, slope_type, r, interpol_type, interpol_var, gamma,
+                     courant_factor, exact_niter, exact_tol, exact_guess, boxlen, 0)
+
+
+def grid_view(g):
+    """rg_grid_view over an object with the AmrGrid scalars and int32 arrays."""
+    v = rg_grid_view()
+    for k in ("ncoarse", "ngridmax", "ncell", "nvar", "nx", "ny", "nz", "ncpu", "nboundary", "nlevelmax"):
+        setattr(v, k, int(getattr(g, k)))
+    keep = []
+    for k in ("son", "father", "nbor", "next", "headl"):
+        a = np.ascontiguousarray(getattr(g, k), dtype=np.int32)
+        keep.append(a)
+        setattr(v, k, a.ctypes.data_as(I32P))
+    v.bound_type = None
+    v.nbound_type = 0
+    v._keep = keep
+    return v
+
+
+_lib = None
+
+
+def lib():
+    """Load librgpu.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: run ramses-cpp_b200/build.py (no CPU fallback exists)")
+    L = C.CDLL(str(LIB_PATH))
+    P = C.POINTER(rg_params)
+    L.rg_create.restype = C.c_void_p
+    L.rg_create.argtypes = [P, C.c_int]
+    L.rg_destroy.argtypes = [C.c_void_p]
+    L.rg_last_error.restype = C.c_char_p
+    L.rg_last_error.argtypes = [C.c_void_p]
+    L.rg_version.restype = C.c_char_p
+    L.rg_riemann_from_string.argtypes = [C.c_char_p]
+    L.rg_set_params.argtypes = [C.c_void_p, P]
+    L.rg_sync_topology.argtypes = [C.c_void_p, C.POINTER(rg_grid_view)]
+    L.rg_upload_state.argtypes = [C.c_void_p, F64P, F64P]
+    L.rg_download_state.argtypes = [C.c_void_p, F64P, F64P]
+    L.rg_device_state.argtypes = [C.c_void_p, C.POINTER(F64P), C.POINTER(F64P)]
+    L.rg_set_unew.argtypes = [C.c_void_p, C.c_int]
+    L.rg_set_uold.argtypes = [C.c_void_p, C.c_int]
+    L.rg_godunov_level.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double]
+    L.rg_courant_step.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_int, F64P]
+    L.rg_level_substep.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, F64P]
+    L.rg_synchronize.argtypes = [C.c_void_p]
+    L.rg_level_octs.argtypes = [C.c_void_p, C.c_int, I32P, C.c_int, I32P]
+    L.rg_level_nbor_cells.argtypes = [C.c_void_p, C.c_int, I32P, C.c_int]
+    L.rg_level_cell_updates.restype = C.c_int64
+    L.rg_level_cell_updates.argtypes = [C.c_void_p, C.c_int]
+    L.rg_last_kernel_ms.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_int]
+    _lib = L
+    return L
+
+
+class RGError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"rgpu error {code}: {msg}")
+        self.code = code
+
+
+def _f64(a):
+    return a.ctypes.data_as(F64P) if a is not None else None
+
+
+class Context:
+    """One rg_ctx: device mirror of an AmrGrid plus the level-step kernels."""
+
+    def __init__(self, params, device=-1):
+        self.L = lib()
+        self.params = params
+        self.h = self.L.rg_create(C.byref(params), device)
+        if not self.h:
+            raise RGError(RG_ERR_NOMEM, "rg_create returned NULL")
+        self._view = None
+        self.ncell = 0
+        self.nvar = params.nvar
+
+    def _chk(self, rc):
+        if rc != RG_OK:
+            raise RGError(rc, self.L.rg_last_error(self.h).decode())
+        return rc
+
+    def close(self):
+        if self.h:
+            self.L.rg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, params):
+        self.params = params
+        self._chk(self.L.rg_set_params(self.h, C.byref(params)))
+
+    def sync_topology(self, g):
+        self._view = grid_view(g)
+        self.ncell = int(g.ncell)
+        self._chk(self.L.rg_sync_topology(self.h, C.byref(self._view)))
+
+    def upload_state(self, uold=None, unew=None):
+        self._chk(self.L.rg_upload_state(self.h, _f64(uold), _f64(unew)))
+
+    def download_state(self, uold=None, unew=None):
+        self._chk(self.L.rg_download_state(self.h, _f64(uold), _f64(unew)))
+
+    def device_state(self):
+        a, b = F64P(), F64P()
+        self._chk(self.L.rg_device_state(self.h, C.byref(a), C.byref(b)))
+        return C.cast(a, C.c_void_p).value, C.cast(b, C.c_void_p).value
+
+    def set_unew(self, il):
+        self._chk(self.L.rg_set_unew(self.h, il))
+
+    def set_uold(self, il):
+        self._chk(self.L.rg_set_uold(self.h, il))
+
+    def godunov_level(self, il, dt, dx):
+        self._chk(self.L.rg_godunov_level(self.h, il, dt, dx))
+
+    def courant_step(self, il, dx, cfl, pressure_cap=True):
+        out = C.c_double(0)
+        self._chk(self.L.rg_courant_step(self.h, il, dx, cfl, 1 if pressure_cap else 0, C.byref(out)))
+        return out.value
+
+    def level_substep(self, il, dx, pressure_cap=False, use_graph=True, want_dt=False):
+        out = C.c_double(0)
+        self._chk(self.L.rg_level_substep(self.h, il, dx, 1 if pressure_cap else 0, 1 if use_graph else 0,
+                                          C.byref(out) if want_dt else None))
+        return out.value if want_dt else None
+
+    def synchronize(self):
+        self._chk(self.L.rg_synchronize(self.h))
+
+    def level_octs(self, il):
+        n = C.c_int(0)
+        self._chk(self.L.rg_level_octs(self.h, il, None, 0, C.byref(n)))
+        out = np.zeros(max(n.value, 1), dtype=np.int32)
+        self._chk(self.L.rg_level_octs(self.h, il, out.ctypes.data_as(I32P), n.value, C.byref(n)))
+        return out[:n.value]
+
+    def level_nbor_cells(self, il, ncells):
+        out = np.zeros(max(ncells * 6, 1), dtype=np.int32)
+        self._chk(self.L.rg_level_nbor_cells(self.h, il, out.ctypes.data_as(I32P), out.size))
+        return out[:ncells * 6].reshape(ncells, 6)
+
+    def cell_updates(self, il):
+        return int(self.L.rg_level_cell_updates(self.h, il))
+
+    def kernel_ms(self):
+        out = (C.c_float * 3)()
+        rc = self.L.rg_last_kernel_ms(self.h, out, 3)
+        return list(out) if rc == RG_OK else None

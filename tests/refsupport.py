@@ -24,28 +24,10 @@ I32P = C.POINTER(C.c_int)
 F64P = C.POINTER(C.c_double)
 
 
-class rg_params(C.Structure):
-    _fields_ = [("ndim", C.c_int), ("nvar", C.c_int), ("slope_type", C.c_int), ("riemann", C.c_int),
-                ("interpol_type", C.c_int), ("interpol_var", C.c_int), ("gamma", C.c_double),
-                ("courant_factor", C.c_double), ("exact_niter", C.c_int), ("exact_tol", C.c_double),
-                ("exact_guess", C.c_int), ("boxlen", C.c_double), ("flags", C.c_int)]
-
-
-class rg_grid_view(C.Structure):
-    _fields_ = [("ncoarse", C.c_int), ("ngridmax", C.c_int), ("ncell", C.c_int), ("nvar", C.c_int),
-                ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("ncpu", C.c_int),
-                ("nboundary", C.c_int), ("nlevelmax", C.c_int),
-                ("son", I32P), ("father", I32P), ("nbor", I32P), ("next", I32P), ("headl", I32P),
-                ("bound_type", I32P), ("nbound_type", C.c_int)]
-
-
-RIEMANN = {"llf": 0, "hll": 1, "hllc": 2, "exact": 3, "acoustic": 4}
-
-
-def make_params(ndim, nvar=None, slope_type=1, riemann="hllc", interpol_type=1, interpol_var=0,
-                gamma=1.4, courant_factor=0.8, exact_niter=10, exact_tol=1e-6, exact_guess=0, boxlen=1.0):
-    return rg_params(ndim, nvar if nvar else ndim + 2, slope_type, RIEMANN.get(riemann, 0), interpol_type,
-                     interpol_var, gamma, courant_factor, exact_niter, exact_tol, exact_guess, boxlen, 0)
+# The ABI structs of include/rgpu.h, shared with the GPU binding.
+import sys as _sys  # noqa: E402
+_sys.path.insert(0, str(ROOT / "ramses-cpp_b200"))
+from rgpu import RIEMANN, make_params, rg_grid_view, rg_params  # noqa: E402,F401
 
 
 def _ptr(a, t):
@@ -294,3 +276,181 @@ class Oracle:
 
     def slope(self, ql, qc, qr, t, theta=1.5, nu=0.0):
         return self.lib.orc_compute_slope(ql, qc, qr, t, theta, nu)
+
+
+# ------------------------------------------------------------------ AMR replay
+
+def harness_cell_centers(h, ids):
+    """Cell centres computed like AmrGrid::get_cell_center, vectorised over ids."""
+    a = h.arrays()
+    ncoarse, ngm, nx, ndim = h.get("ncoarse"), h.get("ngridmax"), h.get("nx"), h.ndim
+    ny, nz = h.get("ny"), h.get("nz")
+    ids = np.asarray(ids, dtype=np.int64)
+    out = np.full((len(ids), 3), 0.5)
+    coarse = ids <= ncoarse
+    if coarse.any():
+        idx = ids[coarse] - 1
+        dxc = 1.0 / max(nx, ny, nz)
+        xyz = [idx % nx, (idx % (nx * ny)) // nx, idx // (nx * ny)]
+        for d in range(ndim):
+            out[coarse, d] = (xyz[d] + 0.5) * dxc
+    fine = ~coarse
+    if fine.any():
+        rel = ids[fine] - ncoarse - 1
+        ig = rel % ngm + 1
+        icx = rel // ngm
+        level = np.ones(len(ig), np.int64)
+        curr = ig.copy()
+        father = a["father"]
+        for _ in range(64):
+            fc = father[curr - 1]
+            step = (curr > 0) & (fc > ncoarse)
+            if not step.any():
+                break
+            curr = np.where(step, (fc - ncoarse - 1) % ngm + 1, curr)
+            level += step
+        dx = 1.0 / (nx * (2.0 ** level))
+        scale = 1.0 / nx
+        xg = a["xg"]
+        for d in range(ndim):
+            bit = (icx >> d) & 1
+            out[fine, d] = xg[d * ngm + ig - 1] * scale + (bit - 0.5) * dx
+    return out
+
+
+def all_level_cells(h, nlevelmax):
+    g = h.grid()
+    ids = [np.arange(1, g.ncoarse + 1)]
+    for L in range(1, nlevelmax + 1):
+        c = g.cell_ids(L, h.ndim)
+        if len(c):
+            ids.append(c)
+    return np.concatenate(ids)
+
+
+def apply_ic(h, nlevelmax, ic_fn, gamma):
+    """Write primitive ICs rho, v, p = ic_fn(xc) into uold (and unew) of every cell."""
+    ids = all_level_cells(h, nlevelmax)
+    xc = harness_cell_centers(h, ids)
+    rho, vel, p = ic_fn(xc)
+    a = h.arrays()
+    nvar, ncell, ndim = h.nvar, h.get("ncell"), h.ndim
+    u = a["uold"].reshape(nvar, ncell)
+    u[0, ids - 1] = rho
+    for d in range(ndim):
+        u[1 + d, ids - 1] = rho * vel[d]
+    u[ndim + 1, ids - 1] = p / (gamma - 1.0) + 0.5 * rho * sum(vel[d] ** 2 for d in range(ndim))
+    a["unew"][:] = a["uold"]
+
+
+def sedov_ic(ndim, base_level, gamma=1.4, rho0=1.0, p0=1e-5, e_blast=1.0, nx=1):
+    dxb = 1.0 / (nx * 2 ** (base_level - 1))
+    p_blast = (gamma - 1.0) * e_blast / (2 * dxb) ** ndim
+
+    def fn(xc):
+        inside = np.all(np.abs(xc[:, :ndim] - 0.5) < dxb, axis=1)
+        n = len(xc)
+        return np.full(n, rho0), [np.zeros(n)] * ndim, np.where(inside, p_blast, p0)
+    return fn
+
+
+class AmrRun:
+    """Replay of Simulation::initialize / run / amr_step (src/core/Simulation.cpp:42-296,
+    366-397, 522-635) on the reference harness, with the CFL step computed by the
+    reference formula without its p <= 100 rho cap (that cap makes the Sedov blast
+    unstable) and an optional hook around every hydro call."""
+
+    def __init__(self, h, levelmin, nlevelmax, gamma, cfl=0.8, ed=-1.0, ep=-1.0, ev=-1.0, nexpand=1,
+                 oracle=None, on_godunov=None):
+        self.h, self.lmin, self.lmax, self.gamma, self.cfl = h, levelmin, nlevelmax, gamma, cfl
+        self.ed, self.ep, self.ev, self.nexp = ed, ep, ev, nexpand
+        self.nsub = [1] * 33
+        for i in range(levelmin, 33):
+            self.nsub[i] = 2
+        self.dtnew = [0.0] * 33
+        self.dtold = [0.0] * 33
+        self.t = 0.0
+        self.nstep = 0
+        self.oracle = oracle or Oracle()
+        self.on_godunov = on_godunov
+        self.cell_updates = 0
+
+    def initialize(self, ic_fn):
+        h = self.h
+        h.refine_uniform(self.lmin, self.nexp)
+        for il_ref in range(self.lmin + 1, self.lmax + 1):
+            self.init_flow(ic_fn)
+            for il in range(1, self.lmax + 1):
+                h.flag_fine(il, self.ed, self.ep, self.ev, -1.0, self.nexp, 1)
+                h.make_grid_fine(il)
+            if h.count_grids(il_ref) == 0:
+                break
+        self.init_flow(ic_fn)
+
+    def init_flow(self, ic_fn):
+        apply_ic(self.h, self.lmax, ic_fn, self.gamma)
+        for il in range(self.lmax - 1, -1, -1):
+            self.h.restrict_fine(il)
+
+    def courant(self, il, dx):
+        g = self.h.grid()
+        a = self.h.arrays()
+        return self.oracle.courant(g, self.h.ndim, self.h.nvar, il, dx, self.gamma, self.cfl, a["uold"],
+                                   pressure_cap=False)
+
+    def godunov(self, il, dt, dx):
+        if self.on_godunov:
+            self.on_godunov(self, il, dt, dx)
+        else:
+            self.h.godunov_fine(il, dt, dx)
+        self.cell_updates += self.oracle.cell_updates(self.h.grid(), self.h.ndim, il)
+
+    def amr_step(self, il, icount):
+        h = self.h
+        if il > self.lmax:
+            return
+        if h.count_grids(il) == 0 and il > 0:
+            return
+        if self.lmin < self.lmax and (il == self.lmin or icount > 1):
+            for i in range(il, self.lmax + 1):
+                h.make_grid_fine(i + 1)
+            for i in range(self.lmax, il - 1, -1):
+                h.remove_grid_fine(i + 1)
+        dx = 1.0 / (h.get("nx") * 2 ** il)
+        self.dtold[il] = self.dtnew[il]
+        self.dtnew[il] = self.courant(il, dx)
+        if il > self.lmin:
+            cand = self.dtnew[il - 1] / self.nsub[il - 1]
+            self.dtnew[il] = cand if cand < self.dtnew[il] else self.dtnew[il]
+        dt = self.dtnew[il]
+        h.set_unew(il)
+        nsub = self.nsub[il]
+        if il < self.lmax:
+            if h.count_grids(il + 1) > 0:
+                for i in range(1, nsub + 1):
+                    self.amr_step(il + 1, i)
+            else:
+                self.dtold[il + 1] = self.dtnew[il] / nsub
+                self.dtnew[il + 1] = self.dtnew[il] / nsub
+                self.t += dt
+                self.nstep += 1
+        else:
+            self.t += dt
+            self.nstep += 1
+        self.godunov(il, dt, dx)
+        h.set_uold(il)
+        if il < self.lmax:
+            h.restrict_fine(il)
+        h.flag_fine(il + 1, self.ed, self.ep, self.ev, -1.0, self.nexp, icount, self.nsub[il - 1] if il > 0 else 1)
+
+    def coarse_step(self):
+        h = self.h
+        if self.lmin < self.lmax:
+            for il in range(1, self.lmin):
+                h.make_grid_fine(il)
+        self.amr_step(self.lmin, 1)
+        for il in range(self.lmin, 0, -1):
+            h.flag_fine(il, self.ed, self.ep, self.ev, -1.0, self.nexp, 2, 2)
+        if self.lmin < self.lmax:
+            for il in range(self.lmin - 1, -1, -1):
+                h.restrict_fine(il)

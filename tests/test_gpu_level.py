@@ -1,0 +1,250 @@
+"""GPU level step (librgpu.so through its C ABI) against the oracle and the
+reference's golden vectors.  Bit-exact for integer work and for the
+HLLC/HLL/LLF/acoustic solvers; the exact solver differs only through pow()
+(CUDA vs glibc) and is held to 3e-12 relative."""
+import numpy as np
+import pytest
+
+import rg_tree
+import rgpu
+from refsupport import GridArrays, make_params
+
+pytestmark = pytest.mark.gpu
+
+RIEMANN_NAMES = ["llf", "hll", "hllc", "exact", "acoustic"]
+EXACT_RTOL = 3e-12
+
+
+def bits_equal(a, b):
+    return np.array_equal(np.ascontiguousarray(a).view(np.int64), np.ascontiguousarray(b).view(np.int64))
+
+
+def close_rel(a, b, rtol=EXACT_RTOL):
+    """|a-b| <= rtol * max(|a|, |b|, floor) per entry; floor avoids 0/0 near zero."""
+    scale = np.maximum(np.maximum(np.abs(a), np.abs(b)), 1e-300)
+    return bool(np.all(np.abs(a - b) <= rtol * scale + 1e-300))
+
+
+def ga_of(g):
+    return GridArrays(ncoarse=g.ncoarse, ngridmax=g.ngridmax, ncell=g.ncell, nvar=g.nvar, nx=g.nx, ny=g.ny,
+                      nz=g.nz, ncpu=1, nboundary=0, nlevelmax=g.nlevelmax, son=g.son, father=g.father, nbor=g.nbor,
+                      next=g.next, headl=g.headl)
+
+
+@pytest.fixture(scope="module")
+def ctx_factory(rgpu_lib):
+    made = []
+
+    def make(params):
+        c = rgpu.Context(params, 0)
+        made.append(c)
+        return c
+    yield make
+    for c in made:
+        c.close()
+
+
+@pytest.mark.parametrize("riem,slope,itype", [("hllc", 2, 1), ("hllc", 1, 2), ("llf", 8, 3), ("hll", 4, 1),
+                                              ("acoustic", 7, 4), ("hllc", 5, 0), ("llf", 6, 1), ("hllc", 0, 2),
+                                              ("exact", 2, 1)])
+def test_uniform_3d_matches_oracle(ctx_factory, oracle, riem, slope, itype):
+    L = 5
+    g = rg_tree.build_uniform(3, L)
+    ga = ga_of(g)
+    params = make_params(3, slope_type=slope, riemann=riem, interpol_type=itype)
+    ctx = ctx_factory(params)
+    ctx.sync_topology(g)
+    uold = rg_tree.random_state(g, L, seed=slope * 11 + itype)
+    unew = uold.copy()
+    ctx.upload_state(uold, unew)
+    dx = 1.0 / 2 ** L
+    for step in range(3):
+        dt = 0.4 * oracle.courant(ga, 3, 5, L, dx, 1.4, 0.8, uold, pressure_cap=False)
+        oracle.set_unew(ga, 3, 5, L, uold, unew)
+        oracle.godunov_fine(ga, params, L, dt, dx, uold, unew)
+        ctx.set_unew(L)
+        ctx.godunov_level(L, dt, dx)
+        got = np.empty_like(unew)
+        ctx.download_state(unew=got)
+        if riem == "exact":
+            assert close_rel(got, unew), f"step {step}"
+            ctx.upload_state(unew=unew)  # continue from the oracle state
+        else:
+            assert bits_equal(got, unew), f"step {step}: {np.count_nonzero(got != unew)} values differ"
+        oracle.set_uold(ga, 3, 5, L, uold, unew)
+        ctx.set_uold(L)
+    got_old = np.empty_like(uold)
+    ctx.download_state(uold=got_old)
+    assert close_rel(got_old, uold) if riem == "exact" else bits_equal(got_old, uold)
+
+
+def test_golden_uniform_cases(ctx_factory, golden):
+    d = golden("uniform")
+    keys = sorted({k.split("_")[0] for k in d.files})
+    for key in keys:
+        ndim, L, slope, riem, itype = (int(x) for x in d[f"{key}_meta"])
+        g = rg_tree.build_uniform(ndim, L)
+        params = make_params(ndim, slope_type=slope, riemann=RIEMANN_NAMES[riem], interpol_type=itype)
+        ctx = ctx_factory(params)
+        ctx.sync_topology(g)
+        dt, dx = (float(x) for x in d[f"{key}_dtdx"])
+        u0 = d[f"{key}_uold"]
+        ctx.upload_state(u0, u0)
+        ctx.godunov_level(L, dt, dx)
+        got = np.empty_like(u0)
+        ctx.download_state(unew=got)
+        want = d[f"{key}_unew"]
+        if RIEMANN_NAMES[riem] == "exact":
+            assert close_rel(got, want), key
+        else:
+            assert bits_equal(got, want), key
+
+
+@pytest.mark.parametrize("fixture", ["amr3d", "amr1d"])
+def test_golden_amr_calls(ctx_factory, golden, fixture):
+    """godunov_fine calls recorded from a sub-cycled AMR run of the reference:
+    coarse-fine ghost states and reflux into coarser cells, bit-exact."""
+    d = golden(fixture)
+    ndim, slope, riem = (int(x) for x in d["params"])
+    params = make_params(ndim, slope_type=slope, riemann=RIEMANN_NAMES[riem])
+    for k in sorted({k.split("_")[0] for k in d.files if k.startswith("L")}):
+        ncoarse, ngm, ncell, nvar, nx, ny, nz, nlevelmax, il = (int(x) for x in d[f"{k}_meta"])
+        g = GridArrays(ncoarse=ncoarse, ngridmax=ngm, ncell=ncell, nvar=nvar, nx=nx, ny=ny, nz=nz, ncpu=1,
+                       nboundary=0, nlevelmax=nlevelmax, son=d[f"{k}_son"], father=d[f"{k}_father"],
+                       nbor=d[f"{k}_nbor"], next=d[f"{k}_next"], headl=d[f"{k}_headl"])
+        ctx = ctx_factory(params)
+        ctx.sync_topology(g)
+        dt, dx = (float(x) for x in d[f"{k}_dtdx"])
+        ctx.upload_state(d[f"{k}_uold"], d[f"{k}_unew_in"])
+        ctx.godunov_level(il, dt, dx)
+        got = np.empty(nvar * ncell)
+        ctx.download_state(unew=got)
+        assert bits_equal(got, d[f"{k}_unew_out"]), f"{fixture} {k}: {np.count_nonzero(got != d[f'{k}_unew_out'])}"
+
+
+def test_level_index_matches_oracle(ctx_factory, oracle, golden):
+    """Oct order (level linked list) and neighbour cells (get_nbor_cells): exact."""
+    d = golden("amr3d")
+    for k in ("L3", "L4", "L5"):
+        ncoarse, ngm, ncell, nvar, nx, ny, nz, nlevelmax, il = (int(x) for x in d[f"{k}_meta"])
+        g = GridArrays(ncoarse=ncoarse, ngridmax=ngm, ncell=ncell, nvar=nvar, nx=nx, ny=ny, nz=nz, ncpu=1,
+                       nboundary=0, nlevelmax=nlevelmax, son=d[f"{k}_son"], father=d[f"{k}_father"],
+                       nbor=d[f"{k}_nbor"], next=d[f"{k}_next"], headl=d[f"{k}_headl"])
+        ctx = ctx_factory(make_params(3, slope_type=2, riemann="hllc"))
+        ctx.sync_topology(g)
+        octs = ctx.level_octs(il)
+        assert np.array_equal(octs, g.level_octs(il))
+        icn = ctx.level_nbor_cells(il, len(octs) * 8)
+        want = np.array([oracle.nbor_cells(g, 3, int(ig), ic) for ig in octs for ic in range(1, 9)])
+        assert np.array_equal(icn, want)
+
+
+def test_courant_matches_oracle(ctx_factory, oracle):
+    L = 5
+    g = rg_tree.build_uniform(3, L)
+    ga = ga_of(g)
+    ctx = ctx_factory(make_params(3))
+    ctx.sync_topology(g)
+    u = rg_tree.random_state(g, L, seed=5, p_range=(-3, 5))
+    ctx.upload_state(u, u)
+    dx = 1.0 / 2 ** L
+    for cap in (True, False):
+        assert ctx.courant_step(L, dx, 0.8, cap) == oracle.courant(ga, 3, 5, L, dx, 1.4, 0.8, u, pressure_cap=cap)
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_device_substep_sedov(ctx_factory, oracle, use_graph):
+    """rg_level_substep (on-device CFL, set_unew, godunov, set_uold; optionally a
+    CUDA graph) against the oracle sequence with the same uncapped CFL."""
+    L = 6
+    g = rg_tree.build_uniform(3, L)
+    ga = ga_of(g)
+    params = make_params(3, slope_type=2, riemann="hllc")
+    ctx = ctx_factory(params)
+    ctx.sync_topology(g)
+    uold = rg_tree.sedov_state(g, L)
+    unew = uold.copy()
+    ctx.upload_state(uold, unew)
+    dx = 1.0 / 2 ** L
+    for step in range(6):
+        dt = oracle.courant(ga, 3, 5, L, dx, 1.4, 0.8, uold, pressure_cap=False)
+        oracle.set_unew(ga, 3, 5, L, uold, unew)
+        oracle.godunov_fine(ga, params, L, dt, dx, uold, unew)
+        oracle.set_uold(ga, 3, 5, L, uold, unew)
+        dt_gpu = ctx.level_substep(L, dx, pressure_cap=False, use_graph=use_graph, want_dt=True)
+        assert dt_gpu == dt, step
+    got = np.empty_like(uold)
+    ctx.download_state(uold=got)
+    assert bits_equal(got, uold)
+    assert ctx.cell_updates(L) == 32 ** 3
+
+
+def test_sod_1d_matches_golden(ctx_factory, golden):
+    d = golden("sod1d")
+    ndim, L = (int(x) for x in d["meta"])
+    g = rg_tree.build_uniform(ndim, L)
+    ctx = ctx_factory(make_params(1, slope_type=1, riemann="hllc"))
+    ctx.sync_topology(g)
+    ctx.upload_state(d["uold0"], d["uold0"])
+    dx = 1.0 / 2 ** L
+    for dt_ref in d["dts"]:
+        dt = ctx.courant_step(L, dx, 0.8, True)
+        assert dt == dt_ref
+        ctx.set_unew(L)
+        ctx.godunov_level(L, dt, dx)
+        ctx.set_uold(L)
+    got = np.empty_like(d["uold0"])
+    ctx.download_state(uold=got)
+    assert bits_equal(got, d["uold_final"])
+
+
+def test_full_size_128_cubed_step_matches_oracle(ctx_factory, oracle):
+    """One step at the benchmark size (128^3, reference level 8) from a
+    developed Sedov state, bit-exact against the oracle."""
+    L = 8
+    g = rg_tree.build_uniform(3, L)
+    ga = ga_of(g)
+    params = make_params(3, slope_type=2, riemann="hllc")
+    ctx = ctx_factory(params)
+    ctx.sync_topology(g)
+    u0 = rg_tree.sedov_state(g, L)
+    ctx.upload_state(u0, u0)
+    dx = 1.0 / 2 ** L
+    for _ in range(10):
+        ctx.level_substep(L, dx, pressure_cap=False, use_graph=True)
+    uold = np.empty_like(u0)
+    unew = np.empty_like(u0)
+    ctx.download_state(uold, unew)
+    dt = oracle.courant(ga, 3, 5, L, dx, 1.4, 0.8, uold, pressure_cap=False)
+    assert ctx.level_substep(L, dx, pressure_cap=False, use_graph=True, want_dt=True) == dt
+    oracle.set_unew(ga, 3, 5, L, uold, unew)
+    oracle.godunov_fine(ga, params, L, dt, dx, uold, unew)
+    oracle.set_uold(ga, 3, 5, L, uold, unew)
+    got = np.empty_like(u0)
+    ctx.download_state(uold=got)
+    assert bits_equal(got, uold)
+
+
+def test_topology_errors_are_reported(ctx_factory):
+    """Host-side fault injection: corrupt tree arrays give error codes, and the
+    context stays usable afterwards (no device fault)."""
+    L = 4
+    g = rg_tree.build_uniform(3, L)
+    ctx = ctx_factory(make_params(3))
+    bad = rg_tree.build_uniform(3, L)
+    octs = bad.level_octs[L]
+    bad.next[octs[-1] - 1] = octs[0]  # the level list becomes a cycle
+    with pytest.raises(rgpu.RGError) as e:
+        ctx.sync_topology(bad)
+    assert e.value.code == rgpu.RG_ERR_TOPOLOGY
+    ctx.sync_topology(g)
+    with pytest.raises(rgpu.RGError) as e:
+        ctx.godunov_level(L, 1e-3, 1.0 / 2 ** L)
+    assert e.value.code == rgpu.RG_ERR_STATE
+    u = rg_tree.random_state(g, L)
+    ctx.upload_state(u, u)
+    with pytest.raises(rgpu.RGError) as e:
+        ctx.godunov_level(L + 5, 1e-3, 0.1)
+    assert e.value.code == rgpu.RG_ERR_ARG
+    ctx.godunov_level(L, 1e-3, 1.0 / 2 ** L)
+    ctx.synchronize()

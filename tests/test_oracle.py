@@ -1,0 +1,196 @@
+"""The C oracle (oracle/rg_oracle.c) against the reference's golden vectors and,
+where the reference sources are present, against the reference itself.
+Bit-exact: every comparison is on the IEEE bit patterns."""
+import numpy as np
+import pytest
+
+import rg_tree
+from refsupport import GridArrays, RefHarness, make_params, namelist
+
+RIEMANN_NAMES = ["llf", "hll", "hllc", "exact", "acoustic"]
+
+
+def bits_equal(a, b):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    return a.shape == b.shape and np.array_equal(a.view(np.int64), b.view(np.int64))
+
+
+@pytest.mark.parametrize("ndim", [1, 3])
+@pytest.mark.parametrize("tag", ["soft", "hard"])
+@pytest.mark.parametrize("name", ["llf", "hll", "hllc", "acoustic", "exact"])
+def test_riemann_golden(oracle, golden, ndim, tag, name):
+    d = golden("riemann")
+    ql, qr = d[f"ql_{ndim}d_{tag}"], d[f"qr_{ndim}d_{tag}"]
+    for gamma in (1.4, 5.0 / 3.0):
+        want = d[f"flux_{name}_{ndim}d_{tag}_g{gamma:.4f}"]
+        got = np.array([oracle.riemann(name, ql[i], qr[i], gamma, ndim)[:ndim + 2] for i in range(len(ql))])
+        assert bits_equal(got, want), f"{name} {ndim}d {tag} gamma={gamma}"
+
+
+def test_slopes_golden(oracle, golden):
+    d = golden("slopes")
+    for t in range(9):
+        got = np.array([oracle.slope(a, b, c, t, 1.5, n) for a, b, c, n in zip(d["ql"], d["qc"], d["qr"], d["nu"])])
+        assert bits_equal(got, d[f"slope_{t}"]), f"slope_type {t}"
+
+
+def _uniform_case(d, key):
+    ndim, L, slope, riem, itype = (int(x) for x in d[f"{key}_meta"])
+    g = rg_tree.build_uniform(ndim, L)
+    return g, ndim, L, make_params(ndim, slope_type=slope, riemann=RIEMANN_NAMES[riem], interpol_type=itype)
+
+
+def test_uniform_golden(oracle, golden):
+    d = golden("uniform")
+    keys = sorted({k.split("_")[0] for k in d.files})
+    assert len(keys) >= 8
+    for key in keys:
+        g, ndim, L, params = _uniform_case(d, key)
+        dt, dx = d[f"{key}_dtdx"]
+        uold = d[f"{key}_uold"].copy()
+        unew = uold.copy()
+        oracle.godunov_fine(GridArrays(**_grid_kwargs(g)), params, L, float(dt), float(dx), uold, unew)
+        assert bits_equal(unew, d[f"{key}_unew"]), key
+
+
+def _grid_kwargs(g):
+    return dict(ncoarse=g.ncoarse, ngridmax=g.ngridmax, ncell=g.ncell, nvar=g.nvar, nx=g.nx, ny=g.ny, nz=g.nz,
+                ncpu=1, nboundary=0, nlevelmax=g.nlevelmax, son=g.son, father=g.father, nbor=g.nbor,
+                next=g.next, headl=g.headl)
+
+
+def test_sod_golden(oracle, golden):
+    d = golden("sod1d")
+    ndim, L = (int(x) for x in d["meta"])
+    g = rg_tree.build_uniform(ndim, L)
+    ga = GridArrays(**_grid_kwargs(g))
+    params = make_params(1, slope_type=1, riemann="hllc")
+    uold = d["uold0"].copy()
+    unew = uold.copy()
+    dx = 1.0 / 2 ** L
+    for dt_ref in d["dts"]:
+        dt = oracle.courant(ga, 1, 3, L, dx, 1.4, 0.8, uold, pressure_cap=True)
+        assert dt == dt_ref
+        oracle.set_unew(ga, 1, 3, L, uold, unew)
+        oracle.godunov_fine(ga, params, L, dt, dx, uold, unew)
+        oracle.set_uold(ga, 1, 3, L, uold, unew)
+    assert bits_equal(uold, d["uold_final"])
+
+
+def amr_grid_from_fixture(d, k):
+    ncoarse, ngm, ncell, nvar, nx, ny, nz, nlevelmax, il = (int(x) for x in d[f"{k}_meta"])
+    return GridArrays(ncoarse=ncoarse, ngridmax=ngm, ncell=ncell, nvar=nvar, nx=nx, ny=ny, nz=nz, ncpu=1,
+                      nboundary=0, nlevelmax=nlevelmax, son=d[f"{k}_son"], father=d[f"{k}_father"],
+                      nbor=d[f"{k}_nbor"], next=d[f"{k}_next"], headl=d[f"{k}_headl"]), il
+
+
+@pytest.mark.parametrize("fixture", ["amr3d", "amr1d"])
+def test_amr_golden(oracle, golden, fixture):
+    d = golden(fixture)
+    ndim, slope, riem = (int(x) for x in d["params"])
+    params = make_params(ndim, slope_type=slope, riemann=RIEMANN_NAMES[riem])
+    levels = sorted({k.split("_")[0] for k in d.files if k.startswith("L")}, key=lambda k: int(k[1:]))
+    assert len(levels) == 3
+    coarse_refluxes = 0
+    for k in levels:
+        g, il = amr_grid_from_fixture(d, k)
+        dt, dx = d[f"{k}_dtdx"]
+        uold = d[f"{k}_uold"].copy()
+        unew = d[f"{k}_unew_in"].copy()
+        oracle.godunov_fine(g, params, il, float(dt), float(dx), uold, unew)
+        assert bits_equal(unew, d[f"{k}_unew_out"]), k
+        # the level has coarse-fine interfaces: some cell outside the level changed
+        changed = np.nonzero(d[f"{k}_unew_in"] != d[f"{k}_unew_out"])[0] % g.ncell + 1
+        lvl_cells = set(g.cell_ids(il, ndim).tolist())
+        coarse_refluxes += sum(c not in lvl_cells for c in changed.tolist())
+    assert coarse_refluxes > 0, "the fixture must exercise reflux into coarser cells"
+
+
+def test_planted_mistake_is_caught(oracle, golden):
+    """A one-ulp change of one input cell must change the result: the
+    bit-exact comparisons above are sensitive enough to catch a wrong kernel."""
+    d = golden("uniform")
+    g, ndim, L, params = _uniform_case(d, "c0")
+    dt, dx = d["c0_dtdx"]
+    uold = d["c0_uold"].copy()
+    c = g.cell_ids(L)[17]
+    uold[c - 1] = np.nextafter(uold[c - 1], np.inf)
+    unew = uold.copy()
+    oracle.godunov_fine(GridArrays(**_grid_kwargs(g)), params, L, float(dt), float(dx), uold, unew)
+    assert not bits_equal(unew, d["c0_unew"])
+
+
+# ---------------------------------------------------------------- live reference
+
+@pytest.fixture(scope="module")
+def ref_ok(reference_available):
+    if not reference_available:
+        pytest.skip("reference sources not present")
+    return True
+
+
+@pytest.mark.parametrize("ndim,L,slope,riem,itype,ivar", [
+    (3, 4, 2, "hllc", 1, 0), (3, 4, 8, "llf", 2, 1), (3, 3, 4, "hll", 3, 2), (3, 4, 5, "acoustic", 4, 0),
+    (3, 3, 6, "exact", 0, 0), (3, 3, 0, "hllc", 1, 0),
+    (1, 6, 1, "hllc", 1, 0), (1, 6, 2, "hllc", 2, 1), (1, 6, 8, "llf", 4, 2), (1, 6, 5, "exact", 3, 2),
+])
+def test_oracle_matches_reference_uniform(ref_ok, oracle, ndim, L, slope, riem, itype, ivar):
+    g = rg_tree.build_uniform(ndim, L)
+    h = RefHarness(ndim).create(namelist(slope_type=slope, riemann=riem, interpol_type=itype, interpol_var=ivar,
+                                         levelmin=L, levelmax=L), ngridmax=g.ngridmax, levelmin=L, nlevelmax=L)
+    h.refine_uniform(L)
+    ga = h.grid()
+    a = h.arrays()
+    a["uold"][:] = rg_tree.random_state(g, L, seed=L * 7 + slope)
+    uo, un = a["uold"].copy(), a["unew"].copy()
+    params = make_params(ndim, slope_type=slope, riemann=riem, interpol_type=itype, interpol_var=ivar)
+    dx = 1.0 / 2 ** L
+    for _ in range(3):
+        dt = 0.4 * h.courant(L, dx, 1.4, 0.8)
+        h.set_unew(L)
+        h.godunov_fine(L, dt, dx)
+        oracle.set_unew(ga, ndim, ndim + 2, L, uo, un)
+        oracle.godunov_fine(ga, params, L, dt, dx, uo, un)
+        assert bits_equal(un, a["unew"])
+        h.set_uold(L)
+        oracle.set_uold(ga, ndim, ndim + 2, L, uo, un)
+    h.close()
+
+
+def test_oracle_matches_reference_amr(ref_ok, oracle):
+    from refsupport import AmrRun, sedov_ic
+    ndim, lmin, lmax = 3, 3, 5
+    h = RefHarness(ndim).create(namelist(slope_type=2, riemann="hllc", levelmin=lmin, levelmax=lmax,
+                                         err_grad_d=0.1, err_grad_p=0.1), ngridmax=700, levelmin=lmin,
+                                nlevelmax=lmax)
+    params = make_params(ndim, slope_type=2, riemann="hllc")
+    ncalls = []
+
+    def hook(run, il, dt, dx):
+        ga = run.h.grid()
+        a = run.h.arrays()
+        uo, un = a["uold"].copy(), a["unew"].copy()
+        run.h.godunov_fine(il, dt, dx)
+        oracle.godunov_fine(ga, params, il, dt, dx, uo, un)
+        assert bits_equal(un, a["unew"]), f"level {il}"
+        ncalls.append(il)
+
+    run = AmrRun(h, lmin, lmax, 1.4, ed=0.1, ep=0.1, on_godunov=hook)
+    run.initialize(sedov_ic(ndim, lmin))
+    for _ in range(2):
+        run.coarse_step()
+    assert set(ncalls) == {3, 4, 5}
+    h.close()
+
+
+def test_courant_matches_reference(ref_ok, oracle):
+    ndim, L = 3, 4
+    g = rg_tree.build_uniform(ndim, L)
+    h = RefHarness(ndim).create(namelist(levelmin=L, levelmax=L), ngridmax=g.ngridmax, levelmin=L, nlevelmax=L)
+    h.refine_uniform(L)
+    a = h.arrays()
+    a["uold"][:] = rg_tree.random_state(g, L, seed=3, p_range=(-2, 4))
+    dx = 1.0 / 2 ** L
+    assert h.courant(L, dx, 1.4, 0.8) == oracle.courant(h.grid(), 3, 5, L, dx, 1.4, 0.8, a["uold"], True)
+    h.close()
