@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Throughput of the B200 Godunov level step (RAMSES-CPP HydroSolver::godunov_fine).
+
+Workload: 3D Sedov blast on a uniform 128^3 grid (the reference's
+levelmin=levelmax=8), MonCen slopes, HLLC, gamma 1.4, FP64, periodic.  One
+step = one level substep through the C ABI: on-device CFL (the reference
+formula without its p <= 100 rho cap), set_unew, godunov_fine, set_uold.
+Steps past the configured 200 continue the same run.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  N > 1 runs one independent replica per GPU
+(the single-grid step has no exchange to shard), weak scaling.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "ramses-cpp_b200"))
+
+METRIC = "cell-updates/s 3D Sedov AMR FP64, %HBM roofline; Newton iters learned vs plain"
+UNIT = "cell-updates/s"
+WORKLOAD = "3D Sedov blast, uniform 128^3 (reference levelmin=levelmax=8), MonCen + HLLC, gamma 1.4, FP64"
+LEVEL = 8
+BYTES_PER_CELL_UPDATE = 80  # uold read once + unew written once, 5 FP64 variables each
+GPU_KERNELS_PER_STEP = 8    # courant init, courant, dt finalize, set_unew, prim, face, fold, set_uold
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """dram bytes per launch of the face kernel from the committed ncu summary."""
+    f = ROOT / "profiles" / "k_face_sedov128.md"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return int(float(line.split(":", 1)[1].strip()))
+            except ValueError:
+                return None
+    return None
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.rows = []
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "50", "-i", str(gpu_index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append((time.time(), line.strip()))
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self, t0, t1):
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for t, line in self.rows:
+            if not (t0 - 0.05 <= t <= t1 + 0.1):
+                continue
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- CPU side
+def cpu_sample(level, steps, kind_pref="reference"):
+    """Time the reference CPU path (or the oracle port) on ``steps`` substeps of
+    the Sedov workload at ``level``; runs in its own process (no CUDA)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import numpy as np
+    import rg_tree
+    import refsupport as rs
+    gamma, cfl = 1.4, 0.8
+    g = rg_tree.build_uniform(3, level)
+    dx = 1.0 / 2 ** level
+    orc = rs.Oracle()
+    ga = rs.GridArrays(ncoarse=g.ncoarse, ngridmax=g.ngridmax, ncell=g.ncell, nvar=g.nvar, nx=1, ny=1, nz=1, ncpu=1,
+                       nboundary=0, nlevelmax=g.nlevelmax, son=g.son, father=g.father, nbor=g.nbor, next=g.next,
+                       headl=g.headl)
+    u0 = rg_tree.sedov_state(g, level, gamma)
+    kind = "port"
+    ref_lib = rs.ORACLE_DIR / "_ref" / "libref_harness3d.so"
+    if kind_pref == "reference" and ref_lib.exists():
+        kind = "reference"
+        h = rs.RefHarness(3).create(rs.namelist(slope_type=2, riemann="hllc", levelmin=level, levelmax=level),
+                                    ngridmax=g.ngridmax, levelmin=level, nlevelmax=level, gamma=gamma)
+        h.refine_uniform(level)
+        a = h.arrays()
+        a["uold"][:] = u0
+        a["unew"][:] = u0
+        el = 0.0
+        for _ in range(steps):
+            dt = orc.courant(ga, 3, 5, level, dx, gamma, cfl, a["uold"], pressure_cap=False)
+            t = time.perf_counter()
+            h.courant(level, dx, gamma, cfl)  # the reference's own CFL pass (value unused: its cap is unstable)
+            h.set_unew(level)
+            h.godunov_fine(level, dt, dx)
+            h.set_uold(level)
+            el += time.perf_counter() - t
+        h.close()
+    else:
+        params = rs.make_params(3, slope_type=2, riemann="hllc")
+        uold, unew = u0.copy(), u0.copy()
+        el = 0.0
+        for _ in range(steps):
+            t = time.perf_counter()
+            dt = orc.courant(ga, 3, 5, level, dx, gamma, cfl, uold, pressure_cap=False)
+            orc.set_unew(ga, 3, 5, level, uold, unew)
+            orc.godunov_fine(ga, params, level, dt, dx, uold, unew)
+            orc.set_uold(ga, 3, 5, level, uold, unew)
+            el += time.perf_counter() - t
+    cells = 8 ** (level - 1) * steps
+    return {"kind": kind, "seconds": el, "cells": cells, "level": level, "steps": steps}
+
+
+def run_cpu_subprocess(level, steps):
+    cmd = [sys.executable, str(Path(__file__).resolve()), "--cpu-sample", str(level), str(steps)]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+    for line in reversed(r.stdout.splitlines()):
+        if line.startswith("{"):
+            return json.loads(line)
+    raise RuntimeError("cpu sample failed: " + r.stderr[-2000:])
+
+
+def reference_arm(args, rank, world):
+    """Times the reference's own CPU implementation of the path on all host cores."""
+    if rank != 0:
+        return None
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    # each step: every core runs one substep of the Sedov workload on a bounded
+    # sample grid, sized so that warmup+steps end within a few minutes
+    total = args.steps + args.warmup
+    level = 6 if total <= 300 else 5  # 32^3 (~0.25 s/step/core) or 16^3
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(cores) as pool:
+        res = pool.map(_ref_worker, [(level, args.steps, args.warmup)] * cores)
+    wall = time.perf_counter() - t0
+    el = max(r["seconds"] for r in res)
+    cells = sum(r["cells"] for r in res)
+    value = cells / el
+    ms = 1e3 * el / args.steps
+    sample = (f"{cores} processes x one substep of the Sedov workload on a {2 ** (level - 1)}^3 grid per step "
+              f"(reference levelmin=levelmax={level}), {args.steps} timed steps after {args.warmup} warm-up")
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "sample_grid": f"{2 ** (level - 1)}^3", "parallelism": "processes"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": res[0]["kind"], "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": wall}
+
+
+def _ref_worker(a):
+    level, steps, warm = a
+    if warm:
+        cpu_sample(level, min(warm, 2))
+    return cpu_sample(level, steps)
+
+
+# ---------------------------------------------------------------- GPU arm
+def gpu_arm(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import rg_tree
+    import rgpu
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    L = LEVEL
+    g = rg_tree.build_uniform(3, L)
+    u0 = rg_tree.sedov_state(g, L)
+    params = rgpu.make_params(3, slope_type=2, riemann="hllc", interpol_type=1, gamma=1.4, courant_factor=0.8)
+    ctx = rgpu.Context(params, local_rank)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    ctx.sync_topology(g)
+    ctx.upload_state(u0, u0)
+    dx = 1.0 / 2 ** L
+    for _ in range(args.warmup):
+        ctx.level_substep(L, dx, pressure_cap=False, use_graph=True)
+    ctx.synchronize()
+    cells = ctx.cell_updates(L)
+
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    tw0 = time.time()
+    e0.record(stream)
+    for _ in range(args.steps):
+        ctx.level_substep(L, dx, pressure_cap=False, use_graph=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    tw1 = time.time()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        dist.barrier()
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    clocks = sampler.summary(tw0, tw1) if sampler else None
+    if sampler:
+        sampler.stop()
+    value = world * cells * args.steps / (ms / 1e3)
+
+    # per-kernel device time (events around prim / face / fold, same stream)
+    ctx.set_timing(True)
+    nk = min(args.steps, 40)
+    acc = np.zeros(3)
+    for _ in range(nk):
+        ctx.level_substep(L, dx, pressure_cap=False, use_graph=False)
+        ctx.synchronize()
+        acc += np.array(ctx.kernel_ms())
+    ctx.set_timing(False)
+    kms = acc / nk
+
+    # end to end through the C ABI with host buffers: H2D uold, substep, D2H uold
+    n = g.nvar * g.ncell
+    host = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    ctx.download_state_ptr(uold_ptr=host.data_ptr())
+    ne = min(args.steps, 40)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(ne):
+        ctx.upload_state_ptr(uold_ptr=host.data_ptr())
+        ctx.level_substep(L, dx, pressure_cap=False, use_graph=True)
+        ctx.download_state_ptr(uold_ptr=host.data_ptr())
+    e3.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e2.elapsed_time(e3)
+    if dist:
+        t = torch.tensor([ms_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e_value = world * cells * ne / (ms_e2e / 1e3)
+    ctx.close()
+    if rank != 0:
+        return None
+
+    peak, peak_kind = peaks()
+    face_s = kms[1] / 1e3
+    alg_bytes = BYTES_PER_CELL_UPDATE * cells
+    achieved = alg_bytes / face_s / 1e9
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "cells_per_step": cells, "riemann": "hllc", "slope_type": 2,
+                   "cfl": "reference compute_courant_step formula, courant_factor 0.8, without the p<=100rho cap",
+                   "l2": "inputs larger than L2: uold+unew 192 MB, primitives 96 MB, flux scratch 503 MB per step",
+                   "parallelism": "replicas" if world > 1 else "single GPU", "cuda_graph": True},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": profile_traffic(), "kernel": "k_face",
+                     "algorithmic_bytes_per_launch": alg_bytes, "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
+                     "step_hbm_frac": (BYTES_PER_CELL_UPDATE * value / world / 1e9) / peak},
+        "kernel_ms": {"prim": kms[0], "face": kms[1], "fold": kms[2]},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
+                "ms_per_step": ms_e2e / ne, "path": "rg_upload_state(pinned host) + rg_level_substep + rg_download_state"},
+        "gpu_launches": GPU_KERNELS_PER_STEP * args.steps,
+        "clocks": clocks,
+    }
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", nargs=2, type=int, metavar=("LEVEL", "STEPS"), help=argparse.SUPPRESS)
+    args = ap.parse_args()
+    if args.cpu_sample:
+        print(json.dumps(cpu_sample(*args.cpu_sample)))
+        return
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if world > 1 and rank != 0:
+            return
+        out = reference_arm(args, rank, world)
+        print(json.dumps(out))
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # one full 128^3 substep of the reference on one core (~15-20 s), before any CUDA work
+        c = run_cpu_subprocess(LEVEL, 1)
+        cpu = {"value": c["cells"] / c["seconds"], "unit": UNIT, "cores": 1, "kind": c["kind"],
+               "sample": f"one substep (CFL, set_unew, godunov_fine, set_uold) of the 128^3 Sedov workload, "
+                         f"single-threaded, {c['seconds']:.1f} s"}
+    out = gpu_arm(args, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        out["cpu_baseline"] = cpu
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

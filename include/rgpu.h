@@ -150,6 +150,12 @@ int rg_courant_step(rg_ctx* ctx, int ilevel, double dx, double courant_factor,
 int rg_level_substep(rg_ctx* ctx, int ilevel, double dx, int pressure_cap,
                      int use_graph, double* dt_used);
 int rg_synchronize(rg_ctx* ctx);
+/* Run the context's work on a caller-owned cudaStream_t (passed as void*,
+ * NULL restores the context's own stream), or read the stream in use, so a
+ * host application can order the level step with its own work and time it
+ * with its own events.  Changing the stream drops captured graphs. */
+int rg_set_stream(rg_ctx* ctx, void* stream);
+int rg_get_stream(rg_ctx* ctx, void** stream);
 
 /* ---- introspection (integer parity checks, profiling) ---------------------- */
 /* Oct ids (1-based) of level ilevel in linked-list order.  *n_out gets the
@@ -164,6 +170,11 @@ int64_t rg_level_cell_updates(rg_ctx* ctx, int ilevel);
 /* Milliseconds of device time of the last godunov kernels (CUDA events on the
  * context stream); per-kernel breakdown in out[0..n) (prim, face, fold). */
 int rg_last_kernel_ms(rg_ctx* ctx, float* out, int n);
+/* Enable (on != 0) or disable the per-kernel CUDA events read by
+ * rg_last_kernel_ms; they are recorded by rg_godunov_level only (captured
+ * graphs carry no events).  The RG_TIMING=1 environment variable sets the
+ * initial value. */
+int rg_set_timing(rg_ctx* ctx, int on);
 
 #ifdef __cplusplus
 }

@@ -167,13 +167,14 @@ rg_ctx* rg_create(const rg_params* params, int device) {
     c->device = device;
     if (check_cuda(c, cudaSetDevice(device), "cudaSetDevice") ||
         check_cuda(c, cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device), "SM count") ||
-        check_cuda(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream") ||
+        check_cuda(c, cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking), "stream") ||
         check_cuda(c, cudaMalloc(&c->d_status, sizeof(DevStatus)), "status") ||
         check_cuda(c, cudaMallocHost(&c->h_status, sizeof(DevStatus)), "pinned status") ||
         check_cuda(c, cudaMemset(c->d_status, 0, sizeof(DevStatus)), "status init")) {
         c->broken = true;
         return c;
     }
+    c->stream = c->own_stream;
     for (auto& e : c->ev) cudaEventCreate(&e);
     const char* t = getenv("RG_TIMING");
     c->timing = t && t[0] == '1';
@@ -196,7 +197,7 @@ void rg_destroy(rg_ctx* c) {
     cudaFree(c->d_flux);
     cudaFree(c->d_status);
     if (c->h_status) cudaFreeHost(c->h_status);
-    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
 }
 
@@ -452,6 +453,27 @@ int rg_synchronize(rg_ctx* c) {
     return check_device_status(c);
 }
 
+int rg_set_stream(rg_ctx* c, void* stream) {
+    CTX_GUARD(c);
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->own_stream;
+    if (s == c->stream) return RG_OK;
+    if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "stream switch")) return rc;
+    for (auto& p : c->plans)
+        if (p.graph) {
+            cudaGraphExecDestroy(p.graph);
+            p.graph = nullptr;
+        }
+    c->stream = s;
+    return RG_OK;
+}
+
+int rg_get_stream(rg_ctx* c, void** stream) {
+    CTX_GUARD(c);
+    if (!stream) return set_error(c, RG_ERR_ARG, "stream is NULL");
+    *stream = (void*)c->stream;
+    return RG_OK;
+}
+
 int rg_level_octs(rg_ctx* c, int ilevel, int* octs_out, int cap, int* n_out) {
     CTX_GUARD(c);
     Plan* P;
@@ -486,6 +508,12 @@ int rg_level_nbor_cells(rg_ctx* c, int ilevel, int* out, int cap) {
 int64_t rg_level_cell_updates(rg_ctx* c, int ilevel) {
     if (!c || ilevel < 0 || ilevel >= (int)c->cell_updates.size()) return 0;
     return c->cell_updates[ilevel];
+}
+
+int rg_set_timing(rg_ctx* c, int on) {
+    CTX_GUARD(c);
+    c->timing = on != 0;
+    return RG_OK;
 }
 
 int rg_last_kernel_ms(rg_ctx* c, float* out, int n) {

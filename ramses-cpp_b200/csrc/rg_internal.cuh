@@ -100,7 +100,8 @@ struct rg_ctx {
     rg_params params{};
     int device = 0;
     int sm_count = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;      // stream in use
+    cudaStream_t own_stream = nullptr;  // created by rg_create
     std::string err;
     bool broken = false;
 

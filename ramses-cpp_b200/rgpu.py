@@ -95,6 +95,9 @@ def lib():
     L.rg_level_cell_updates.restype = C.c_int64
     L.rg_level_cell_updates.argtypes = [C.c_void_p, C.c_int]
     L.rg_last_kernel_ms.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_int]
+    L.rg_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+    L.rg_set_timing.argtypes = [C.c_void_p, C.c_int]
+    L.rg_get_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
     _lib = L
     return L
 
@@ -178,6 +181,23 @@ class Context:
                                           C.byref(out) if want_dt else None))
         return out.value if want_dt else None
 
+    def set_stream(self, stream_handle):
+        self._chk(self.L.rg_set_stream(self.h, C.c_void_p(stream_handle) if stream_handle else None))
+
+    def get_stream(self):
+        out = C.c_void_p()
+        self._chk(self.L.rg_get_stream(self.h, C.byref(out)))
+        return out.value
+
+    def upload_state_ptr(self, uold_ptr=None, unew_ptr=None):
+        """Upload from raw host addresses (e.g. pinned torch tensors)."""
+        self._chk(self.L.rg_upload_state(self.h, C.cast(C.c_void_p(uold_ptr), F64P) if uold_ptr else None,
+                                         C.cast(C.c_void_p(unew_ptr), F64P) if unew_ptr else None))
+
+    def download_state_ptr(self, uold_ptr=None, unew_ptr=None):
+        self._chk(self.L.rg_download_state(self.h, C.cast(C.c_void_p(uold_ptr), F64P) if uold_ptr else None,
+                                           C.cast(C.c_void_p(unew_ptr), F64P) if unew_ptr else None))
+
     def synchronize(self):
         self._chk(self.L.rg_synchronize(self.h))
 
@@ -195,6 +215,9 @@ class Context:
 
     def cell_updates(self, il):
         return int(self.L.rg_level_cell_updates(self.h, il))
+
+    def set_timing(self, on):
+        self._chk(self.L.rg_set_timing(self.h, 1 if on else 0))
 
     def kernel_ms(self):
         out = (C.c_float * 3)()
