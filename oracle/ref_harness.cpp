@@ -12,6 +12,10 @@
 //     are the hot path under test;
 //   - RiemannSolver::solve_* and SlopeLimiter::compute_slope are exposed for
 //     unit-level parity.
+// Built with -DRG_GPU_PATCH (oracle/Makefile target "dropin") the same
+// harness gets its solver from ramses-cpp_b200/host/GpuHydroSolver.cpp through
+// the reference's create_hydro_solver seam, so tests run the unmodified
+// reference API with the GPU level step dropped in.
 // The namelist text is written to a temporary file because Config can only
 // parse files (src/core/Config.cpp:25).
 #include <cstdio>
@@ -28,6 +32,9 @@
 #include "ramses/solvers/hydro/HydroSolver.hpp"
 #include "ramses/solvers/hydro/RiemannSolver.hpp"
 #include "ramses/solvers/hydro/SlopeLimiter.hpp"
+#ifdef RG_GPU_PATCH
+#include "ramses/core/SolverFactory.hpp"
+#endif
 
 namespace {
 struct Harness {
@@ -62,7 +69,12 @@ void* rh_create(const char* nml_text, int nx, int ny, int nz, int ngridmax, int 
     ramses::params::nlevelmax = nlevelmax;
     h->grid.allocate(nx, ny, nz, ngridmax, nvar, 1, nlevelmax);
     h->grid.gamma = gamma;
+#ifdef RG_GPU_PATCH
+    // the drop-in build: the solver comes from the patch's create_hydro_solver
+    h->hydro = ramses::create_hydro_solver(h->grid, h->config);
+#else
     h->hydro = std::make_unique<ramses::HydroSolver>(h->grid, h->config);
+#endif
     h->hydro->set_nener(0);
     h->hydro->set_nvar_hydro(nvar);
     ramses::HydroSolver* hs = h->hydro.get();

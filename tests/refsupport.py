@@ -37,10 +37,11 @@ def _ptr(a, t):
 def ensure_built(target):
     """Build oracle targets on demand (``oracle`` always; ``ref`` needs the reference tree)."""
     lib = {"oracle": ORACLE_DIR / "_build" / "liboracle.so",
-           "ref": ORACLE_DIR / "_ref" / "libref_harness3d.so"}[target]
+           "ref": ORACLE_DIR / "_ref" / "libref_harness3d.so",
+           "dropin": ORACLE_DIR / "_ref" / "libref_harness_gpu3d.so"}[target]
     if lib.exists():
         return True
-    if target == "ref" and not REF_SRC.exists():
+    if target in ("ref", "dropin") and not REF_SRC.exists():
         return False
     subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), target, f"REF={REF_SRC}", "-j8"], check=True)
     return lib.exists()
@@ -79,10 +80,15 @@ class GridArrays:
 
 
 class RefHarness:
-    def __init__(self, ndim):
-        assert ensure_built("ref"), "reference sources unavailable"
+    """The reference driven through its own API.  variant="gpu" loads the
+    drop-in build whose HydroSolver is the GpuHydroSolver patch."""
+
+    def __init__(self, ndim, variant="cpu"):
+        target = "dropin" if variant == "gpu" else "ref"
+        assert ensure_built(target), "reference sources unavailable"
         self.ndim = ndim
-        self.lib = C.CDLL(str(ORACLE_DIR / "_ref" / f"libref_harness{ndim}d.so"))
+        name = f"libref_harness_gpu{ndim}d.so" if variant == "gpu" else f"libref_harness{ndim}d.so"
+        self.lib = C.CDLL(str(ORACLE_DIR / "_ref" / name))
         L = self.lib
         L.rh_create.restype = C.c_void_p
         L.rh_create.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
