@@ -157,6 +157,26 @@ int rg_synchronize(rg_ctx* ctx);
 int rg_set_stream(rg_ctx* ctx, void* stream);
 int rg_get_stream(rg_ctx* ctx, void** stream);
 
+/* ---- allocation-free variant ---------------------------------------------- */
+/* No counterpart in the reference.  The same level step as rg_godunov_level
+ * for callers that must not allocate device memory once set-up is over (a
+ * device-memory budget committed at start-up, a framework allocator that owns
+ * the free memory, a time loop that may not call cudaMalloc/cudaFree because
+ * they synchronise): it calls no allocating routine.  State comes from the
+ * caller's device buffers, [nvar][ncell] like the grid: uold_dev is read,
+ * unew_dev is updated in place.  The flux scratch is a 64 MiB static device
+ * array inside the library (levels of at most 279,620 cells in 3D, 1,398,101
+ * in 1D; larger levels return RG_ERR_ARG); every GPU that loads the library
+ * keeps those 64 MiB until exit.  The level's plan must already exist (one
+ * earlier rg_godunov_level or rg_set_unew call for the level after
+ * rg_sync_topology builds it), else RG_ERR_STATE.  The first call on each
+ * device resolves the scratch address with cudaGetSymbolAddress, so make that
+ * first call before any stream capture.  All calls share the one scratch
+ * array: calls whose kernels overlap on the GPU race and must be ordered by
+ * the caller; nothing in it needs to start at zero. */
+int rg_godunov_level_noalloc(rg_ctx* ctx, int ilevel, double dt, double dx, const double* uold_dev,
+                             double* unew_dev);
+
 /* ---- introspection (integer parity checks, profiling) ---------------------- */
 /* Oct ids (1-based) of level ilevel in linked-list order.  *n_out gets the
  * count; at most cap entries are written. */

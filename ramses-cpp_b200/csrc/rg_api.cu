@@ -138,6 +138,14 @@ void record_updates(rg_ctx* c, int ilevel, const Plan& P) {
 
 }  // namespace
 
+namespace rg {
+Plan* existing_plan(rg_ctx* c, int ilevel) {
+    if (!c->have_topology || ilevel < 0 || ilevel >= (int)c->plans.size()) return nullptr;
+    Plan& p = c->plans[ilevel];
+    return p.valid ? &p : nullptr;
+}
+}  // namespace rg
+
 extern "C" {
 
 const char* rg_version(void) { return "rgpu 1 (sm_100a, FP64 Godunov level step)"; }

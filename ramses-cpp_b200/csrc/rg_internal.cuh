@@ -147,6 +147,7 @@ int check_device_status(rg_ctx* c);  // synchronises
 int build_plan(rg_ctx* c, int ilevel, Plan& plan);
 void free_plan(Plan& plan);
 int rank_lists(rg_ctx* c);
+Plan* existing_plan(rg_ctx* c, int ilevel);  // built plan or nullptr; never builds
 int compute_cell_levels(rg_ctx* c);
 // step launchers (enqueue only)
 int launch_set_unew(rg_ctx* c, const Plan& p);
@@ -155,5 +156,6 @@ int launch_courant(rg_ctx* c, const Plan& p, double dx, int pressure_cap, double
 int launch_set_dt_host(rg_ctx* c, double dt, double dx);
 int launch_finalize_dt(rg_ctx* c, double dx);
 int launch_godunov(rg_ctx* c, const Plan& p);
+int launch_godunov_ext(rg_ctx* c, const Plan& p, const double* uold, double* unew, double* prim, double* flux);
 TreeView tree_view(const rg_ctx* c);
 }  // namespace rg

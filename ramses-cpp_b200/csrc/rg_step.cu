@@ -532,11 +532,45 @@ int launch_godunov_t(rg_ctx* c, const Plan& P) {
     return check_cuda(c, cudaGetLastError(), "godunov kernels");
 }
 
+template <int NDIM, int RS>
+void launch_face_ext_t(rg_ctx* c, const Plan& P, const StepK& K, const double* uold, const double* prim,
+                       double* flux) {
+    long long work = (long long)P.ncells * NDIM;
+    k_face<NDIM, RS><<<grid_for(c, work, 128), 128, 0, c->stream>>>(tree_view(c), P.view(), prim, uold, flux,
+                                                                     c->d_status, K, nullptr);
+}
+
+// Same kernels as launch_godunov_t, on caller-given state, primitive and flux
+// buffers (used by the entry point whose flux scratch is a static array).
+template <int NDIM>
+int launch_godunov_ext_t(rg_ctx* c, const Plan& P, const double* uold, double* unew, double* prim, double* flux) {
+    if (P.ncells == 0) return RG_OK;
+    StepK K = step_consts(c);
+    TreeView T = tree_view(c);
+    PlanView V = P.view();
+    int nprim = P.ncells + P.nextra_prim;
+    k_prim<NDIM><<<grid_for(c, nprim, 256), 256, 0, c->stream>>>(T, V, uold, prim, K.gamma, K.smalle);
+    switch (c->params.riemann) {
+        case RG_RIEMANN_HLLC: launch_face_ext_t<NDIM, RG_RIEMANN_HLLC>(c, P, K, uold, prim, flux); break;
+        case RG_RIEMANN_HLL: launch_face_ext_t<NDIM, RG_RIEMANN_HLL>(c, P, K, uold, prim, flux); break;
+        case RG_RIEMANN_EXACT: launch_face_ext_t<NDIM, RG_RIEMANN_EXACT>(c, P, K, uold, prim, flux); break;
+        case RG_RIEMANN_ACOUSTIC: launch_face_ext_t<NDIM, RG_RIEMANN_ACOUSTIC>(c, P, K, uold, prim, flux); break;
+        default: launch_face_ext_t<NDIM, RG_RIEMANN_LLF>(c, P, K, uold, prim, flux); break;
+    }
+    k_fold<NDIM><<<grid_for(c, P.ntarg, 256), 256, 0, c->stream>>>(T, V, flux, unew, c->d_status, K.gamma);
+    return check_cuda(c, cudaGetLastError(), "godunov kernels (caller buffers)");
+}
+
 }  // namespace
 
 int launch_godunov(rg_ctx* c, const Plan& P) {
     if (c->params.ndim == 1) return launch_godunov_t<1>(c, P);
     return launch_godunov_t<3>(c, P);
+}
+
+int launch_godunov_ext(rg_ctx* c, const Plan& P, const double* uold, double* unew, double* prim, double* flux) {
+    if (c->params.ndim == 1) return launch_godunov_ext_t<1>(c, P, uold, unew, prim, flux);
+    return launch_godunov_ext_t<3>(c, P, uold, unew, prim, flux);
 }
 
 int launch_set_unew(rg_ctx* c, const Plan& P) {

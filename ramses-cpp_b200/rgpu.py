@@ -97,6 +97,7 @@ def lib():
     L.rg_last_kernel_ms.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_int]
     L.rg_set_stream.argtypes = [C.c_void_p, C.c_void_p]
     L.rg_set_timing.argtypes = [C.c_void_p, C.c_int]
+    L.rg_godunov_level_noalloc.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p]
     L.rg_get_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
     _lib = L
     return L
@@ -169,6 +170,11 @@ class Context:
 
     def godunov_level(self, il, dt, dx):
         self._chk(self.L.rg_godunov_level(self.h, il, dt, dx))
+
+    def godunov_level_noalloc(self, il, dt, dx, uold_dev_ptr, unew_dev_ptr):
+        """Allocation-free level step on caller-owned device buffers (raw addresses)."""
+        self._chk(self.L.rg_godunov_level_noalloc(self.h, il, dt, dx, C.c_void_p(uold_dev_ptr),
+                                                  C.c_void_p(unew_dev_ptr)))
 
     def courant_step(self, il, dx, cfl, pressure_cap=True):
         out = C.c_double(0)
