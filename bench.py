@@ -30,7 +30,9 @@ UNIT = "cell-updates/s"
 WORKLOAD = "3D Sedov blast, uniform 128^3 (reference levelmin=levelmax=8), MonCen + HLLC, gamma 1.4, FP64"
 LEVEL = 8
 BYTES_PER_CELL_UPDATE = 80  # uold read once + unew written once, 5 FP64 variables each
-GPU_KERNELS_PER_STEP = 8    # courant init, courant, dt finalize, set_unew, prim, face, fold, set_uold
+# kernels per substep of a level without refined cells: courant init,
+# courant+primitives, dt finalize, face, fold (set_unew/set_uold fused into fold)
+GPU_KERNELS_PER_STEP = 5
 
 
 def peaks():

@@ -402,7 +402,9 @@ int rg_level_substep(rg_ctx* c, int ilevel, double dx, int pressure_cap, int use
     if (int rc = get_plan(c, ilevel, &P)) return rc;
     record_updates(c, ilevel, *P);
     if (int rc = ensure_flux(c, *P)) return rc;
+    const bool leaf = P->nactive == P->ncells;  // no refined cell: fused substep
     auto enqueue = [&]() -> int {
+        if (leaf) return launch_leaf_substep(c, *P, dx, pressure_cap, c->params.courant_factor);
         if (int rc = launch_courant(c, *P, dx, pressure_cap, c->params.courant_factor)) return rc;
         if (int rc = launch_finalize_dt(c, dx)) return rc;
         if (int rc = launch_set_unew(c, *P)) return rc;

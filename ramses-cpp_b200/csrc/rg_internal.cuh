@@ -48,6 +48,8 @@ struct DevStatus {
     unsigned long long dtmin_bits;  // CFL min-reduction scratch
     double dt, dx, dtdx;            // values of the current step (read by kernels)
     unsigned long long cell_updates;
+    double inv_dx;                  // 1/dx, used only when dx_pow2 != 0
+    int dx_pow2;
 };
 
 // Read-only view of the mirrored tree handed to kernels.
@@ -156,6 +158,7 @@ int launch_courant(rg_ctx* c, const Plan& p, double dx, int pressure_cap, double
 int launch_set_dt_host(rg_ctx* c, double dt, double dx);
 int launch_finalize_dt(rg_ctx* c, double dx);
 int launch_godunov(rg_ctx* c, const Plan& p);
+int launch_leaf_substep(rg_ctx* c, const Plan& p, double dx, int pressure_cap, double courant_factor);
 int launch_godunov_ext(rg_ctx* c, const Plan& p, const double* uold, double* unew, double* prim, double* flux);
 TreeView tree_view(const rg_ctx* c);
 }  // namespace rg

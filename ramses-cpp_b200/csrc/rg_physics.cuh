@@ -62,6 +62,23 @@ __device__ __forceinline__ void rot_swap(double* q, int idim) {
     }
 }
 
+// Division by the cell size.  When dx is a power of two (the usual
+// boxlen / (nx 2^L) with power-of-two nx and boxlen), x / dx and x * (1/dx)
+// are the same correctly rounded value of the same real number for every x,
+// so the multiply replaces the divide without changing a bit.
+struct DxDiv {
+    double dx, inv;
+    bool pow2;
+    __device__ __forceinline__ double div(double x) const { return pow2 ? x * inv : x / dx; }
+};
+
+__device__ __forceinline__ bool is_pow2_with_normal_inverse(double dx, double inv) {
+    unsigned long long b = (unsigned long long)__double_as_longlong(dx);
+    unsigned long long bi = (unsigned long long)__double_as_longlong(inv);
+    unsigned e = (unsigned)((b >> 52) & 0x7ff), ei = (unsigned)((bi >> 52) & 0x7ff);
+    return dx > 0.0 && (b & 0xfffffffffffffULL) == 0 && e != 0 && e != 0x7ff && ei != 0 && ei != 0x7ff;
+}
+
 __device__ __forceinline__ double cs2_of(double d, double p, double gamma) {
     double cs2 = gamma * p;
     return smax(cs2 / smax(d, 1e-10), 1e-20);
@@ -230,10 +247,12 @@ __device__ __forceinline__ void solve_hll(const double* ql, const double* qr, do
     }
 }
 
+// smallp = 1e-10*1e-10/gamma (RiemannSolver.cpp:71) is the same value in every
+// call, so the caller computes it once, in the same operation order.
 template <int NDIM>
-__device__ __forceinline__ void solve_hllc(const double* ql, const double* qr, double* flux, double gamma) {
+__device__ __forceinline__ void solve_hllc(const double* ql, const double* qr, double* flux, double gamma,
+                                           double smallp) {
     constexpr int NV = Dims<NDIM>::NV, IP = Dims<NDIM>::IP;
-    const double smallp = 1e-10 * 1e-10 / gamma;
     double rl = smax(ql[0], 1e-10), ul = ql[1], pl = smax(ql[IP], rl * smallp);
     double rr = smax(qr[0], 1e-10), ur = qr[1], pr = smax(qr[IP], rr * smallp);
     double cl = sqrt(cs2_of(rl, ql[IP], gamma));
@@ -286,10 +305,10 @@ __device__ __forceinline__ void solve_hllc(const double* ql, const double* qr, d
 }
 
 template <int NDIM>
-__device__ __forceinline__ void solve_acoustic(const double* ql, const double* qr, double* flux, double gamma) {
+__device__ __forceinline__ void solve_acoustic(const double* ql, const double* qr, double* flux, double gamma,
+                                               double smallp) {
     constexpr int NV = Dims<NDIM>::NV, IP = Dims<NDIM>::IP;
     const double smallc = 1e-10;
-    const double smallp = smallc * smallc / gamma;
     double rl = smax(ql[0], 1e-10), ul = ql[1], pl = smax(ql[IP], rl * smallp);
     double rr = smax(qr[0], 1e-10), ur = qr[1], pr = smax(qr[IP], rr * smallp);
     double cl = sqrt(cs2_of(rl, ql[IP], gamma));
@@ -333,9 +352,8 @@ __device__ __forceinline__ void solve_acoustic(const double* ql, const double* q
 // initial guess of :215 (learned mode).  Returns the Newton update count.
 template <int NDIM>
 __device__ __forceinline__ int solve_exact(const double* ql, const double* qr, double* flux, double gamma,
-                                           int niter, double tol, double p_guess) {
+                                           double smallp, int niter, double tol, double p_guess) {
     constexpr int IP = Dims<NDIM>::IP;
-    const double smallp = 1e-10 * 1e-10 / gamma;
     const double gamma6 = (gamma + 1.0) / (2.0 * gamma);
     double rl = smax(ql[0], 1e-10), ul = ql[1], pl = smax(ql[IP], rl * smallp);
     double rr = smax(qr[0], 1e-10), ur = qr[1], pr = smax(qr[IP], rr * smallp);

@@ -60,50 +60,50 @@ __device__ __forceinline__ void load_nb_rot(const TreeView& T, const double* __r
 }
 
 struct StepK {
-    double gamma, smalle;
+    double gamma, smalle, smallp;
     int slope_type, interpol_type, interpol_var, exact_niter;
     double exact_tol;
 };
 
 // Own trace (compute_slopes + trace, HydroSolver.cpp:653-732) on rotated data.
 template <int NDIM>
-__device__ __forceinline__ void own_trace(const double* qc, const double* ql, const double* qr, double dt, double dx,
-                                          const StepK& K, double* qm, double* qp) {
+__device__ __forceinline__ void own_trace(const double* qc, const double* ql, const double* qr, double dt,
+                                          const DxDiv& D, const StepK& K, double* qm, double* qp) {
     constexpr int NV = Dims<NDIM>::NV;
     double dq[NV];
-    double nu = qc[1] * dt / dx;
+    double nu = D.div(qc[1] * dt);
 #pragma unroll
     for (int iv = 0; iv < NV; ++iv) {
         if (K.slope_type == 0) dq[iv] = 0.0;
         else if ((K.slope_type == 5 || K.slope_type == 6) && iv != 0) dq[iv] = 0.0;
-        else dq[iv] = compute_slope(ql[iv], qc[iv], qr[iv], K.slope_type, 1.5, nu) / dx;
+        else dq[iv] = D.div(compute_slope(ql[iv], qc[iv], qr[iv], K.slope_type, 1.5, nu));
     }
-    trace<NDIM>(qc, dq, dt, dx, qm, qp, K.gamma);
+    trace<NDIM>(qc, dq, dt, D.dx, qm, qp, K.gamma);
 }
 
 // Ghost trace of a coarser (or same-level) neighbour, 2D/3D form
 // (HydroSolver.cpp:357-440): interpolation slopes over 2dx.
 template <int NDIM>
 __device__ __forceinline__ void ghost_trace(const double* qc, const double* ql, const double* qr, double dt,
-                                            double dx, const StepK& K, double* qm, double* qp) {
+                                            const DxDiv& D, const StepK& K, double* qm, double* qp) {
     constexpr int NV = Dims<NDIM>::NV;
     double dq[NV];
-    double dxc = 2.0 * dx;
+    const DxDiv Dc{2.0 * D.dx, 0.5 * D.inv, D.pow2};  // dx_coarse = 2 dx, still a power of two
 #pragma unroll
     for (int iv = 0; iv < NV; ++iv) {
         double dlft = qc[iv] - ql[iv];
         double drgt = qr[iv] - qc[iv];
         double slope = 0.0;
         if (K.interpol_type > 0 && dlft * drgt > 0.0) slope = interp_slope(dlft, drgt, K.interpol_type);
-        dq[iv] = slope / dxc;
+        dq[iv] = Dc.div(slope);
     }
-    trace<NDIM>(qc, dq, dt, dxc, qm, qp, K.gamma);
+    trace<NDIM>(qc, dq, dt, Dc.dx, qm, qp, K.gamma);
 }
 
 // Ghost face state of the 1D build (HydroSolver.cpp:219-356): the coarse
 // neighbour's child states, then a slope_type slope against the active cell.
 __device__ void ghost_1d(const double* __restrict__ uold, size_t ncell, const TreeView& T, int n, int nl, int nr,
-                         int side, const double* q_act, double dt, double dx, const StepK& K, double* qm,
+                         int side, const double* q_act, double dt, const DxDiv& D, const StepK& K, double* qm,
                          double* qp) {
     constexpr int NV = 3;
     double uc[NV], ul[NV], ur[NV];
@@ -181,7 +181,7 @@ __device__ void ghost_1d(const double* __restrict__ uold, size_t ncell, const Tr
     ctoprim<1>(uch[side == 0 ? 0 : 1], qg2, gamma, K.smalle);
     ctoprim<1>(uch[side == 0 ? 1 : 0], qg, gamma, K.smalle);
     double dq[NV];
-    double nu = qg[1] * dt / dx;
+    double nu = D.div(qg[1] * dt);
 #pragma unroll
     for (int iv = 0; iv < NV; ++iv) {
         double dlft, drgt;
@@ -193,17 +193,17 @@ __device__ void ghost_1d(const double* __restrict__ uold, size_t ncell, const Tr
             drgt = qg2[iv] - qg[iv];
         }
         if ((K.slope_type == 5 || K.slope_type == 6) && iv != 0) dq[iv] = 0.0;
-        else dq[iv] = compute_slope(qg[iv] - dlft, qg[iv], qg[iv] + drgt, K.slope_type, 1.5, nu) / dx;
+        else dq[iv] = D.div(compute_slope(qg[iv] - dlft, qg[iv], qg[iv] + drgt, K.slope_type, 1.5, nu));
     }
-    trace<1>(qg, dq, dt, dx, qm, qp, gamma);
+    trace<1>(qg, dq, dt, D.dx, qm, qp, gamma);
 }
 
 template <int NDIM, int RS>
 __device__ __forceinline__ int riemann(const double* ql, const double* qr, double* f, const StepK& K) {
-    if constexpr (RS == RG_RIEMANN_HLLC) solve_hllc<NDIM>(ql, qr, f, K.gamma);
+    if constexpr (RS == RG_RIEMANN_HLLC) solve_hllc<NDIM>(ql, qr, f, K.gamma, K.smallp);
     else if constexpr (RS == RG_RIEMANN_HLL) solve_hll<NDIM>(ql, qr, f, K.gamma);
-    else if constexpr (RS == RG_RIEMANN_ACOUSTIC) solve_acoustic<NDIM>(ql, qr, f, K.gamma);
-    else if constexpr (RS == RG_RIEMANN_EXACT) return solve_exact<NDIM>(ql, qr, f, K.gamma, K.exact_niter, K.exact_tol, -1.0);
+    else if constexpr (RS == RG_RIEMANN_ACOUSTIC) solve_acoustic<NDIM>(ql, qr, f, K.gamma, K.smallp);
+    else if constexpr (RS == RG_RIEMANN_EXACT) return solve_exact<NDIM>(ql, qr, f, K.gamma, K.smallp, K.exact_niter, K.exact_tol, -1.0);
     else solve_llf<NDIM>(ql, qr, f, K.gamma);
     return 0;
 }
@@ -214,8 +214,8 @@ __device__ __forceinline__ int riemann(const double* ql, const double* qr, doubl
 template <int NDIM>
 __device__ __forceinline__ void neighbour_face(const TreeView& T, const PlanView& P, const double* __restrict__ prim,
                                                const double* __restrict__ uold, size_t ncell, int p, int c, int idim,
-                                               int side, int kd, int n, const double* qc, double dt, double dx,
-                                               const StepK& K, double* qf) {
+                                               int side, int kd, int n, const double* qc, double dt,
+                                               const DxDiv& D, const StepK& K, double* qf) {
     constexpr int NV = Dims<NDIM>::NV;
     double qm[NV], qp[NV];
     int kind = kd & KIND_MASK;
@@ -228,7 +228,7 @@ __device__ __forceinline__ void neighbour_face(const TreeView& T, const PlanView
             dq0[iv] = 0.0;
         }
         if (kd & KIND_REFLECT) qb[1] *= -1.0;
-        trace<NDIM>(qb, dq0, dt, dx, qm, qp, K.gamma);
+        trace<NDIM>(qb, dq0, dt, D.dx, qm, qp, K.gamma);
     } else {
         if (P.level0) {
             // level 0 traces are unrotated first-order states (HydroSolver.cpp:77-91)
@@ -236,7 +236,7 @@ __device__ __forceinline__ void neighbour_face(const TreeView& T, const PlanView
             load_rot<NDIM>(prim, ncell, n, 0, qn);
 #pragma unroll
             for (int iv = 0; iv < NV; ++iv) dq0[iv] = 0.0;
-            trace<NDIM>(qn, dq0, dt, dx, qmn, qpn, K.gamma);
+            trace<NDIM>(qn, dq0, dt, D.dx, qmn, qpn, K.gamma);
 #pragma unroll
             for (int iv = 0; iv < NV; ++iv) {
                 qm[iv] = qmn[iv];
@@ -249,7 +249,7 @@ __device__ __forceinline__ void neighbour_face(const TreeView& T, const PlanView
             int nr = P.stc[((size_t)s * 2 + 1) * P.ncells + p];
             if constexpr (NDIM == 1) {
                 if (kind == K_GHOST) {
-                    ghost_1d(uold, ncell, T, n, nl, nr, side, qc, dt, dx, K, qm, qp);
+                    ghost_1d(uold, ncell, T, n, nl, nr, side, qc, dt, D, K, qm, qp);
                     goto have_face;
                 }
             }
@@ -258,8 +258,8 @@ __device__ __forceinline__ void neighbour_face(const TreeView& T, const PlanView
                 load_rot<NDIM>(prim, ncell, n, idim, qn);
                 load_nb_rot<NDIM>(T, prim, ncell, nl, idim, qn, qnl);
                 load_nb_rot<NDIM>(T, prim, ncell, nr, idim, qn, qnr);
-                if (kind == K_GHOST) ghost_trace<NDIM>(qn, qnl, qnr, dt, dx, K, qm, qp);
-                else own_trace<NDIM>(qn, qnl, qnr, dt, dx, K, qm, qp);
+                if (kind == K_GHOST) ghost_trace<NDIM>(qn, qnl, qnr, dt, D, K, qm, qp);
+                else own_trace<NDIM>(qn, qnl, qnr, dt, D, K, qm, qp);
             }
         have_face:;
         }
@@ -276,7 +276,8 @@ __global__ void __launch_bounds__(128) k_face(TreeView T, PlanView P, const doub
     constexpr int NV = Dims<NDIM>::NV;
     const size_t ncell = (size_t)T.ncell;
     const int nc = P.ncells;
-    const double dt = st->dt, dx = st->dx;
+    const double dt = st->dt;
+    const DxDiv D{st->dx, st->inv_dx, st->dx_pow2 != 0};
     const long long total = (long long)nc * NDIM;
     unsigned long long iters = 0;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
@@ -294,7 +295,7 @@ __global__ void __launch_bounds__(128) k_face(TreeView T, PlanView P, const doub
             load_rot<NDIM>(prim, ncell, c, 0, qn);
 #pragma unroll
             for (int iv = 0; iv < NV; ++iv) dq0[iv] = 0.0;
-            trace<NDIM>(qn, dq0, dt, dx, qmo, qpo, K.gamma);
+            trace<NDIM>(qn, dq0, dt, D.dx, qmo, qpo, K.gamma);
             rot_swap<NDIM>(qmo, idim);
             rot_swap<NDIM>(qpo, idim);
         } else {
@@ -302,7 +303,7 @@ __global__ void __launch_bounds__(128) k_face(TreeView T, PlanView P, const doub
             double ql[NV], qr[NV];
             load_nb_rot<NDIM>(T, prim, ncell, l, idim, qc, ql);
             load_nb_rot<NDIM>(T, prim, ncell, r, idim, qc, qr);
-            own_trace<NDIM>(qc, ql, qr, dt, dx, K, qmo, qpo);
+            own_trace<NDIM>(qc, ql, qr, dt, D, K, qmo, qpo);
         }
 #pragma unroll
         for (int side = 0; side < 2; ++side) {
@@ -315,7 +316,7 @@ __global__ void __launch_bounds__(128) k_face(TreeView T, PlanView P, const doub
             } else {
                 int n = P.icn[(size_t)s * nc + p];
                 double qf[NV];
-                neighbour_face<NDIM>(T, P, prim, uold, ncell, p, c, idim, side, kd, n, qc, dt, dx, K, qf);
+                neighbour_face<NDIM>(T, P, prim, uold, ncell, p, c, idim, side, kd, n, qc, dt, D, K, qf);
                 if (side == 0) iters += riemann<NDIM, RS>(qf, qpo, f, K);
                 else iters += riemann<NDIM, RS>(qmo, qf, f, K);
                 rot_swap<NDIM>(f, idim);
@@ -344,9 +345,13 @@ __global__ void k_prim(TreeView T, PlanView P, const double* __restrict__ uold, 
     }
 }
 
-template <int NDIM>
+// LEAF: the level has no refined cell, so set_unew (unew <- uold) and
+// set_uold (uold <- unew) of its cells are folded in: a level target starts
+// from uold and its result is written to both arrays.  Coarser targets start
+// from unew as always.
+template <int NDIM, bool LEAF = false>
 __global__ void k_fold(TreeView T, PlanView P, const double* __restrict__ flux, double* __restrict__ unew,
-                       const DevStatus* __restrict__ st, double gamma) {
+                       const DevStatus* __restrict__ st, double gamma, double* __restrict__ uold = nullptr) {
     constexpr int NV = Dims<NDIM>::NV, NS = Dims<NDIM>::NS, TTD = Dims<NDIM>::TTD;
     const size_t ncell = (size_t)T.ncell;
     const int nc = P.ncells;
@@ -356,9 +361,11 @@ __global__ void k_fold(TreeView T, PlanView P, const double* __restrict__ flux, 
         int a = P.toff[t], b = P.toff[t + 1];
         if (a == b) continue;
         int cell = (t < nc) ? cell_of(T, P, t) : P.textra[t - nc];
+        const bool from_old = LEAF && t < nc;
+        const double* src = from_old ? uold : unew;
         double u[NV];
 #pragma unroll
-        for (int iv = 0; iv < NV; ++iv) u[iv] = unew[(size_t)iv * ncell + cell - 1];
+        for (int iv = 0; iv < NV; ++iv) u[iv] = src[(size_t)iv * ncell + cell - 1];
         for (int e = a; e < b; ++e) {
             int key = P.tev[e];
             int slot = key & 7, cp = key >> 3;
@@ -402,6 +409,10 @@ __global__ void k_fold(TreeView T, PlanView P, const double* __restrict__ flux, 
         }
 #pragma unroll
         for (int iv = 0; iv < NV; ++iv) unew[(size_t)iv * ncell + cell - 1] = u[iv];
+        if (from_old) {
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) uold[(size_t)iv * ncell + cell - 1] = u[iv];
+        }
     }
 }
 
@@ -458,20 +469,69 @@ __global__ void k_courant(TreeView T, PlanView P, const double* __restrict__ uol
     if ((threadIdx.x & 31) == 0 && best != ~0ULL) atomicMin(&st->dtmin_bits, best);
 }
 
+// CFL candidate and primitives in one pass over uold (leaf-level substep).
+template <int NDIM>
+__global__ void k_courant_prim(TreeView T, PlanView P, const double* __restrict__ uold, double* __restrict__ prim,
+                               DevStatus* st, double dx, double gamma, double smalle, double cfl, int pressure_cap) {
+    constexpr int NV = Dims<NDIM>::NV;
+    const size_t ncell = (size_t)T.ncell;
+    const int total = P.ncells + P.nextra_prim;
+    unsigned long long best = ~0ULL;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        int id = (t < P.ncells) ? cell_of(T, P, t) : P.xprim[t - P.ncells];
+        double u[NV], q[NV];
+#pragma unroll
+        for (int iv = 0; iv < NV; ++iv) u[iv] = uold[(size_t)iv * ncell + id - 1];
+        ctoprim<NDIM>(u, q, gamma, smalle);
+#pragma unroll
+        for (int iv = 0; iv < NV; ++iv) prim[(size_t)iv * ncell + id - 1] = q[iv];
+        if (t >= P.ncells || T.son[id - 1] > 0) continue;
+        double d = smax(u[0], 1e-10), v2 = 0.0;
+#pragma unroll
+        for (int i = 1; i <= NDIM; ++i) {
+            double v = u[i] / d;
+            v2 = v2 + v * v;
+        }
+        double e_non = 0.0, sum_gamma_p = 0.0;
+        double pr = smax((u[NDIM + 1] - 0.5 * d * v2 - e_non) * (gamma - 1.0), d * 1e-10);
+        if (pressure_cap) pr = smin(pr, d * 1e2);
+        double cs2 = cs2_of(d, pr, gamma);
+        cs2 = cs2 + sum_gamma_p / d;
+        double cs = sqrt(smax(cs2, 1e-10));
+        double u_wave = NDIM * cs;
+#pragma unroll
+        for (int i = 1; i <= NDIM; ++i) u_wave = u_wave + fabs(u[i] / d);
+        double a_grav = 0.0;
+#pragma unroll
+        for (int i = 1; i <= NDIM; ++i) a_grav = a_grav + fabs(0.0);
+        double alpha = a_grav * dx / (u_wave * u_wave);
+        alpha = smax(alpha, 0.0001);
+        double dtc = (dx / u_wave) * (sqrt(1.0 + 2.0 * cfl * alpha) - 1.0) / alpha;
+        unsigned long long b = (unsigned long long)__double_as_longlong(dtc);
+        if (dtc >= 0.0 && b < best) best = b;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
+        best = other < best ? other : best;
+    }
+    if ((threadIdx.x & 31) == 0 && best != ~0ULL) atomicMin(&st->dtmin_bits, best);
+}
+
 __global__ void k_courant_init(DevStatus* st, double dt_start) {
     st->dtmin_bits = (unsigned long long)__double_as_longlong(dt_start);
 }
+__device__ __forceinline__ void set_step_values(DevStatus* st, double dt, double dx) {
+    st->dt = dt;
+    st->dx = dx;
+    st->dtdx = dt / dx;
+    double inv = 1.0 / dx;
+    st->inv_dx = inv;
+    st->dx_pow2 = is_pow2_with_normal_inverse(dx, inv) ? 1 : 0;
+}
 __global__ void k_dt_finalize(DevStatus* st, double dx) {
-    double dt = __longlong_as_double((long long)st->dtmin_bits);
-    st->dt = dt;
-    st->dx = dx;
-    st->dtdx = dt / dx;
+    set_step_values(st, __longlong_as_double((long long)st->dtmin_bits), dx);
 }
-__global__ void k_dt_set(DevStatus* st, double dt, double dx) {
-    st->dt = dt;
-    st->dx = dx;
-    st->dtdx = dt / dx;
-}
+__global__ void k_dt_set(DevStatus* st, double dt, double dx) { set_step_values(st, dt, dx); }
 
 inline int grid_for(rg_ctx* c, long long work, int block) {
     long long b = (work + block - 1) / block;
@@ -485,6 +545,7 @@ StepK step_consts(const rg_ctx* c) {
     StepK K;
     K.gamma = p.gamma;
     K.smalle = 1e-10 * 1e-10 / p.gamma / (p.gamma - 1.0);
+    K.smallp = 1e-10 * 1e-10 / p.gamma;
     K.slope_type = p.slope_type;
     K.interpol_type = p.interpol_type;
     K.interpol_var = p.interpol_var;
@@ -571,6 +632,32 @@ int launch_godunov(rg_ctx* c, const Plan& P) {
 int launch_godunov_ext(rg_ctx* c, const Plan& P, const double* uold, double* unew, double* prim, double* flux) {
     if (c->params.ndim == 1) return launch_godunov_ext_t<1>(c, P, uold, unew, prim, flux);
     return launch_godunov_ext_t<3>(c, P, uold, unew, prim, flux);
+}
+
+template <int NDIM>
+int launch_leaf_substep_t(rg_ctx* c, const Plan& P, double dx, int pressure_cap, double cfl) {
+    StepK K = step_consts(c);
+    TreeView T = tree_view(c);
+    PlanView V = P.view();
+    k_courant_init<<<1, 1, 0, c->stream>>>(c->d_status, c->params.boxlen / 1e-10);
+    int nprim = P.ncells + P.nextra_prim;
+    k_courant_prim<NDIM><<<grid_for(c, nprim, 256), 256, 0, c->stream>>>(T, V, c->d_uold, c->d_prim, c->d_status, dx,
+                                                                         K.gamma, K.smalle, cfl, pressure_cap);
+    k_dt_finalize<<<1, 1, 0, c->stream>>>(c->d_status, dx);
+    launch_face_n<NDIM>(c, P, K);
+    k_fold<NDIM, true><<<grid_for(c, P.ntarg, 256), 256, 0, c->stream>>>(T, V, c->d_flux, c->d_unew, c->d_status,
+                                                                         K.gamma, c->d_uold);
+    return check_cuda(c, cudaGetLastError(), "leaf substep kernels");
+}
+
+// Substep of a level without refined cells: CFL + primitives in one pass,
+// set_unew/set_uold folded into the fold kernel (five launches instead of eight).
+int launch_leaf_substep(rg_ctx* c, const Plan& P, double dx, int pressure_cap, double cfl) {
+    if (P.ncells == 0) return RG_OK;
+    if (c->cap_flux < (size_t)(2 * c->params.ndim) * (c->params.ndim + 2) * P.ncells)
+        return set_error(c, RG_ERR_STATE, "flux scratch not sized");
+    if (c->params.ndim == 1) return launch_leaf_substep_t<1>(c, P, dx, pressure_cap, cfl);
+    return launch_leaf_substep_t<3>(c, P, dx, pressure_cap, cfl);
 }
 
 int launch_set_unew(rg_ctx* c, const Plan& P) {
