@@ -195,6 +195,17 @@ int rg_last_kernel_ms(rg_ctx* ctx, float* out, int n);
  * graphs carry no events).  The RG_TIMING=1 environment variable sets the
  * initial value. */
 int rg_set_timing(rg_ctx* ctx, int on);
+/* Exact-solver statistics accumulated by the face kernels: Newton updates
+ * and Riemann solves since the last reset (reset != 0 clears them). */
+int rg_exact_stats(rg_ctx* ctx, int64_t* iters, int64_t* calls, int reset);
+/* The face kernel's launch shape (tiles per block, register cap, batch of
+ * tiles per queue grab) is timed on each level's first substep and the
+ * fastest kept; on == 0 keeps the default shape instead. */
+int rg_set_autotune(rg_ctx* ctx, int on);
+/* Shape chosen for a level: variant index, batch, and its timed ms. */
+int rg_face_config(rg_ctx* ctx, int ilevel, int* variant, int* batch, float* ms);
+/* Pin the face-kernel shape of a level (variant 0..4, batch >= 1). */
+int rg_set_face_config(rg_ctx* ctx, int ilevel, int variant, int batch);
 
 #ifdef __cplusplus
 }

@@ -10,6 +10,7 @@
 #include <new>
 #include <string>
 
+#include "rg_face.cuh"
 #include "rg_internal.cuh"
 
 namespace rg {
@@ -120,7 +121,7 @@ int get_plan(rg_ctx* c, int ilevel, Plan** out) {
 // The flux scratch is shared by all levels and baked into captured graphs:
 // growing it invalidates every graph.
 int ensure_flux(rg_ctx* c, const Plan& P) {
-    size_t need = (size_t)(2 * c->params.ndim) * (c->params.ndim + 2) * (size_t)P.ncells;
+    size_t need = (size_t)(2 * c->params.ndim + 1) * (c->params.ndim + 2) * (size_t)P.ncells;
     if (c->cap_flux >= need && c->d_flux) return RG_OK;
     cudaStreamSynchronize(c->stream);
     for (auto& p : c->plans)
@@ -373,7 +374,11 @@ int rg_godunov_level(rg_ctx* c, int ilevel, double dt, double dx) {
     if (P->ncells == 0) return RG_OK;
     if (int rc = ensure_flux(c, *P)) return rc;
     if (int rc = launch_set_dt_host(c, dt, dx)) return rc;
-    return launch_godunov(c, *P);
+    if (int rc = launch_godunov(c, *P)) return rc;
+    // after the first real call the primitives of this level are in place:
+    // time the face-kernel shapes on them (writes only the flux scratch)
+    if (P->face_variant < 0 && ++P->substeps_run >= 1) return autotune_face(c, *P, step_consts(c));
+    return RG_OK;
 }
 
 int rg_courant_step(rg_ctx* c, int ilevel, double dx, double courant_factor, int pressure_cap, double* dt_out) {
@@ -411,7 +416,12 @@ int rg_level_substep(rg_ctx* c, int ilevel, double dx, int pressure_cap, int use
         if (int rc = launch_godunov(c, *P)) return rc;
         return launch_set_uold(c, *P);
     };
-    if (use_graph) {
+    if (P->face_variant < 0) {
+        // first substep of this plan: run it eagerly, then tune the face
+        // kernel on its primitives before any graph captures the launch shape
+        if (int rc = enqueue()) return rc;
+        if (int rc = autotune_face(c, *P, step_consts(c))) return rc;
+    } else if (use_graph) {
         int cap_key = pressure_cap ? 1 : 0;
         if (!P->graph || P->graph_cap != cap_key ) {
             if (P->graph) {
@@ -518,6 +528,53 @@ int rg_level_nbor_cells(rg_ctx* c, int ilevel, int* out, int cap) {
 int64_t rg_level_cell_updates(rg_ctx* c, int ilevel) {
     if (!c || ilevel < 0 || ilevel >= (int)c->cell_updates.size()) return 0;
     return c->cell_updates[ilevel];
+}
+
+int rg_exact_stats(rg_ctx* c, int64_t* iters, int64_t* calls, int reset) {
+    CTX_GUARD(c);
+    if (int rc = check_cuda(c, cudaMemcpyAsync(c->h_status, c->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                                               c->stream),
+                            "stats copy"))
+        return rc;
+    if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "stats sync")) return rc;
+    if (iters) *iters = (int64_t)c->h_status->exact_iters;
+    if (calls) *calls = (int64_t)c->h_status->exact_calls;
+    if (reset) {
+        // exact_iters and exact_calls are adjacent in DevStatus
+        cudaMemsetAsync(&c->d_status->exact_iters, 0, 2 * sizeof(unsigned long long), c->stream);
+        return check_cuda(c, cudaStreamSynchronize(c->stream), "stats reset");
+    }
+    return RG_OK;
+}
+
+int rg_set_autotune(rg_ctx* c, int on) {
+    CTX_GUARD(c);
+    c->no_autotune = (on == 0);
+    return RG_OK;
+}
+
+int rg_face_config(rg_ctx* c, int ilevel, int* variant, int* batch, float* ms) {
+    CTX_GUARD(c);
+    Plan* P = existing_plan(c, ilevel);
+    if (!P) return set_error(c, RG_ERR_STATE, "no plan for this level yet");
+    if (variant) *variant = P->face_variant;
+    if (batch) *batch = P->face_batch;
+    if (ms) *ms = P->face_ms;
+    return RG_OK;
+}
+
+int rg_set_face_config(rg_ctx* c, int ilevel, int variant, int batch) {
+    CTX_GUARD(c);
+    if (variant < 0 || variant > 4 || batch < 1) return set_error(c, RG_ERR_ARG, "variant must be 0..4, batch >= 1");
+    Plan* P;
+    if (int rc = get_plan(c, ilevel, &P)) return rc;
+    P->face_variant = variant;
+    P->face_batch = batch;
+    if (P->graph) {
+        cudaGraphExecDestroy(P->graph);
+        P->graph = nullptr;
+    }
+    return RG_OK;
 }
 
 int rg_set_timing(rg_ctx* c, int on) {

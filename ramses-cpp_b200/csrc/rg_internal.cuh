@@ -50,6 +50,8 @@ struct DevStatus {
     unsigned long long cell_updates;
     double inv_dx;                  // 1/dx, used only when dx_pow2 != 0
     int dx_pow2;
+    unsigned int face_next, face_done;  // persistent face-kernel work queue
+    unsigned long long exact_iters, exact_calls;  // exact-solver Newton statistics
 };
 
 // Read-only view of the mirrored tree handed to kernels.
@@ -85,6 +87,9 @@ struct Plan {
     int8_t* kind = nullptr;
     cudaGraphExec_t graph = nullptr;  // substep graph (set_unew..set_uold)
     int graph_cap = -1;
+    int face_variant = -1, face_batch = 4;  // autotuned face-kernel shape (-1: not tuned yet)
+    float face_ms = 0.f;
+    int substeps_run = 0;
     PlanView view() const {
         return PlanView{ilevel, level0, noct, ncells, ntarg, nextra_prim, octs, icn, stc, kind, toff, tev, textra, xprim};
     }
@@ -138,6 +143,7 @@ struct rg_ctx {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     float last_ms[3] = {0, 0, 0};
     bool timing = false;
+    bool no_autotune = false;
     std::vector<long long> cell_updates;
 };
 

@@ -97,6 +97,10 @@ def lib():
     L.rg_last_kernel_ms.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_int]
     L.rg_set_stream.argtypes = [C.c_void_p, C.c_void_p]
     L.rg_set_timing.argtypes = [C.c_void_p, C.c_int]
+    L.rg_exact_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_int]
+    L.rg_set_autotune.argtypes = [C.c_void_p, C.c_int]
+    L.rg_set_face_config.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+    L.rg_face_config.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float)]
     L.rg_godunov_level_noalloc.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p]
     L.rg_get_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
     _lib = L
@@ -221,6 +225,22 @@ class Context:
 
     def cell_updates(self, il):
         return int(self.L.rg_level_cell_updates(self.h, il))
+
+    def exact_stats(self, reset=False):
+        it, ca = C.c_int64(0), C.c_int64(0)
+        self._chk(self.L.rg_exact_stats(self.h, C.byref(it), C.byref(ca), 1 if reset else 0))
+        return it.value, ca.value
+
+    def set_autotune(self, on):
+        self._chk(self.L.rg_set_autotune(self.h, 1 if on else 0))
+
+    def face_config(self, il):
+        v, b, ms = C.c_int(0), C.c_int(0), C.c_float(0)
+        self._chk(self.L.rg_face_config(self.h, il, C.byref(v), C.byref(b), C.byref(ms)))
+        return v.value, b.value, ms.value
+
+    def set_face_config(self, il, variant, batch):
+        self._chk(self.L.rg_set_face_config(self.h, il, variant, batch))
 
     def set_timing(self, on):
         self._chk(self.L.rg_set_timing(self.h, 1 if on else 0))

@@ -248,3 +248,44 @@ def test_topology_errors_are_reported(ctx_factory):
     assert e.value.code == rgpu.RG_ERR_ARG
     ctx.godunov_level(L, 1e-3, 1.0 / 2 ** L)
     ctx.synchronize()
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+def test_every_face_kernel_shape_is_bit_identical(ctx_factory, oracle, variant):
+    """The autotuner may pick any shape: each must give the oracle's bits."""
+    L = 5
+    g = rg_tree.build_uniform(3, L)
+    ga = ga_of(g)
+    params = make_params(3, slope_type=2, riemann="hllc")
+    ctx = ctx_factory(params)
+    ctx.sync_topology(g)
+    u = rg_tree.random_state(g, L, seed=variant)
+    want = u.copy()
+    dx = 1.0 / 2 ** L
+    dt = 0.3 * oracle.courant(ga, 3, 5, L, dx, 1.4, 0.8, u, pressure_cap=False)
+    oracle.godunov_fine(ga, params, L, dt, dx, u.copy(), want)
+    for batch in (1, 3, 16):
+        ctx.set_face_config(L, variant, batch)
+        ctx.upload_state(u, u)
+        ctx.godunov_level(L, dt, dx)
+        got = np.empty_like(u)
+        ctx.download_state(unew=got)
+        assert bits_equal(got, want), (variant, batch)
+
+
+def test_autotuner_picks_a_shape_and_exact_stats_count(ctx_factory):
+    L = 6
+    g = rg_tree.build_uniform(3, L)
+    ctx = ctx_factory(make_params(3, slope_type=2, riemann="exact"))
+    ctx.sync_topology(g)
+    u = rg_tree.sedov_state(g, L)
+    ctx.upload_state(u, u)
+    dx = 1.0 / 2 ** L
+    ctx.level_substep(L, dx, use_graph=True)  # eager first substep + autotune
+    v, b, ms = ctx.face_config(L)
+    assert 0 <= v <= 4 and b >= 1 and ms > 0
+    ctx.exact_stats(reset=True)
+    ctx.level_substep(L, dx, use_graph=True)
+    ctx.synchronize()
+    iters, calls = ctx.exact_stats()
+    assert calls == 6 * 32 ** 3 and iters >= calls
