@@ -204,7 +204,7 @@ int rg_exact_stats(rg_ctx* ctx, int64_t* iters, int64_t* calls, int reset);
 int rg_set_autotune(rg_ctx* ctx, int on);
 /* Shape chosen for a level: variant index, batch, and its timed ms. */
 int rg_face_config(rg_ctx* ctx, int ilevel, int* variant, int* batch, float* ms);
-/* Pin the face-kernel shape of a level (variant 0..4, batch >= 1). */
+/* Pin the face-kernel shape of a level (variant 0..6, batch >= 1). */
 int rg_set_face_config(rg_ctx* ctx, int ilevel, int variant, int batch);
 
 #ifdef __cplusplus

@@ -23,7 +23,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC,-O2",
                 "--expt-relaxed-constexpr", f"-I{ROOT / 'include'}"]
-SOURCES = ["rg_api.cu", "rg_plan.cu", "rg_step.cu", "rg_face.cu", "rg_noalloc.cu"]
+SOURCES = ["rg_api.cu", "rg_plan.cu", "rg_step.cu", "rg_face.cu", "rg_face_1d.cu", "rg_face_3d.cu",
+           "rg_noalloc.cu"]
 
 
 def _newer(target: Path, deps) -> bool:

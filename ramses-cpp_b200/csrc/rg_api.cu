@@ -565,7 +565,8 @@ int rg_face_config(rg_ctx* c, int ilevel, int* variant, int* batch, float* ms) {
 
 int rg_set_face_config(rg_ctx* c, int ilevel, int variant, int batch) {
     CTX_GUARD(c);
-    if (variant < 0 || variant > 4 || batch < 1) return set_error(c, RG_ERR_ARG, "variant must be 0..4, batch >= 1");
+    if (variant < 0 || variant >= kNumFaceVariants || batch < 1)
+        return set_error(c, RG_ERR_ARG, "variant must be 0..6, batch >= 1");
     Plan* P;
     if (int rc = get_plan(c, ilevel, &P)) return rc;
     P->face_variant = variant;

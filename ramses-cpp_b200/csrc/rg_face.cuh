@@ -254,6 +254,186 @@ __device__ __forceinline__ void neighbour_face(const TreeView& T, const PlanView
     for (int iv = 0; iv < NV; ++iv) qf[iv] = side == 0 ? qm[iv] : qp[iv];
 }
 
+// The persistent tiled face kernel.  Work unit: a tile of 32 consecutive
+// level cells (one warp wide).  A block holds R tiles x ndim directions, one
+// warp per (tile, direction): the warp computes, for its 32 cells, the own
+// trace along the direction, the two neighbour face states and the two Riemann
+// fluxes (HydroSolver.cpp:93-474).  The fluxes go to global memory (the
+// neighbours' reflux events read them) and to shared memory, where the
+// direction-0 warp then forms each cell's own flux sum in the reference's
+// (idim, side) order (HydroSolver.cpp:485-486), so the fold reads 5 doubles
+// for the own update instead of 2*ndim*5.  Blocks are persistent: a grid sized
+// from the occupancy of the chosen variant pulls batches of tiles from a
+// counter in device memory; the last block to finish resets the counter for
+// the next launch (nothing ever waits on another block).
+constexpr int TILE = 32;
+
+template <int NDIM, int RS, int R, int MINB>
+__global__ void __launch_bounds__(TILE * NDIM * R, MINB)
+    k_face_tiles(TreeView T, PlanView P, const double* __restrict__ prim, const double* __restrict__ uold,
+                 double* __restrict__ flux, double* __restrict__ fsum, DevStatus* st, StepK K, int batch) {
+    constexpr int NV = Dims<NDIM>::NV, NS = Dims<NDIM>::NS;
+    __shared__ double sf[R][NS][NV][TILE];
+    __shared__ int s_base;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r = warp / NDIM, idim = warp - r * NDIM;
+    const size_t ncell = (size_t)T.ncell;
+    const int nc = P.ncells;
+    const int ntiles = (nc + TILE - 1) / TILE;
+    const double dt = st->dt;
+    const DxDiv D{st->dx, st->inv_dx, st->dx_pow2 != 0};
+    unsigned long long iters = 0, calls = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_base = (int)atomicAdd(&st->face_next, (unsigned)(batch * R));
+        __syncthreads();
+        const int base = s_base;
+        __syncthreads();
+        if (base >= ntiles) break;
+        const int end = min(base + batch * R, ntiles);
+        for (int t0 = base; t0 < end; t0 += R) {
+            const int tile = t0 + r;
+            const int p = tile * TILE + lane;
+            const bool valid = tile < end && p < nc;
+            int kd0 = K_NONE;
+            if (valid) {
+                const int s0 = 2 * idim;
+                kd0 = P.kind[(size_t)s0 * nc + p];
+                if (kd0 != K_NONE) {
+                    const int kd1 = P.kind[(size_t)(s0 + 1) * nc + p];
+                    const int c = cell_of(T, P, p);
+                    double qc[NV], qmo[NV], qpo[NV];
+                    load_rot<NDIM>(prim, ncell, c, idim, qc);
+                    if (P.level0) {
+                        double qn[NV], dq0[NV];
+                        load_rot<NDIM>(prim, ncell, c, 0, qn);
+#pragma unroll
+                        for (int iv = 0; iv < NV; ++iv) dq0[iv] = 0.0;
+                        trace<NDIM>(qn, dq0, dt, D.dx, qmo, qpo, K.gamma);
+                        rot_swap<NDIM>(qmo, idim);
+                        rot_swap<NDIM>(qpo, idim);
+                    } else {
+                        const int l = P.icn[(size_t)s0 * nc + p], rr = P.icn[(size_t)(s0 + 1) * nc + p];
+                        double ql[NV], qr[NV];
+                        load_nb_rot<NDIM>(T, prim, ncell, l, idim, qc, ql);
+                        load_nb_rot<NDIM>(T, prim, ncell, rr, idim, qc, qr);
+                        own_trace<NDIM>(qc, ql, qr, dt, D, K, qmo, qpo);
+                    }
+#pragma unroll
+                    for (int side = 0; side < 2; ++side) {
+                        const int kd = side ? kd1 : kd0;
+                        const int s = s0 + side;
+                        double f[NV];
+                        if ((kd & KIND_MASK) == K_ZERO) {
+#pragma unroll
+                            for (int iv = 0; iv < NV; ++iv) f[iv] = 0.0;
+                        } else {
+                            const int n = P.icn[(size_t)s * nc + p];
+                            double qf[NV];
+                            neighbour_face<NDIM>(T, P, prim, uold, ncell, p, c, idim, side, kd, n, qc, dt, D, K, qf);
+                            if (side == 0) iters += riemann<NDIM, RS>(qf, qpo, f, K);
+                            else iters += riemann<NDIM, RS>(qmo, qf, f, K);
+                            ++calls;
+                            rot_swap<NDIM>(f, idim);
+                        }
+#pragma unroll
+                        for (int iv = 0; iv < NV; ++iv) {
+                            flux[((size_t)s * NV + iv) * nc + p] = f[iv];
+                            sf[r][s][iv][lane] = f[iv];
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            if (idim == 0 && valid && kd0 != K_NONE) {
+#pragma unroll
+                for (int iv = 0; iv < NV; ++iv) {
+                    double fs = 0.0;
+#pragma unroll
+                    for (int s = 0; s < NS; ++s) {
+                        const double sign = (s & 1) ? -1.0 : 1.0;
+                        fs = fs + sign * sf[r][s][iv][lane];
+                    }
+                    fsum[(size_t)iv * nc + p] = fs;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (RS == RG_RIEMANN_EXACT) {
+        for (int o = 16; o > 0; o >>= 1) {
+            iters += __shfl_xor_sync(0xffffffffu, iters, o);
+            calls += __shfl_xor_sync(0xffffffffu, calls, o);
+        }
+        if (lane == 0 && calls) {
+            atomicAdd(&st->exact_iters, iters);
+            atomicAdd(&st->exact_calls, calls);
+        }
+    }
+    // the last block out resets the work counter for the next launch
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&st->face_done, 1u) == gridDim.x - 1) {
+            st->face_next = 0;
+            st->face_done = 0;
+            __threadfence();
+        }
+    }
+}
+
+// Variant table: tiles per block (R) and the launch-bounds minimum of
+// resident blocks (caps registers per thread).  Index = variant id.
+#define RG_FACE_VARIANTS(X) X(0, 1, 6) X(1, 1, 8) X(2, 1, 10) X(3, 1, 12) X(4, 2, 4) X(5, 2, 5) X(6, 2, 6)
+constexpr int kNumFaceVariants = 7;
+constexpr int kDefaultFaceVariant = 1;
+
+template <int NDIM, int RS, int R, int MINB>
+int launch_face_one(rg_ctx* c, const Plan& P, const StepK& K, int batch, const double* uold, const double* prim,
+                    double* flux, double* fsum) {
+    auto kern = k_face_tiles<NDIM, RS, R, MINB>;
+    const int block = TILE * NDIM * R;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, 0);
+    per_sm = per_sm > 1 ? per_sm : 1;
+    const int ntiles = (P.ncells + TILE - 1) / TILE;
+    const int grabs = (ntiles + batch * R - 1) / (batch * R);
+    int grid = per_sm * c->sm_count;
+    if (grabs < grid) grid = grabs;
+    if (grid < 1) grid = 1;
+    kern<<<grid, block, 0, c->stream>>>(tree_view(c), P.view(), prim, uold, flux, fsum, c->d_status, K, batch);
+    return check_cuda(c, cudaGetLastError(), "face kernel");
+}
+
+template <int NDIM, int RS>
+int launch_face_rs(rg_ctx* c, const Plan& P, const StepK& K, int variant, int batch, const double* uold,
+                   const double* prim, double* flux, double* fsum) {
+#define RG_FACE_CASE(id, r, mb) \
+    case id: return launch_face_one<NDIM, RS, r, mb>(c, P, K, batch, uold, prim, flux, fsum);
+    switch (variant) {
+        RG_FACE_VARIANTS(RG_FACE_CASE)
+        default: return launch_face_one<NDIM, RS, 1, 8>(c, P, K, batch, uold, prim, flux, fsum);
+    }
+#undef RG_FACE_CASE
+}
+
+template <int NDIM>
+int launch_face_nd(rg_ctx* c, const Plan& P, const StepK& K, int variant, int batch, const double* uold,
+                   const double* prim, double* flux, double* fsum) {
+    switch (c->params.riemann) {
+        case RG_RIEMANN_HLLC: return launch_face_rs<NDIM, RG_RIEMANN_HLLC>(c, P, K, variant, batch, uold, prim, flux, fsum);
+        case RG_RIEMANN_HLL: return launch_face_rs<NDIM, RG_RIEMANN_HLL>(c, P, K, variant, batch, uold, prim, flux, fsum);
+        case RG_RIEMANN_EXACT: return launch_face_rs<NDIM, RG_RIEMANN_EXACT>(c, P, K, variant, batch, uold, prim, flux, fsum);
+        case RG_RIEMANN_ACOUSTIC:
+            return launch_face_rs<NDIM, RG_RIEMANN_ACOUSTIC>(c, P, K, variant, batch, uold, prim, flux, fsum);
+        default: return launch_face_rs<NDIM, RG_RIEMANN_LLF>(c, P, K, variant, batch, uold, prim, flux, fsum);
+    }
+}
+
+// instantiated in rg_face_1d.cu / rg_face_3d.cu (compiled in parallel)
+int launch_face_nd1(rg_ctx* c, const Plan& P, const StepK& K, int variant, int batch, const double* uold,
+                    const double* prim, double* flux, double* fsum);
+int launch_face_nd3(rg_ctx* c, const Plan& P, const StepK& K, int variant, int batch, const double* uold,
+                    const double* prim, double* flux, double* fsum);
+
 StepK step_consts(const rg_ctx* c);
 int launch_face_tiles(rg_ctx* c, const Plan& P, const StepK& K, const double* uold, const double* prim,
                       double* flux, double* fsum);
