@@ -157,6 +157,44 @@ int rg_synchronize(rg_ctx* ctx);
 int rg_set_stream(rg_ctx* ctx, void* stream);
 int rg_get_stream(rg_ctx* ctx, void** stream);
 
+/* ---- exact solver and its learned Newton start ----------------------------- */
+/* Exact two-shock Newton solves (RiemannSolver::solve_godunov_nr,
+ * RiemannSolver.cpp:194-307) of n independent interfaces.  Device arrays:
+ * ql/qr [ndim+2][n] rotated primitives (rho, u_n, u_t..., p), gamma [n] or
+ * NULL (params.gamma), outputs flux [ndim+2][n], pstar [n], iters [n] (Newton
+ * updates), each may be NULL.  guess: RG_GUESS_TWO_SHOCK (the reference's
+ * :215) or RG_GUESS_LEARNED.  niter/tol: 10/1e-6 reproduce the reference;
+ * a tol of 1e-14 with a larger cap is the converged mode. */
+int rg_exact_batch(rg_ctx* ctx, int n, const double* ql_dev, const double* qr_dev, const double* gamma_dev,
+                   double* flux_dev, double* pstar_dev, int* iters_dev, int guess, int niter, double tol);
+/* The exact solver's stress workload, seeded: density ratios log-uniform to
+ * 1e4, pressure ratios to 1e6, 30 % strong double rarefactions, gamma 5/3 or
+ * 1.4 per interface; layout as rg_exact_batch. */
+int rg_stress_states(rg_ctx* ctx, int n, uint64_t seed, double* ql_dev, double* qr_dev, double* gamma_dev);
+/* Learned Newton start (no reference counterpart): an 8-64-64-1 SiLU MLP
+ * predicting log(pstar / base), base = max(two-shock, two-rarefaction estimate),
+ * from the interface states, trained on the GPU
+ * (BF16 tensor-core forward/backward, FP32 master weights, Adam) on nsamples
+ * stress states labelled by the converged Newton root.  Used by
+ * rg_exact_batch and by the level step when params.exact_guess ==
+ * RG_GUESS_LEARNED; the two-shock guess is kept whenever the prediction is not
+ * a finite positive number or lies within the gate band of it (near-linear
+ * waves, where the linearised start is already exact).  *loss_out: mean
+ * squared error (standardised target) over the last epoch. */
+int rg_mlp_train(rg_ctx* ctx, int nsamples, int epochs, int batch, float lr, uint64_t seed, float* loss_out);
+int rg_mlp_nparam(void);
+/* Parameter block of rg_mlp_nparam() floats: W1[64][8], b1, W2[64][64], b2,
+ * w3, b3, feature means and scales [8]+[8], target mean and scale, gate
+ * (|log(prediction / two-shock guess)| below which the two-shock guess is
+ * kept; 0.2 after training). */
+int rg_mlp_get(rg_ctx* ctx, float* params);
+int rg_mlp_set(rg_ctx* ctx, const float* params);
+/* Gradient check: loss (sum of squared errors) and gradients of the mean
+ * squared error w.r.t. the first 4801 parameters for n samples of
+ * standardised features x [8][n] and targets t [n] (host arrays), computed by
+ * the training kernel without updating the weights. */
+int rg_mlp_grad(rg_ctx* ctx, int n, const float* x, const float* t, float* grad, float* loss);
+
 /* ---- allocation-free variant ---------------------------------------------- */
 /* No counterpart in the reference.  The same level step as rg_godunov_level
  * for callers that must not allocate device memory once set-up is over (a

@@ -204,6 +204,7 @@ void rg_destroy(rg_ctx* c) {
     cudaFree(c->d_unew);
     cudaFree(c->d_prim);
     cudaFree(c->d_flux);
+    cudaFree(c->d_mlp);
     cudaFree(c->d_status);
     if (c->h_status) cudaFreeHost(c->h_status);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -365,9 +366,16 @@ int rg_set_uold(rg_ctx* c, int ilevel) {
     return launch_set_uold(c, *P);
 }
 
+static int check_learned(rg_ctx* c) {
+    if (c->params.riemann == RG_RIEMANN_EXACT && c->params.exact_guess == RG_GUESS_LEARNED && !c->mlp_valid)
+        return set_error(c, RG_ERR_STATE, "exact_guess is RG_GUESS_LEARNED but no network was trained or set");
+    return RG_OK;
+}
+
 int rg_godunov_level(rg_ctx* c, int ilevel, double dt, double dx) {
     CTX_GUARD(c);
     if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state uploaded");
+    if (int rc = check_learned(c)) return rc;
     Plan* P;
     if (int rc = get_plan(c, ilevel, &P)) return rc;
     record_updates(c, ilevel, *P);
@@ -403,6 +411,7 @@ int rg_courant_step(rg_ctx* c, int ilevel, double dx, double courant_factor, int
 int rg_level_substep(rg_ctx* c, int ilevel, double dx, int pressure_cap, int use_graph, double* dt_used) {
     CTX_GUARD(c);
     if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state uploaded");
+    if (int rc = check_learned(c)) return rc;
     Plan* P;
     if (int rc = get_plan(c, ilevel, &P)) return rc;
     record_updates(c, ilevel, *P);
@@ -576,6 +585,63 @@ int rg_set_face_config(rg_ctx* c, int ilevel, int variant, int batch) {
         P->graph = nullptr;
     }
     return RG_OK;
+}
+
+int rg_exact_batch(rg_ctx* c, int n, const double* ql_dev, const double* qr_dev, const double* gamma_dev,
+                   double* flux_dev, double* pstar_dev, int* iters_dev, int guess, int niter, double tol) {
+    CTX_GUARD(c);
+    if (n < 0 || !ql_dev || !qr_dev) return set_error(c, RG_ERR_ARG, "bad batch arguments");
+    if (niter < 1 || !(tol > 0)) return set_error(c, RG_ERR_ARG, "niter >= 1 and tol > 0 required");
+    const float* mlp = nullptr;
+    if (guess == RG_GUESS_LEARNED) {
+        if (!c->mlp_valid) return set_error(c, RG_ERR_STATE, "no network trained or set");
+        mlp = c->d_mlp;
+    }
+    if (n == 0) return RG_OK;
+    return launch_exact_batch(c, n, ql_dev, qr_dev, gamma_dev, flux_dev, pstar_dev, iters_dev, mlp, niter, tol);
+}
+
+int rg_stress_states(rg_ctx* c, int n, uint64_t seed, double* ql_dev, double* qr_dev, double* gamma_dev) {
+    CTX_GUARD(c);
+    if (n < 1 || !ql_dev || !qr_dev) return set_error(c, RG_ERR_ARG, "bad stress arguments");
+    return launch_stress_states(c, n, (unsigned long long)seed, ql_dev, qr_dev, gamma_dev);
+}
+
+int rg_mlp_nparam(void) { return MLP_NPARAM; }
+
+int rg_mlp_train(rg_ctx* c, int nsamples, int epochs, int batch, float lr, uint64_t seed, float* loss_out) {
+    CTX_GUARD(c);
+    return mlp_train(c, nsamples, epochs, batch, lr, (unsigned long long)seed, loss_out);
+}
+
+int rg_mlp_get(rg_ctx* c, float* params) {
+    CTX_GUARD(c);
+    if (!params) return set_error(c, RG_ERR_ARG, "params is NULL");
+    if (!c->mlp_valid) return set_error(c, RG_ERR_STATE, "no network trained or set");
+    if (int rc = check_cuda(c, cudaMemcpyAsync(params, c->d_mlp, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost,
+                                               c->stream),
+                            "mlp copy"))
+        return rc;
+    return check_cuda(c, cudaStreamSynchronize(c->stream), "mlp sync");
+}
+
+int rg_mlp_set(rg_ctx* c, const float* params) {
+    CTX_GUARD(c);
+    if (!params) return set_error(c, RG_ERR_ARG, "params is NULL");
+    if (int rc = mlp_ensure(c)) return rc;
+    if (int rc = check_cuda(c, cudaMemcpyAsync(c->d_mlp, params, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice,
+                                               c->stream),
+                            "mlp copy"))
+        return rc;
+    c->mlp_valid = true;
+    return check_cuda(c, cudaStreamSynchronize(c->stream), "mlp sync");
+}
+
+int rg_mlp_grad(rg_ctx* c, int n, const float* x, const float* t, float* grad, float* loss) {
+    CTX_GUARD(c);
+    if (n < 1 || !x || !t || !grad || !loss) return set_error(c, RG_ERR_ARG, "bad gradient-check arguments");
+    if (!c->mlp_valid) return set_error(c, RG_ERR_STATE, "no network trained or set");
+    return mlp_grad(c, n, x, t, grad, loss);
 }
 
 int rg_set_timing(rg_ctx* c, int on) {

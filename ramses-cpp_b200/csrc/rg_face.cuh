@@ -8,6 +8,7 @@
 #pragma once
 
 #include "rg_internal.cuh"
+#include "rg_mlp.cuh"
 #include "rg_physics.cuh"
 
 namespace rg {
@@ -16,6 +17,7 @@ struct StepK {
     double gamma, smalle, smallp;
     int slope_type, interpol_type, interpol_var, exact_niter;
     double exact_tol;
+    const float* mlp;  // learned Newton start of the exact solver, or nullptr
 };
 
 __device__ __forceinline__ int cell_of(const TreeView& T, const PlanView& P, int p) {
@@ -189,7 +191,9 @@ __device__ __forceinline__ int riemann(const double* ql, const double* qr, doubl
     if constexpr (RS == RG_RIEMANN_HLLC) solve_hllc<NDIM>(ql, qr, f, K.gamma, K.smallp);
     else if constexpr (RS == RG_RIEMANN_HLL) solve_hll<NDIM>(ql, qr, f, K.gamma);
     else if constexpr (RS == RG_RIEMANN_ACOUSTIC) solve_acoustic<NDIM>(ql, qr, f, K.gamma, K.smallp);
-    else if constexpr (RS == RG_RIEMANN_EXACT) return solve_exact<NDIM>(ql, qr, f, K.gamma, K.smallp, K.exact_niter, K.exact_tol, -1.0);
+    else if constexpr (RS == RG_RIEMANN_EXACT)
+        return solve_exact<NDIM>(ql, qr, f, K.gamma, K.smallp, K.exact_niter, K.exact_tol,
+                                 mlp_guess<NDIM>(K.mlp, ql, qr, K.gamma, K.smallp));
     else solve_llf<NDIM>(ql, qr, f, K.gamma);
     return 0;
 }

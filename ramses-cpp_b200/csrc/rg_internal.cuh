@@ -144,6 +144,8 @@ struct rg_ctx {
     float last_ms[3] = {0, 0, 0};
     bool timing = false;
     bool no_autotune = false;
+    float* d_mlp = nullptr;  // learned Newton start: parameters + Adam state
+    bool mlp_valid = false;
     std::vector<long long> cell_updates;
 };
 
@@ -167,4 +169,10 @@ int launch_godunov(rg_ctx* c, const Plan& p);
 int launch_leaf_substep(rg_ctx* c, const Plan& p, double dx, int pressure_cap, double courant_factor);
 int launch_godunov_ext(rg_ctx* c, const Plan& p, const double* uold, double* unew, double* prim, double* flux);
 TreeView tree_view(const rg_ctx* c);
+int mlp_ensure(rg_ctx* c);
+int mlp_train(rg_ctx* c, int nsamples, int epochs, int batch, float lr, unsigned long long seed, float* loss_out);
+int mlp_grad(rg_ctx* c, int n, const float* x_host, const float* t_host, float* grad_host, float* loss_host);
+int launch_exact_batch(rg_ctx* c, int n, const double* ql, const double* qr, const double* gam, double* flux,
+                       double* pstar, int* iters, const float* mlp, int niter, double tol);
+int launch_stress_states(rg_ctx* c, int n, unsigned long long seed, double* ql, double* qr, double* gam);
 }  // namespace rg

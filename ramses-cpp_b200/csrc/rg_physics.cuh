@@ -351,8 +351,9 @@ __device__ __forceinline__ void solve_acoustic(const double* ql, const double* q
 // niter/tol default to the reference's 10 and 1e-6; p_guess > 0 replaces the
 // initial guess of :215 (learned mode).  Returns the Newton update count.
 template <int NDIM>
-__device__ __forceinline__ int solve_exact(const double* ql, const double* qr, double* flux, double gamma,
-                                           double smallp, int niter, double tol, double p_guess) {
+__device__ __forceinline__ int solve_exact_p(const double* ql, const double* qr, double* flux, double gamma,
+                                             double smallp, int niter, double tol, double p_guess,
+                                             double* pstar_out) {
     constexpr int IP = Dims<NDIM>::IP;
     const double gamma6 = (gamma + 1.0) / (2.0 * gamma);
     double rl = smax(ql[0], 1e-10), ul = ql[1], pl = smax(ql[IP], rl * smallp);
@@ -382,6 +383,7 @@ __device__ __forceinline__ int solve_exact(const double* ql, const double* qr, d
         if (fabs(delp / (pold + 1e-10)) < tol) break;
     }
     pstar = pold;
+    if (pstar_out) *pstar_out = pstar;
     double wwl_f = sqrt(smax(cl_sq * (1.0 + gamma6 * (pstar - pl) / (pl + 1e-20)), 0.0));
     double wwr_f = sqrt(smax(cr_sq * (1.0 + gamma6 * (pstar - pr) / (pr + 1e-20)), 0.0));
     double ustar = 0.5 * (ul + (pl - pstar) / (wwl_f + 1e-20) + ur - (pr - pstar) / (wwr_f + 1e-20));
@@ -417,6 +419,12 @@ __device__ __forceinline__ int solve_exact(const double* ql, const double* qr, d
     for (int i = 2; i <= NDIM; ++i) flux[i] = flux[0] * (left ? ql[i] : qr[i]);
     flux[IP] = (E + po) * uo;
     return it;
+}
+
+template <int NDIM>
+__device__ __forceinline__ int solve_exact(const double* ql, const double* qr, double* flux, double gamma,
+                                           double smallp, int niter, double tol, double p_guess) {
+    return solve_exact_p<NDIM>(ql, qr, flux, gamma, smallp, niter, tol, p_guess, nullptr);
 }
 
 }  // namespace rg

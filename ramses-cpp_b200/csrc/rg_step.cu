@@ -313,6 +313,7 @@ StepK step_consts(const rg_ctx* c) {
     K.interpol_var = p.interpol_var;
     K.exact_niter = p.exact_niter > 0 ? p.exact_niter : 10;
     K.exact_tol = p.exact_tol > 0 ? p.exact_tol : 1e-6;
+    K.mlp = (p.riemann == RG_RIEMANN_EXACT && p.exact_guess == RG_GUESS_LEARNED && c->mlp_valid) ? c->d_mlp : nullptr;
     return K;
 }
 

@@ -100,6 +100,14 @@ def lib():
     L.rg_exact_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_int]
     L.rg_set_autotune.argtypes = [C.c_void_p, C.c_int]
     L.rg_set_face_config.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+    VP = C.c_void_p
+    L.rg_exact_batch.argtypes = [VP, C.c_int, VP, VP, VP, VP, VP, VP, C.c_int, C.c_int, C.c_double]
+    L.rg_stress_states.argtypes = [VP, C.c_int, C.c_uint64, VP, VP, VP]
+    L.rg_mlp_train.argtypes = [VP, C.c_int, C.c_int, C.c_int, C.c_float, C.c_uint64, C.POINTER(C.c_float)]
+    L.rg_mlp_get.argtypes = [VP, C.POINTER(C.c_float)]
+    L.rg_mlp_set.argtypes = [VP, C.POINTER(C.c_float)]
+    L.rg_mlp_grad.argtypes = [VP, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                              C.POINTER(C.c_float)]
     L.rg_face_config.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float)]
     L.rg_godunov_level_noalloc.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p]
     L.rg_get_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
@@ -241,6 +249,39 @@ class Context:
 
     def set_face_config(self, il, variant, batch):
         self._chk(self.L.rg_set_face_config(self.h, il, variant, batch))
+
+    # ---- exact solver / learned guess (device buffers passed as raw addresses)
+    def exact_batch(self, n, ql, qr, gamma=None, flux=None, pstar=None, iters=None, learned=False, niter=10,
+                    tol=1e-6):
+        self._chk(self.L.rg_exact_batch(self.h, n, ql, qr, gamma, flux, pstar, iters, 1 if learned else 0, niter,
+                                        tol))
+
+    def stress_states(self, n, seed, ql, qr, gamma):
+        self._chk(self.L.rg_stress_states(self.h, n, seed, ql, qr, gamma))
+
+    def mlp_train(self, nsamples=10_000_000, epochs=30, batch=8192, lr=2e-3, seed=1):
+        loss = C.c_float(0)
+        self._chk(self.L.rg_mlp_train(self.h, nsamples, epochs, batch, lr, seed, C.byref(loss)))
+        return loss.value
+
+    def mlp_get(self):
+        out = np.zeros(self.L.rg_mlp_nparam(), dtype=np.float32)
+        self._chk(self.L.rg_mlp_get(self.h, out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out
+
+    def mlp_set(self, params):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        self._chk(self.L.rg_mlp_set(self.h, p.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def mlp_grad(self, x, t):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        g = np.zeros(4801, dtype=np.float32)
+        loss = C.c_float(0)
+        FP = C.POINTER(C.c_float)
+        self._chk(self.L.rg_mlp_grad(self.h, len(t), x.ctypes.data_as(FP), t.ctypes.data_as(FP),
+                                     g.ctypes.data_as(FP), C.byref(loss)))
+        return g, loss.value
 
     def set_timing(self, on):
         self._chk(self.L.rg_set_timing(self.h, 1 if on else 0))
