@@ -10,7 +10,13 @@ Steps past the configured 200 continue the same run.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Prints one JSON line (rank 0).  N > 1 runs one independent replica per GPU
-(the single-grid step has no exchange to shard), weak scaling.
+(weak scaling): the single-grid step of this workload is not partitioned, so
+the ranks exchange nothing but the final timing maximum.
+
+The line also carries a "newton" object for the exact Riemann solver: the
+stress workload (256^3 independent interface pairs) with the plain two-shock
+Newton start against the learned start (network trained on the GPU first),
+and the same Sedov step run with the exact solver under both starts.
 """
 import argparse
 import json
@@ -307,7 +313,7 @@ def gpu_arm(args, rank, world, local_rank):
                    "l2": "inputs larger than L2: uold+unew 192 MB, primitives 96 MB, flux scratch 503 MB per step",
                    "parallelism": "replicas" if world > 1 else "single GPU", "cuda_graph": True},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": profile_traffic(), "kernel": "k_face",
+                     "traffic": profile_traffic(), "kernel": "k_face_tiles",
                      "algorithmic_bytes_per_launch": alg_bytes, "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
                      "step_hbm_frac": (BYTES_PER_CELL_UPDATE * value / world / 1e9) / peak},
         "kernel_ms": {"prim": kms[0], "face": kms[1], "fold": kms[2]},
@@ -319,6 +325,98 @@ def gpu_arm(args, rank, world, local_rank):
     return out
 
 
+def newton_report(local_rank, stream, steps):
+    """Exact solver, plain vs learned Newton start (converged mode |dp|/p < 1e-14)."""
+    import numpy as np
+    import torch
+    import rg_tree
+    import rgpu
+    out = {"tolerance": 1e-14, "iteration_cap": 100}
+    ctx = rgpu.Context(rgpu.make_params(3, riemann="exact"), local_rank)
+    ctx.set_stream(stream.cuda_stream)
+    t0 = time.perf_counter()
+    loss = ctx.mlp_train()
+    ctx.synchronize()
+    out["training"] = {"samples": 10_000_000, "epochs": 30, "loss": loss, "seconds": time.perf_counter() - t0,
+                       "precision": "BF16 tensor-core products, FP32 master weights, Adam"}
+    w = ctx.mlp_get()
+    n = 256 ** 3
+    dev = torch.device("cuda", local_rank)
+    ql = torch.empty(5 * n, dtype=torch.float64, device=dev)
+    qr = torch.empty_like(ql)
+    gam = torch.empty(n, dtype=torch.float64, device=dev)
+    ctx.stress_states(n, 20261203, ql.data_ptr(), qr.data_ptr(), gam.data_ptr())
+    res = {}
+    for learned in (False, True):
+        f = torch.empty(5 * n, dtype=torch.float64, device=dev)
+        ps = torch.empty(n, dtype=torch.float64, device=dev)
+        it = torch.empty(n, dtype=torch.int32, device=dev)
+        call = lambda: ctx.exact_batch(n, ql.data_ptr(), qr.data_ptr(), gam.data_ptr(), f.data_ptr(), ps.data_ptr(),
+                                       it.data_ptr(), learned=learned, niter=100, tol=1e-14)
+        call()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(5):
+            call()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 5
+        hist = torch.bincount(it.long(), minlength=101).cpu().numpy()
+        cdf = np.cumsum(hist) / n
+        res[learned] = (f, ps, {"mean_iters": float((hist * np.arange(len(hist))).sum() / n),
+                                "p99_iters": int(np.searchsorted(cdf, 0.99)),
+                                "at_cap_frac": float(hist[100:].sum() / n), "ms": ms,
+                                "interfaces_per_s": n / (ms / 1e3)})
+    (f0, p0, a), (f1, p1, b) = res[False], res[True]
+    rel = ((p1 - p0).abs() / p0.abs().clamp_min(1e-300))
+    frel = ((f1 - f0).abs() / f0.abs().clamp_min(1e-300))
+    out["stress"] = {"workload": "256^3 independent interface pairs: rho ratio to 1e4, p ratio to 1e6, "
+                                 "30% strong double rarefactions, gamma 5/3 or 1.4, seed 20261203",
+                     "interfaces": n, "plain": a, "learned": b,
+                     "iteration_ratio": a["mean_iters"] / b["mean_iters"],
+                     "pstar_rel_max": float(rel.max()), "pstar_rel_gt_1e-13_frac": float((rel > 1e-13).double().mean()),
+                     "flux_rel_gt_1e-12_frac": float((frel > 1e-12).double().mean())}
+    del ql, qr, gam, f0, f1, p0, p1, res, rel, frel
+    ctx.close()
+    torch.cuda.empty_cache()
+
+    L = LEVEL
+    g = rg_tree.build_uniform(3, L)
+    u0 = rg_tree.sedov_state(g, L)
+    dx = 1.0 / 2 ** L
+    sed = {}
+    for learned in (False, True):
+        c = rgpu.Context(rgpu.make_params(3, slope_type=2, riemann="exact", interpol_type=1, gamma=1.4,
+                                          courant_factor=0.8, exact_niter=100, exact_tol=1e-14,
+                                          exact_guess=1 if learned else 0), local_rank)
+        c.set_stream(stream.cuda_stream)
+        if learned:
+            c.mlp_set(w)
+        c.sync_topology(g)
+        c.upload_state(u0, u0)
+        for _ in range(3):
+            c.level_substep(L, dx, pressure_cap=False, use_graph=True)
+        c.synchronize()
+        c.exact_stats(reset=True)
+        cells = c.cell_updates(L)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            c.level_substep(L, dx, pressure_cap=False, use_graph=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        iters, calls = c.exact_stats()
+        sed["learned" if learned else "plain"] = {"cell_updates_per_s": cells / (ms / 1e3), "ms_per_step": ms,
+                                                   "iters_per_interface": iters / max(calls, 1)}
+        c.close()
+    sed["workload"] = WORKLOAD.replace("HLLC", "exact solver (converged mode)") + f", {steps} substeps after 3"
+    out["sedov_exact"] = sed
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -326,6 +424,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-newton", action="store_true", help="skip the exact-solver plain/learned report")
     ap.add_argument("--cpu-sample", nargs=2, type=int, metavar=("LEVEL", "STEPS"), help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.cpu_sample:
@@ -355,6 +454,9 @@ def main():
                "sample": f"one substep (CFL, set_unew, godunov_fine, set_uold) of the 128^3 Sedov workload, "
                          f"single-threaded, {c['seconds']:.1f} s"}
     out = gpu_arm(args, rank, world, local_rank)
+    if rank == 0 and not args.no_newton:
+        import torch
+        out["newton"] = newton_report(local_rank, torch.cuda.Stream(), min(max(args.steps // 20, 5), 40))
     if world > 1:
         import torch.distributed as dist
         dist.barrier()

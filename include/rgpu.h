@@ -226,11 +226,12 @@ int rg_level_nbor_cells(rg_ctx* ctx, int ilevel, int* out, int cap);
  * rg_level_substep of this level processed. */
 int64_t rg_level_cell_updates(rg_ctx* ctx, int ilevel);
 /* Milliseconds of device time of the last godunov kernels (CUDA events on the
- * context stream); per-kernel breakdown in out[0..n) (prim, face, fold). */
+ * context stream); per-kernel breakdown in out[0..n) (prim, face, fold; in a
+ * fused leaf substep "prim" covers the CFL + primitive pass). */
 int rg_last_kernel_ms(rg_ctx* ctx, float* out, int n);
 /* Enable (on != 0) or disable the per-kernel CUDA events read by
- * rg_last_kernel_ms; they are recorded by rg_godunov_level only (captured
- * graphs carry no events).  The RG_TIMING=1 environment variable sets the
+ * rg_last_kernel_ms; they are recorded by rg_godunov_level and by eager
+ * (use_graph == 0) rg_level_substep calls (captured graphs carry no events).  The RG_TIMING=1 environment variable sets the
  * initial value. */
 int rg_set_timing(rg_ctx* ctx, int on);
 /* Exact-solver statistics accumulated by the face kernels: Newton updates

@@ -8,14 +8,15 @@
 // while fewer iterations are needed.  The two-shock guess stays the fallback
 // whenever the prediction is not a finite positive number, and also when the
 // prediction lies within a relative band (MLP_GATE in log space) of the
-// two-shock guess: there the linearised start is already as good as the
+// two-shock guess, and without evaluating the network at all for weak waves
+// (MLP_WEAK_*): there the linearised start is already as good as the
 // network (it is exact for weak waves, where Newton stops after one update),
 // and replacing it by a prediction carrying the network's few-percent error
 // would add iterations.
 //
 // Network: 8 features -> 64 -> 64 -> 1, SiLU activations.
 // Features of a rotated pair (ql, qr) with floors as in the solver, pref =
-// max(pl, pr), c = sqrt(gamma p / rho):
+// max(pl, pr), c = sqrt(gamma p / rho), FP32:
 //   x0 log(rl/rr)            x1 log(pl/pr)
 //   x2 asinh((ul-ur)/(cl+cr)) x3 asinh(ul/cl)   x4 asinh(ur/cr)
 //   x5 gamma                  x6 log(max(p_twoshock, 1e-30 pref)/pref)
@@ -47,6 +48,10 @@ constexpr int MLP_YS = MLP_YM + 1;                 // target scale
 constexpr int MLP_GATE = MLP_YS + 1;               // keep the two-shock start when |log(guess/p2s)| < gate
 constexpr int MLP_NPARAM = MLP_GATE + 1;           // 4820 floats in the parameter block
 constexpr float MLP_GATE_DEFAULT = 0.2f;
+// Weak-wave pre-gate: with pmax/pmin < MLP_WEAK_P and |ul-ur| < MLP_WEAK_U
+// (cl+cr) the two-shock guess is within a few percent of p* (its error is
+// second order in the wave strength) and the network is not evaluated.
+constexpr double MLP_WEAK_P = 1.3, MLP_WEAK_U = 0.3;
 constexpr float MLP_LOG_FLOOR = 1e-30f;
 
 __device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
@@ -55,45 +60,63 @@ __device__ __forceinline__ float silu_grad(float z) {
     return s * (1.0f + z * (1.0f - s));
 }
 
-// Features of a rotated pair; returns pref and the base estimate b.
+// Features of a rotated pair; returns pref and the base estimate b (and the
+// two-shock guess).  Computed in FP32 on scale-free quantities -- pressures
+// in units of pref, densities of rref = max(rl, rr), velocities of
+// sqrt(pref/rref) -- so that every intermediate stays in FP32 range whatever
+// the states' scale; the features are ratios and do not depend on the units.
 template <int NDIM>
 __device__ __forceinline__ void mlp_features(const double* ql, const double* qr, double gamma, double smallp,
                                              float* x, double* pref_out, double* base_out,
                                              double* p2s_out = nullptr) {
     constexpr int IP = Dims<NDIM>::IP;
-    double rl = smax(ql[0], 1e-10), ul = ql[1], pl = smax(ql[IP], rl * smallp);
-    double rr = smax(qr[0], 1e-10), ur = qr[1], pr = smax(qr[IP], rr * smallp);
-    double cl = sqrt(gamma * pl / rl), cr = sqrt(gamma * pr / rr);
-    double wl = sqrt(gamma * pl * rl), wr = sqrt(gamma * pr * rr);
-    double p2s = smax((wr * pl + wl * pr + wl * wr * (ul - ur)) / (wl + wr + 1e-20), 0.0);
-    double pref = smax(pl, pr);
-    double z = (gamma - 1.0) / (2.0 * gamma);
-    double num = cl + cr - 0.5 * (gamma - 1.0) * (ur - ul);
-    double den = cl / pow(pl, z) + cr / pow(pr, z);
-    double ptr = num > 0.0 ? pow(num / den, 1.0 / z) : 0.0;
-    x[0] = (float)log(rl / rr);
-    x[1] = (float)log(pl / pr);
-    x[2] = (float)asinh((ul - ur) / (cl + cr));
-    x[3] = (float)asinh(ul / cl);
-    x[4] = (float)asinh(ur / cr);
-    x[5] = (float)gamma;
-    x[6] = (float)log(smax(p2s, 1e-30 * pref) / pref);
-    x[7] = (float)log(smax(ptr, 1e-30 * pref) / pref);
+    double rl = smax(ql[0], 1e-10), pl = smax(ql[IP], rl * smallp);
+    double rr = smax(qr[0], 1e-10), pr = smax(qr[IP], rr * smallp);
+    double pref = smax(pl, pr), rref = smax(rl, rr);
+    double ip = 1.0 / pref, ir = 1.0 / rref, iv = sqrt(rref * ip);
+    const float g = (float)gamma;
+    const float al = (float)(rl * ir), ar = (float)(rr * ir);
+    const float bl = (float)(pl * ip), br = (float)(pr * ip);
+    const float vl = (float)(ql[1] * iv), vr = (float)(qr[1] * iv);
+    float cl = sqrtf(g * bl / al), cr = sqrtf(g * br / ar);
+    float wl = sqrtf(g * bl * al), wr = sqrtf(g * br * ar);
+    float p2s = fmaxf((wr * bl + wl * br + wl * wr * (vl - vr)) / (wl + wr + 1e-30f), 0.f);
+    float z = (g - 1.f) / (2.f * g);
+    float num = cl + cr - 0.5f * (g - 1.f) * (vr - vl);
+    float den = cl / powf(bl, z) + cr / powf(br, z);
+    float ptr = num > 0.f ? fminf(powf(num / den, 1.f / z), 1e30f) : 0.f;
+    x[0] = logf(al / ar);
+    x[1] = logf(bl / br);
+    x[2] = asinhf((vl - vr) / (cl + cr));
+    x[3] = asinhf(vl / cl);
+    x[4] = asinhf(vr / cr);
+    x[5] = g;
+    x[6] = logf(fmaxf(p2s, MLP_LOG_FLOOR));
+    x[7] = logf(fmaxf(ptr, MLP_LOG_FLOOR));
     *pref_out = pref;
-    *base_out = smax(smax(p2s, ptr), 1e-30 * pref);
-    if (p2s_out) *p2s_out = p2s;
+    *base_out = pref * (double)fmaxf(fmaxf(p2s, ptr), MLP_LOG_FLOOR);
+    if (p2s_out) *p2s_out = pref * (double)p2s;
 }
 
 // FP32 forward pass on standardised features xs; w points to MLP_NPARAM
-// floats (global memory, read through the read-only cache: every lane reads
-// the same weight).  Returns the standardised prediction.
+// floats (global memory, 16-byte aligned, read through the read-only cache
+// as float4: every lane reads the same weights, so each load is a broadcast
+// feeding four FMAs).  Returns the standardised prediction.
 __device__ __forceinline__ float mlp_forward_std(const float* __restrict__ w, const float* x) {
+    const float4* __restrict__ w4 = reinterpret_cast<const float4*>(w);
     float h1[MLP_H];
 #pragma unroll 8
     for (int j = 0; j < MLP_H; ++j) {
         float z = __ldg(w + MLP_B1 + j);
-#pragma unroll
-        for (int k = 0; k < MLP_IN; ++k) z = fmaf(__ldg(w + MLP_W1 + j * MLP_IN + k), x[k], z);
+        float4 a = __ldg(w4 + (MLP_W1 + j * MLP_IN) / 4), b = __ldg(w4 + (MLP_W1 + j * MLP_IN) / 4 + 1);
+        z = fmaf(a.x, x[0], z);
+        z = fmaf(a.y, x[1], z);
+        z = fmaf(a.z, x[2], z);
+        z = fmaf(a.w, x[3], z);
+        z = fmaf(b.x, x[4], z);
+        z = fmaf(b.y, x[5], z);
+        z = fmaf(b.z, x[6], z);
+        z = fmaf(b.w, x[7], z);
         h1[j] = silu(z);
     }
     float y = __ldg(w + MLP_B3);
@@ -101,7 +124,13 @@ __device__ __forceinline__ float mlp_forward_std(const float* __restrict__ w, co
     for (int j = 0; j < MLP_H; ++j) {
         float z = __ldg(w + MLP_B2 + j);
 #pragma unroll
-        for (int k = 0; k < MLP_H; ++k) z = fmaf(__ldg(w + MLP_W2 + j * MLP_H + k), h1[k], z);
+        for (int k = 0; k < MLP_H; k += 4) {
+            float4 a = __ldg(w4 + (MLP_W2 + j * MLP_H + k) / 4);
+            z = fmaf(a.x, h1[k], z);
+            z = fmaf(a.y, h1[k + 1], z);
+            z = fmaf(a.z, h1[k + 2], z);
+            z = fmaf(a.w, h1[k + 3], z);
+        }
         y = fmaf(__ldg(w + MLP_W3 + j), silu(z), y);
     }
     return y;
@@ -113,6 +142,15 @@ template <int NDIM>
 __device__ __forceinline__ double mlp_guess(const float* __restrict__ w, const double* ql, const double* qr,
                                             double gamma, double smallp) {
     if (!w) return -1.0;
+    {
+        constexpr int IP = Dims<NDIM>::IP;
+        double rl = smax(ql[0], 1e-10), pl = smax(ql[IP], rl * smallp);
+        double rr = smax(qr[0], 1e-10), pr = smax(qr[IP], rr * smallp);
+        if (smax(pl, pr) < MLP_WEAK_P * smin(pl, pr)) {
+            double du = ql[1] - qr[1], cs = sqrt(gamma * pl / rl) + sqrt(gamma * pr / rr);
+            if (fabs(du) < MLP_WEAK_U * cs) return -1.0;
+        }
+    }
     float x[MLP_IN];
     double pref, base, p2s;
     mlp_features<NDIM>(ql, qr, gamma, smallp, x, &pref, &base, &p2s);

@@ -414,15 +414,19 @@ int launch_leaf_substep_t(rg_ctx* c, const Plan& P, double dx, int pressure_cap,
     StepK K = step_consts(c);
     TreeView T = tree_view(c);
     PlanView V = P.view();
+    if (c->timing) cudaEventRecord(c->ev[0], c->stream);
     k_courant_init<<<1, 1, 0, c->stream>>>(c->d_status, c->params.boxlen / 1e-10);
     int nprim = P.ncells + P.nextra_prim;
     k_courant_prim<NDIM><<<grid_for(c, nprim, 256), 256, 0, c->stream>>>(T, V, c->d_uold, c->d_prim, c->d_status, dx,
                                                                          K.gamma, K.smalle, cfl, pressure_cap);
     k_dt_finalize<<<1, 1, 0, c->stream>>>(c->d_status, dx);
+    if (c->timing) cudaEventRecord(c->ev[1], c->stream);
     double* fsum = c->d_flux + (size_t)(2 * NDIM) * (NDIM + 2) * P.ncells;
     if (int rc = launch_face_tiles(c, P, K, c->d_uold, c->d_prim, c->d_flux, fsum)) return rc;
+    if (c->timing) cudaEventRecord(c->ev[2], c->stream);
     k_fold<NDIM, true, true><<<grid_for(c, P.ntarg, 256), 256, 0, c->stream>>>(T, V, c->d_flux, c->d_unew,
                                                                                c->d_status, K.gamma, c->d_uold, fsum);
+    if (c->timing) cudaEventRecord(c->ev[3], c->stream);
     return check_cuda(c, cudaGetLastError(), "leaf substep kernels");
 }
 
