@@ -241,9 +241,29 @@ int rg_exact_stats(rg_ctx* ctx, int64_t* iters, int64_t* calls, int reset);
  * tiles per queue grab) is timed on each level's first substep and the
  * fastest kept; on == 0 keeps the default shape instead. */
 int rg_set_autotune(rg_ctx* ctx, int on);
+/* ---- ensembles of independent boxes (no reference counterpart) ----------
+ * Many independent periodic boxes, each a uniform grid the reference would
+ * run as its own simulation, stepped together: the host merges their trees
+ * into one forest whose level list `ilevel` chains every box's leaf octs,
+ * box after box (so each box keeps the oct order, hence the update order, it
+ * has alone), and tells the library which list positions belong to which
+ * box.  rg_level_substep then computes one CFL step per box (the reference
+ * formula with that box's dx) and advances every box by its own dt in the
+ * same launches.  first_oct[nbox+1]: box b owns level-list positions
+ * [first_oct[b], first_oct[b+1]); dx[nbox]: the dx the reference passes for
+ * that box's level (boxlen / (nx 2^level)).  The level must have no refined
+ * cell.  The table is dropped when rg_sync_topology rebuilds the plans.
+ * rg_godunov_level, rg_courant_step and the allocation-free entry point
+ * refuse a level with boxes (they take one dt for the whole level). */
+int rg_set_level_boxes(rg_ctx* ctx, int ilevel, int nbox, const int* first_oct, const double* dx);
+/* dt of every box in the last substep (nbox must equal the level's count);
+ * rg_level_substep's dt_used reports the smallest of them. */
+int rg_level_box_dt(rg_ctx* ctx, int ilevel, double* dt_out, int nbox);
+
 /* Shape chosen for a level: variant index, batch, and its timed ms. */
 int rg_face_config(rg_ctx* ctx, int ilevel, int* variant, int* batch, float* ms);
-/* Pin the face-kernel shape of a level (variant 0..6, batch >= 1). */
+/* Pin the face-kernel shape of a level (variant 0..8, batch >= 1; 7 and 8
+ * select the software-pipelined kernel on levels above level 0 in 2D/3D). */
 int rg_set_face_config(rg_ctx* ctx, int ilevel, int variant, int batch);
 
 #ifdef __cplusplus

@@ -6,6 +6,8 @@
 // int status and never throws across the boundary.
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <new>
 #include <string>
@@ -101,6 +103,18 @@ int validate_params(rg_ctx* c, const rg_params* p) {
 
 void invalidate_plans(rg_ctx* c) {
     for (auto& p : c->plans) free_plan(p);
+}
+
+// dt of every box of an ensemble level (synchronises the stream)
+int box_dts(rg_ctx* c, const Plan& P, double* out) {
+    std::vector<BoxStep> h((size_t)P.nbox);
+    if (int rc = check_cuda(c, cudaMemcpyAsync(h.data(), P.boxes, h.size() * sizeof(BoxStep), cudaMemcpyDeviceToHost,
+                                               c->stream),
+                            "box dt copy"))
+        return rc;
+    if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "box dt sync")) return rc;
+    for (size_t b = 0; b < h.size(); ++b) out[b] = h[b].dt;
+    return RG_OK;
 }
 
 int get_plan(rg_ctx* c, int ilevel, Plan** out) {
@@ -378,6 +392,7 @@ int rg_godunov_level(rg_ctx* c, int ilevel, double dt, double dx) {
     if (int rc = check_learned(c)) return rc;
     Plan* P;
     if (int rc = get_plan(c, ilevel, &P)) return rc;
+    if (P->nbox > 0) return set_error(c, RG_ERR_STATE, "ensemble level: every box has its own dt, use rg_level_substep");
     record_updates(c, ilevel, *P);
     if (P->ncells == 0) return RG_OK;
     if (int rc = ensure_flux(c, *P)) return rc;
@@ -395,6 +410,7 @@ int rg_courant_step(rg_ctx* c, int ilevel, double dx, double courant_factor, int
     if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state uploaded");
     Plan* P;
     if (int rc = get_plan(c, ilevel, &P)) return rc;
+    if (P->nbox > 0) return set_error(c, RG_ERR_STATE, "ensemble level: read the per-box steps with rg_level_box_dt");
     if (int rc = launch_courant(c, *P, dx, pressure_cap, courant_factor)) return rc;
     if (int rc = check_cuda(c, cudaMemcpyAsync(c->h_status, c->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
                                                c->stream),
@@ -462,6 +478,12 @@ int rg_level_substep(rg_ctx* c, int ilevel, double dx, int pressure_cap, int use
         if (int rc = enqueue()) return rc;
     }
     if (dt_used) {
+        if (P->nbox > 0) {
+            std::vector<double> dts((size_t)P->nbox);
+            if (int rc = box_dts(c, *P, dts.data())) return rc;
+            *dt_used = *std::min_element(dts.begin(), dts.end());
+            return RG_OK;
+        }
         if (int rc = check_cuda(c, cudaMemcpyAsync(c->h_status, c->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
                                                    c->stream),
                                 "dt copy"))
@@ -470,6 +492,55 @@ int rg_level_substep(rg_ctx* c, int ilevel, double dx, int pressure_cap, int use
         *dt_used = c->h_status->dt;
     }
     return RG_OK;
+}
+
+int rg_set_level_boxes(rg_ctx* c, int ilevel, int nbox, const int* first_oct, const double* dx) {
+    CTX_GUARD(c);
+    if (nbox < 1 || !first_oct || !dx) return set_error(c, RG_ERR_ARG, "nbox >= 1, first_oct[nbox+1] and dx[nbox] required");
+    Plan* P;
+    if (int rc = get_plan(c, ilevel, &P)) return rc;
+    if (P->level0) return set_error(c, RG_ERR_ARG, "ensemble boxes need a level above the coarse level");
+    if (P->nactive != P->ncells) return set_error(c, RG_ERR_STATE, "ensemble level has refined cells");
+    if (first_oct[0] != 0 || first_oct[nbox] != P->noct)
+        return set_error(c, RG_ERR_ARG, "first_oct must start at 0 and end at the level's oct count " +
+                                            std::to_string(P->noct));
+    std::vector<int> obox((size_t)P->noct);
+    std::vector<BoxStep> boxes((size_t)nbox);
+    for (int b = 0; b < nbox; ++b) {
+        if (first_oct[b + 1] <= first_oct[b]) return set_error(c, RG_ERR_ARG, "box " + std::to_string(b) + " is empty");
+        if (!(dx[b] > 0.0) || !std::isfinite(dx[b])) return set_error(c, RG_ERR_ARG, "dx must be positive");
+        for (int k = first_oct[b]; k < first_oct[b + 1]; ++k) obox[(size_t)k] = b;
+        boxes[(size_t)b] = BoxStep{0ULL, 0.0, dx[b], 0.0, 0.0, 0, 0};
+    }
+    if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "boxes sync")) return rc;
+    cudaFree(P->obox);
+    cudaFree(P->boxes);
+    P->obox = nullptr;
+    P->boxes = nullptr;
+    P->nbox = 0;
+    if (int rc = check_cuda(c, cudaMalloc(&P->obox, obox.size() * sizeof(int)), "cudaMalloc(boxes)")) return rc;
+    if (int rc = check_cuda(c, cudaMalloc(&P->boxes, boxes.size() * sizeof(BoxStep)), "cudaMalloc(boxes)")) return rc;
+    if (int rc = check_cuda(c, cudaMemcpy(P->obox, obox.data(), obox.size() * sizeof(int), cudaMemcpyHostToDevice),
+                            "boxes upload"))
+        return rc;
+    if (int rc = check_cuda(c, cudaMemcpy(P->boxes, boxes.data(), boxes.size() * sizeof(BoxStep),
+                                          cudaMemcpyHostToDevice),
+                            "boxes upload"))
+        return rc;
+    P->nbox = nbox;
+    if (P->graph) {
+        cudaGraphExecDestroy(P->graph);
+        P->graph = nullptr;
+    }
+    return RG_OK;
+}
+
+int rg_level_box_dt(rg_ctx* c, int ilevel, double* dt_out, int nbox) {
+    CTX_GUARD(c);
+    Plan* P = existing_plan(c, ilevel);
+    if (!P || P->nbox == 0) return set_error(c, RG_ERR_STATE, "level has no ensemble boxes");
+    if (!dt_out || nbox != P->nbox) return set_error(c, RG_ERR_ARG, "dt_out must hold the level's box count");
+    return box_dts(c, *P, dt_out);
 }
 
 int rg_synchronize(rg_ctx* c) {
@@ -575,7 +646,7 @@ int rg_face_config(rg_ctx* c, int ilevel, int* variant, int* batch, float* ms) {
 int rg_set_face_config(rg_ctx* c, int ilevel, int variant, int batch) {
     CTX_GUARD(c);
     if (variant < 0 || variant >= kNumFaceVariants || batch < 1)
-        return set_error(c, RG_ERR_ARG, "variant must be 0..6, batch >= 1");
+        return set_error(c, RG_ERR_ARG, "variant must be in [0, 9), batch >= 1");
     Plan* P;
     if (int rc = get_plan(c, ilevel, &P)) return rc;
     P->face_variant = variant;

@@ -186,6 +186,13 @@ __device__ __forceinline__ void ghost_1d(const double* __restrict__ uold, size_t
     trace<1>(qg, dq, dt, D.dx, qm, qp, gamma);
 }
 
+// Step values of the box of level cell p (ensemble levels).
+__device__ __forceinline__ void step_of_box(const PlanView& P, int p, double& dt, DxDiv& D) {
+    const BoxStep& B = P.boxes[box_of(P, p)];
+    dt = B.dt;
+    D = DxDiv{B.dx, B.inv_dx, B.dx_pow2 != 0};
+}
+
 template <int NDIM, int RS>
 __device__ __forceinline__ int riemann(const double* ql, const double* qr, double* f, const StepK& K) {
     if constexpr (RS == RG_RIEMANN_HLLC) solve_hllc<NDIM>(ql, qr, f, K.gamma, K.smallp);
@@ -200,12 +207,14 @@ __device__ __forceinline__ int riemann(const double* ql, const double* qr, doubl
 
 // Face state of the neighbour across slot (idim, side), rotated.  Writes the
 // state the Riemann problem needs: the neighbour's right-face state (qm) for
-// side 0, its left-face state (qp) for side 1.
+// side 0, its left-face state (qp) for side 1.  qside is the rotated primitive
+// state of neighbour cell n (the own trace's stencil cell on that side; only
+// read off level 0 outside the boundary branch).
 template <int NDIM>
 __device__ __forceinline__ void neighbour_face(const TreeView& T, const PlanView& P, const double* __restrict__ prim,
                                                const double* __restrict__ uold, size_t ncell, int p, int c, int idim,
-                                               int side, int kd, int n, const double* qc, double dt,
-                                               const DxDiv& D, const StepK& K, double* qf) {
+                                               int side, int kd, int n, const double* qc, const double* qside,
+                                               double dt, const DxDiv& D, const StepK& K, double* qf) {
     constexpr int NV = Dims<NDIM>::NV;
     double qm[NV], qp[NV];
     int kind = kd & KIND_MASK;
@@ -244,10 +253,23 @@ __device__ __forceinline__ void neighbour_face(const TreeView& T, const PlanView
                 }
             }
             {
-                double qn[NV], qnl[NV], qnr[NV];
-                load_rot<NDIM>(prim, ncell, n, idim, qn);
-                load_nb_rot<NDIM>(T, prim, ncell, nl, idim, qn, qnl);
-                load_nb_rot<NDIM>(T, prim, ncell, nr, idim, qn, qnr);
+                // the neighbour's state is the own trace's stencil cell on this
+                // side (qside, already loaded), and on a same-level face the
+                // neighbour's stencil cell towards this cell is the cell itself
+                double qnl[NV], qnr[NV];
+                const double* qn = qside;
+                if (side == 0 && nr == c) {
+#pragma unroll
+                    for (int iv = 0; iv < NV; ++iv) qnr[iv] = qc[iv];
+                } else {
+                    load_nb_rot<NDIM>(T, prim, ncell, nr, idim, qn, qnr);
+                }
+                if (side == 1 && nl == c) {
+#pragma unroll
+                    for (int iv = 0; iv < NV; ++iv) qnl[iv] = qc[iv];
+                } else {
+                    load_nb_rot<NDIM>(T, prim, ncell, nl, idim, qn, qnl);
+                }
                 if (kind == K_GHOST) ghost_trace<NDIM>(qn, qnl, qnr, dt, D, K, qm, qp);
                 else own_trace<NDIM>(qn, qnl, qnr, dt, D, K, qm, qp);
             }
@@ -284,8 +306,8 @@ __global__ void __launch_bounds__(TILE * NDIM * R, MINB)
     const size_t ncell = (size_t)T.ncell;
     const int nc = P.ncells;
     const int ntiles = (nc + TILE - 1) / TILE;
-    const double dt = st->dt;
-    const DxDiv D{st->dx, st->inv_dx, st->dx_pow2 != 0};
+    const double dt0 = st->dt;
+    const DxDiv D0{st->dx, st->inv_dx, st->dx_pow2 != 0};
     unsigned long long iters = 0, calls = 0;
     for (;;) {
         if (threadIdx.x == 0) s_base = (int)atomicAdd(&st->face_next, (unsigned)(batch * R));
@@ -305,7 +327,10 @@ __global__ void __launch_bounds__(TILE * NDIM * R, MINB)
                 if (kd0 != K_NONE) {
                     const int kd1 = P.kind[(size_t)(s0 + 1) * nc + p];
                     const int c = cell_of(T, P, p);
-                    double qc[NV], qmo[NV], qpo[NV];
+                    double dt = dt0;
+                    DxDiv D = D0;
+                    if (P.obox) step_of_box(P, p, dt, D);
+                    double qc[NV], qmo[NV], qpo[NV], ql[NV], qr[NV];
                     load_rot<NDIM>(prim, ncell, c, idim, qc);
                     if (P.level0) {
                         double qn[NV], dq0[NV];
@@ -317,7 +342,6 @@ __global__ void __launch_bounds__(TILE * NDIM * R, MINB)
                         rot_swap<NDIM>(qpo, idim);
                     } else {
                         const int l = P.icn[(size_t)s0 * nc + p], rr = P.icn[(size_t)(s0 + 1) * nc + p];
-                        double ql[NV], qr[NV];
                         load_nb_rot<NDIM>(T, prim, ncell, l, idim, qc, ql);
                         load_nb_rot<NDIM>(T, prim, ncell, rr, idim, qc, qr);
                         own_trace<NDIM>(qc, ql, qr, dt, D, K, qmo, qpo);
@@ -333,7 +357,8 @@ __global__ void __launch_bounds__(TILE * NDIM * R, MINB)
                         } else {
                             const int n = P.icn[(size_t)s * nc + p];
                             double qf[NV];
-                            neighbour_face<NDIM>(T, P, prim, uold, ncell, p, c, idim, side, kd, n, qc, dt, D, K, qf);
+                            neighbour_face<NDIM>(T, P, prim, uold, ncell, p, c, idim, side, kd, n, qc,
+                                                 side ? qr : ql, dt, D, K, qf);
                             if (side == 0) iters += riemann<NDIM, RS>(qf, qpo, f, K);
                             else iters += riemann<NDIM, RS>(qmo, qf, f, K);
                             ++calls;
@@ -385,9 +410,13 @@ __global__ void __launch_bounds__(TILE * NDIM * R, MINB)
 }
 
 // Variant table: tiles per block (R) and the launch-bounds minimum of
-// resident blocks (caps registers per thread).  Index = variant id.
+// resident blocks (caps registers per thread).  Index = variant id.  Ids
+// kFirstPipeVariant.. select the software-pipelined kernel (rg_face_pipe.cuh)
+// with launch-bounds minimum 4 and 3 (levels above level 0 in 2D/3D builds;
+// elsewhere they fall back to the default variant).
 #define RG_FACE_VARIANTS(X) X(0, 1, 6) X(1, 1, 8) X(2, 1, 10) X(3, 1, 12) X(4, 2, 4) X(5, 2, 5) X(6, 2, 6)
-constexpr int kNumFaceVariants = 7;
+constexpr int kFirstPipeVariant = 7;
+constexpr int kNumFaceVariants = 9;
 constexpr int kDefaultFaceVariant = 1;
 
 template <int NDIM, int RS, int R, int MINB>

@@ -54,6 +54,15 @@ struct DevStatus {
     unsigned long long exact_iters, exact_calls;  // exact-solver Newton statistics
 };
 
+// Step values of one box of an ensemble level (independent periodic boxes
+// whose leaf octs share one level list, each with its own dx and CFL step):
+// the box's CFL min-reduction word and the values derived from it.
+struct BoxStep {
+    unsigned long long dtmin_bits;
+    double dt, dx, dtdx, inv_dx;
+    int dx_pow2, pad;
+};
+
 // Read-only view of the mirrored tree handed to kernels.
 struct TreeView {
     int ncoarse, ngridmax, ncell, nx, ny, nz;
@@ -76,7 +85,12 @@ struct PlanView {
     const int* tev;        // [toff[ntarg]] event keys: (cpu_pos*8 + slot)
     const int* textra;     // [ntarg-ncells] cell ids of extra (coarser) targets
     const int* xprim;      // [nextra_prim] cells outside the level needing primitives
+    const int* obox;       // [noct] box of each oct position (ensemble levels), else nullptr
+    BoxStep* boxes;        // [nbox] per-box step values (ensemble levels), else nullptr
 };
+
+// Box of level cell p (ensemble levels only).
+__device__ __forceinline__ int box_of(const PlanView& P, int p) { return P.obox[p % P.noct]; }
 
 struct Plan {
     bool valid = false;
@@ -90,8 +104,12 @@ struct Plan {
     int face_variant = -1, face_batch = 4;  // autotuned face-kernel shape (-1: not tuned yet)
     float face_ms = 0.f;
     int substeps_run = 0;
+    int nbox = 0;              // ensemble level: number of boxes (0: one grid)
+    int* obox = nullptr;       // [noct]
+    BoxStep* boxes = nullptr;  // [nbox]
     PlanView view() const {
-        return PlanView{ilevel, level0, noct, ncells, ntarg, nextra_prim, octs, icn, stc, kind, toff, tev, textra, xprim};
+        return PlanView{ilevel, level0, noct, ncells, ntarg, nextra_prim, octs, icn, stc, kind, toff, tev, textra,
+                        xprim, obox, boxes};
     }
 };
 

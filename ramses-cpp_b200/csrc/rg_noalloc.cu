@@ -62,6 +62,7 @@ extern "C" int rg_godunov_level_noalloc(rg_ctx* c, int ilevel, double dt, double
     if (!uold_dev || !unew_dev) return rg::set_error(c, RG_ERR_ARG, "uold_dev and unew_dev must be device pointers");
     if (int rc = rg::check_cuda(c, cudaSetDevice(c->device), "cudaSetDevice")) return rc;
     rg::Plan* P = rg::existing_plan(c, ilevel);
+    if (P && P->nbox > 0) return rg::set_error(c, RG_ERR_STATE, "ensemble level: every box has its own dt");
     if (!P)
         return rg::set_error(c, RG_ERR_STATE,
                              "no level plan: building one allocates, so call rg_godunov_level (or rg_set_unew) "

@@ -362,6 +362,8 @@ void free_plan(Plan& p) {
     cudaFree(p.tev);
     cudaFree(p.textra);
     cudaFree(p.xprim);
+    cudaFree(p.obox);
+    cudaFree(p.boxes);
     p = Plan();
 }
 

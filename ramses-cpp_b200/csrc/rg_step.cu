@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(128) k_face(TreeView T, PlanView P, const doub
         if (kd0 == K_NONE) continue;
         int kd1 = P.kind[(size_t)(s0 + 1) * nc + p];
         int c = cell_of(T, P, p);
-        double qc[NV], qmo[NV], qpo[NV];
+        double qc[NV], qmo[NV], qpo[NV], ql[NV], qr[NV];
         load_rot<NDIM>(prim, ncell, c, idim, qc);
         if (P.level0) {
             double qn[NV], dq0[NV];
@@ -59,7 +59,6 @@ __global__ void __launch_bounds__(128) k_face(TreeView T, PlanView P, const doub
             rot_swap<NDIM>(qpo, idim);
         } else {
             int l = P.icn[(size_t)s0 * nc + p], r = P.icn[(size_t)(s0 + 1) * nc + p];
-            double ql[NV], qr[NV];
             load_nb_rot<NDIM>(T, prim, ncell, l, idim, qc, ql);
             load_nb_rot<NDIM>(T, prim, ncell, r, idim, qc, qr);
             own_trace<NDIM>(qc, ql, qr, dt, D, K, qmo, qpo);
@@ -75,7 +74,8 @@ __global__ void __launch_bounds__(128) k_face(TreeView T, PlanView P, const doub
             } else {
                 int n = P.icn[(size_t)s * nc + p];
                 double qf[NV];
-                neighbour_face<NDIM>(T, P, prim, uold, ncell, p, c, idim, side, kd, n, qc, dt, D, K, qf);
+                neighbour_face<NDIM>(T, P, prim, uold, ncell, p, c, idim, side, kd, n, qc, side ? qr : ql, dt, D, K,
+                                     qf);
                 if (side == 0) iters += riemann<NDIM, RS>(qf, qpo, f, K);
                 else iters += riemann<NDIM, RS>(qmo, qf, f, K);
                 rot_swap<NDIM>(f, idim);
@@ -117,11 +117,17 @@ __global__ void k_fold(TreeView T, PlanView P, const double* __restrict__ flux, 
     constexpr int NV = Dims<NDIM>::NV, NS = Dims<NDIM>::NS, TTD = Dims<NDIM>::TTD;
     const size_t ncell = (size_t)T.ncell;
     const int nc = P.ncells;
-    const double dtdx = st->dtdx;
+    const double dtdx0 = st->dtdx;
     const double factor = 1.0 / (1 << NDIM);
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < P.ntarg; t += gridDim.x * blockDim.x) {
         int a = P.toff[t], b = P.toff[t + 1];
         if (a == b) continue;
+        double dtdx = dtdx0;
+        if (P.obox) {
+            // ensemble level: a target's updates all come from its own box
+            const int cp = P.tev[a] >> 3;
+            dtdx = P.boxes[box_of(P, P.level0 ? cp : (cp % TTD) * P.noct + cp / TTD)].dtdx;
+        }
         int cell = (t < nc) ? cell_of(T, P, t) : P.textra[t - nc];
         const bool from_old = LEAF && t < nc;
         const double* src = from_old ? uold : unew;
@@ -300,6 +306,89 @@ __global__ void k_dt_finalize(DevStatus* st, double dx) {
 }
 __global__ void k_dt_set(DevStatus* st, double dt, double dx) { set_step_values(st, dt, dx); }
 
+// ---- ensemble levels: one CFL step per box
+__global__ void k_box_courant_init(BoxStep* boxes, int nbox, double dt_start) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nbox; b += gridDim.x * blockDim.x)
+        boxes[b].dtmin_bits = (unsigned long long)__double_as_longlong(dt_start);
+}
+__global__ void k_box_dt_finalize(BoxStep* boxes, int nbox) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nbox; b += gridDim.x * blockDim.x) {
+        BoxStep& B = boxes[b];
+        const double dt = __longlong_as_double((long long)B.dtmin_bits), dx = B.dx;
+        B.dt = dt;
+        B.dtdx = dt / dx;
+        const double inv = 1.0 / dx;
+        B.inv_dx = inv;
+        B.dx_pow2 = is_pow2_with_normal_inverse(dx, inv) ? 1 : 0;
+    }
+}
+
+// k_courant_prim of an ensemble level: each cell's CFL candidate uses its
+// box's dx and goes to its box's min-reduction word.  Warps walk aligned runs
+// of 32 consecutive level cells; a box owns contiguous oct positions, so the
+// lanes of one box form one run and a segmented shuffle min leaves one atomic
+// per run.
+template <int NDIM>
+__global__ void k_courant_prim_boxes(TreeView T, PlanView P, const double* __restrict__ uold,
+                                     double* __restrict__ prim, double gamma, double smalle, double cfl,
+                                     int pressure_cap) {
+    constexpr int NV = Dims<NDIM>::NV;
+    const size_t ncell = (size_t)T.ncell;
+    const int total = P.ncells + P.nextra_prim;
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long base = warp * 32; base < total; base += nwarps * 32) {
+        const int t = (int)(base + lane);
+        unsigned long long best = ~0ULL;
+        int box = -1;
+        if (t < total) {
+            int id = (t < P.ncells) ? cell_of(T, P, t) : P.xprim[t - P.ncells];
+            double u[NV], q[NV];
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) u[iv] = uold[(size_t)iv * ncell + id - 1];
+            ctoprim<NDIM>(u, q, gamma, smalle);
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) prim[(size_t)iv * ncell + id - 1] = q[iv];
+            if (t < P.ncells && T.son[id - 1] == 0) {
+                box = box_of(P, t);
+                const double dx = P.boxes[box].dx;
+                double d = smax(u[0], 1e-10), v2 = 0.0;
+#pragma unroll
+                for (int i = 1; i <= NDIM; ++i) {
+                    double v = u[i] / d;
+                    v2 = v2 + v * v;
+                }
+                double e_non = 0.0, sum_gamma_p = 0.0;
+                double pr = smax((u[NDIM + 1] - 0.5 * d * v2 - e_non) * (gamma - 1.0), d * 1e-10);
+                if (pressure_cap) pr = smin(pr, d * 1e2);
+                double cs2 = cs2_of(d, pr, gamma);
+                cs2 = cs2 + sum_gamma_p / d;
+                double cs = sqrt(smax(cs2, 1e-10));
+                double u_wave = NDIM * cs;
+#pragma unroll
+                for (int i = 1; i <= NDIM; ++i) u_wave = u_wave + fabs(u[i] / d);
+                double a_grav = 0.0;
+#pragma unroll
+                for (int i = 1; i <= NDIM; ++i) a_grav = a_grav + fabs(0.0);
+                double alpha = a_grav * dx / (u_wave * u_wave);
+                alpha = smax(alpha, 0.0001);
+                double dtc = (dx / u_wave) * (sqrt(1.0 + 2.0 * cfl * alpha) - 1.0) / alpha;
+                unsigned long long b = (unsigned long long)__double_as_longlong(dtc);
+                if (dtc >= 0.0) best = b;
+            }
+        }
+        // segmented min over runs of equal box in lane order
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long ob = __shfl_down_sync(0xffffffffu, best, o);
+            const int obx = __shfl_down_sync(0xffffffffu, box, o);
+            if (lane + o < 32 && obx == box && ob < best) best = ob;
+        }
+        const int prev = __shfl_up_sync(0xffffffffu, box, 1);
+        if (box >= 0 && (lane == 0 || prev != box) && best != ~0ULL) atomicMin(&P.boxes[box].dtmin_bits, best);
+    }
+}
+
 }  // namespace
 
 StepK step_consts(const rg_ctx* c) {
@@ -415,11 +504,21 @@ int launch_leaf_substep_t(rg_ctx* c, const Plan& P, double dx, int pressure_cap,
     TreeView T = tree_view(c);
     PlanView V = P.view();
     if (c->timing) cudaEventRecord(c->ev[0], c->stream);
-    k_courant_init<<<1, 1, 0, c->stream>>>(c->d_status, c->params.boxlen / 1e-10);
     int nprim = P.ncells + P.nextra_prim;
-    k_courant_prim<NDIM><<<grid_for(c, nprim, 256), 256, 0, c->stream>>>(T, V, c->d_uold, c->d_prim, c->d_status, dx,
-                                                                         K.gamma, K.smalle, cfl, pressure_cap);
-    k_dt_finalize<<<1, 1, 0, c->stream>>>(c->d_status, dx);
+    if (P.nbox > 0) {
+        const int bb = (P.nbox + 127) / 128;
+        k_box_courant_init<<<bb, 128, 0, c->stream>>>(P.boxes, P.nbox, c->params.boxlen / 1e-10);
+        k_courant_prim_boxes<NDIM><<<grid_for(c, nprim, 256), 256, 0, c->stream>>>(T, V, c->d_uold, c->d_prim,
+                                                                                   K.gamma, K.smalle, cfl,
+                                                                                   pressure_cap);
+        k_box_dt_finalize<<<bb, 128, 0, c->stream>>>(P.boxes, P.nbox);
+    } else {
+        k_courant_init<<<1, 1, 0, c->stream>>>(c->d_status, c->params.boxlen / 1e-10);
+        k_courant_prim<NDIM><<<grid_for(c, nprim, 256), 256, 0, c->stream>>>(T, V, c->d_uold, c->d_prim,
+                                                                             c->d_status, dx, K.gamma, K.smalle,
+                                                                             cfl, pressure_cap);
+        k_dt_finalize<<<1, 1, 0, c->stream>>>(c->d_status, dx);
+    }
     if (c->timing) cudaEventRecord(c->ev[1], c->stream);
     double* fsum = c->d_flux + (size_t)(2 * NDIM) * (NDIM + 2) * P.ncells;
     if (int rc = launch_face_tiles(c, P, K, c->d_uold, c->d_prim, c->d_flux, fsum)) return rc;

@@ -111,6 +111,8 @@ def lib():
     L.rg_face_config.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float)]
     L.rg_godunov_level_noalloc.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p]
     L.rg_get_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+    L.rg_set_level_boxes.argtypes = [VP, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    L.rg_level_box_dt.argtypes = [VP, C.c_int, C.POINTER(C.c_double), C.c_int]
     _lib = L
     return L
 
@@ -249,6 +251,20 @@ class Context:
 
     def set_face_config(self, il, variant, batch):
         self._chk(self.L.rg_set_face_config(self.h, il, variant, batch))
+
+    # ---- ensembles of independent boxes sharing one level list
+    def set_level_boxes(self, il, first_oct, dx):
+        first = np.ascontiguousarray(first_oct, dtype=np.int32)
+        dxs = np.ascontiguousarray(dx, dtype=np.float64)
+        if len(first) != len(dxs) + 1:
+            raise ValueError("first_oct needs one entry more than dx")
+        self._chk(self.L.rg_set_level_boxes(self.h, il, len(dxs), first.ctypes.data_as(C.POINTER(C.c_int)),
+                                            dxs.ctypes.data_as(C.POINTER(C.c_double))))
+
+    def level_box_dt(self, il, nbox):
+        out = np.zeros(nbox, dtype=np.float64)
+        self._chk(self.L.rg_level_box_dt(self.h, il, out.ctypes.data_as(C.POINTER(C.c_double)), nbox))
+        return out
 
     # ---- exact solver / learned guess (device buffers passed as raw addresses)
     def exact_batch(self, n, ql, qr, gamma=None, flux=None, pstar=None, iters=None, learned=False, niter=10,

@@ -100,10 +100,13 @@ def test_golden_uniform_cases(ctx_factory, golden):
             assert bits_equal(got, want), key
 
 
-@pytest.mark.parametrize("fixture", ["amr3d", "amr1d"])
-def test_golden_amr_calls(ctx_factory, golden, fixture):
+@pytest.mark.parametrize("fixture,variant", [("amr3d", None), ("amr1d", None), ("amr3d", 7), ("amr3d", 8),
+                                             ("amr1d", 7)])
+def test_golden_amr_calls(ctx_factory, golden, fixture, variant):
     """godunov_fine calls recorded from a sub-cycled AMR run of the reference:
-    coarse-fine ghost states and reflux into coarser cells, bit-exact."""
+    coarse-fine ghost states and reflux into coarser cells, bit-exact; also
+    with the software-pipelined face kernel forced on every level (its
+    coarse-fine faces load the neighbour's inner stencil cell directly)."""
     d = golden(fixture)
     ndim, slope, riem = (int(x) for x in d["params"])
     params = make_params(ndim, slope_type=slope, riemann=RIEMANN_NAMES[riem])
@@ -115,6 +118,8 @@ def test_golden_amr_calls(ctx_factory, golden, fixture):
         ctx = ctx_factory(params)
         ctx.sync_topology(g)
         dt, dx = (float(x) for x in d[f"{k}_dtdx"])
+        if variant is not None:
+            ctx.set_face_config(il, variant, 1)
         ctx.upload_state(d[f"{k}_uold"], d[f"{k}_unew_in"])
         ctx.godunov_level(il, dt, dx)
         got = np.empty(nvar * ncell)
@@ -250,7 +255,7 @@ def test_topology_errors_are_reported(ctx_factory):
     ctx.synchronize()
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8])
 def test_every_face_kernel_shape_is_bit_identical(ctx_factory, oracle, variant):
     """The autotuner may pick any shape: each must give the oracle's bits."""
     L = 5
@@ -283,7 +288,7 @@ def test_autotuner_picks_a_shape_and_exact_stats_count(ctx_factory):
     dx = 1.0 / 2 ** L
     ctx.level_substep(L, dx, use_graph=True)  # eager first substep + autotune
     v, b, ms = ctx.face_config(L)
-    assert 0 <= v <= 6 and b >= 1 and ms > 0
+    assert 0 <= v <= 8 and b >= 1 and ms > 0
     ctx.exact_stats(reset=True)
     ctx.level_substep(L, dx, use_graph=True)
     ctx.synchronize()
