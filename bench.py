@@ -13,10 +13,17 @@ Prints one JSON line (rank 0).  N > 1 runs one independent replica per GPU
 (weak scaling): the single-grid step of this workload is not partitioned, so
 the ranks exchange nothing but the final timing maximum.
 
-The line also carries a "newton" object for the exact Riemann solver: the
-stress workload (256^3 independent interface pairs) with the plain two-shock
-Newton start against the learned start (network trained on the GPU first),
-and the same Sedov step run with the exact solver under both starts.
+The line also carries the other workloads of the path, each measured on the
+same box:
+- "newton": the exact Riemann solver on the stress workload (256^3
+  independent interface pairs), plain two-shock Newton start against the
+  learned start (network trained on the GPU first), and the Sedov step run
+  with the exact solver under both starts;
+- "ensemble": 512 independent uneven boxes stepped together (sharded over
+  the ranks when N > 1);
+- "amr": the sub-cycled Sedov AMR run through the reference's own
+  AmrGrid/TreeUpdater step, CPU reference against the GPU drop-in (N = 1);
+- "sod1d": the 1D Sod run to t = 0.245, CPU reference against the GPU (N = 1).
 """
 import argparse
 import json
@@ -417,6 +424,182 @@ def newton_report(local_rank, stream, steps):
     return out
 
 
+def ensemble_report(rank, world, local_rank, steps):
+    """Config 4: 512 independent periodic boxes (edges 16..64, nx 1 and 3,
+    planar Riemann problems, gamma 5/3) in one launch sequence per substep,
+    each box with its own CFL step.  N > 1: the boxes are partitioned over the
+    ranks by cell count and each rank steps its shard (no exchange)."""
+    import torch
+    import rg_ensemble as ens
+    import rgpu
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    t0 = time.perf_counter()
+    specs = ens.box_specs(512)
+    f = ens.Forest(ens.shard_boxes(specs, world)[rank])
+    u0 = f.initial_state()
+    build_s = time.perf_counter() - t0
+    ctx = rgpu.Context(rgpu.make_params(3, slope_type=2, riemann="hllc", gamma=5.0 / 3.0, courant_factor=0.8),
+                       local_rank)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    ctx.sync_topology(f.grid)
+    ctx.upload_state(u0, u0)
+    ctx.set_level_boxes(f.level, f.first_oct, f.dx)
+    for _ in range(3):
+        ctx.level_substep(f.level, 0.0, pressure_cap=False, use_graph=True)
+    ctx.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        ctx.level_substep(f.level, 0.0, pressure_cap=False, use_graph=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    cells = f.cells
+    if dist:
+        t = torch.tensor([ms, float(cells)], device="cuda", dtype=torch.float64)
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        ms, cells = float(mx[0].item()), int(t[1].item())
+    variant = ctx.face_config(f.level)
+    ctx.close()
+    if rank != 0:
+        return None
+    return {"workload": "512 periodic boxes, edges uniform in {16,24,32,48,64} (24, 48: nx=3), planar Riemann "
+                        "problem with random normal, rho log-U[1e-3,1e3], p log-U[1e-4,1e4], u_n U[-3,3], gamma 5/3, "
+                        "MonCen + HLLC, per-box CFL, seed 20261203",
+            "boxes": 512, "cells_per_step": cells, "steps": steps, "ms_per_step": ms / steps,
+            "value": cells * steps / (ms / 1e3), "unit": UNIT, "n_gpus": world,
+            "sharding": "boxes partitioned over ranks by cell count, no exchange" if world > 1 else "one GPU",
+            "face_variant": list(variant), "host_build_s": build_s}
+
+
+def amr_sample(variant, steps, lmin=7, lmax=10, ngridmax=400000):
+    """Config 3 through the reference's own AmrGrid / TreeUpdater / HydroSolver
+    (the CPU reference, or the reference with the GPU drop-in); runs in its own
+    process: the reference prints a line per flagged cell."""
+    import hashlib
+    sys.path.insert(0, str(ROOT / "tests"))
+    from refsupport import AmrRun, RefHarness, namelist, sedov_ic
+    nml = namelist(slope_type=2, riemann="hllc", levelmin=lmin, levelmax=lmax, err_grad_d=0.1, err_grad_p=0.1)
+    h = RefHarness(3, variant).create(nml, ngridmax=ngridmax, levelmin=lmin, nlevelmax=lmax, gamma=1.4)
+    hyd = [0.0]
+
+    def on_g(run, il, dt, dx):
+        t = time.perf_counter()
+        run.h.godunov_fine(il, dt, dx)
+        hyd[0] += time.perf_counter() - t
+
+    r = AmrRun(h, lmin, lmax, 1.4, ed=0.1, ep=0.1, on_godunov=on_g)
+    r.initialize(sedov_ic(3, lmin))
+    r.coarse_step()  # warm-up step (first-call costs)
+    hyd[0] = 0.0
+    cu0 = r.cell_updates
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        r.coarse_step()
+    wall = time.perf_counter() - t0
+    a = h.arrays()
+    out = {"variant": variant, "coarse_steps": steps, "wall_s": wall, "hydro_s": hyd[0],
+           "cell_updates": r.cell_updates - cu0, "t": r.t,
+           "octs_per_level": [h.count_grids(il) for il in range(lmin, lmax + 1)],
+           "digest": hashlib.sha1(a["uold"].tobytes() + a["son"].tobytes()).hexdigest()}
+    h.close()
+    return out
+
+
+def sod_sample(variant):
+    """Config 1: 1D Sod, 1024 cells (reference levelmin=levelmax=11), MinMod +
+    HLLC, reference CFL (courant 0.8; p <= 100 rho holds), to t = 0.245."""
+    import hashlib
+
+    import numpy as np
+    import rg_tree
+    L, gamma, tend = 11, 1.4, 0.245
+    g = rg_tree.build_uniform(1, L)
+    ids = g.cell_ids(L)
+    dx = 1.0 / 2 ** L
+    t, n = 0.0, 0
+    if variant == "cpu":
+        sys.path.insert(0, str(ROOT / "tests"))
+        import refsupport as rs
+        h = rs.RefHarness(1).create(rs.namelist(slope_type=1, riemann="hllc", levelmin=L, levelmax=L),
+                                    ngridmax=g.ngridmax, levelmin=L, nlevelmax=L, gamma=gamma)
+        h.refine_uniform(L)
+        a = h.arrays()
+        u = rg_tree.sod_state(g, L, gamma)
+        a["uold"][:] = u
+        a["unew"][:] = u
+        t0 = time.perf_counter()
+        while t < tend:
+            dt = h.courant(L, dx, gamma, 0.8)
+            h.set_unew(L)
+            h.godunov_fine(L, dt, dx)
+            h.set_uold(L)
+            t += dt
+            n += 1
+        wall = time.perf_counter() - t0
+        final = np.array(a["uold"]).reshape(3, -1)[:, ids - 1]
+        h.close()
+    else:
+        import rgpu
+        ctx = rgpu.Context(rgpu.make_params(1, slope_type=1, riemann="hllc", gamma=gamma, courant_factor=0.8), 0)
+        ctx.sync_topology(g)
+        u = rg_tree.sod_state(g, L, gamma)
+        ctx.upload_state(u, u)
+        t0 = time.perf_counter()
+        while t < tend:
+            t += ctx.level_substep(L, dx, pressure_cap=True, use_graph=True, want_dt=True)
+            n += 1
+        ctx.synchronize()
+        wall = time.perf_counter() - t0
+        out = np.empty_like(u)
+        ctx.download_state(uold=out)
+        ctx.close()
+        final = out.reshape(3, -1)[:, ids - 1]
+    return {"variant": variant, "steps": n, "t": t, "wall_s": wall, "cell_updates": n * len(ids),
+            "digest": hashlib.sha1(np.ascontiguousarray(final).tobytes()).hexdigest()}
+
+
+def run_sample(flag, *args, timeout=900):
+    cmd = [sys.executable, str(Path(__file__).resolve()), flag, *[str(a) for a in args]]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+    for line in reversed(r.stdout.splitlines()):
+        if line.startswith("{"):
+            return json.loads(line)
+    raise RuntimeError(f"{flag} failed: " + r.stderr[-2000:])
+
+
+def amr_report(steps):
+    ref = run_sample("--amr-sample", "cpu", steps)
+    gpu = run_sample("--amr-sample", "gpu", steps)
+    return {"workload": "3D Sedov AMR, reference levelmin 7, levelmax 10 (64^3 base, 512^3 effective), "
+                        "err_grad_d = err_grad_p = 0.1, sub-cycled, MonCen + HLLC, through the reference's own "
+                        "AmrGrid/TreeUpdater/Simulation step with the hydro solver swapped by create_hydro_solver",
+            "coarse_steps": steps, "after": "initialisation and one warm-up coarse step",
+            "reference_cpu": ref, "gpu_dropin": gpu, "bit_identical": ref["digest"] == gpu["digest"],
+            "wall_speedup": ref["wall_s"] / gpu["wall_s"], "hydro_speedup": ref["hydro_s"] / gpu["hydro_s"],
+            "gpu_hydro_cell_updates_per_s": gpu["cell_updates"] / gpu["hydro_s"],
+            "note": "tree maintenance (flag/refine/restrict) stays on the host in both arms; GPU hydro time "
+                    "includes the level-sparse host<->device copies of every godunov_fine call"}
+
+
+def sod_report():
+    ref = run_sample("--sod-sample", "cpu")
+    gpu = run_sample("--sod-sample", "gpu")
+    return {"workload": "1D Sod, 1024 cells (reference levelmin=levelmax=11), MinMod + HLLC, courant 0.8, "
+                        "to t=0.245", "reference_cpu": ref, "gpu": gpu,
+            "bit_identical": ref["digest"] == gpu["digest"] and ref["steps"] == gpu["steps"],
+            "wall_speedup": ref["wall_s"] / gpu["wall_s"],
+            "note": "GPU run reads dt back every step (the run stops at t >= 0.245), so it is launch/latency bound"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -425,10 +608,19 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-newton", action="store_true", help="skip the exact-solver plain/learned report")
+    ap.add_argument("--no-extra", action="store_true", help="skip the ensemble, AMR and Sod reports")
     ap.add_argument("--cpu-sample", nargs=2, type=int, metavar=("LEVEL", "STEPS"), help=argparse.SUPPRESS)
+    ap.add_argument("--amr-sample", nargs=2, metavar=("VARIANT", "STEPS"), help=argparse.SUPPRESS)
+    ap.add_argument("--sod-sample", metavar="VARIANT", help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.cpu_sample:
         print(json.dumps(cpu_sample(*args.cpu_sample)))
+        return
+    if args.amr_sample:
+        print(json.dumps(amr_sample(args.amr_sample[0], int(args.amr_sample[1]))))
+        return
+    if args.sod_sample:
+        print(json.dumps(sod_sample(args.sod_sample)))
         return
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -457,6 +649,13 @@ def main():
     if rank == 0 and not args.no_newton:
         import torch
         out["newton"] = newton_report(local_rank, torch.cuda.Stream(), min(max(args.steps // 20, 5), 40))
+    if not args.no_extra:
+        ens_out = ensemble_report(rank, world, local_rank, 100)
+        if rank == 0:
+            out["ensemble"] = ens_out
+            if world == 1:
+                out["amr"] = amr_report(3)
+                out["sod1d"] = sod_report()
     if world > 1:
         import torch.distributed as dist
         dist.barrier()

@@ -195,6 +195,16 @@ int rg_mlp_set(rg_ctx* ctx, const float* params);
  * the training kernel without updating the weights. */
 int rg_mlp_grad(rg_ctx* ctx, int n, const float* x, const float* t, float* grad, float* loss);
 
+/* Level step on state held in host memory: the drop-in form of
+ * HydroSolver::godunov_fine (HydroSolver.cpp:18-573) for callers whose
+ * AmrGrid keeps uold/unew on the host between calls.  Uploads uold only at
+ * the cells the step reads (the level's cells and the stencil cells outside
+ * it) and unew only at its update targets, runs the step, and writes back
+ * unew at the targets alone; every other host value is left untouched, as
+ * the reference leaves it.  uold/unew: host arrays of nvar*ncell doubles in
+ * AmrGrid's layout.  Synchronises the context stream before returning. */
+int rg_godunov_level_host(rg_ctx* ctx, int ilevel, double dt, double dx, const double* uold, double* unew);
+
 /* ---- allocation-free variant ---------------------------------------------- */
 /* No counterpart in the reference.  The same level step as rg_godunov_level
  * for callers that must not allocate device memory once set-up is over (a

@@ -127,6 +127,14 @@ int get_plan(rg_ctx* c, int ilevel, Plan** out) {
             free_plan(p);
             return rc;
         }
+        if ((int)c->tuned.size() > ilevel) {
+            const TunedShape& t = c->tuned[ilevel];
+            if (t.variant >= 0 && p.ncells <= 2LL * t.ncells && 2LL * p.ncells >= t.ncells) {
+                p.face_variant = t.variant;
+                p.face_batch = t.batch;
+                p.face_ms = t.ms;
+            }
+        }
     }
     *out = &p;
     return RG_OK;
@@ -154,6 +162,12 @@ void record_updates(rg_ctx* c, int ilevel, const Plan& P) {
 }  // namespace
 
 namespace rg {
+void remember_shape(rg_ctx* c, const Plan& P) {
+    if (P.ilevel < 0) return;
+    if ((int)c->tuned.size() <= P.ilevel) c->tuned.resize((size_t)P.ilevel + 1);
+    c->tuned[(size_t)P.ilevel] = TunedShape{P.face_variant, P.face_batch, P.ncells, P.face_ms};
+}
+
 Plan* existing_plan(rg_ctx* c, int ilevel) {
     if (!c->have_topology || ilevel < 0 || ilevel >= (int)c->plans.size()) return nullptr;
     Plan& p = c->plans[ilevel];
@@ -219,8 +233,10 @@ void rg_destroy(rg_ctx* c) {
     cudaFree(c->d_prim);
     cudaFree(c->d_flux);
     cudaFree(c->d_mlp);
+    cudaFree(c->d_stage);
     cudaFree(c->d_status);
     if (c->h_status) cudaFreeHost(c->h_status);
+    if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
 }
@@ -238,6 +254,8 @@ int rg_set_params(rg_ctx* c, const rg_params* params) {
     c->params = *params;
     if (c->params.boxlen <= 0) c->params.boxlen = 1.0;
     // graphs bake the solver choice and constants in: drop them, keep the plans
+    // (and forget tuned shapes: another solver may prefer another one)
+    c->tuned.clear();
     for (auto& p : c->plans)
         if (p.graph) {
             cudaGraphExecDestroy(p.graph);
@@ -402,6 +420,25 @@ int rg_godunov_level(rg_ctx* c, int ilevel, double dt, double dx) {
     // time the face-kernel shapes on them (writes only the flux scratch)
     if (P->face_variant < 0 && ++P->substeps_run >= 1) return autotune_face(c, *P, step_consts(c));
     return RG_OK;
+}
+
+int rg_godunov_level_host(rg_ctx* c, int ilevel, double dt, double dx, const double* uold, double* unew) {
+    CTX_GUARD(c);
+    if (!uold || !unew) return set_error(c, RG_ERR_ARG, "uold and unew must be host arrays of nvar*ncell doubles");
+    if (int rc = check_learned(c)) return rc;
+    Plan* P;
+    if (int rc = get_plan(c, ilevel, &P)) return rc;
+    if (P->nbox > 0) return set_error(c, RG_ERR_STATE, "ensemble level: every box has its own dt, use rg_level_substep");
+    record_updates(c, ilevel, *P);
+    if (P->ncells == 0) return RG_OK;
+    if (int rc = ensure_flux(c, *P)) return rc;
+    if (int rc = upload_level_host(c, *P, uold, unew)) return rc;
+    if (int rc = launch_set_dt_host(c, dt, dx)) return rc;
+    if (int rc = launch_godunov(c, *P)) return rc;
+    if (P->face_variant < 0 && ++P->substeps_run >= 1)
+        if (int rc = autotune_face(c, *P, step_consts(c))) return rc;
+    if (int rc = download_level_host(c, *P, unew)) return rc;
+    return check_device_status(c);
 }
 
 int rg_courant_step(rg_ctx* c, int ilevel, double dx, double courant_factor, int pressure_cap, double* dt_out) {
@@ -651,6 +688,7 @@ int rg_set_face_config(rg_ctx* c, int ilevel, int variant, int batch) {
     if (int rc = get_plan(c, ilevel, &P)) return rc;
     P->face_variant = variant;
     P->face_batch = batch;
+    remember_shape(c, *P);
     if (P->graph) {
         cudaGraphExecDestroy(P->graph);
         P->graph = nullptr;

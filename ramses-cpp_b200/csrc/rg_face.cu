@@ -42,6 +42,8 @@ int autotune_face(rg_ctx* c, Plan& P, const StepK& K) {
     int bv = kDefaultFaceVariant, bb = 1;
     for (int v = 0; v < kNumFaceVariants; ++v) {
         for (int b : kBatches) {
+            if (v >= kFirstPipeVariant && b != 1) continue;  // round-robin tiles: no batch
+            if (P.nbox > 0 && !boxed_variant_distinct(v)) continue;
             float tmin = 1e30f;
             for (int rep = 0; rep < 3; ++rep) {
                 cudaEventRecord(e0, c->stream);
@@ -68,6 +70,7 @@ int autotune_face(rg_ctx* c, Plan& P, const StepK& K) {
     P.face_variant = bv;
     P.face_batch = bb;
     P.face_ms = best;
+    remember_shape(c, P);
     return check_cuda(c, cudaGetLastError(), "face autotune");
 }
 

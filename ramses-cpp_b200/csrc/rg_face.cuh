@@ -207,9 +207,9 @@ __device__ __forceinline__ int riemann(const double* ql, const double* qr, doubl
 
 // Face state of the neighbour across slot (idim, side), rotated.  Writes the
 // state the Riemann problem needs: the neighbour's right-face state (qm) for
-// side 0, its left-face state (qp) for side 1.  qside is the rotated primitive
-// state of neighbour cell n (the own trace's stencil cell on that side; only
-// read off level 0 outside the boundary branch).
+// side 0, its left-face state (qp) for side 1.  qside, if not null, is the
+// rotated primitive state of neighbour cell n already in registers (the own
+// trace's stencil cell on that side); otherwise it is loaded here.
 template <int NDIM>
 __device__ __forceinline__ void neighbour_face(const TreeView& T, const PlanView& P, const double* __restrict__ prim,
                                                const double* __restrict__ uold, size_t ncell, int p, int c, int idim,
@@ -256,8 +256,12 @@ __device__ __forceinline__ void neighbour_face(const TreeView& T, const PlanView
                 // the neighbour's state is the own trace's stencil cell on this
                 // side (qside, already loaded), and on a same-level face the
                 // neighbour's stencil cell towards this cell is the cell itself
-                double qnl[NV], qnr[NV];
+                double qnl[NV], qnr[NV], qload[NV];
                 const double* qn = qside;
+                if (!qn) {
+                    load_rot<NDIM>(prim, ncell, n, idim, qload);
+                    qn = qload;
+                }
                 if (side == 0 && nr == c) {
 #pragma unroll
                     for (int iv = 0; iv < NV; ++iv) qnr[iv] = qc[iv];
@@ -294,7 +298,7 @@ __device__ __forceinline__ void neighbour_face(const TreeView& T, const PlanView
 // the next launch (nothing ever waits on another block).
 constexpr int TILE = 32;
 
-template <int NDIM, int RS, int R, int MINB>
+template <int NDIM, int RS, int R, int MINB, bool BOXED>
 __global__ void __launch_bounds__(TILE * NDIM * R, MINB)
     k_face_tiles(TreeView T, PlanView P, const double* __restrict__ prim, const double* __restrict__ uold,
                  double* __restrict__ flux, double* __restrict__ fsum, DevStatus* st, StepK K, int batch) {
@@ -329,8 +333,8 @@ __global__ void __launch_bounds__(TILE * NDIM * R, MINB)
                     const int c = cell_of(T, P, p);
                     double dt = dt0;
                     DxDiv D = D0;
-                    if (P.obox) step_of_box(P, p, dt, D);
-                    double qc[NV], qmo[NV], qpo[NV], ql[NV], qr[NV];
+                    if constexpr (BOXED) step_of_box(P, p, dt, D);
+                    double qc[NV], qmo[NV], qpo[NV];
                     load_rot<NDIM>(prim, ncell, c, idim, qc);
                     if (P.level0) {
                         double qn[NV], dq0[NV];
@@ -342,6 +346,7 @@ __global__ void __launch_bounds__(TILE * NDIM * R, MINB)
                         rot_swap<NDIM>(qpo, idim);
                     } else {
                         const int l = P.icn[(size_t)s0 * nc + p], rr = P.icn[(size_t)(s0 + 1) * nc + p];
+                        double ql[NV], qr[NV];
                         load_nb_rot<NDIM>(T, prim, ncell, l, idim, qc, ql);
                         load_nb_rot<NDIM>(T, prim, ncell, rr, idim, qc, qr);
                         own_trace<NDIM>(qc, ql, qr, dt, D, K, qmo, qpo);
@@ -357,8 +362,8 @@ __global__ void __launch_bounds__(TILE * NDIM * R, MINB)
                         } else {
                             const int n = P.icn[(size_t)s * nc + p];
                             double qf[NV];
-                            neighbour_face<NDIM>(T, P, prim, uold, ncell, p, c, idim, side, kd, n, qc,
-                                                 side ? qr : ql, dt, D, K, qf);
+                            neighbour_face<NDIM>(T, P, prim, uold, ncell, p, c, idim, side, kd, n, qc, nullptr,
+                                                 dt, D, K, qf);
                             if (side == 0) iters += riemann<NDIM, RS>(qf, qpo, f, K);
                             else iters += riemann<NDIM, RS>(qmo, qf, f, K);
                             ++calls;
@@ -418,11 +423,18 @@ __global__ void __launch_bounds__(TILE * NDIM * R, MINB)
 constexpr int kFirstPipeVariant = 7;
 constexpr int kNumFaceVariants = 9;
 constexpr int kDefaultFaceVariant = 1;
+// Ensemble levels (per-box dt and dx read per cell) instantiate only the
+// default tiled shape, this one, and the first pipelined variant; every other
+// id runs the default shape there.
+constexpr int kBoxedAltVariant = 4;
+inline bool boxed_variant_distinct(int v) {
+    return v == kDefaultFaceVariant || v == kBoxedAltVariant || v == kFirstPipeVariant;
+}
 
-template <int NDIM, int RS, int R, int MINB>
+template <int NDIM, int RS, int R, int MINB, bool BOXED = false>
 int launch_face_one(rg_ctx* c, const Plan& P, const StepK& K, int batch, const double* uold, const double* prim,
                     double* flux, double* fsum) {
-    auto kern = k_face_tiles<NDIM, RS, R, MINB>;
+    auto kern = k_face_tiles<NDIM, RS, R, MINB, BOXED>;
     const int block = TILE * NDIM * R;
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, 0);
@@ -439,6 +451,11 @@ int launch_face_one(rg_ctx* c, const Plan& P, const StepK& K, int batch, const d
 template <int NDIM, int RS>
 int launch_face_rs(rg_ctx* c, const Plan& P, const StepK& K, int variant, int batch, const double* uold,
                    const double* prim, double* flux, double* fsum) {
+    if (P.nbox > 0) {
+        // ensemble levels (per-box dt and dx): two shapes are instantiated
+        if (variant == kBoxedAltVariant) return launch_face_one<NDIM, RS, 2, 4, true>(c, P, K, batch, uold, prim, flux, fsum);
+        return launch_face_one<NDIM, RS, 1, 8, true>(c, P, K, batch, uold, prim, flux, fsum);
+    }
 #define RG_FACE_CASE(id, r, mb) \
     case id: return launch_face_one<NDIM, RS, r, mb>(c, P, K, batch, uold, prim, flux, fsum);
     switch (variant) {

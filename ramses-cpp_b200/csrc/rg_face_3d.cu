@@ -9,6 +9,7 @@ namespace {
 template <int RS>
 int launch_pipe_rs(rg_ctx* c, const Plan& P, const StepK& K, int variant, const double* prim, double* flux,
                    double* fsum) {
+    if (P.nbox > 0) return launch_face_pipe<3, RS, 4, true>(c, P, K, prim, flux, fsum);
     if (variant == kFirstPipeVariant) return launch_face_pipe<3, RS, 4>(c, P, K, prim, flux, fsum);
     return launch_face_pipe<3, RS, 3>(c, P, K, prim, flux, fsum);
 }

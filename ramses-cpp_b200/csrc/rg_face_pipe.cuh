@@ -110,7 +110,7 @@ __device__ __forceinline__ void pipe_state(const TreeView& T, const double* B, i
     if (ib > 0 && ib <= T.nbound_type && T.bound_type[ib - 1] == 1) q[1] *= -1.0;
 }
 
-template <int NDIM, int RS, int MINB>
+template <int NDIM, int RS, int MINB, bool BOXED>
 __global__ void __launch_bounds__(TILE * NDIM, MINB)
     k_face_pipe(TreeView T, PlanView P, const double* __restrict__ prim, double* __restrict__ flux,
                 double* __restrict__ fsum, DevStatus* st, StepK K) {
@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(TILE * NDIM, MINB)
             const int c = I0.c;
             double dt = dt0;
             DxDiv D = D0;
-            if (P.obox) step_of_box(P, p, dt, D);
+            if constexpr (BOXED) step_of_box(P, p, dt, D);
             double qc[NV], ql[NV], qr[NV], qmo[NV], qpo[NV];
             pipe_state<NDIM>(T, B, lane, 0, c, idim, nullptr, qc);
             pipe_state<NDIM>(T, B, lane, 1, I0.l, idim, qc, ql);
@@ -241,9 +241,9 @@ __global__ void __launch_bounds__(TILE * NDIM, MINB)
     }
 }
 
-template <int NDIM, int RS, int MINB>
+template <int NDIM, int RS, int MINB, bool BOXED = false>
 int launch_face_pipe(rg_ctx* c, const Plan& P, const StepK& K, const double* prim, double* flux, double* fsum) {
-    auto kern = k_face_pipe<NDIM, RS, MINB>;
+    auto kern = k_face_pipe<NDIM, RS, MINB, BOXED>;
     const int block = TILE * NDIM;
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, 0);

@@ -1,0 +1,169 @@
+// rg_host_level.cu -- level-sparse host <-> device state transfer for
+// callers whose state lives in host memory between level steps.
+//
+// In a RAMSES-CPP run the tree maintenance (TreeUpdater) and Simulation read
+// and write AmrGrid's host uold/unew between hydro calls, so a drop-in hydro
+// solver must take its inputs from, and return its outputs to, host memory
+// on every godunov_fine call (HydroSolver.cpp:18-573).  The step of level L
+// reads uold only at the level's cells and at the cells outside the level
+// that its stencils reach (the plan's extra primitive cells), reads unew only
+// at its update targets (the level's cells and the coarser cells that
+// receive refluxes), and writes unew only at those targets.  So instead of
+// the whole state (2 x nvar x ncell doubles up, nvar x ncell down) a call
+// moves exactly those cells: gathered on the host into pinned staging, one
+// copy each way, scattered on the device.
+#include <algorithm>
+#include <vector>
+
+#include "rg_internal.cuh"
+
+namespace rg {
+
+namespace {
+
+__device__ __forceinline__ int plan_cell(const TreeView& T, const PlanView& P, int p) {
+    if (P.level0) return p + 1;
+    int icx = p / P.noct, k = p - icx * P.noct;
+    return T.ncoarse + icx * T.ngridmax + P.octs[k];
+}
+
+// read ids: level cells then extra primitive cells; target ids: level cells
+// then extra targets
+__global__ void k_level_ids(TreeView T, PlanView P, int* read_ids, int* targ_ids) {
+    const int nread = P.ncells + P.nextra_prim;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nread || t < P.ntarg; t += gridDim.x * blockDim.x) {
+        const int lvl = t < P.ncells ? plan_cell(T, P, t) : 0;
+        if (t < nread) read_ids[t] = t < P.ncells ? lvl : P.xprim[t - P.ncells];
+        if (t < P.ntarg) targ_ids[t] = t < P.ncells ? lvl : P.textra[t - P.ncells];
+    }
+}
+
+// staging layout: [nvar][nread] uold values, then [nvar][ntarg] unew values
+__global__ void k_scatter_level(const int* __restrict__ read_ids, int nread, const int* __restrict__ targ_ids,
+                                int ntarg, int nvar, size_t ncell, const double* __restrict__ stage, double* uold,
+                                double* unew) {
+    const double* sn = stage + (size_t)nvar * nread;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nread || t < ntarg; t += gridDim.x * blockDim.x) {
+        if (t < nread) {
+            const size_t id = (size_t)read_ids[t] - 1;
+            for (int iv = 0; iv < nvar; ++iv) uold[iv * ncell + id] = stage[(size_t)iv * nread + t];
+        }
+        if (t < ntarg) {
+            const size_t id = (size_t)targ_ids[t] - 1;
+            for (int iv = 0; iv < nvar; ++iv) unew[iv * ncell + id] = sn[(size_t)iv * ntarg + t];
+        }
+    }
+}
+
+__global__ void k_gather_targets(const int* __restrict__ targ_ids, int ntarg, int nvar, size_t ncell,
+                                  const double* __restrict__ unew, double* stage) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntarg; t += gridDim.x * blockDim.x) {
+        const size_t id = (size_t)targ_ids[t] - 1;
+        for (int iv = 0; iv < nvar; ++iv) stage[(size_t)iv * ntarg + t] = unew[iv * ncell + id];
+    }
+}
+
+int blocks(rg_ctx* c, long long n) {
+    long long b = (n + 255) / 256, cap = (long long)c->sm_count * 16;
+    return (int)std::max(1LL, std::min(b, cap));
+}
+
+int grow_stage(rg_ctx* c, size_t doubles) {
+    if (c->cap_hstage < doubles) {
+        if (c->h_stage) cudaFreeHost(c->h_stage);
+        c->h_stage = nullptr;
+        c->cap_hstage = 0;
+        if (int rc = check_cuda(c, cudaMallocHost(&c->h_stage, doubles * sizeof(double)), "pinned level staging"))
+            return rc;
+        c->cap_hstage = doubles;
+    }
+    if (c->cap_dstage < doubles) {
+        cudaFree(c->d_stage);
+        c->d_stage = nullptr;
+        c->cap_dstage = 0;
+        if (int rc = check_cuda(c, cudaMalloc(&c->d_stage, doubles * sizeof(double)), "device level staging"))
+            return rc;
+        c->cap_dstage = doubles;
+    }
+    return RG_OK;
+}
+
+}  // namespace
+
+// Host and device copies of the plan's read and target cell ids (built once
+// per plan; synchronises the stream).
+int level_ids(rg_ctx* c, Plan& P) {
+    if (P.ids_ready) return RG_OK;
+    const int nread = P.ncells + P.nextra_prim;
+    cudaFree(P.read_ids);
+    P.read_ids = nullptr;
+    if (int rc = check_cuda(c, cudaMalloc(&P.read_ids, sizeof(int) * ((size_t)nread + P.ntarg + 1)), "level ids"))
+        return rc;
+    P.targ_ids = P.read_ids + nread;
+    k_level_ids<<<blocks(c, std::max(nread, P.ntarg)), 256, 0, c->stream>>>(tree_view(c), P.view(), P.read_ids,
+                                                                          P.targ_ids);
+    P.h_read.resize((size_t)nread);
+    P.h_targ.resize((size_t)P.ntarg);
+    if (nread && check_cuda(c, cudaMemcpyAsync(P.h_read.data(), P.read_ids, sizeof(int) * nread,
+                                               cudaMemcpyDeviceToHost, c->stream),
+                            "level ids copy"))
+        return RG_ERR_CUDA;
+    if (P.ntarg && check_cuda(c, cudaMemcpyAsync(P.h_targ.data(), P.targ_ids, sizeof(int) * P.ntarg,
+                                                 cudaMemcpyDeviceToHost, c->stream),
+                              "level ids copy"))
+        return RG_ERR_CUDA;
+    if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "level ids sync")) return rc;
+    P.ids_ready = true;
+    return RG_OK;
+}
+
+int upload_level_host(rg_ctx* c, Plan& P, const double* uold, const double* unew) {
+    if (int rc = level_ids(c, P)) return rc;
+    const int nv = c->nvar, nread = (int)P.h_read.size(), ntarg = (int)P.h_targ.size();
+    const size_t ncell = (size_t)c->ncell;
+    const size_t n = (size_t)nv * ((size_t)nread + ntarg);
+    if (n == 0) return RG_OK;
+    if (int rc = grow_stage(c, n)) return rc;
+    // the previous call's download has completed (it synchronised), so the
+    // pinned buffer is free to refill
+    double* s = c->h_stage;
+    for (int iv = 0; iv < nv; ++iv) {
+        const double* src = uold + (size_t)iv * ncell;
+        double* dst = s + (size_t)iv * nread;
+        for (int t = 0; t < nread; ++t) dst[t] = src[P.h_read[(size_t)t] - 1];
+    }
+    double* sn = s + (size_t)nv * nread;
+    for (int iv = 0; iv < nv; ++iv) {
+        const double* src = unew + (size_t)iv * ncell;
+        double* dst = sn + (size_t)iv * ntarg;
+        for (int t = 0; t < ntarg; ++t) dst[t] = src[P.h_targ[(size_t)t] - 1];
+    }
+    if (int rc = check_cuda(c, cudaMemcpyAsync(c->d_stage, s, n * sizeof(double), cudaMemcpyHostToDevice, c->stream),
+                            "level upload"))
+        return rc;
+    k_scatter_level<<<blocks(c, std::max(nread, ntarg)), 256, 0, c->stream>>>(
+        P.read_ids, nread, P.targ_ids, ntarg, nv, ncell, c->d_stage, c->d_uold, c->d_unew);
+    return check_cuda(c, cudaGetLastError(), "level scatter");
+}
+
+int download_level_host(rg_ctx* c, Plan& P, double* unew) {
+    const int nv = c->nvar, ntarg = (int)P.h_targ.size();
+    const size_t ncell = (size_t)c->ncell;
+    const size_t n = (size_t)nv * ntarg;
+    if (n == 0) return check_cuda(c, cudaStreamSynchronize(c->stream), "level download sync");
+    if (int rc = grow_stage(c, n)) return rc;
+    k_gather_targets<<<blocks(c, ntarg), 256, 0, c->stream>>>(P.targ_ids, ntarg, nv, ncell, c->d_unew, c->d_stage);
+    if (int rc = check_cuda(c, cudaMemcpyAsync(c->h_stage, c->d_stage, n * sizeof(double), cudaMemcpyDeviceToHost,
+                                               c->stream),
+                            "level download"))
+        return rc;
+    if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "level download sync")) return rc;
+    for (int iv = 0; iv < nv; ++iv) {
+        double* dst = unew + (size_t)iv * ncell;
+        const double* src = c->h_stage + (size_t)iv * ntarg;
+        for (int t = 0; t < ntarg; ++t) dst[P.h_targ[(size_t)t] - 1] = src[t];
+    }
+    return RG_OK;
+}
+
+}  // namespace rg

@@ -104,6 +104,10 @@ struct Plan {
     int face_variant = -1, face_batch = 4;  // autotuned face-kernel shape (-1: not tuned yet)
     float face_ms = 0.f;
     int substeps_run = 0;
+    bool ids_ready = false;    // level-sparse host transfer: cell ids read / written
+    int* read_ids = nullptr;   // [ncells + nextra_prim] then targ_ids [ntarg] (one allocation)
+    int* targ_ids = nullptr;
+    std::vector<int> h_read, h_targ;
     int nbox = 0;              // ensemble level: number of boxes (0: one grid)
     int* obox = nullptr;       // [noct]
     BoxStep* boxes = nullptr;  // [nbox]
@@ -111,6 +115,14 @@ struct Plan {
         return PlanView{ilevel, level0, noct, ncells, ntarg, nextra_prim, octs, icn, stc, kind, toff, tev, textra,
                         xprim, obox, boxes};
     }
+};
+
+// Face-kernel shape chosen for a level, kept across plan rebuilds (an AMR run
+// rebuilds its plans whenever the tree changes) and reused while the level's
+// cell count stays within a factor two of the one it was tuned on.
+struct TunedShape {
+    int variant = -1, batch = 1, ncells = 0;
+    float ms = 0.f;
 };
 
 struct Tuning {
@@ -157,11 +169,16 @@ struct rg_ctx {
     rg::DevStatus* h_status = nullptr;  // pinned mirror
 
     std::vector<rg::Plan> plans;
+    std::vector<rg::TunedShape> tuned;  // per level
     rg::Tuning tuning;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     float last_ms[3] = {0, 0, 0};
     bool timing = false;
     bool no_autotune = false;
+    double* h_stage = nullptr;  // pinned staging of level-sparse host transfers
+    size_t cap_hstage = 0;
+    double* d_stage = nullptr;
+    size_t cap_dstage = 0;
     float* d_mlp = nullptr;  // learned Newton start: parameters + Adam state
     bool mlp_valid = false;
     std::vector<long long> cell_updates;
@@ -187,6 +204,9 @@ int launch_godunov(rg_ctx* c, const Plan& p);
 int launch_leaf_substep(rg_ctx* c, const Plan& p, double dx, int pressure_cap, double courant_factor);
 int launch_godunov_ext(rg_ctx* c, const Plan& p, const double* uold, double* unew, double* prim, double* flux);
 TreeView tree_view(const rg_ctx* c);
+void remember_shape(rg_ctx* c, const Plan& P);
+int upload_level_host(rg_ctx* c, Plan& P, const double* uold, const double* unew);
+int download_level_host(rg_ctx* c, Plan& P, double* unew);
 int mlp_ensure(rg_ctx* c);
 int mlp_train(rg_ctx* c, int nsamples, int epochs, int batch, float lr, unsigned long long seed, float* loss_out);
 int mlp_grad(rg_ctx* c, int n, const float* x_host, const float* t_host, float* grad_host, float* loss_host);

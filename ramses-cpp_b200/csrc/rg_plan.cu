@@ -364,6 +364,7 @@ void free_plan(Plan& p) {
     cudaFree(p.xprim);
     cudaFree(p.obox);
     cudaFree(p.boxes);
+    cudaFree(p.read_ids);
     p = Plan();
 }
 

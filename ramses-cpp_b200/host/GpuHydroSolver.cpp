@@ -11,9 +11,10 @@
 // State ownership: AmrGrid keeps owning the host vectors.  The tree
 // maintenance (TreeUpdater) and the rest of Simulation read and write
 // grid_.uold/unew between hydro calls, so godunov_fine uploads the state it
-// reads, runs the step on the device and writes the updated unew back; the
-// tree arrays are re-sent only when they changed (compared with the copy sent
-// last time).  set_unew/set_uold stay plain host copies here: they are memory
+// reads -- only the level's cells, the stencil cells around it and the update
+// targets (rg_godunov_level_host) -- runs the step on the device and writes
+// the updated targets back; the tree arrays are re-sent only when they
+// changed (compared with the copy sent last time).  set_unew/set_uold stay plain host copies here: they are memory
 // copies the host has to see anyway.  Unsupported configurations (non-thermal
 // energies, passive scalars, barotropic EOS, boundary patches) throw: there is
 // no silent CPU fallback.
@@ -40,9 +41,8 @@ public:
     void godunov_fine(int ilevel, real_t dt, real_t dx) override {
         ensure_context();
         sync_topology();
-        check(rg_upload_state(ctx_, grid_.uold_vec.data(), grid_.unew_vec.data()), "rg_upload_state");
-        check(rg_godunov_level(ctx_, ilevel, dt, dx), "rg_godunov_level");
-        check(rg_download_state(ctx_, nullptr, grid_.unew_vec.data()), "rg_download_state");
+        check(rg_godunov_level_host(ctx_, ilevel, dt, dx, grid_.uold_vec.data(), grid_.unew_vec.data()),
+              "rg_godunov_level_host");
     }
 
 private:

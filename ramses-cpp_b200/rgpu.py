@@ -111,6 +111,8 @@ def lib():
     L.rg_face_config.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float)]
     L.rg_godunov_level_noalloc.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p]
     L.rg_get_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+    L.rg_godunov_level_host.argtypes = [VP, C.c_int, C.c_double, C.c_double, C.POINTER(C.c_double),
+                                        C.POINTER(C.c_double)]
     L.rg_set_level_boxes.argtypes = [VP, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]
     L.rg_level_box_dt.argtypes = [VP, C.c_int, C.POINTER(C.c_double), C.c_int]
     _lib = L
@@ -184,6 +186,15 @@ class Context:
 
     def godunov_level(self, il, dt, dx):
         self._chk(self.L.rg_godunov_level(self.h, il, dt, dx))
+
+    def godunov_level_host(self, il, dt, dx, uold, unew):
+        """Level step on host arrays: unew (float64, C-contiguous) is updated in place
+        at the step's targets only."""
+        if uold.dtype != np.float64 or unew.dtype != np.float64 or not unew.flags.c_contiguous:
+            raise ValueError("uold/unew must be contiguous float64 arrays")
+        uo = np.ascontiguousarray(uold)
+        self._chk(self.L.rg_godunov_level_host(self.h, il, dt, dx, uo.ctypes.data_as(C.POINTER(C.c_double)),
+                                               unew.ctypes.data_as(C.POINTER(C.c_double))))
 
     def godunov_level_noalloc(self, il, dt, dx, uold_dev_ptr, unew_dev_ptr):
         """Allocation-free level step on caller-owned device buffers (raw addresses)."""

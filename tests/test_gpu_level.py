@@ -127,6 +127,27 @@ def test_golden_amr_calls(ctx_factory, golden, fixture, variant):
         assert bits_equal(got, d[f"{k}_unew_out"]), f"{fixture} {k}: {np.count_nonzero(got != d[f'{k}_unew_out'])}"
 
 
+@pytest.mark.parametrize("fixture", ["amr3d", "amr1d"])
+def test_golden_amr_calls_host_sparse(ctx_factory, golden, fixture):
+    """rg_godunov_level_host on host arrays: moves only the cells the step reads
+    and writes, gives the reference's bits at the targets and leaves every other
+    host value as it was."""
+    d = golden(fixture)
+    ndim, slope, riem = (int(x) for x in d["params"])
+    params = make_params(ndim, slope_type=slope, riemann=RIEMANN_NAMES[riem])
+    ctx = ctx_factory(params)
+    for k in sorted({k.split("_")[0] for k in d.files if k.startswith("L")}):
+        ncoarse, ngm, ncell, nvar, nx, ny, nz, nlevelmax, il = (int(x) for x in d[f"{k}_meta"])
+        g = GridArrays(ncoarse=ncoarse, ngridmax=ngm, ncell=ncell, nvar=nvar, nx=nx, ny=ny, nz=nz, ncpu=1,
+                       nboundary=0, nlevelmax=nlevelmax, son=d[f"{k}_son"], father=d[f"{k}_father"],
+                       nbor=d[f"{k}_nbor"], next=d[f"{k}_next"], headl=d[f"{k}_headl"])
+        ctx.sync_topology(g)
+        dt, dx = (float(x) for x in d[f"{k}_dtdx"])
+        unew = np.array(d[f"{k}_unew_in"], dtype=np.float64)
+        ctx.godunov_level_host(il, dt, dx, np.array(d[f"{k}_uold"], dtype=np.float64), unew)
+        assert bits_equal(unew, d[f"{k}_unew_out"]), f"{fixture} {k}: {np.count_nonzero(unew != d[f'{k}_unew_out'])}"
+
+
 def test_level_index_matches_oracle(ctx_factory, oracle, golden):
     """Oct order (level linked list) and neighbour cells (get_nbor_cells): exact."""
     d = golden("amr3d")
