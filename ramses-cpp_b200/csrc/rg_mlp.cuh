@@ -136,12 +136,25 @@ __device__ __forceinline__ float mlp_forward_std(const float* __restrict__ w, co
     return y;
 }
 
+// Features, network and gate: out of line, so the face kernels that inline
+// the exact solver carry the network's 64-wide hidden layer only in the
+// frame of this call, not in their own register allocation.
+template <int NDIM>
+__device__ __noinline__ double mlp_guess_eval(const float* __restrict__ w, const double* ql, const double* qr,
+                                              double gamma, double smallp);
+
 // Learned Newton start: pref * exp(prediction), or -1 (use the two-shock
 // guess) when the network is absent or its output is not usable.
 template <int NDIM>
 __device__ __forceinline__ double mlp_guess(const float* __restrict__ w, const double* ql, const double* qr,
                                             double gamma, double smallp) {
     if (!w) return -1.0;
+    return mlp_guess_eval<NDIM>(w, ql, qr, gamma, smallp);
+}
+
+template <int NDIM>
+__device__ __noinline__ double mlp_guess_eval(const float* __restrict__ w, const double* ql, const double* qr,
+                                              double gamma, double smallp) {
     {
         constexpr int IP = Dims<NDIM>::IP;
         double rl = smax(ql[0], 1e-10), pl = smax(ql[IP], rl * smallp);

@@ -372,8 +372,11 @@ __device__ __forceinline__ int solve_exact_p(const double* ql, const double* qr,
         double wwr_sq = cr_sq * (1.0 + gamma6 * (pold - pr) / (pr + 1e-20));
         double wwl = sqrt(smax(wwl_sq, 0.0));
         double wwr = sqrt(smax(wwr_sq, 0.0));
-        double ql_nr = (2.0 * pow(wwl, 3.0)) / (wwl * wwl + cl_sq + 1e-20);
-        double qr_nr = (2.0 * pow(wwr, 3.0)) / (wwr * wwr + cr_sq + 1e-20);
+        // std::pow(w, 3.0) in the reference (RiemannSolver.cpp:226): the cube
+        // by two products is as close to glibc's result (a few ulp at most)
+        // as CUDA's general pow, at a fraction of its cost
+        double ql_nr = (2.0 * (wwl * wwl * wwl)) / (wwl * wwl + cl_sq + 1e-20);
+        double qr_nr = (2.0 * (wwr * wwr * wwr)) / (wwr * wwr + cr_sq + 1e-20);
         double usl = ul - (pold - pl) / (wwl + 1e-20);
         double usr = ur + (pold - pr) / (wwr + 1e-20);
         double delp = (qr_nr * ql_nr / (qr_nr + ql_nr + 1e-20)) * (usl - usr);
