@@ -272,8 +272,10 @@ int rg_level_box_dt(rg_ctx* ctx, int ilevel, double* dt_out, int nbox);
 
 /* Shape chosen for a level: variant index, batch, and its timed ms. */
 int rg_face_config(rg_ctx* ctx, int ilevel, int* variant, int* batch, float* ms);
-/* Pin the face-kernel shape of a level (variant 0..8, batch >= 1; 7 and 8
- * select the software-pipelined kernel on levels above level 0 in 2D/3D). */
+/* Pin the face-kernel shape of a level (variant 0..10, batch >= 1; 7 and 8
+ * select the software-pipelined kernel on levels above level 0 in 2D/3D,
+ * 9 and 10 the brick kernel on levels that form one complete periodic
+ * lattice; elsewhere those ids run the default shape). */
 int rg_set_face_config(rg_ctx* ctx, int ilevel, int variant, int batch);
 
 #ifdef __cplusplus

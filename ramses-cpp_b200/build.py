@@ -24,7 +24,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC,-O2",
                 "--expt-relaxed-constexpr", f"-I{ROOT / 'include'}"]
 SOURCES = ["rg_api.cu", "rg_plan.cu", "rg_step.cu", "rg_face.cu", "rg_face_1d.cu", "rg_face_3d.cu",
-           "rg_noalloc.cu", "rg_exact.cu", "rg_mlp.cu", "rg_host_level.cu"]
+           "rg_noalloc.cu", "rg_exact.cu", "rg_mlp.cu", "rg_host_level.cu",
+           "rg_lattice.cu"]
 
 
 def _newer(target: Path, deps) -> bool:

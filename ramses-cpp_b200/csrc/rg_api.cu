@@ -127,6 +127,10 @@ int get_plan(rg_ctx* c, int ilevel, Plan** out) {
             free_plan(p);
             return rc;
         }
+        if (int rc = build_lattice(c, p)) {
+            free_plan(p);
+            return rc;
+        }
         if ((int)c->tuned.size() > ilevel) {
             const TunedShape& t = c->tuned[ilevel];
             if (t.variant >= 0 && p.ncells <= 2LL * t.ncells && 2LL * p.ncells >= t.ncells) {
@@ -683,7 +687,7 @@ int rg_face_config(rg_ctx* c, int ilevel, int* variant, int* batch, float* ms) {
 int rg_set_face_config(rg_ctx* c, int ilevel, int variant, int batch) {
     CTX_GUARD(c);
     if (variant < 0 || variant >= kNumFaceVariants || batch < 1)
-        return set_error(c, RG_ERR_ARG, "variant must be in [0, 9), batch >= 1");
+        return set_error(c, RG_ERR_ARG, "variant must be in [0, 11), batch >= 1");
     Plan* P;
     if (int rc = get_plan(c, ilevel, &P)) return rc;
     P->face_variant = variant;

@@ -42,7 +42,8 @@ int autotune_face(rg_ctx* c, Plan& P, const StepK& K) {
     int bv = kDefaultFaceVariant, bb = 1;
     for (int v = 0; v < kNumFaceVariants; ++v) {
         for (int b : kBatches) {
-            if (v >= kFirstPipeVariant && b != 1) continue;  // round-robin tiles: no batch
+            if (v >= kFirstPipeVariant && b != 1) continue;  // round-robin tiles / bricks: no batch
+            if (v >= kFirstBrickVariant && !(P.lattice && P.nbox == 0)) continue;
             if (P.nbox > 0 && !boxed_variant_distinct(v)) continue;
             float tmin = 1e30f;
             for (int rep = 0; rep < 3; ++rep) {

@@ -104,6 +104,11 @@ struct Plan {
     int face_variant = -1, face_batch = 4;  // autotuned face-kernel shape (-1: not tuned yet)
     float face_ms = 0.f;
     int substeps_run = 0;
+    int lattice = 0;           // the level is one complete periodic lattice (rg_lattice.cu)
+    int lat_e[3] = {0, 0, 0};  // its extent
+    int lat_kind = 0;          // the (single) interface kind of its faces
+    int* lat_id = nullptr;     // [ex*ey*ez] cell id of each lattice site (x fastest)
+    int* lat_p = nullptr;      // [ex*ey*ez] plan position of each site
     bool ids_ready = false;    // level-sparse host transfer: cell ids read / written
     int* read_ids = nullptr;   // [ncells + nextra_prim] then targ_ids [ntarg] (one allocation)
     int* targ_ids = nullptr;
@@ -205,6 +210,7 @@ int launch_leaf_substep(rg_ctx* c, const Plan& p, double dx, int pressure_cap, d
 int launch_godunov_ext(rg_ctx* c, const Plan& p, const double* uold, double* unew, double* prim, double* flux);
 TreeView tree_view(const rg_ctx* c);
 void remember_shape(rg_ctx* c, const Plan& P);
+int build_lattice(rg_ctx* c, Plan& P);
 int upload_level_host(rg_ctx* c, Plan& P, const double* uold, const double* unew);
 int download_level_host(rg_ctx* c, Plan& P, double* unew);
 int mlp_ensure(rg_ctx* c);

@@ -365,6 +365,8 @@ void free_plan(Plan& p) {
     cudaFree(p.obox);
     cudaFree(p.boxes);
     cudaFree(p.read_ids);
+    cudaFree(p.lat_id);
+    cudaFree(p.lat_p);
     p = Plan();
 }
 

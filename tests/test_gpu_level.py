@@ -276,7 +276,7 @@ def test_topology_errors_are_reported(ctx_factory):
     ctx.synchronize()
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("variant", list(range(11)))
 def test_every_face_kernel_shape_is_bit_identical(ctx_factory, oracle, variant):
     """The autotuner may pick any shape: each must give the oracle's bits."""
     L = 5
@@ -309,7 +309,7 @@ def test_autotuner_picks_a_shape_and_exact_stats_count(ctx_factory):
     dx = 1.0 / 2 ** L
     ctx.level_substep(L, dx, use_graph=True)  # eager first substep + autotune
     v, b, ms = ctx.face_config(L)
-    assert 0 <= v <= 8 and b >= 1 and ms > 0
+    assert 0 <= v <= 10 and b >= 1 and ms > 0
     ctx.exact_stats(reset=True)
     ctx.level_substep(L, dx, use_graph=True)
     ctx.synchronize()
