@@ -56,9 +56,9 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
+def profile_traffic(kernel):
     """dram bytes per launch of the face kernel from the committed ncu summary."""
-    f = ROOT / "profiles" / "k_face_sedov128.md"
+    f = ROOT / "profiles" / f"{kernel}_sedov128.md"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
@@ -270,6 +270,10 @@ def gpu_arm(args, rank, world, local_rank):
         sampler.stop()
     value = world * cells * args.steps / (ms / 1e3)
 
+    # the face-kernel shape the autotuner kept for this level
+    variant = ctx.face_config(L)[0]
+    face_kernel = "k_face_brick" if variant >= 9 else ("k_face_pipe" if variant >= 7 else "k_face_tiles")
+
     # per-kernel device time (events around prim / face / fold, same stream)
     ctx.set_timing(True)
     nk = min(args.steps, 40)
@@ -320,7 +324,7 @@ def gpu_arm(args, rank, world, local_rank):
                    "l2": "inputs larger than L2: uold+unew 192 MB, primitives 96 MB, flux scratch 503 MB per step",
                    "parallelism": "replicas" if world > 1 else "single GPU", "cuda_graph": True},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": profile_traffic(), "kernel": "k_face_tiles",
+                     "traffic": profile_traffic(face_kernel), "kernel": face_kernel, "variant": variant,
                      "algorithmic_bytes_per_launch": alg_bytes, "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
                      "step_hbm_frac": (BYTES_PER_CELL_UPDATE * value / world / 1e9) / peak},
         "kernel_ms": {"prim": kms[0], "face": kms[1], "fold": kms[2]},
