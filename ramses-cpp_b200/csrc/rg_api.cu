@@ -133,7 +133,7 @@ int get_plan(rg_ctx* c, int ilevel, Plan** out) {
         }
         if ((int)c->tuned.size() > ilevel) {
             const TunedShape& t = c->tuned[ilevel];
-            if (t.variant >= 0 && p.ncells <= 2LL * t.ncells && 2LL * p.ncells >= t.ncells) {
+            if (t.variant >= 0 && p.ncells <= 8LL * t.ncells && 8LL * p.ncells >= t.ncells) {
                 p.face_variant = t.variant;
                 p.face_batch = t.batch;
                 p.face_ms = t.ms;

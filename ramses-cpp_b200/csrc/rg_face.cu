@@ -27,12 +27,15 @@ int launch_face_tiles(rg_ctx* c, const Plan& P, const StepK& K, const double* uo
 
 // Times every (variant, batch) on the level's current data (the face kernel
 // only writes the flux scratch, so repeating it changes no state) and keeps
-// the fastest.  Small levels keep the default.  Must run outside a capture.
+// the fastest.  Levels below 2^17 cells keep the default.  Must run outside a
+// capture.
 int autotune_face(rg_ctx* c, Plan& P, const StepK& K) {
     if (P.face_variant >= 0) return RG_OK;
     P.face_variant = kDefaultFaceVariant;
     P.face_batch = 1;
-    if (P.ncells < (1 << 14) || c->no_autotune) return RG_OK;
+    // small levels keep the default: timing 75 launches would cost more than
+    // any shape can save, and AMR rebuilds its small levels every coarse step
+    if (P.ncells < (1 << 17) || c->no_autotune) return RG_OK;
     const int ns = 2 * c->params.ndim, nv = c->params.ndim + 2;
     double* fsum = c->d_flux + (size_t)ns * nv * P.ncells;
     cudaEvent_t e0, e1;

@@ -124,7 +124,7 @@ struct Plan {
 
 // Face-kernel shape chosen for a level, kept across plan rebuilds (an AMR run
 // rebuilds its plans whenever the tree changes) and reused while the level's
-// cell count stays within a factor two of the one it was tuned on.
+// cell count stays within a factor eight of the one it was tuned on.
 struct TunedShape {
     int variant = -1, batch = 1, ncells = 0;
     float ms = 0.f;
