@@ -451,6 +451,7 @@ def ensemble_report(rank, world, local_rank, steps):
     ctx.sync_topology(f.grid)
     ctx.upload_state(u0, u0)
     ctx.set_level_boxes(f.level, f.first_oct, f.dx)
+    ctx.set_level_lattices(f.level, *f.lattices())
     for _ in range(3):
         ctx.level_substep(f.level, 0.0, pressure_cap=False, use_graph=True)
     ctx.synchronize()

@@ -266,6 +266,15 @@ int rg_set_autotune(rg_ctx* ctx, int on);
  * rg_godunov_level, rg_courant_step and the allocation-free entry point
  * refuse a level with boxes (they take one dt for the whole level). */
 int rg_set_level_boxes(rg_ctx* ctx, int ilevel, int nbox, const int* first_oct, const double* dx);
+/* Optional, after rg_set_level_boxes: each box is one periodic lattice of
+ * extent[3b..3b+2] cells (multiples of 8); lat_id / lat_p give, for every
+ * site of every box (box after box, x fastest), its cell id and its position
+ * p = (ic-1)*noct + k in the level (k = position of its oct in the level
+ * list).  The library checks every site against the level's neighbours,
+ * ghost stencils and interface kinds before it uses the brick face kernel on
+ * the boxes; a mismatch returns RG_ERR_ARG and changes nothing. */
+int rg_set_level_lattices(rg_ctx* ctx, int ilevel, int nbox, const int* extent, const int* lat_id,
+                          const int* lat_p);
 /* dt of every box in the last substep (nbox must equal the level's count);
  * rg_level_substep's dt_used reports the smallest of them. */
 int rg_level_box_dt(rg_ctx* ctx, int ilevel, double* dt_out, int nbox);

@@ -576,6 +576,22 @@ int rg_set_level_boxes(rg_ctx* c, int ilevel, int nbox, const int* first_oct, co
     return RG_OK;
 }
 
+int rg_set_level_lattices(rg_ctx* c, int ilevel, int nbox, const int* extent, const int* lat_id, const int* lat_p) {
+    CTX_GUARD(c);
+    if (nbox < 1 || !extent || !lat_id || !lat_p) return set_error(c, RG_ERR_ARG, "nbox, extent, lat_id and lat_p required");
+    Plan* P = existing_plan(c, ilevel);
+    if (!P || P->nbox != nbox) return set_error(c, RG_ERR_STATE, "set the level's boxes (rg_set_level_boxes) first");
+    if (c->params.ndim != 3) return set_error(c, RG_ERR_UNSUPPORTED, "box lattices are a 3D form");
+    if (int rc = set_box_lattices(c, *P, extent, lat_id, lat_p)) return rc;
+    if (P->graph) {
+        cudaGraphExecDestroy(P->graph);
+        P->graph = nullptr;
+    }
+    // the tuned shape was timed without the brick kernel
+    P->face_variant = -1;
+    return RG_OK;
+}
+
 int rg_level_box_dt(rg_ctx* c, int ilevel, double* dt_out, int nbox) {
     CTX_GUARD(c);
     Plan* P = existing_plan(c, ilevel);

@@ -46,7 +46,8 @@ int autotune_face(rg_ctx* c, Plan& P, const StepK& K) {
     for (int v = 0; v < kNumFaceVariants; ++v) {
         for (int b : kBatches) {
             if (v >= kFirstPipeVariant && b != 1) continue;  // round-robin tiles / bricks: no batch
-            if (v >= kFirstBrickVariant && !(P.lattice && P.nbox == 0)) continue;
+            if (v >= kFirstBrickVariant && !(P.nbox > 0 ? P.box_lattice : P.lattice)) continue;
+            if (v > kFirstBrickVariant && P.nbox > 0) continue;  // one boxed brick shape
             if (P.nbox > 0 && !boxed_variant_distinct(v)) continue;
             float tmin = 1e30f;
             for (int rep = 0; rep < 3; ++rep) {

@@ -431,7 +431,7 @@ constexpr int kDefaultFaceVariant = 1;
 // id runs the default shape there.
 constexpr int kBoxedAltVariant = 4;
 inline bool boxed_variant_distinct(int v) {
-    return v == kDefaultFaceVariant || v == kBoxedAltVariant || v == kFirstPipeVariant;
+    return v == kDefaultFaceVariant || v == kBoxedAltVariant || v == kFirstPipeVariant || v == kFirstBrickVariant;
 }
 
 template <int NDIM, int RS, int R, int MINB, bool BOXED = false>

@@ -18,6 +18,7 @@ int launch_pipe_rs(rg_ctx* c, const Plan& P, const StepK& K, int variant, const 
 template <int RS>
 int launch_brick_rs(rg_ctx* c, const Plan& P, const StepK& K, int variant, const double* prim, double* flux,
                     double* fsum) {
+    if (P.nbox > 0) return launch_face_brick<RS, 2, true>(c, P, K, prim, flux, fsum);
     if (variant == kFirstBrickVariant) return launch_face_brick<RS, 3>(c, P, K, prim, flux, fsum);
     return launch_face_brick<RS, 2>(c, P, K, prim, flux, fsum);
 }
@@ -26,7 +27,8 @@ int launch_brick_rs(rg_ctx* c, const Plan& P, const StepK& K, int variant, const
 int launch_face_nd3(rg_ctx* c, const Plan& P, const StepK& K, int variant, int batch, const double* uold,
                     const double* prim, double* flux, double* fsum) {
     if (variant >= kFirstBrickVariant) {
-        if (!P.lattice || P.nbox > 0) return launch_face_nd<3>(c, P, K, kDefaultFaceVariant, batch, uold, prim, flux, fsum);
+        const bool ok = P.nbox > 0 ? P.box_lattice != 0 : P.lattice != 0;
+        if (!ok) return launch_face_nd<3>(c, P, K, kDefaultFaceVariant, batch, uold, prim, flux, fsum);
         switch (c->params.riemann) {
             case RG_RIEMANN_HLLC: return launch_brick_rs<RG_RIEMANN_HLLC>(c, P, K, variant, prim, flux, fsum);
             case RG_RIEMANN_HLL: return launch_brick_rs<RG_RIEMANN_HLL>(c, P, K, variant, prim, flux, fsum);

@@ -8,7 +8,8 @@
 // 93-474); fluxes to the scratch and each cell's own flux sum in the
 // reference's (idim, side) order.
 //
-// A block owns an 8x8x8 brick of cells.  It first copies the primitives of
+// A block owns an 8x8x8 brick of cells (on ensemble levels: of one box, whose
+// own dt and dx it uses).  It first copies the primitives of
 // the brick and a 2-cell periodic halo (12^3 cells, the reach of the own and
 // ghost stencils) from HBM into shared memory -- one read of each value per
 // brick, through the lattice's id map, instead of per-thread gathers through
@@ -32,15 +33,45 @@ __device__ __forceinline__ void brick_state(const double* __restrict__ sq, int s
     rot_swap<3>(q, idim);
 }
 
-template <int RS, int MINB>
+// Lattice geometry of a level: one lattice (nbox == 0: extents ex, ey, ez) or
+// one lattice per ensemble box (extents ext[3b..3b+2], sites from off[b] in
+// the concatenated maps, bricks from brick_off[b]).
+struct BrickGeom {
+    int ex, ey, ez, nbox;
+    const int* ext;
+    const int* off;
+    const int* brick_off;
+};
+
+template <int RS, int MINB, bool BOXED>
 __global__ void __launch_bounds__(BRICK_THREADS, MINB)
-    k_face_brick(PlanView P, int ex, int ey, int ez, const int* __restrict__ lat_id, const int* __restrict__ lat_p,
-                 int kind, const double* __restrict__ prim, size_t ncell, double* __restrict__ flux,
+    k_face_brick(PlanView P, BrickGeom G, const int* __restrict__ lat_id, const int* __restrict__ lat_p, int kind,
+                 const double* __restrict__ prim, size_t ncell, double* __restrict__ flux,
                  double* __restrict__ fsum, DevStatus* st, StepK K) {
     constexpr int NV = 5;
     extern __shared__ __align__(16) double sq[];  // [NV][BSITES]
+    int ex = G.ex, ey = G.ey, ez = G.ez, local = blockIdx.x;
+    double dt = st->dt;
+    DxDiv D{st->dx, st->inv_dx, st->dx_pow2 != 0};
+    if constexpr (BOXED) {
+        int lo = 0, hi = G.nbox - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (G.brick_off[mid] <= (int)blockIdx.x) lo = mid;
+            else hi = mid - 1;
+        }
+        local = blockIdx.x - G.brick_off[lo];
+        ex = G.ext[3 * lo];
+        ey = G.ext[3 * lo + 1];
+        ez = G.ext[3 * lo + 2];
+        lat_id += G.off[lo];
+        lat_p += G.off[lo];
+        const BoxStep& B = P.boxes[lo];
+        dt = B.dt;
+        D = DxDiv{B.dx, B.inv_dx, B.dx_pow2 != 0};
+    }
     const int nbx = ex / BRICK, nby = ey / BRICK;
-    const int bx = blockIdx.x % nbx, by = (blockIdx.x / nbx) % nby, bz = blockIdx.x / (nbx * nby);
+    const int bx = local % nbx, by = (local / nbx) % nby, bz = local / (nbx * nby);
     const int x0 = bx * BRICK - BHALO, y0 = by * BRICK - BHALO, z0 = bz * BRICK - BHALO;
     for (int t = threadIdx.x; t < BSITES; t += blockDim.x) {
         const int a = t % BSIDE, b = (t / BSIDE) % BSIDE, cz = t / (BSIDE * BSIDE);
@@ -53,8 +84,6 @@ __global__ void __launch_bounds__(BRICK_THREADS, MINB)
         for (int iv = 0; iv < NV; ++iv) sq[iv * BSITES + t] = __ldg(prim + iv * ncell + id);
     }
     __syncthreads();
-    const double dt = st->dt;
-    const DxDiv D{st->dx, st->inv_dx, st->dx_pow2 != 0};
     const int nc = P.ncells;
     const bool ghost = (kind & KIND_MASK) == K_GHOST;
     unsigned long long iters = 0, calls = 0;
@@ -111,9 +140,9 @@ __global__ void __launch_bounds__(BRICK_THREADS, MINB)
     }
 }
 
-template <int RS, int MINB>
+template <int RS, int MINB, bool BOXED = false>
 int launch_face_brick(rg_ctx* c, const Plan& P, const StepK& K, const double* prim, double* flux, double* fsum) {
-    auto kern = k_face_brick<RS, MINB>;
+    auto kern = k_face_brick<RS, MINB, BOXED>;
     static bool attr_set[64] = {};  // per device: the shared-memory opt-in is a function attribute
     const int dev = c->device & 63;
     if (!attr_set[dev]) {
@@ -123,10 +152,11 @@ int launch_face_brick(rg_ctx* c, const Plan& P, const StepK& K, const double* pr
             return rc;
         attr_set[dev] = true;
     }
-    const int nbricks = (P.lat_e[0] / BRICK) * (P.lat_e[1] / BRICK) * (P.lat_e[2] / BRICK);
-    kern<<<nbricks, BRICK_THREADS, BRICK_SMEM, c->stream>>>(P.view(), P.lat_e[0], P.lat_e[1], P.lat_e[2], P.lat_id,
-                                                            P.lat_p, P.lat_kind, prim, (size_t)c->ncell, flux, fsum,
-                                                            c->d_status, K);
+    const BrickGeom G{P.lat_e[0], P.lat_e[1], P.lat_e[2], P.nbox, P.bl_ext, P.bl_off, P.bl_brick_off};
+    const int nbricks =
+        BOXED ? P.bl_nbricks : (P.lat_e[0] / BRICK) * (P.lat_e[1] / BRICK) * (P.lat_e[2] / BRICK);
+    kern<<<nbricks, BRICK_THREADS, BRICK_SMEM, c->stream>>>(P.view(), G, P.lat_id, P.lat_p, P.lat_kind, prim,
+                                                            (size_t)c->ncell, flux, fsum, c->d_status, K);
     return check_cuda(c, cudaGetLastError(), "brick face kernel");
 }
 

@@ -109,6 +109,13 @@ struct Plan {
     int lat_kind = 0;          // the (single) interface kind of its faces
     int* lat_id = nullptr;     // [ex*ey*ez] cell id of each lattice site (x fastest)
     int* lat_p = nullptr;      // [ex*ey*ez] plan position of each site
+    // ensemble levels whose boxes are each one periodic lattice: per box its
+    // extent, its first site in lat_id/lat_p and its first brick
+    int box_lattice = 0;
+    int* bl_ext = nullptr;        // [3*nbox]
+    int* bl_off = nullptr;        // [nbox]
+    int* bl_brick_off = nullptr;  // [nbox+1]
+    int bl_nbricks = 0;
     bool ids_ready = false;    // level-sparse host transfer: cell ids read / written
     int* read_ids = nullptr;   // [ncells + nextra_prim] then targ_ids [ntarg] (one allocation)
     int* targ_ids = nullptr;
@@ -211,6 +218,7 @@ int launch_godunov_ext(rg_ctx* c, const Plan& p, const double* uold, double* une
 TreeView tree_view(const rg_ctx* c);
 void remember_shape(rg_ctx* c, const Plan& P);
 int build_lattice(rg_ctx* c, Plan& P);
+int set_box_lattices(rg_ctx* c, Plan& P, const int* ext, const int* lat_id, const int* lat_p);
 int upload_level_host(rg_ctx* c, Plan& P, const double* uold, const double* unew);
 int download_level_host(rg_ctx* c, Plan& P, double* unew);
 int mlp_ensure(rg_ctx* c);

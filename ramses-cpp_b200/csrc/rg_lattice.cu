@@ -103,6 +103,53 @@ __global__ void k_lattice_check(TreeView T, PlanView P, int ex, int ey, int ez, 
     }
 }
 
+// Box lattices supplied by the host (one periodic lattice per ensemble box):
+// every site's plan position must hold that site's cell, every plan position
+// must appear once, and the plan's neighbours, ghost stencils and kinds must
+// be the box lattice's (periodic inside the box).
+__global__ void k_box_lattice_check(TreeView T, PlanView P, int nbox, const int* __restrict__ ext,
+                                    const int* __restrict__ off, const int* __restrict__ lat_id,
+                                    const int* __restrict__ lat_p, int kind0, int* seen, int* bad) {
+    const int n = P.ncells;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) {
+        int lo = 0, hi = nbox - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (off[mid] <= g) lo = mid;
+            else hi = mid - 1;
+        }
+        const int b = lo, ex = ext[3 * b], ey = ext[3 * b + 1], ez = ext[3 * b + 2];
+        const int site = g - off[b];
+        const int x = site % ex, y = (site / ex) % ey, z = site / (ex * ey);
+        const int p = lat_p[g], c = lat_id[g];
+        if (p < 0 || p >= n || atomicExch(&seen[p], 1) != 0) {
+            atomicExch(bad, 1);
+            continue;
+        }
+        const int icx = p / P.noct;
+        if (c != T.ncoarse + icx * T.ngridmax + P.octs[p - icx * P.noct]) {
+            atomicExch(bad, 1);
+            continue;
+        }
+        for (int s = 0; s < 6; ++s) {
+            const int idim = s >> 1, side = s & 1, d = side ? 1 : -1;
+            auto at = [&](int o) {
+                int xx = x, yy = y, zz = z;
+                if (idim == 0) xx = wrap(x + o, ex);
+                else if (idim == 1) yy = wrap(y + o, ey);
+                else zz = wrap(z + o, ez);
+                return lat_id[off[b] + xx + ex * (yy + ey * zz)];
+            };
+            const int nb = at(d), far = at(2 * d);
+            const size_t nc = (size_t)n;
+            const int want_nl = side ? c : far, want_nr = side ? far : c;
+            if (P.icn[s * nc + p] != nb || P.stc[((size_t)s * 2 + 0) * nc + p] != want_nl ||
+                P.stc[((size_t)s * 2 + 1) * nc + p] != want_nr || P.kind[s * nc + p] != kind0)
+                atomicExch(bad, 1);
+        }
+    }
+}
+
 int lblocks(rg_ctx* c, long long n) {
     long long b = (n + LTPB - 1) / LTPB, cap = (long long)c->sm_count * 16;
     return (int)(b < 1 ? 1 : (b > cap ? cap : b));
@@ -159,6 +206,73 @@ int build_lattice(rg_ctx* c, Plan& P) {
     P.lat_e[1] = (int)ey;
     P.lat_e[2] = (int)ez;
     P.lat_kind = kd;
+    return RG_OK;
+}
+
+int set_box_lattices(rg_ctx* c, Plan& P, const int* ext, const int* lat_id, const int* lat_p) {
+    const int nbox = P.nbox;
+    std::vector<int> hext(ext, ext + 3 * (size_t)nbox), hoff((size_t)nbox), hbrick((size_t)nbox + 1);
+    long long sites = 0, bricks = 0;
+    for (int b = 0; b < nbox; ++b) {
+        const int ex = hext[3 * b], ey = hext[3 * b + 1], ez = hext[3 * b + 2];
+        if (ex < 8 || ey < 8 || ez < 8 || ex % 8 || ey % 8 || ez % 8)
+            return set_error(c, RG_ERR_ARG, "box " + std::to_string(b) + ": lattice extents must be multiples of 8");
+        hoff[(size_t)b] = (int)sites;
+        hbrick[(size_t)b] = (int)bricks;
+        sites += (long long)ex * ey * ez;
+        bricks += (long long)(ex / 8) * (ey / 8) * (ez / 8);
+    }
+    hbrick[(size_t)nbox] = (int)bricks;
+    if (sites != P.ncells) return set_error(c, RG_ERR_ARG, "box lattices do not cover the level's cells once");
+    int8_t kind0 = 0;
+    int* d_bad = nullptr;
+    int* d_seen = nullptr;
+    auto fail = [&](int rc) {
+        cudaFree(d_bad);
+        cudaFree(d_seen);
+        cudaFree(P.lat_id);
+        cudaFree(P.lat_p);
+        cudaFree(P.bl_ext);
+        cudaFree(P.bl_off);
+        cudaFree(P.bl_brick_off);
+        P.lat_id = P.lat_p = P.bl_ext = P.bl_off = P.bl_brick_off = nullptr;
+        P.box_lattice = 0;
+        return rc;
+    };
+    fail(RG_OK);
+    const size_t n = (size_t)P.ncells;
+    if (check_cuda(c, cudaMalloc(&d_bad, sizeof(int)), "box lattice flag") ||
+        check_cuda(c, cudaMalloc(&d_seen, sizeof(int) * n), "box lattice marks") ||
+        check_cuda(c, cudaMalloc(&P.lat_id, sizeof(int) * n), "box lattice ids") ||
+        check_cuda(c, cudaMalloc(&P.lat_p, sizeof(int) * n), "box lattice positions") ||
+        check_cuda(c, cudaMalloc(&P.bl_ext, sizeof(int) * hext.size()), "box lattice extents") ||
+        check_cuda(c, cudaMalloc(&P.bl_off, sizeof(int) * hoff.size()), "box lattice offsets") ||
+        check_cuda(c, cudaMalloc(&P.bl_brick_off, sizeof(int) * hbrick.size()), "box lattice bricks"))
+        return fail(RG_ERR_NOMEM);
+    cudaStream_t s = c->stream;
+    cudaMemcpyAsync(&kind0, P.kind, 1, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(P.lat_id, lat_id, sizeof(int) * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(P.lat_p, lat_p, sizeof(int) * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(P.bl_ext, hext.data(), sizeof(int) * hext.size(), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(P.bl_off, hoff.data(), sizeof(int) * hoff.size(), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(P.bl_brick_off, hbrick.data(), sizeof(int) * hbrick.size(), cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(d_seen, 0, sizeof(int) * n, s);
+    cudaMemsetAsync(d_bad, 0, sizeof(int), s);
+    if (int rc = check_cuda(c, cudaStreamSynchronize(s), "box lattice upload")) return fail(rc);
+    if ((kind0 & KIND_MASK) != K_GHOST && (kind0 & KIND_MASK) != K_SAME)
+        return fail(set_error(c, RG_ERR_ARG, "box lattices need a level whose faces are all ghost faces"));
+    k_box_lattice_check<<<lblocks(c, P.ncells), LTPB, 0, s>>>(tree_view(c), P.view(), nbox, P.bl_ext, P.bl_off,
+                                                             P.lat_id, P.lat_p, kind0, d_seen, d_bad);
+    int bad = 1;
+    cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (int rc = check_cuda(c, cudaStreamSynchronize(s), "box lattice check")) return fail(rc);
+    cudaFree(d_bad);
+    cudaFree(d_seen);
+    d_bad = d_seen = nullptr;
+    if (bad) return fail(set_error(c, RG_ERR_ARG, "box lattices do not match the level's neighbours"));
+    P.box_lattice = 1;
+    P.bl_nbricks = (int)bricks;
+    P.lat_kind = kind0;
     return RG_OK;
 }
 

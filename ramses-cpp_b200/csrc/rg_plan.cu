@@ -367,6 +367,9 @@ void free_plan(Plan& p) {
     cudaFree(p.read_ids);
     cudaFree(p.lat_id);
     cudaFree(p.lat_p);
+    cudaFree(p.bl_ext);
+    cudaFree(p.bl_off);
+    cudaFree(p.bl_brick_off);
     p = Plan();
 }
 

@@ -175,6 +175,29 @@ class Forest:
             u[:, self.map_cells(b, cells) - 1] = ub
         return u.reshape(-1)
 
+    def lattices(self):
+        """Per box: its periodic lattice of cells (x fastest) as forest cell ids and as
+        positions p = (ic-1)*noct + k in the leaf level (k = oct position in the level
+        list), concatenated box after box, with the extents [nbox][3]."""
+        noct = int(self.first_oct[-1])
+        ids_all, p_all, ext = [], [], []
+        for b, (sp, gb) in enumerate(zip(self.specs, self.boxes)):
+            E = sp.edge
+            octs = gb.level_octs[sp.level]
+            ids = gb.cell_ids(sp.level)                       # oct-major, ic minor
+            ijk = np.rint(gb.cell_centers(sp.level) * E - 0.5).astype(np.int64)
+            site = ijk[:, 0] + E * (ijk[:, 1] + E * ijk[:, 2])
+            k = np.repeat(np.arange(len(octs)), 8) + int(self.first_oct[b])
+            icx = np.tile(np.arange(8), len(octs))
+            lat_id = np.zeros(E ** 3, np.int32)
+            lat_p = np.full(E ** 3, -1, np.int32)
+            lat_id[site] = self.map_cells(b, ids)
+            lat_p[site] = icx * noct + k
+            ids_all.append(lat_id)
+            p_all.append(lat_p)
+            ext.append((E, E, E))
+        return np.array(ext, np.int32), np.concatenate(ids_all), np.concatenate(p_all)
+
     def extract(self, u, b):
         """Leaf-cell state of box ``b`` from a forest state, as [nvar][leaf cells] in the
         box's own cell order (Grid.cell_ids of its leaf level)."""

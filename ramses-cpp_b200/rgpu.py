@@ -115,6 +115,8 @@ def lib():
                                         C.POINTER(C.c_double)]
     L.rg_set_level_boxes.argtypes = [VP, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]
     L.rg_level_box_dt.argtypes = [VP, C.c_int, C.POINTER(C.c_double), C.c_int]
+    IP = C.POINTER(C.c_int)
+    L.rg_set_level_lattices.argtypes = [VP, C.c_int, C.c_int, IP, IP, IP]
     _lib = L
     return L
 
@@ -271,6 +273,14 @@ class Context:
             raise ValueError("first_oct needs one entry more than dx")
         self._chk(self.L.rg_set_level_boxes(self.h, il, len(dxs), first.ctypes.data_as(C.POINTER(C.c_int)),
                                             dxs.ctypes.data_as(C.POINTER(C.c_double))))
+
+    def set_level_lattices(self, il, extent, lat_id, lat_p):
+        ext = np.ascontiguousarray(extent, dtype=np.int32).reshape(-1)
+        lid = np.ascontiguousarray(lat_id, dtype=np.int32)
+        lp = np.ascontiguousarray(lat_p, dtype=np.int32)
+        IP = C.POINTER(C.c_int)
+        self._chk(self.L.rg_set_level_lattices(self.h, il, len(ext) // 3, ext.ctypes.data_as(IP),
+                                               lid.ctypes.data_as(IP), lp.ctypes.data_as(IP)))
 
     def level_box_dt(self, il, nbox):
         out = np.zeros(nbox, dtype=np.float64)

@@ -71,6 +71,24 @@ def test_forest_keeps_boxes_closed():
     assert np.all(g.son[g.father[octs - 1] - 1] == octs)
 
 
+def test_box_lattices_are_permutations_of_the_level():
+    f = ens.Forest(specs_of([16, 24, 32]))
+    ext, lat_id, lat_p = f.lattices()
+    g = f.grid
+    noct = int(f.first_oct[-1])
+    assert len(lat_p) == len(lat_id) == noct * 8 == int((ext.prod(axis=1)).sum())
+    assert np.array_equal(np.sort(lat_p), np.arange(noct * 8))
+    leaf = g.level_octs[f.level]
+    icx, k = lat_p // noct, lat_p % noct
+    assert np.array_equal(lat_id, g.ncoarse + icx * g.ngridmax + leaf[k])
+    # x neighbours inside a box are the +x lattice sites (periodic)
+    E = int(ext[0, 0])
+    box0 = lat_id[:E ** 3].reshape(E, E, E)  # [z][y][x]
+    cid = box0[0, 0, 0]
+    ig, ic = (cid - g.ncoarse - 1) % g.ngridmax + 1, (cid - g.ncoarse - 1) // g.ngridmax
+    assert ic & 1 == 0 and box0[0, 0, 1] == cid + g.ngridmax  # same oct, x bit set
+
+
 @pytest.mark.parametrize("edges", [[16, 16, 16], [24, 24]])
 def test_forest_step_equals_each_box_alone(edges):
     """Same dx across the forest (the oracle takes one dx per call): the forest's
@@ -129,7 +147,9 @@ def test_sharding_covers_every_box_once_gloo(tmp_path):
 
 
 @pytest.mark.gpu
-def test_ensemble_substeps_match_each_box_alone(rgpu_lib):
+@pytest.mark.parametrize("bricks", [False, True])
+def test_ensemble_substeps_match_each_box_alone(rgpu_lib, bricks):
+    """Tiled face kernel, or (bricks) the brick kernel over the boxes' lattices."""
     import rgpu
     specs = specs_of([16, 24, 32, 16, 24, 32, 16], seed=11)
     f = ens.Forest(specs)
@@ -142,6 +162,9 @@ def test_ensemble_substeps_match_each_box_alone(rgpu_lib):
         u0 = f.initial_state()
         ctx.upload_state(u0, u0)
         ctx.set_level_boxes(f.level, f.first_oct, f.dx)
+        if bricks:
+            ctx.set_level_lattices(f.level, *f.lattices())
+            ctx.set_face_config(f.level, 9, 1)
         nsteps = 3
         dts = []
         for k in range(nsteps):
