@@ -187,3 +187,30 @@ def test_ensemble_substeps_match_each_box_alone(rgpu_lib, bricks):
             orc.set_uold(ga, 3, 5, s.level, uold, unew)
         want = uold.reshape(5, b.ncell)[:, b.cell_ids(s.level) - 1]
         assert bits_equal(f.extract(got, i), want), i
+
+
+@pytest.mark.gpu
+def test_wrong_lattice_map_is_rejected(rgpu_lib):
+    import rgpu
+    f = ens.Forest(specs_of([16, 24], seed=5))
+    ctx = rgpu.Context(rgpu.make_params(3, slope_type=2, riemann="hllc", gamma=f.gamma), 0)
+    try:
+        ctx.sync_topology(f.grid)
+        u0 = f.initial_state()
+        ctx.upload_state(u0, u0)
+        ctx.set_level_boxes(f.level, f.first_oct, f.dx)
+        ext, lat_id, lat_p = f.lattices()
+        bad_p = lat_p.copy()
+        bad_p[[5, 6]] = bad_p[[6, 5]]          # two sites swapped: positions no longer hold their cells
+        with pytest.raises(rgpu.RGError) as e:
+            ctx.set_level_lattices(f.level, ext, lat_id, bad_p)
+        assert e.value.code == rgpu.RG_ERR_ARG
+        bad_id = lat_id.copy()
+        bad_id[:16 ** 3] = np.roll(bad_id[:16 ** 3].reshape(16, 16, 16), 1, axis=2).reshape(-1)
+        with pytest.raises(rgpu.RGError):
+            ctx.set_level_lattices(f.level, ext, bad_id, lat_p)
+        ctx.set_level_lattices(f.level, ext, lat_id, lat_p)  # the right maps are still accepted
+        ctx.level_substep(f.level, 0.0, use_graph=False)
+        ctx.synchronize()
+    finally:
+        ctx.close()

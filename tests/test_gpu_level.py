@@ -315,3 +315,50 @@ def test_autotuner_picks_a_shape_and_exact_stats_count(ctx_factory):
     ctx.synchronize()
     iters, calls = ctx.exact_stats()
     assert calls == 6 * 64 ** 3 and iters >= calls
+
+
+def test_empty_level_is_a_no_op(ctx_factory):
+    """A level list with no octs (headl = 0): every entry point returns OK and
+    leaves the state as it was."""
+    g = rg_tree.build_uniform(3, 4, nlevelmax=6)
+    ctx = ctx_factory(make_params(3, slope_type=2, riemann="hllc"))
+    ctx.sync_topology(g)
+    u = rg_tree.random_state(g, 4, seed=3)
+    ctx.upload_state(u, u)
+    for il in (5, 6):
+        ctx.set_unew(il)
+        ctx.godunov_level(il, 1e-3, 1.0 / 2 ** il)
+        ctx.set_uold(il)
+        ctx.level_substep(il, 1.0 / 2 ** il, use_graph=False)
+        unew = u.copy()
+        ctx.godunov_level_host(il, 1e-3, 1.0 / 2 ** il, u, unew)
+        assert bits_equal(unew, u)
+        assert ctx.cell_updates(il) == 0
+    a, b = np.empty_like(u), np.empty_like(u)
+    ctx.download_state(uold=a, unew=b)
+    assert bits_equal(a, u) and bits_equal(b, u)
+
+
+@pytest.mark.parametrize("variant", [1, 9])
+def test_nx3_grid_with_non_power_of_two_dx(ctx_factory, oracle, variant):
+    """3x3x3 coarse cells refined to 24^3 (dx = 1/48, not a power of two: true
+    divisions in the slopes and traces); tiled and brick kernels."""
+    L = 4
+    g = rg_tree.build_uniform(3, L, nx=3, ny=3, nz=3)
+    ga = ga_of(g)
+    params = make_params(3, slope_type=2, riemann="hllc")
+    ctx = ctx_factory(params)
+    ctx.sync_topology(g)
+    u = rg_tree.random_state(g, L, seed=21)
+    dx = 1.0 / (3 * 2 ** L)
+    dt = 0.3 * oracle.courant(ga, 3, 5, L, dx, 1.4, 0.8, u, pressure_cap=False)
+    want = u.copy()
+    oracle.godunov_fine(ga, params, L, dt, dx, u.copy(), want)
+    ctx.set_face_config(L, variant, 1)
+    ctx.upload_state(u, u)
+    ctx.godunov_level(L, dt, dx)
+    got = np.empty_like(u)
+    ctx.download_state(unew=got)
+    assert bits_equal(got, want)
+    assert ctx.courant_step(L, dx, 0.8, pressure_cap=False) == oracle.courant(ga, 3, 5, L, dx, 1.4, 0.8, u,
+                                                                               pressure_cap=False)
