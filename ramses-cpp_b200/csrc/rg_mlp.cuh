@@ -47,7 +47,7 @@ constexpr int MLP_YM = MLP_SD + MLP_IN;            // target mean
 constexpr int MLP_YS = MLP_YM + 1;                 // target scale
 constexpr int MLP_GATE = MLP_YS + 1;               // keep the two-shock start when |log(guess/p2s)| < gate
 constexpr int MLP_NPARAM = MLP_GATE + 1;           // 4820 floats in the parameter block
-constexpr float MLP_GATE_DEFAULT = 0.2f;
+constexpr float MLP_GATE_DEFAULT = 0.05f;
 // Weak-wave pre-gate: with pmax/pmin < MLP_WEAK_P and |ul-ur| < MLP_WEAK_U
 // (cl+cr) the two-shock guess is within a few percent of p* (its error is
 // second order in the wave strength) and the network is not evaluated.
@@ -81,10 +81,14 @@ __device__ __forceinline__ void mlp_features(const double* ql, const double* qr,
     float cl = sqrtf(g * bl / al), cr = sqrtf(g * br / ar);
     float wl = sqrtf(g * bl * al), wr = sqrtf(g * br * ar);
     float p2s = fmaxf((wr * bl + wl * br + wl * wr * (vl - vr)) / (wl + wr + 1e-30f), 0.f);
-    float z = (g - 1.f) / (2.f * g);
-    float num = cl + cr - 0.5f * (g - 1.f) * (vr - vl);
-    float den = cl / powf(bl, z) + cr / powf(br, z);
-    float ptr = num > 0.f ? fminf(powf(num / den, 1.f / z), 1e30f) : 0.f;
+    // Toro's two-shock estimate: the linearised formula above with each wave's
+    // mass flux W_k(p) = sqrt(gamma p_k rho_k (1 + (gamma+1)/(2 gamma) (p-p_k)/p_k))
+    // -- the function the solver's Newton iteration works on -- taken at the
+    // plain guess instead of at p_k
+    const float g6 = (g + 1.f) / (2.f * g);
+    const float wl0 = sqrtf(fmaxf(wl * wl * (1.f + g6 * (p2s - bl) / bl), 0.f));
+    const float wr0 = sqrtf(fmaxf(wr * wr * (1.f + g6 * (p2s - br) / br), 0.f));
+    const float pts = fmaxf((wr0 * bl + wl0 * br + wl0 * wr0 * (vl - vr)) / (wl0 + wr0 + 1e-30f), 0.f);
     x[0] = logf(al / ar);
     x[1] = logf(bl / br);
     x[2] = asinhf((vl - vr) / (cl + cr));
@@ -92,9 +96,9 @@ __device__ __forceinline__ void mlp_features(const double* ql, const double* qr,
     x[4] = asinhf(vr / cr);
     x[5] = g;
     x[6] = logf(fmaxf(p2s, MLP_LOG_FLOOR));
-    x[7] = logf(fmaxf(ptr, MLP_LOG_FLOOR));
+    x[7] = logf(fmaxf(pts, MLP_LOG_FLOOR));
     *pref_out = pref;
-    *base_out = pref * (double)fmaxf(fmaxf(p2s, ptr), MLP_LOG_FLOOR);
+    *base_out = pref * (double)fmaxf(pts, MLP_LOG_FLOOR);
     if (p2s_out) *p2s_out = pref * (double)p2s;
 }
 
