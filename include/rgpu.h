@@ -172,7 +172,8 @@ int rg_exact_batch(rg_ctx* ctx, int n, const double* ql_dev, const double* qr_de
  * 1.4 per interface; layout as rg_exact_batch. */
 int rg_stress_states(rg_ctx* ctx, int n, uint64_t seed, double* ql_dev, double* qr_dev, double* gamma_dev);
 /* Learned Newton start (no reference counterpart): an 8-64-64-1 SiLU MLP
- * predicting log(pstar / base), base = max(two-shock, two-rarefaction estimate),
+ * predicting log(pstar / base), base = Toro's two-shock estimate (the plain
+ * guess's formula with the wave mass fluxes evaluated at the plain guess),
  * from the interface states, trained on the GPU
  * (BF16 tensor-core forward/backward, FP32 master weights, Adam) on nsamples
  * stress states labelled by the converged Newton root.  Used by

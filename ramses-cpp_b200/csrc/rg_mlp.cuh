@@ -20,8 +20,9 @@
 //   x0 log(rl/rr)            x1 log(pl/pr)
 //   x2 asinh((ul-ur)/(cl+cr)) x3 asinh(ul/cl)   x4 asinh(ur/cr)
 //   x5 gamma                  x6 log(max(p_twoshock, 1e-30 pref)/pref)
-//   x7 log(max(p_tworarefaction, 1e-30 pref)/pref)  (Toro's TRRS estimate)
-// Base estimate: b = max(p_twoshock, p_tworarefaction, 1e-30 pref).
+//   x7 log(max(p_ts, 1e-30 pref)/pref), p_ts = Toro's two-shock estimate (the
+//      linearised formula with the wave mass fluxes taken at the plain guess)
+// Base estimate: b = max(p_ts, 1e-30 pref).
 // Target: log(max(p*, 1e-30 pref) / b); the guess is b * exp(prediction).
 #pragma once
 
