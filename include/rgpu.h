@@ -206,6 +206,14 @@ int rg_mlp_grad(rg_ctx* ctx, int n, const float* x, const float* t, float* grad,
  * AmrGrid's layout.  Synchronises the context stream before returning. */
 int rg_godunov_level_host(rg_ctx* ctx, int ilevel, double dt, double dx, const double* uold, double* unew);
 
+/* Snapshot records of level ilevel from the device state, as
+ * RamsesWriter::write_hydro (src/io/RamsesWriter.cpp:145-226) writes them:
+ * out[((ic-1)*nvar + iv-1)*noct + k] for child slot ic, variable iv (density
+ * floored at 1e-10, velocities, pressure) and the level's k-th oct in list
+ * order.  cap: doubles available at out (needs 2^ndim * nvar * noct).
+ * Synchronises the context stream. */
+int rg_level_output(rg_ctx* ctx, int ilevel, double* out, int64_t cap);
+
 /* ---- allocation-free variant ---------------------------------------------- */
 /* No counterpart in the reference.  The same level step as rg_godunov_level
  * for callers that must not allocate device memory once set-up is over (a

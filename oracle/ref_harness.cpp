@@ -29,6 +29,7 @@
 #include "ramses/core/Config.hpp"
 #include "ramses/core/Parameters.hpp"
 #include "ramses/core/TreeUpdater.hpp"
+#include "ramses/io/RamsesWriter.hpp"
 #include "ramses/solvers/hydro/HydroSolver.hpp"
 #include "ramses/solvers/hydro/RiemannSolver.hpp"
 #include "ramses/solvers/hydro/SlopeLimiter.hpp"
@@ -141,6 +142,14 @@ void rh_interpol_hydro(void* hp, const double* u1, double* u2) {
     memcpy(a, u1, sizeof(a));
     static_cast<Harness*>(hp)->hydro->interpol_hydro(a, b);
     memcpy(u2, b, sizeof(b));
+}
+
+// The reference's hydro snapshot file (RamsesWriter::write_hydro,
+// src/io/RamsesWriter.cpp:145-226) for the harness's current state.
+void rh_write_hydro(void* hp, const char* path) {
+    ramses::SnapshotInfo info{};
+    info.gamma = static_cast<Harness*>(hp)->grid.gamma;
+    ramses::RamsesWriter(path).write_hydro(static_cast<Harness*>(hp)->grid, info);
 }
 
 // Direct access to the public static kernels of the hot path.

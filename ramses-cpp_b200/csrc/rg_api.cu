@@ -592,6 +592,27 @@ int rg_set_level_lattices(rg_ctx* c, int ilevel, int nbox, const int* extent, co
     return RG_OK;
 }
 
+int rg_level_output(rg_ctx* c, int ilevel, double* out, int64_t cap) {
+    CTX_GUARD(c);
+    if (!out) return set_error(c, RG_ERR_ARG, "out is NULL");
+    if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state on the device");
+    if (c->params.nvar != c->params.ndim + 2)
+        return set_error(c, RG_ERR_UNSUPPORTED, "snapshot records of extra variables are not formed on the device");
+    Plan* P;
+    if (int rc = get_plan(c, ilevel, &P)) return rc;
+    const size_t n = (size_t)(1 << c->params.ndim) * c->params.nvar * (size_t)P->noct;
+    if (P->level0) return set_error(c, RG_ERR_ARG, "the coarse level has no octs to write");
+    if ((int64_t)n > cap) return set_error(c, RG_ERR_ARG, "out holds fewer than 2^ndim * nvar * noct doubles");
+    if (n == 0) return RG_OK;
+    if (int rc = ensure_flux(c, *P)) return rc;  // the flux scratch is large enough to stage the records
+    if (c->cap_flux < n) return set_error(c, RG_ERR_STATE, "staging too small");
+    if (int rc = launch_level_output(c, *P, c->d_flux)) return rc;
+    if (int rc = check_cuda(c, cudaMemcpyAsync(out, c->d_flux, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
+                            "level output copy"))
+        return rc;
+    return check_cuda(c, cudaStreamSynchronize(c->stream), "level output sync");
+}
+
 int rg_level_box_dt(rg_ctx* c, int ilevel, double* dt_out, int nbox) {
     CTX_GUARD(c);
     Plan* P = existing_plan(c, ilevel);

@@ -218,6 +218,7 @@ int launch_godunov_ext(rg_ctx* c, const Plan& p, const double* uold, double* une
 TreeView tree_view(const rg_ctx* c);
 void remember_shape(rg_ctx* c, const Plan& P);
 int build_lattice(rg_ctx* c, Plan& P);
+int launch_level_output(rg_ctx* c, const Plan& P, double* out_dev);
 int set_box_lattices(rg_ctx* c, Plan& P, const int* ext, const int* lat_id, const int* lat_p);
 int upload_level_host(rg_ctx* c, Plan& P, const double* uold, const double* unew);
 int download_level_host(rg_ctx* c, Plan& P, double* unew);

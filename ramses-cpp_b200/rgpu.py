@@ -117,6 +117,7 @@ def lib():
     L.rg_level_box_dt.argtypes = [VP, C.c_int, C.POINTER(C.c_double), C.c_int]
     IP = C.POINTER(C.c_int)
     L.rg_set_level_lattices.argtypes = [VP, C.c_int, C.c_int, IP, IP, IP]
+    L.rg_level_output.argtypes = [VP, C.c_int, C.POINTER(C.c_double), C.c_int64]
     _lib = L
     return L
 
@@ -281,6 +282,14 @@ class Context:
         IP = C.POINTER(C.c_int)
         self._chk(self.L.rg_set_level_lattices(self.h, il, len(ext) // 3, ext.ctypes.data_as(IP),
                                                lid.ctypes.data_as(IP), lp.ctypes.data_as(IP)))
+
+    def level_output(self, il, ndim, nvar):
+        """Snapshot records of level il: array [2^ndim][nvar][noct] (list order)."""
+        noct = len(self.level_octs(il))
+        out = np.empty(((1 << ndim), nvar, noct), dtype=np.float64)
+        if noct:
+            self._chk(self.L.rg_level_output(self.h, il, out.ctypes.data_as(C.POINTER(C.c_double)), out.size))
+        return out
 
     def level_box_dt(self, il, nbox):
         out = np.zeros(nbox, dtype=np.float64)

@@ -111,6 +111,7 @@ class RefHarness:
         L.rh_slope.restype = C.c_double
         L.rh_slope.argtypes = [C.c_double] * 3 + [C.c_int, C.c_double, C.c_double]
         L.rh_interpol_hydro.argtypes = [C.c_void_p, F64P, F64P]
+        L.rh_write_hydro.argtypes = [C.c_void_p, C.c_char_p]
         self.h = None
 
     # -- construction -----------------------------------------------------------
@@ -122,6 +123,10 @@ class RefHarness:
         self.nvar = nvar
         self.levelmin, self.nlevelmax = levelmin, nlevelmax
         return self
+
+    def write_hydro(self, path):
+        """The reference's RamsesWriter::write_hydro of the current state."""
+        self.lib.rh_write_hydro(self.h, str(path).encode())
 
     def close(self):
         if self.h:
