@@ -572,6 +572,32 @@ def sod_sample(variant):
             "digest": hashlib.sha1(np.ascontiguousarray(final).tobytes()).hexdigest()}
 
 
+def profile_case_learned():
+    """A small run of the learned part for ncu captures: training on 1e6 stress
+    states for 2 epochs (launches: one k_exact_batch for the labels, then
+    k_mlp_grad + k_adam per batch), then the exact solver on 4M stress pairs
+    with the plain start (k_exact_batch #1) and the learned start (#2)."""
+    import torch
+    import rgpu
+    ctx = rgpu.Context(rgpu.make_params(3, riemann="exact"), 0)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    ctx.mlp_train(nsamples=1_000_000, epochs=2)
+    n = 1 << 22
+    ql = torch.empty(5 * n, dtype=torch.float64, device="cuda")
+    qr = torch.empty_like(ql)
+    gam = torch.empty(n, dtype=torch.float64, device="cuda")
+    f = torch.empty_like(ql)
+    ps = torch.empty(n, dtype=torch.float64, device="cuda")
+    it = torch.empty(n, dtype=torch.int32, device="cuda")
+    ctx.stress_states(n, 2026, ql.data_ptr(), qr.data_ptr(), gam.data_ptr())
+    for learned in (False, True):
+        ctx.exact_batch(n, ql.data_ptr(), qr.data_ptr(), gam.data_ptr(), f.data_ptr(), ps.data_ptr(), it.data_ptr(),
+                        learned=learned, niter=100, tol=1e-14)
+    ctx.synchronize()
+    ctx.close()
+
+
 def run_sample(flag, *args, timeout=900):
     cmd = [sys.executable, str(Path(__file__).resolve()), flag, *[str(a) for a in args]]
     # load every kernel when the context is created (in the sample's untimed
@@ -620,6 +646,7 @@ def main():
     ap.add_argument("--cpu-sample", nargs=2, type=int, metavar=("LEVEL", "STEPS"), help=argparse.SUPPRESS)
     ap.add_argument("--amr-sample", nargs=2, metavar=("VARIANT", "STEPS"), help=argparse.SUPPRESS)
     ap.add_argument("--sod-sample", metavar="VARIANT", help=argparse.SUPPRESS)
+    ap.add_argument("--profile-case", choices=["learned"], help="small run for ncu captures (no timing output)")
     args = ap.parse_args()
     if args.cpu_sample:
         print(json.dumps(cpu_sample(*args.cpu_sample)))
@@ -629,6 +656,9 @@ def main():
         return
     if args.sod_sample:
         print(json.dumps(sod_sample(args.sod_sample)))
+        return
+    if args.profile_case == "learned":
+        profile_case_learned()
         return
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
