@@ -362,3 +362,27 @@ def test_nx3_grid_with_non_power_of_two_dx(ctx_factory, oracle, variant):
     assert bits_equal(got, want)
     assert ctx.courant_step(L, dx, 0.8, pressure_cap=False) == oracle.courant(ga, 3, 5, L, dx, 1.4, 0.8, u,
                                                                                pressure_cap=False)
+
+
+@pytest.mark.parametrize("riem,slope,itype", [("llf", 1, 1), ("hll", 8, 3), ("hllc", 2, 2), ("acoustic", 7, 4),
+                                              ("exact", 2, 1), ("hllc", 5, 0)])
+def test_brick_kernel_every_solver(ctx_factory, oracle, riem, slope, itype):
+    """The brick face kernel (forced) on a 16^3 lattice level, every Riemann
+    solver, slope and interpolation family: the oracle's bits (exact: 3e-12)."""
+    L = 5
+    g = rg_tree.build_uniform(3, L)
+    ga = ga_of(g)
+    params = make_params(3, slope_type=slope, riemann=riem, interpol_type=itype)
+    ctx = ctx_factory(params)
+    ctx.sync_topology(g)
+    ctx.set_face_config(L, 10, 1)
+    u = rg_tree.random_state(g, L, seed=slope * 7 + itype)
+    dx = 1.0 / 2 ** L
+    dt = 0.4 * oracle.courant(ga, 3, 5, L, dx, 1.4, 0.8, u, pressure_cap=False)
+    want = u.copy()
+    oracle.godunov_fine(ga, params, L, dt, dx, u.copy(), want)
+    ctx.upload_state(u, u)
+    ctx.godunov_level(L, dt, dx)
+    got = np.empty_like(u)
+    ctx.download_state(unew=got)
+    assert close_rel(got, want) if riem == "exact" else bits_equal(got, want)
