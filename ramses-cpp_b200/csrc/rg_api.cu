@@ -252,6 +252,7 @@ const char* rg_last_error(const rg_ctx* c) {
 
 int rg_set_params(rg_ctx* c, const rg_params* params) {
     CTX_GUARD(c);
+    c->next_level = -1;  // the state or the CFL word may change
     if (int rc = validate_params(c, params)) return rc;
     if (params->ndim != c->params.ndim && c->have_topology)
         return set_error(c, RG_ERR_ARG, "ndim cannot change after rg_sync_topology");
@@ -270,6 +271,7 @@ int rg_set_params(rg_ctx* c, const rg_params* params) {
 
 int rg_sync_topology(rg_ctx* c, const rg_grid_view* g) {
     CTX_GUARD(c);
+    c->next_level = -1;  // the state or the CFL word may change
     if (!g || !g->son || !g->father || !g->nbor || !g->next || !g->headl) return set_error(c, RG_ERR_ARG, "null grid array");
     if (g->ngridmax < 1 || g->ncoarse < 1 || g->nx < 1 || g->ny < 1 || g->nz < 1 || g->ncpu < 1 || g->nlevelmax < 1)
         return set_error(c, RG_ERR_ARG, "bad grid sizes");
@@ -358,6 +360,7 @@ int rg_sync_topology(rg_ctx* c, const rg_grid_view* g) {
 
 int rg_upload_state(rg_ctx* c, const double* uold, const double* unew) {
     CTX_GUARD(c);
+    c->next_level = -1;  // the state or the CFL word may change
     if (!c->have_topology) return set_error(c, RG_ERR_STATE, "rg_sync_topology has not been called");
     size_t bytes = sizeof(double) * (size_t)c->nvar * c->ncell;
     if (uold && check_cuda(c, cudaMemcpyAsync(c->d_uold, uold, bytes, cudaMemcpyHostToDevice, c->stream), "uold upload"))
@@ -381,6 +384,7 @@ int rg_download_state(rg_ctx* c, double* uold, double* unew) {
 
 int rg_device_state(rg_ctx* c, double** uold_dev, double** unew_dev) {
     CTX_GUARD(c);
+    c->next_level = -1;  // the state or the CFL word may change
     if (!c->have_topology) return set_error(c, RG_ERR_STATE, "rg_sync_topology has not been called");
     if (uold_dev) *uold_dev = c->d_uold;
     if (unew_dev) *unew_dev = c->d_unew;
@@ -390,6 +394,7 @@ int rg_device_state(rg_ctx* c, double** uold_dev, double** unew_dev) {
 
 int rg_set_unew(rg_ctx* c, int ilevel) {
     CTX_GUARD(c);
+    c->next_level = -1;  // the state or the CFL word may change
     Plan* P;
     if (int rc = get_plan(c, ilevel, &P)) return rc;
     return launch_set_unew(c, *P);
@@ -397,6 +402,7 @@ int rg_set_unew(rg_ctx* c, int ilevel) {
 
 int rg_set_uold(rg_ctx* c, int ilevel) {
     CTX_GUARD(c);
+    c->next_level = -1;  // the state or the CFL word may change
     Plan* P;
     if (int rc = get_plan(c, ilevel, &P)) return rc;
     return launch_set_uold(c, *P);
@@ -410,6 +416,7 @@ static int check_learned(rg_ctx* c) {
 
 int rg_godunov_level(rg_ctx* c, int ilevel, double dt, double dx) {
     CTX_GUARD(c);
+    c->next_level = -1;  // the state or the CFL word may change
     if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state uploaded");
     if (int rc = check_learned(c)) return rc;
     Plan* P;
@@ -428,6 +435,7 @@ int rg_godunov_level(rg_ctx* c, int ilevel, double dt, double dx) {
 
 int rg_godunov_level_host(rg_ctx* c, int ilevel, double dt, double dx, const double* uold, double* unew) {
     CTX_GUARD(c);
+    c->next_level = -1;  // the state or the CFL word may change
     if (!uold || !unew) return set_error(c, RG_ERR_ARG, "uold and unew must be host arrays of nvar*ncell doubles");
     if (int rc = check_learned(c)) return rc;
     Plan* P;
@@ -447,6 +455,7 @@ int rg_godunov_level_host(rg_ctx* c, int ilevel, double dt, double dx, const dou
 
 int rg_courant_step(rg_ctx* c, int ilevel, double dx, double courant_factor, int pressure_cap, double* dt_out) {
     CTX_GUARD(c);
+    c->next_level = -1;  // the state or the CFL word may change
     if (!dt_out) return set_error(c, RG_ERR_ARG, "dt_out is NULL");
     if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state uploaded");
     Plan* P;
@@ -474,9 +483,23 @@ int rg_level_substep(rg_ctx* c, int ilevel, double dx, int pressure_cap, int use
     record_updates(c, ilevel, *P);
     if (int rc = ensure_flux(c, *P)) return rc;
     const bool leaf = P->nactive == P->ncells;  // no refined cell: fused substep
+    const double cfl = c->params.courant_factor;
+    const int cap_key = pressure_cap ? 1 : 0;
+    if (leaf) {
+        // the CFL word and primitives are current if the previous call was a
+        // fused substep of this level with the same arguments
+        const bool ready = leaf_fusable(*P) && c->next_level == ilevel && c->next_cap == cap_key &&
+                           c->next_dx == dx && c->next_cfl == cfl;
+        c->next_level = -1;
+        if (!ready) {
+            if (int rc = launch_leaf_prefix(c, *P, dx, pressure_cap, cfl)) return rc;
+        } else if (c->timing) {
+            cudaEventRecord(c->ev[0], c->stream);
+        }
+    }
     auto enqueue = [&]() -> int {
-        if (leaf) return launch_leaf_substep(c, *P, dx, pressure_cap, c->params.courant_factor);
-        if (int rc = launch_courant(c, *P, dx, pressure_cap, c->params.courant_factor)) return rc;
+        if (leaf) return launch_leaf_core(c, *P, dx, pressure_cap, cfl);
+        if (int rc = launch_courant(c, *P, dx, pressure_cap, cfl)) return rc;
         if (int rc = launch_finalize_dt(c, dx)) return rc;
         if (int rc = launch_set_unew(c, *P)) return rc;
         if (int rc = launch_godunov(c, *P)) return rc;
@@ -488,8 +511,8 @@ int rg_level_substep(rg_ctx* c, int ilevel, double dx, int pressure_cap, int use
         if (int rc = enqueue()) return rc;
         if (int rc = autotune_face(c, *P, step_consts(c))) return rc;
     } else if (use_graph) {
-        int cap_key = pressure_cap ? 1 : 0;
-        if (!P->graph || P->graph_cap != cap_key ) {
+        // a graph bakes dx, the courant factor and the pressure cap into its launches
+        if (!P->graph || P->graph_cap != cap_key || P->graph_dx != dx || P->graph_cfl != cfl) {
             if (P->graph) {
                 cudaGraphExecDestroy(P->graph);
                 P->graph = nullptr;
@@ -513,10 +536,18 @@ int rg_level_substep(rg_ctx* c, int ilevel, double dx, int pressure_cap, int use
             cudaGraphDestroy(g);
             if (int rc = check_cuda(c, ei, "graph instantiate")) return rc;
             P->graph_cap = cap_key;
+            P->graph_dx = dx;
+            P->graph_cfl = cfl;
         }
         if (int rc = check_cuda(c, cudaGraphLaunch(P->graph, c->stream), "graph launch")) return rc;
     } else {
         if (int rc = enqueue()) return rc;
+    }
+    if (leaf && leaf_fusable(*P) && P->ncells > 0) {
+        c->next_level = ilevel;
+        c->next_cap = cap_key;
+        c->next_dx = dx;
+        c->next_cfl = cfl;
     }
     if (dt_used) {
         if (P->nbox > 0) {
@@ -537,6 +568,7 @@ int rg_level_substep(rg_ctx* c, int ilevel, double dx, int pressure_cap, int use
 
 int rg_set_level_boxes(rg_ctx* c, int ilevel, int nbox, const int* first_oct, const double* dx) {
     CTX_GUARD(c);
+    c->next_level = -1;  // the state or the CFL word may change
     if (nbox < 1 || !first_oct || !dx) return set_error(c, RG_ERR_ARG, "nbox >= 1, first_oct[nbox+1] and dx[nbox] required");
     Plan* P;
     if (int rc = get_plan(c, ilevel, &P)) return rc;
@@ -578,6 +610,7 @@ int rg_set_level_boxes(rg_ctx* c, int ilevel, int nbox, const int* first_oct, co
 
 int rg_set_level_lattices(rg_ctx* c, int ilevel, int nbox, const int* extent, const int* lat_id, const int* lat_p) {
     CTX_GUARD(c);
+    c->next_level = -1;  // the state or the CFL word may change
     if (nbox < 1 || !extent || !lat_id || !lat_p) return set_error(c, RG_ERR_ARG, "nbox, extent, lat_id and lat_p required");
     Plan* P = existing_plan(c, ilevel);
     if (!P || P->nbox != nbox) return set_error(c, RG_ERR_STATE, "set the level's boxes (rg_set_level_boxes) first");

@@ -101,6 +101,7 @@ struct Plan {
     int8_t* kind = nullptr;
     cudaGraphExec_t graph = nullptr;  // substep graph (set_unew..set_uold)
     int graph_cap = -1;
+    double graph_dx = 0.0, graph_cfl = 0.0;
     int face_variant = -1, face_batch = 4;  // autotuned face-kernel shape (-1: not tuned yet)
     float face_ms = 0.f;
     int substeps_run = 0;
@@ -182,6 +183,11 @@ struct rg_ctx {
 
     std::vector<rg::Plan> plans;
     std::vector<rg::TunedShape> tuned;  // per level
+    // the CFL word and primitives the last fused fold prepared: valid for the
+    // next substep of this level with these arguments, until any call that
+    // touches the state or the CFL word
+    int next_level = -1, next_cap = 0;
+    double next_dx = 0.0, next_cfl = 0.0;
     rg::Tuning tuning;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     float last_ms[3] = {0, 0, 0};
@@ -213,7 +219,11 @@ int launch_courant(rg_ctx* c, const Plan& p, double dx, int pressure_cap, double
 int launch_set_dt_host(rg_ctx* c, double dt, double dx);
 int launch_finalize_dt(rg_ctx* c, double dx);
 int launch_godunov(rg_ctx* c, const Plan& p);
-int launch_leaf_substep(rg_ctx* c, const Plan& p, double dx, int pressure_cap, double courant_factor);
+int launch_leaf_prefix(rg_ctx* c, const Plan& p, double dx, int pressure_cap, double courant_factor);
+int launch_leaf_core(rg_ctx* c, const Plan& p, double dx, int pressure_cap, double courant_factor);
+// a leaf level whose stencils and updates stay inside it: its fold can prepare
+// the next substep
+inline bool leaf_fusable(const Plan& P) { return P.nextra_prim == 0 && P.ntarg == P.ncells && !P.level0; }
 int launch_godunov_ext(rg_ctx* c, const Plan& p, const double* uold, double* unew, double* prim, double* flux);
 TreeView tree_view(const rg_ctx* c);
 void remember_shape(rg_ctx* c, const Plan& P);

@@ -60,6 +60,7 @@ extern "C" int rg_godunov_level_noalloc(rg_ctx* c, int ilevel, double dt, double
     if (!c) return RG_ERR_ARG;
     if (c->broken) return rg::set_error(c, RG_ERR_CUDA, c->err.empty() ? "context unusable after a device fault" : c->err);
     if (!uold_dev || !unew_dev) return rg::set_error(c, RG_ERR_ARG, "uold_dev and unew_dev must be device pointers");
+    c->next_level = -1;  // this call uses the context's CFL word and primitive array
     if (int rc = rg::check_cuda(c, cudaSetDevice(c->device), "cudaSetDevice")) return rc;
     rg::Plan* P = rg::existing_plan(c, ilevel);
     if (P && P->nbox > 0) return rg::set_error(c, RG_ERR_STATE, "ensemble level: every box has its own dt");

@@ -104,88 +104,205 @@ __global__ void k_prim(TreeView T, PlanView P, const double* __restrict__ uold, 
     }
 }
 
+// The ordered updates of one target (HydroSolver.cpp:476-547): refluxes from
+// neighbours and the cell's own flux-sum update with its clamps, applied in
+// the CPU loop order to u (the target's starting state).
+// FSUM: the face kernel stored each cell's own flux sum (fsum [nvar][ncells]),
+// so the own update reads it instead of re-adding the 2*ndim slots.
+template <int NDIM, bool FSUM>
+__device__ __forceinline__ void fold_events(const PlanView& P, int a, int b, const double* __restrict__ flux,
+                                            const double* __restrict__ fsum, double gamma, double dtdx, double* u) {
+    constexpr int NV = Dims<NDIM>::NV, NS = Dims<NDIM>::NS, TTD = Dims<NDIM>::TTD;
+    const int nc = P.ncells;
+    const double factor = 1.0 / (1 << NDIM);
+    for (int e = a; e < b; ++e) {
+        int key = P.tev[e];
+        int slot = key & 7, cp = key >> 3;
+        int ps = P.level0 ? cp : (cp % TTD) * P.noct + cp / TTD;
+        if (slot == OWN_SLOT) {
+            double fs[NV];
+            if constexpr (FSUM) {
+#pragma unroll
+                for (int iv = 0; iv < NV; ++iv) fs[iv] = fsum[(size_t)iv * nc + ps];
+            } else {
+#pragma unroll
+                for (int iv = 0; iv < NV; ++iv) fs[iv] = 0.0;
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    double sign = (s & 1) ? -1.0 : 1.0;
+#pragma unroll
+                    for (int iv = 0; iv < NV; ++iv) fs[iv] = fs[iv] + sign * flux[((size_t)s * NV + iv) * nc + ps];
+                }
+            }
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) u[iv] = u[iv] + dtdx * fs[iv];
+            // clamps (HydroSolver.cpp:534-547)
+            double d = sclamp(u[0], 1e-10, 1e6);
+            u[0] = d;
+#pragma unroll
+            for (int i = 1; i <= NDIM; ++i) u[i] = sclamp(u[i], -d * 10.0, d * 10.0);
+            double v2 = 0.0;
+#pragma unroll
+            for (int i = 1; i <= NDIM; ++i) {
+                double v = u[i] / d;
+                v2 = v2 + v * v;
+            }
+            constexpr int IE = NDIM + 1;
+            double ei = u[IE] - 0.5 * d * v2;
+            if (ei < d * 1e-10 / (gamma - 1.0)) {
+                double e_non = 0;
+                u[IE] = d * 1e-10 / (gamma - 1.0) + 0.5 * d * v2 + e_non;
+            }
+            u[IE] = smin(u[IE], d * 1e8);
+        } else {
+            double sign = (slot & 1) ? -1.0 : 1.0;
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv)
+                u[iv] = u[iv] - dtdx * sign * flux[((size_t)slot * NV + iv) * nc + ps] * factor;
+        }
+    }
+}
+
+// dt/dx of the box a target belongs to (ensemble levels): a target's updates
+// all come from its own box, so its first event's source tells the box.
+template <int NDIM>
+__device__ __forceinline__ double box_dtdx(const PlanView& P, int a) {
+    constexpr int TTD = Dims<NDIM>::TTD;
+    const int cp = P.tev[a] >> 3;
+    return P.boxes[box_of(P, P.level0 ? cp : (cp % TTD) * P.noct + cp / TTD)].dtdx;
+}
+
 // LEAF: the level has no refined cell, so set_unew (unew <- uold) and
 // set_uold (uold <- unew) of its cells are folded in: a level target starts
 // from uold and its result is written to both arrays.  Coarser targets start
 // from unew as always.
-// FSUM: the face kernel stored each cell's own flux sum (fsum [nvar][ncells]),
-// so the own update reads it instead of re-adding the 2*ndim slots.
 template <int NDIM, bool LEAF = false, bool FSUM = false>
 __global__ void k_fold(TreeView T, PlanView P, const double* __restrict__ flux, double* __restrict__ unew,
                        const DevStatus* __restrict__ st, double gamma, double* __restrict__ uold = nullptr,
                        const double* __restrict__ fsum = nullptr) {
-    constexpr int NV = Dims<NDIM>::NV, NS = Dims<NDIM>::NS, TTD = Dims<NDIM>::TTD;
+    constexpr int NV = Dims<NDIM>::NV;
     const size_t ncell = (size_t)T.ncell;
     const int nc = P.ncells;
     const double dtdx0 = st->dtdx;
-    const double factor = 1.0 / (1 << NDIM);
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < P.ntarg; t += gridDim.x * blockDim.x) {
         int a = P.toff[t], b = P.toff[t + 1];
         if (a == b) continue;
-        double dtdx = dtdx0;
-        if (P.obox) {
-            // ensemble level: a target's updates all come from its own box
-            const int cp = P.tev[a] >> 3;
-            dtdx = P.boxes[box_of(P, P.level0 ? cp : (cp % TTD) * P.noct + cp / TTD)].dtdx;
-        }
+        const double dtdx = P.obox ? box_dtdx<NDIM>(P, a) : dtdx0;
         int cell = (t < nc) ? cell_of(T, P, t) : P.textra[t - nc];
         const bool from_old = LEAF && t < nc;
         const double* src = from_old ? uold : unew;
         double u[NV];
 #pragma unroll
         for (int iv = 0; iv < NV; ++iv) u[iv] = src[(size_t)iv * ncell + cell - 1];
-        for (int e = a; e < b; ++e) {
-            int key = P.tev[e];
-            int slot = key & 7, cp = key >> 3;
-            int ps = P.level0 ? cp : (cp % TTD) * P.noct + cp / TTD;
-            if (slot == OWN_SLOT) {
-                double fs[NV];
-                if constexpr (FSUM) {
-#pragma unroll
-                    for (int iv = 0; iv < NV; ++iv) fs[iv] = fsum[(size_t)iv * nc + ps];
-                } else {
-#pragma unroll
-                    for (int iv = 0; iv < NV; ++iv) fs[iv] = 0.0;
-#pragma unroll
-                    for (int s = 0; s < NS; ++s) {
-                        double sign = (s & 1) ? -1.0 : 1.0;
-#pragma unroll
-                        for (int iv = 0; iv < NV; ++iv) fs[iv] = fs[iv] + sign * flux[((size_t)s * NV + iv) * nc + ps];
-                    }
-                }
-#pragma unroll
-                for (int iv = 0; iv < NV; ++iv) u[iv] = u[iv] + dtdx * fs[iv];
-                // clamps (HydroSolver.cpp:534-547)
-                double d = sclamp(u[0], 1e-10, 1e6);
-                u[0] = d;
-#pragma unroll
-                for (int i = 1; i <= NDIM; ++i) u[i] = sclamp(u[i], -d * 10.0, d * 10.0);
-                double v2 = 0.0;
-#pragma unroll
-                for (int i = 1; i <= NDIM; ++i) {
-                    double v = u[i] / d;
-                    v2 = v2 + v * v;
-                }
-                constexpr int IE = NDIM + 1;
-                double ei = u[IE] - 0.5 * d * v2;
-                if (ei < d * 1e-10 / (gamma - 1.0)) {
-                    double e_non = 0;
-                    u[IE] = d * 1e-10 / (gamma - 1.0) + 0.5 * d * v2 + e_non;
-                }
-                u[IE] = smin(u[IE], d * 1e8);
-            } else {
-                double sign = (slot & 1) ? -1.0 : 1.0;
-#pragma unroll
-                for (int iv = 0; iv < NV; ++iv)
-                    u[iv] = u[iv] - dtdx * sign * flux[((size_t)slot * NV + iv) * nc + ps] * factor;
-            }
-        }
+        fold_events<NDIM, FSUM>(P, a, b, flux, fsum, gamma, dtdx, u);
 #pragma unroll
         for (int iv = 0; iv < NV; ++iv) unew[(size_t)iv * ncell + cell - 1] = u[iv];
         if (from_old) {
 #pragma unroll
             for (int iv = 0; iv < NV; ++iv) uold[(size_t)iv * ncell + cell - 1] = u[iv];
         }
+    }
+}
+
+// CFL candidate of one cell from its conservative state, the reference
+// formula (HydroSolver::compute_courant_step, HydroSolver.cpp:878-977) with or
+// without its p <= 100 rho cap; negative or NaN candidates are not returned
+// (flag false), matching std::min's NaN fall-through.
+template <int NDIM>
+__device__ __forceinline__ bool cfl_candidate(const double* u, double dx, double gamma, double cfl, int pressure_cap,
+                                              unsigned long long* bits) {
+    double d = smax(u[0], 1e-10), v2 = 0.0;
+#pragma unroll
+    for (int i = 1; i <= NDIM; ++i) {
+        double v = u[i] / d;
+        v2 = v2 + v * v;
+    }
+    double e_non = 0.0, sum_gamma_p = 0.0;
+    double pr = smax((u[NDIM + 1] - 0.5 * d * v2 - e_non) * (gamma - 1.0), d * 1e-10);
+    if (pressure_cap) pr = smin(pr, d * 1e2);
+    double cs2 = cs2_of(d, pr, gamma);
+    cs2 = cs2 + sum_gamma_p / d;
+    double cs = sqrt(smax(cs2, 1e-10));
+    double u_wave = NDIM * cs;
+#pragma unroll
+    for (int i = 1; i <= NDIM; ++i) u_wave = u_wave + fabs(u[i] / d);
+    double a_grav = 0.0;
+#pragma unroll
+    for (int i = 1; i <= NDIM; ++i) a_grav = a_grav + fabs(0.0);
+    double alpha = a_grav * dx / (u_wave * u_wave);
+    alpha = smax(alpha, 0.0001);
+    double dtc = (dx / u_wave) * (sqrt(1.0 + 2.0 * cfl * alpha) - 1.0) / alpha;
+    *bits = (unsigned long long)__double_as_longlong(dtc);
+    return dtc >= 0.0;
+}
+
+// Leaf-level fold that also prepares the next substep: on a level whose
+// stencils and updates stay inside it (no extra primitive cells, no extra
+// targets), the new state of every level cell is in registers here, so its
+// primitives (the next face step's input) and its CFL candidate (min-reduced
+// into the re-armed CFL word; per box on ensemble levels) are formed at once
+// instead of in a separate pass over uold.  Warps walk aligned runs of 32
+// targets so the per-box min can use a segmented shuffle.
+template <int NDIM, bool BOXED>
+__global__ void k_fold_next(TreeView T, PlanView P, const double* __restrict__ flux, double* __restrict__ unew,
+                            DevStatus* st, double gamma, double smalle, double* __restrict__ uold,
+                            const double* __restrict__ fsum, double* __restrict__ prim, double dx, double cfl,
+                            int pressure_cap) {
+    constexpr int NV = Dims<NDIM>::NV;
+    const size_t ncell = (size_t)T.ncell;
+    const int nt = P.ntarg;
+    const double dtdx0 = st->dtdx;
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    unsigned long long best_all = ~0ULL;
+    for (long long base = warp * 32; base < nt; base += nwarps * 32) {
+        const int t = (int)(base + lane);
+        unsigned long long best = ~0ULL;
+        int box = -1;
+        if (t < nt) {
+            const int a = P.toff[t], b = P.toff[t + 1];
+            const int cell = cell_of(T, P, t);
+            double u[NV], q[NV];
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) u[iv] = uold[(size_t)iv * ncell + cell - 1];
+            if (a < b) {
+                const double dtdx = BOXED ? box_dtdx<NDIM>(P, a) : dtdx0;
+                fold_events<NDIM, true>(P, a, b, flux, fsum, gamma, dtdx, u);
+#pragma unroll
+                for (int iv = 0; iv < NV; ++iv) {
+                    unew[(size_t)iv * ncell + cell - 1] = u[iv];
+                    uold[(size_t)iv * ncell + cell - 1] = u[iv];
+                }
+            }
+            ctoprim<NDIM>(u, q, gamma, smalle);
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) prim[(size_t)iv * ncell + cell - 1] = q[iv];
+            if (T.son[cell - 1] == 0) {
+                if (BOXED) box = box_of(P, t);
+                unsigned long long bits;
+                if (cfl_candidate<NDIM>(u, BOXED ? P.boxes[box].dx : dx, gamma, cfl, pressure_cap, &bits))
+                    best = bits;
+            }
+        }
+        if constexpr (BOXED) {
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long ob = __shfl_down_sync(0xffffffffu, best, o);
+                const int obx = __shfl_down_sync(0xffffffffu, box, o);
+                if (lane + o < 32 && obx == box && ob < best) best = ob;
+            }
+            const int prev = __shfl_up_sync(0xffffffffu, box, 1);
+            if (box >= 0 && (lane == 0 || prev != box) && best != ~0ULL) atomicMin(&P.boxes[box].dtmin_bits, best);
+        } else {
+            best_all = best < best_all ? best : best_all;
+        }
+    }
+    if constexpr (!BOXED) {
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long other = __shfl_xor_sync(0xffffffffu, best_all, o);
+            best_all = other < best_all ? other : best_all;
+        }
+        if (lane == 0 && best_all != ~0ULL) atomicMin(&st->dtmin_bits, best_all);
     }
 }
 
@@ -259,29 +376,8 @@ __global__ void k_courant_prim(TreeView T, PlanView P, const double* __restrict_
 #pragma unroll
         for (int iv = 0; iv < NV; ++iv) prim[(size_t)iv * ncell + id - 1] = q[iv];
         if (t >= P.ncells || T.son[id - 1] > 0) continue;
-        double d = smax(u[0], 1e-10), v2 = 0.0;
-#pragma unroll
-        for (int i = 1; i <= NDIM; ++i) {
-            double v = u[i] / d;
-            v2 = v2 + v * v;
-        }
-        double e_non = 0.0, sum_gamma_p = 0.0;
-        double pr = smax((u[NDIM + 1] - 0.5 * d * v2 - e_non) * (gamma - 1.0), d * 1e-10);
-        if (pressure_cap) pr = smin(pr, d * 1e2);
-        double cs2 = cs2_of(d, pr, gamma);
-        cs2 = cs2 + sum_gamma_p / d;
-        double cs = sqrt(smax(cs2, 1e-10));
-        double u_wave = NDIM * cs;
-#pragma unroll
-        for (int i = 1; i <= NDIM; ++i) u_wave = u_wave + fabs(u[i] / d);
-        double a_grav = 0.0;
-#pragma unroll
-        for (int i = 1; i <= NDIM; ++i) a_grav = a_grav + fabs(0.0);
-        double alpha = a_grav * dx / (u_wave * u_wave);
-        alpha = smax(alpha, 0.0001);
-        double dtc = (dx / u_wave) * (sqrt(1.0 + 2.0 * cfl * alpha) - 1.0) / alpha;
-        unsigned long long b = (unsigned long long)__double_as_longlong(dtc);
-        if (dtc >= 0.0 && b < best) best = b;
+        unsigned long long b;
+        if (cfl_candidate<NDIM>(u, dx, gamma, cfl, pressure_cap, &b) && b < best) best = b;
     }
     for (int o = 16; o > 0; o >>= 1) {
         unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
@@ -301,8 +397,11 @@ __device__ __forceinline__ void set_step_values(DevStatus* st, double dt, double
     st->inv_dx = inv;
     st->dx_pow2 = is_pow2_with_normal_inverse(dx, inv) ? 1 : 0;
 }
-__global__ void k_dt_finalize(DevStatus* st, double dx) {
+// Takes the step from the CFL word and re-arms the word at dt_start, ready for
+// the candidates of the next step (the fused fold adds them).
+__global__ void k_dt_finalize(DevStatus* st, double dx, double dt_start) {
     set_step_values(st, __longlong_as_double((long long)st->dtmin_bits), dx);
+    st->dtmin_bits = (unsigned long long)__double_as_longlong(dt_start);
 }
 __global__ void k_dt_set(DevStatus* st, double dt, double dx) { set_step_values(st, dt, dx); }
 
@@ -311,10 +410,11 @@ __global__ void k_box_courant_init(BoxStep* boxes, int nbox, double dt_start) {
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nbox; b += gridDim.x * blockDim.x)
         boxes[b].dtmin_bits = (unsigned long long)__double_as_longlong(dt_start);
 }
-__global__ void k_box_dt_finalize(BoxStep* boxes, int nbox) {
+__global__ void k_box_dt_finalize(BoxStep* boxes, int nbox, double dt_start) {
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nbox; b += gridDim.x * blockDim.x) {
         BoxStep& B = boxes[b];
         const double dt = __longlong_as_double((long long)B.dtmin_bits), dx = B.dx;
+        B.dtmin_bits = (unsigned long long)__double_as_longlong(dt_start);
         B.dt = dt;
         B.dtdx = dt / dx;
         const double inv = 1.0 / dx;
@@ -352,30 +452,8 @@ __global__ void k_courant_prim_boxes(TreeView T, PlanView P, const double* __res
             for (int iv = 0; iv < NV; ++iv) prim[(size_t)iv * ncell + id - 1] = q[iv];
             if (t < P.ncells && T.son[id - 1] == 0) {
                 box = box_of(P, t);
-                const double dx = P.boxes[box].dx;
-                double d = smax(u[0], 1e-10), v2 = 0.0;
-#pragma unroll
-                for (int i = 1; i <= NDIM; ++i) {
-                    double v = u[i] / d;
-                    v2 = v2 + v * v;
-                }
-                double e_non = 0.0, sum_gamma_p = 0.0;
-                double pr = smax((u[NDIM + 1] - 0.5 * d * v2 - e_non) * (gamma - 1.0), d * 1e-10);
-                if (pressure_cap) pr = smin(pr, d * 1e2);
-                double cs2 = cs2_of(d, pr, gamma);
-                cs2 = cs2 + sum_gamma_p / d;
-                double cs = sqrt(smax(cs2, 1e-10));
-                double u_wave = NDIM * cs;
-#pragma unroll
-                for (int i = 1; i <= NDIM; ++i) u_wave = u_wave + fabs(u[i] / d);
-                double a_grav = 0.0;
-#pragma unroll
-                for (int i = 1; i <= NDIM; ++i) a_grav = a_grav + fabs(0.0);
-                double alpha = a_grav * dx / (u_wave * u_wave);
-                alpha = smax(alpha, 0.0001);
-                double dtc = (dx / u_wave) * (sqrt(1.0 + 2.0 * cfl * alpha) - 1.0) / alpha;
-                unsigned long long b = (unsigned long long)__double_as_longlong(dtc);
-                if (dtc >= 0.0) best = b;
+                unsigned long long b;
+                if (cfl_candidate<NDIM>(u, P.boxes[box].dx, gamma, cfl, pressure_cap, &b)) best = b;
             }
         }
         // segmented min over runs of equal box in lane order
@@ -498,45 +576,81 @@ int launch_godunov_ext(rg_ctx* c, const Plan& P, const double* uold, double* une
     return launch_godunov_ext_t<3>(c, P, uold, unew, prim, flux);
 }
 
+// CFL candidates and primitives of a leaf level from uold, into the armed CFL
+// word (the first substep, or any substep whose previous one did not prepare
+// them).
 template <int NDIM>
-int launch_leaf_substep_t(rg_ctx* c, const Plan& P, double dx, int pressure_cap, double cfl) {
+void launch_leaf_prefix_t(rg_ctx* c, const Plan& P, double dx, int pressure_cap, double cfl) {
     StepK K = step_consts(c);
     TreeView T = tree_view(c);
     PlanView V = P.view();
-    if (c->timing) cudaEventRecord(c->ev[0], c->stream);
-    int nprim = P.ncells + P.nextra_prim;
+    const int nprim = P.ncells + P.nextra_prim;
+    const double start = c->params.boxlen / 1e-10;
     if (P.nbox > 0) {
         const int bb = (P.nbox + 127) / 128;
-        k_box_courant_init<<<bb, 128, 0, c->stream>>>(P.boxes, P.nbox, c->params.boxlen / 1e-10);
+        k_box_courant_init<<<bb, 128, 0, c->stream>>>(P.boxes, P.nbox, start);
         k_courant_prim_boxes<NDIM><<<grid_for(c, nprim, 256), 256, 0, c->stream>>>(T, V, c->d_uold, c->d_prim,
                                                                                    K.gamma, K.smalle, cfl,
                                                                                    pressure_cap);
-        k_box_dt_finalize<<<bb, 128, 0, c->stream>>>(P.boxes, P.nbox);
     } else {
-        k_courant_init<<<1, 1, 0, c->stream>>>(c->d_status, c->params.boxlen / 1e-10);
+        k_courant_init<<<1, 1, 0, c->stream>>>(c->d_status, start);
         k_courant_prim<NDIM><<<grid_for(c, nprim, 256), 256, 0, c->stream>>>(T, V, c->d_uold, c->d_prim,
                                                                              c->d_status, dx, K.gamma, K.smalle,
                                                                              cfl, pressure_cap);
-        k_dt_finalize<<<1, 1, 0, c->stream>>>(c->d_status, dx);
     }
+}
+
+// dt from the CFL word, the face step and the fold (the fused fold on levels
+// that allow it, which leaves the next substep's CFL word and primitives).
+template <int NDIM>
+int launch_leaf_core_t(rg_ctx* c, const Plan& P, double dx, int pressure_cap, double cfl) {
+    StepK K = step_consts(c);
+    TreeView T = tree_view(c);
+    PlanView V = P.view();
+    const double start = c->params.boxlen / 1e-10;
+    if (P.nbox > 0) k_box_dt_finalize<<<(P.nbox + 127) / 128, 128, 0, c->stream>>>(P.boxes, P.nbox, start);
+    else k_dt_finalize<<<1, 1, 0, c->stream>>>(c->d_status, dx, start);
     if (c->timing) cudaEventRecord(c->ev[1], c->stream);
     double* fsum = c->d_flux + (size_t)(2 * NDIM) * (NDIM + 2) * P.ncells;
     if (int rc = launch_face_tiles(c, P, K, c->d_uold, c->d_prim, c->d_flux, fsum)) return rc;
     if (c->timing) cudaEventRecord(c->ev[2], c->stream);
-    k_fold<NDIM, true, true><<<grid_for(c, P.ntarg, 256), 256, 0, c->stream>>>(T, V, c->d_flux, c->d_unew,
-                                                                               c->d_status, K.gamma, c->d_uold, fsum);
+    const int g = grid_for(c, P.ntarg, 256);
+    if (leaf_fusable(P)) {
+        if (P.nbox > 0)
+            k_fold_next<NDIM, true><<<g, 256, 0, c->stream>>>(T, V, c->d_flux, c->d_unew, c->d_status, K.gamma,
+                                                              K.smalle, c->d_uold, fsum, c->d_prim, dx, cfl,
+                                                              pressure_cap);
+        else
+            k_fold_next<NDIM, false><<<g, 256, 0, c->stream>>>(T, V, c->d_flux, c->d_unew, c->d_status, K.gamma,
+                                                               K.smalle, c->d_uold, fsum, c->d_prim, dx, cfl,
+                                                               pressure_cap);
+    } else {
+        k_fold<NDIM, true, true><<<g, 256, 0, c->stream>>>(T, V, c->d_flux, c->d_unew, c->d_status, K.gamma,
+                                                           c->d_uold, fsum);
+    }
     if (c->timing) cudaEventRecord(c->ev[3], c->stream);
     return check_cuda(c, cudaGetLastError(), "leaf substep kernels");
 }
 
 // Substep of a level without refined cells: CFL + primitives in one pass,
-// set_unew/set_uold folded into the fold kernel (five launches instead of eight).
-int launch_leaf_substep(rg_ctx* c, const Plan& P, double dx, int pressure_cap, double cfl) {
+// set_unew/set_uold folded into the fold kernel; on levels whose stencils stay
+// inside them the fold also prepares the next substep's CFL word and
+// primitives, and the prefix is skipped while they are current (three
+// launches instead of five).
+int launch_leaf_prefix(rg_ctx* c, const Plan& P, double dx, int pressure_cap, double cfl) {
+    if (P.ncells == 0) return RG_OK;
+    if (c->timing) cudaEventRecord(c->ev[0], c->stream);
+    if (c->params.ndim == 1) launch_leaf_prefix_t<1>(c, P, dx, pressure_cap, cfl);
+    else launch_leaf_prefix_t<3>(c, P, dx, pressure_cap, cfl);
+    return check_cuda(c, cudaGetLastError(), "leaf substep CFL");
+}
+
+int launch_leaf_core(rg_ctx* c, const Plan& P, double dx, int pressure_cap, double cfl) {
     if (P.ncells == 0) return RG_OK;
     if (c->cap_flux < (size_t)(2 * c->params.ndim + 1) * (c->params.ndim + 2) * P.ncells)
         return set_error(c, RG_ERR_STATE, "flux scratch not sized");
-    if (c->params.ndim == 1) return launch_leaf_substep_t<1>(c, P, dx, pressure_cap, cfl);
-    return launch_leaf_substep_t<3>(c, P, dx, pressure_cap, cfl);
+    if (c->params.ndim == 1) return launch_leaf_core_t<1>(c, P, dx, pressure_cap, cfl);
+    return launch_leaf_core_t<3>(c, P, dx, pressure_cap, cfl);
 }
 
 int launch_set_unew(rg_ctx* c, const Plan& P) {
@@ -570,7 +684,7 @@ int launch_courant(rg_ctx* c, const Plan& P, double dx, int pressure_cap, double
 }
 
 int launch_finalize_dt(rg_ctx* c, double dx) {
-    k_dt_finalize<<<1, 1, 0, c->stream>>>(c->d_status, dx);
+    k_dt_finalize<<<1, 1, 0, c->stream>>>(c->d_status, dx, c->params.boxlen / 1e-10);
     return check_cuda(c, cudaGetLastError(), "dt finalize");
 }
 

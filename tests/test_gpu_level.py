@@ -386,3 +386,43 @@ def test_brick_kernel_every_solver(ctx_factory, oracle, riem, slope, itype):
     got = np.empty_like(u)
     ctx.download_state(unew=got)
     assert close_rel(got, want) if riem == "exact" else bits_equal(got, want)
+
+
+def test_substep_sequence_with_interruptions(ctx_factory, oracle):
+    """Consecutive substeps reuse the CFL word and primitives the previous fused
+    fold prepared; a state upload, a change of the pressure cap, a manual
+    godunov_level and graph/eager switches must each be seen (oracle bits and
+    dt at every step)."""
+    L = 5
+    g = rg_tree.build_uniform(3, L)
+    ga = ga_of(g)
+    params = make_params(3, slope_type=2, riemann="hllc")
+    ctx = ctx_factory(params)
+    ctx.sync_topology(g)
+    uold = rg_tree.sedov_state(g, L)
+    unew = uold.copy()
+    ctx.upload_state(uold, unew)
+    dx = 1.0 / 2 ** L
+    plan = [(False, True), (False, True), (False, False), ("upload", None), (False, True), (True, True),
+            (True, False), (False, True), ("godunov", None), (False, True), (False, False)]
+    for step, (cap, graph) in enumerate(plan):
+        if cap == "upload":
+            uold = rg_tree.random_state(g, L, seed=step)
+            unew = uold.copy()
+            ctx.upload_state(uold, unew)
+            continue
+        if cap == "godunov":
+            # a direct level step between substeps (the reference's godunov_fine)
+            dt = 0.5 * oracle.courant(ga, 3, 5, L, dx, 1.4, 0.8, uold, pressure_cap=False)
+            oracle.godunov_fine(ga, params, L, dt, dx, uold, unew)
+            ctx.godunov_level(L, dt, dx)
+            continue
+        dt = oracle.courant(ga, 3, 5, L, dx, 1.4, 0.8, uold, pressure_cap=cap)
+        oracle.set_unew(ga, 3, 5, L, uold, unew)
+        oracle.godunov_fine(ga, params, L, dt, dx, uold, unew)
+        oracle.set_uold(ga, 3, 5, L, uold, unew)
+        dt_gpu = ctx.level_substep(L, dx, pressure_cap=cap, use_graph=graph, want_dt=True)
+        assert dt_gpu == dt, step
+        got = np.empty_like(uold)
+        ctx.download_state(uold=got)
+        assert bits_equal(got, uold), step
