@@ -43,9 +43,10 @@ UNIT = "cell-updates/s"
 WORKLOAD = "3D Sedov blast, uniform 128^3 (reference levelmin=levelmax=8), MonCen + HLLC, gamma 1.4, FP64"
 LEVEL = 8
 BYTES_PER_CELL_UPDATE = 80  # uold read once + unew written once, 5 FP64 variables each
-# kernels per substep of a level without refined cells: courant init,
-# courant+primitives, dt finalize, face, fold (set_unew/set_uold fused into fold)
-GPU_KERNELS_PER_STEP = 5
+# kernels per substep of the timed loop (a uniform level after its first
+# substep): dt finalize, face, fold (set_unew/set_uold and the next substep's
+# CFL candidates and primitives fused into the fold)
+GPU_KERNELS_PER_STEP = 3
 
 
 def peaks():
