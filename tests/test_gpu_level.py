@@ -426,3 +426,34 @@ def test_substep_sequence_with_interruptions(ctx_factory, oracle):
         got = np.empty_like(uold)
         ctx.download_state(uold=got)
         assert bits_equal(got, uold), step
+
+
+@pytest.mark.parametrize("key", ["L3", "L4", "L5"])
+def test_substep_on_amr_levels(ctx_factory, oracle, golden, key):
+    """rg_level_substep on the levels of a sub-cycled AMR tree (coarse levels
+    with refined cells take the unfused path: CFL, set_unew, godunov_fine,
+    set_uold; the finest level the leaf path), two substeps each, against the
+    oracle's sequence with the same uncapped CFL."""
+    d = golden("amr3d")
+    ndim, slope, riem = (int(x) for x in d["params"])
+    params = make_params(ndim, slope_type=slope, riemann=RIEMANN_NAMES[riem])
+    ncoarse, ngm, ncell, nvar, nx, ny, nz, nlevelmax, il = (int(x) for x in d[f"{key}_meta"])
+    g = GridArrays(ncoarse=ncoarse, ngridmax=ngm, ncell=ncell, nvar=nvar, nx=nx, ny=ny, nz=nz, ncpu=1,
+                   nboundary=0, nlevelmax=nlevelmax, son=d[f"{key}_son"], father=d[f"{key}_father"],
+                   nbor=d[f"{key}_nbor"], next=d[f"{key}_next"], headl=d[f"{key}_headl"])
+    ctx = ctx_factory(params)
+    ctx.sync_topology(g)
+    uold = np.array(d[f"{key}_uold"], dtype=np.float64)
+    unew = np.array(d[f"{key}_unew_in"], dtype=np.float64)
+    ctx.upload_state(uold, unew)
+    dx = 1.0 / (nx * 2 ** il)
+    for step in range(2):
+        dt = oracle.courant(g, ndim, nvar, il, dx, 1.4, 0.8, uold, pressure_cap=False)
+        oracle.set_unew(g, ndim, nvar, il, uold, unew)
+        oracle.godunov_fine(g, params, il, dt, dx, uold, unew)
+        oracle.set_uold(g, ndim, nvar, il, uold, unew)
+        dt_gpu = ctx.level_substep(il, dx, pressure_cap=False, use_graph=(step == 1), want_dt=True)
+        assert dt_gpu == dt, (key, step)
+    a, b = np.empty_like(uold), np.empty_like(unew)
+    ctx.download_state(uold=a, unew=b)
+    assert bits_equal(a, uold) and bits_equal(b, unew)
