@@ -217,21 +217,30 @@ __device__ __forceinline__ bool cfl_candidate(const double* u, double dx, double
         double v = u[i] / d;
         v2 = v2 + v * v;
     }
-    double e_non = 0.0, sum_gamma_p = 0.0;
+    double e_non = 0.0;
     double pr = smax((u[NDIM + 1] - 0.5 * d * v2 - e_non) * (gamma - 1.0), d * 1e-10);
     if (pressure_cap) pr = smin(pr, d * 1e2);
+    // The reference adds sum_gamma_p / d with sum_gamma_p = 0 (no non-thermal
+    // energies): +0 leaves cs2 unchanged (cs2 > 0, or NaN stays NaN).
     double cs2 = cs2_of(d, pr, gamma);
-    cs2 = cs2 + sum_gamma_p / d;
     double cs = sqrt(smax(cs2, 1e-10));
     double u_wave = NDIM * cs;
 #pragma unroll
     for (int i = 1; i <= NDIM; ++i) u_wave = u_wave + fabs(u[i] / d);
-    double a_grav = 0.0;
-#pragma unroll
-    for (int i = 1; i <= NDIM; ++i) a_grav = a_grav + fabs(0.0);
-    double alpha = a_grav * dx / (u_wave * u_wave);
-    alpha = smax(alpha, 0.0001);
-    double dtc = (dx / u_wave) * (sqrt(1.0 + 2.0 * cfl * alpha) - 1.0) / alpha;
+    // alpha = max(a_grav dx / u_wave^2, 1e-4) with a_grav = 0 (no gravity) is
+    // exactly 1e-4 when dx is finite and u_wave^2 > 0; the sqrt term then
+    // depends on cfl alone.  Other cases take the literal formula.
+    const double uw2 = u_wave * u_wave;
+    double alpha, sq;
+    if (isfinite(dx) && uw2 > 0.0) {
+        alpha = 0.0001;
+        sq = sqrt(1.0 + 2.0 * cfl * 0.0001) - 1.0;
+    } else {
+        const double a_grav = 0.0;
+        alpha = smax(a_grav * dx / uw2, 0.0001);
+        sq = sqrt(1.0 + 2.0 * cfl * alpha) - 1.0;
+    }
+    double dtc = (dx / u_wave) * sq / alpha;
     *bits = (unsigned long long)__double_as_longlong(dtc);
     return dtc >= 0.0;
 }
