@@ -109,12 +109,68 @@ __global__ void k_prim(TreeView T, PlanView P, const double* __restrict__ uold, 
 // the CPU loop order to u (the target's starting state).
 // FSUM: the face kernel stored each cell's own flux sum (fsum [nvar][ncells]),
 // so the own update reads it instead of re-adding the 2*ndim slots.
-template <int NDIM, bool FSUM>
+// Own update with its clamps (HydroSolver.cpp:485-547).
+template <int NDIM>
+__device__ __forceinline__ void own_update(const double* fs, double gamma, double dtdx, double* u) {
+    constexpr int NV = Dims<NDIM>::NV;
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) u[iv] = u[iv] + dtdx * fs[iv];
+    double d = sclamp(u[0], 1e-10, 1e6);
+    u[0] = d;
+#pragma unroll
+    for (int i = 1; i <= NDIM; ++i) u[i] = sclamp(u[i], -d * 10.0, d * 10.0);
+    double v2 = 0.0;
+#pragma unroll
+    for (int i = 1; i <= NDIM; ++i) {
+        double v = u[i] / d;
+        v2 = v2 + v * v;
+    }
+    constexpr int IE = NDIM + 1;
+    double ei = u[IE] - 0.5 * d * v2;
+    if (ei < d * 1e-10 / (gamma - 1.0)) {
+        double e_non = 0;
+        u[IE] = d * 1e-10 / (gamma - 1.0) + 0.5 * d * v2 + e_non;
+    }
+    u[IE] = smin(u[IE], d * 1e8);
+}
+
+// BATCH: fetch all events' values before applying them (more loads in flight
+// per thread).  It pays on a single grid; on a 43M-cell ensemble, with a
+// 12 GB flux scratch, 35 planes in flight per warp measured slower.
+template <int NDIM, bool FSUM, bool BATCH = true>
 __device__ __forceinline__ void fold_events(const PlanView& P, int a, int b, const double* __restrict__ flux,
                                             const double* __restrict__ fsum, double gamma, double dtdx, double* u) {
     constexpr int NV = Dims<NDIM>::NV, NS = Dims<NDIM>::NS, TTD = Dims<NDIM>::TTD;
     const int nc = P.ncells;
     const double factor = 1.0 / (1 << NDIM);
+    if (BATCH && FSUM && b - a == NS + 1) {
+        // a cell with all 2*ndim neighbours refluxing into it and its own
+        // update (every cell of a uniform level): fetch every event's values
+        // first, then apply them in the same order with the same arithmetic
+        double v[NS + 1][NV];
+        int slots[NS + 1];
+#pragma unroll
+        for (int e = 0; e <= NS; ++e) {
+            const int key = P.tev[a + e];
+            const int slot = key & 7, cp = key >> 3;
+            const int ps = P.level0 ? cp : (cp % TTD) * P.noct + cp / TTD;
+            slots[e] = slot;
+            const double* src = slot == OWN_SLOT ? fsum + ps : flux + (size_t)slot * NV * nc + ps;
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) v[e][iv] = src[(size_t)iv * nc];
+        }
+#pragma unroll
+        for (int e = 0; e <= NS; ++e) {
+            if (slots[e] == OWN_SLOT) {
+                own_update<NDIM>(v[e], gamma, dtdx, u);
+            } else {
+                const double sign = (slots[e] & 1) ? -1.0 : 1.0;
+#pragma unroll
+                for (int iv = 0; iv < NV; ++iv) u[iv] = u[iv] - dtdx * sign * v[e][iv] * factor;
+            }
+        }
+        return;
+    }
     for (int e = a; e < b; ++e) {
         int key = P.tev[e];
         int slot = key & 7, cp = key >> 3;
@@ -134,26 +190,7 @@ __device__ __forceinline__ void fold_events(const PlanView& P, int a, int b, con
                     for (int iv = 0; iv < NV; ++iv) fs[iv] = fs[iv] + sign * flux[((size_t)s * NV + iv) * nc + ps];
                 }
             }
-#pragma unroll
-            for (int iv = 0; iv < NV; ++iv) u[iv] = u[iv] + dtdx * fs[iv];
-            // clamps (HydroSolver.cpp:534-547)
-            double d = sclamp(u[0], 1e-10, 1e6);
-            u[0] = d;
-#pragma unroll
-            for (int i = 1; i <= NDIM; ++i) u[i] = sclamp(u[i], -d * 10.0, d * 10.0);
-            double v2 = 0.0;
-#pragma unroll
-            for (int i = 1; i <= NDIM; ++i) {
-                double v = u[i] / d;
-                v2 = v2 + v * v;
-            }
-            constexpr int IE = NDIM + 1;
-            double ei = u[IE] - 0.5 * d * v2;
-            if (ei < d * 1e-10 / (gamma - 1.0)) {
-                double e_non = 0;
-                u[IE] = d * 1e-10 / (gamma - 1.0) + 0.5 * d * v2 + e_non;
-            }
-            u[IE] = smin(u[IE], d * 1e8);
+            own_update<NDIM>(fs, gamma, dtdx, u);
         } else {
             double sign = (slot & 1) ? -1.0 : 1.0;
 #pragma unroll
@@ -194,7 +231,8 @@ __global__ void k_fold(TreeView T, PlanView P, const double* __restrict__ flux, 
         double u[NV];
 #pragma unroll
         for (int iv = 0; iv < NV; ++iv) u[iv] = src[(size_t)iv * ncell + cell - 1];
-        fold_events<NDIM, FSUM>(P, a, b, flux, fsum, gamma, dtdx, u);
+        if (P.obox) fold_events<NDIM, FSUM, false>(P, a, b, flux, fsum, gamma, dtdx, u);
+        else fold_events<NDIM, FSUM>(P, a, b, flux, fsum, gamma, dtdx, u);
 #pragma unroll
         for (int iv = 0; iv < NV; ++iv) unew[(size_t)iv * ncell + cell - 1] = u[iv];
         if (from_old) {
@@ -277,7 +315,7 @@ __global__ void k_fold_next(TreeView T, PlanView P, const double* __restrict__ f
             for (int iv = 0; iv < NV; ++iv) u[iv] = uold[(size_t)iv * ncell + cell - 1];
             if (a < b) {
                 const double dtdx = BOXED ? box_dtdx<NDIM>(P, a) : dtdx0;
-                fold_events<NDIM, true>(P, a, b, flux, fsum, gamma, dtdx, u);
+                fold_events<NDIM, true, !BOXED>(P, a, b, flux, fsum, gamma, dtdx, u);
 #pragma unroll
                 for (int iv = 0; iv < NV; ++iv) {
                     unew[(size_t)iv * ncell + cell - 1] = u[iv];
