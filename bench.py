@@ -286,7 +286,9 @@ def gpu_arm(args, rank, world, local_rank):
     ctx.set_timing(False)
     kms = acc / nk
 
-    # end to end through the C ABI with host buffers: H2D uold, substep, D2H uold
+    # end to end through the C ABI with the state in (pinned) host memory: each
+    # step uploads the cells the substep reads, runs it, and downloads the
+    # cells it updated (rg_level_substep_host)
     n = g.nvar * g.ncell
     host = torch.empty(n, dtype=torch.float64, pin_memory=True)
     ctx.download_state_ptr(uold_ptr=host.data_ptr())
@@ -297,9 +299,7 @@ def gpu_arm(args, rank, world, local_rank):
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e2.record(stream)
     for _ in range(ne):
-        ctx.upload_state_ptr(uold_ptr=host.data_ptr())
-        ctx.level_substep(L, dx, pressure_cap=False, use_graph=True)
-        ctx.download_state_ptr(uold_ptr=host.data_ptr())
+        ctx.level_substep_host_ptr(L, dx, host.data_ptr(), want_dt=False)
     e3.record(stream)
     torch.cuda.synchronize()
     ms_e2e = e2.elapsed_time(e3)
@@ -329,8 +329,9 @@ def gpu_arm(args, rank, world, local_rank):
                      "algorithmic_bytes_per_launch": alg_bytes, "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
                      "step_hbm_frac": (BYTES_PER_CELL_UPDATE * value / world / 1e9) / peak},
         "kernel_ms": {"prim": kms[0], "face": kms[1], "fold": kms[2]},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
-                "ms_per_step": ms_e2e / ne, "path": "rg_upload_state(pinned host) + rg_level_substep + rg_download_state"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * g.nvar * cells,
+                "d2h_bytes_per_step": 8 * g.nvar * cells, "ms_per_step": ms_e2e / ne,
+                "path": "rg_level_substep_host on pinned host memory: the level's cells up, substep, its cells down"},
         "gpu_launches": GPU_KERNELS_PER_STEP * args.steps,
         "clocks": clocks,
     }

@@ -214,6 +214,14 @@ int rg_godunov_level_host(rg_ctx* ctx, int ilevel, double dt, double dx, const d
  * Synchronises the context stream. */
 int rg_level_output(rg_ctx* ctx, int ilevel, double* out, int64_t cap);
 
+/* One substep (rg_level_substep) of a level without refined cells on state
+ * held in host memory: uploads uold only at the cells the substep reads, runs
+ * it, and writes back uold (and unew, if not null) at the level's update
+ * targets only.  For callers that keep the state on the host between
+ * substeps.  Synchronises the context stream before returning. */
+int rg_level_substep_host(rg_ctx* ctx, int ilevel, double dx, int pressure_cap, double* uold, double* unew,
+                          double* dt_used);
+
 /* ---- allocation-free variant ---------------------------------------------- */
 /* No counterpart in the reference.  The same level step as rg_godunov_level
  * for callers that must not allocate device memory once set-up is over (a

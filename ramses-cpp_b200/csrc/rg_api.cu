@@ -566,6 +566,30 @@ int rg_level_substep(rg_ctx* c, int ilevel, double dx, int pressure_cap, int use
     return RG_OK;
 }
 
+int rg_level_substep_host(rg_ctx* c, int ilevel, double dx, int pressure_cap, double* uold, double* unew,
+                          double* dt_used) {
+    CTX_GUARD(c);
+    c->next_level = -1;  // the state comes from the host
+    if (!uold) return set_error(c, RG_ERR_ARG, "uold must be a host array of nvar*ncell doubles");
+    Plan* P;
+    if (int rc = get_plan(c, ilevel, &P)) return rc;
+    if (P->nactive != P->ncells) return set_error(c, RG_ERR_STATE, "host substeps need a level without refined cells");
+    if (P->ncells == 0) return RG_OK;
+    if (int rc = upload_level_host(c, *P, uold, nullptr)) return rc;
+    c->have_state = true;
+    if (int rc = rg_level_substep(c, ilevel, dx, pressure_cap, 1, nullptr)) return rc;
+    if (unew)
+        if (int rc = download_level_host(c, *P, unew, c->d_unew)) return rc;
+    if (int rc = download_level_host(c, *P, uold, c->d_uold)) return rc;
+    if (dt_used) {
+        if (int rc = check_cuda(c, cudaMemcpy(c->h_status, c->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost),
+                                "dt copy"))
+            return rc;
+        *dt_used = c->h_status->dt;
+    }
+    return RG_OK;
+}
+
 int rg_set_level_boxes(rg_ctx* c, int ilevel, int nbox, const int* first_oct, const double* dx) {
     CTX_GUARD(c);
     c->next_level = -1;  // the state or the CFL word may change

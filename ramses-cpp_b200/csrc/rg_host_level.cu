@@ -10,8 +10,10 @@
 // at its update targets (the level's cells and the coarser cells that
 // receive refluxes), and writes unew only at those targets.  So instead of
 // the whole state (2 x nvar x ncell doubles up, nvar x ncell down) a call
-// moves exactly those cells: gathered on the host into pinned staging, one
-// copy each way, scattered on the device.
+// moves exactly those cells: as plain copies of their runs of consecutive
+// cell ids when there are few (a uniform level: one run per child slot), else
+// gathered on the host into pinned staging, one copy each way, scattered on
+// the device.
 #include <algorithm>
 #include <vector>
 
@@ -39,6 +41,7 @@ __global__ void k_level_ids(TreeView T, PlanView P, int* read_ids, int* targ_ids
 }
 
 // staging layout: [nvar][nread] uold values, then [nvar][ntarg] unew values
+// (ntarg = 0 when only uold is uploaded)
 __global__ void k_scatter_level(const int* __restrict__ read_ids, int nread, const int* __restrict__ targ_ids,
                                 int ntarg, int nvar, size_t ncell, const double* __restrict__ stage, double* uold,
                                 double* unew) {
@@ -113,13 +116,49 @@ int level_ids(rg_ctx* c, Plan& P) {
                               "level ids copy"))
         return RG_ERR_CUDA;
     if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "level ids sync")) return rc;
+    auto runs = [](const std::vector<int>& ids) {
+        std::vector<std::pair<int, int>> r;
+        for (size_t t = 0; t < ids.size(); ++t) {
+            if (!r.empty() && ids[t] == r.back().first + r.back().second) ++r.back().second;
+            else r.emplace_back(ids[t], 1);
+        }
+        return r;
+    };
+    P.read_runs = runs(P.h_read);
+    P.targ_runs = runs(P.h_targ);
     P.ids_ready = true;
     return RG_OK;
 }
 
+namespace {
+// Levels whose cells form at most this many id runs are moved run by run
+// (DMA straight between the caller's arrays and the device state); more
+// fragmented levels are gathered into pinned staging instead.
+constexpr size_t kMaxRuns = 256;
+
+// one 2D copy per run covers the run in all nvar planes (pitch = one plane)
+int copy_runs(rg_ctx* c, const std::vector<std::pair<int, int>>& runs, double* dst, const double* src,
+              cudaMemcpyKind kind) {
+    const size_t pitch = sizeof(double) * (size_t)c->ncell;
+    for (const auto& r : runs) {
+        const size_t off = (size_t)r.first - 1;
+        if (int rc = check_cuda(c, cudaMemcpy2DAsync(dst + off, pitch, src + off, pitch, sizeof(double) * (size_t)r.second,
+                                                     (size_t)c->nvar, kind, c->stream),
+                                "level run copy"))
+            return rc;
+    }
+    return RG_OK;
+}
+}  // namespace
+
 int upload_level_host(rg_ctx* c, Plan& P, const double* uold, const double* unew) {
     if (int rc = level_ids(c, P)) return rc;
-    const int nv = c->nvar, nread = (int)P.h_read.size(), ntarg = (int)P.h_targ.size();
+    if (P.read_runs.size() <= kMaxRuns && (!unew || P.targ_runs.size() <= kMaxRuns)) {
+        if (int rc = copy_runs(c, P.read_runs, c->d_uold, uold, cudaMemcpyHostToDevice)) return rc;
+        if (unew) return copy_runs(c, P.targ_runs, c->d_unew, unew, cudaMemcpyHostToDevice);
+        return RG_OK;
+    }
+    const int nv = c->nvar, nread = (int)P.h_read.size(), ntarg = unew ? (int)P.h_targ.size() : 0;
     const size_t ncell = (size_t)c->ncell;
     const size_t n = (size_t)nv * ((size_t)nread + ntarg);
     if (n == 0) return RG_OK;
@@ -146,13 +185,18 @@ int upload_level_host(rg_ctx* c, Plan& P, const double* uold, const double* unew
     return check_cuda(c, cudaGetLastError(), "level scatter");
 }
 
-int download_level_host(rg_ctx* c, Plan& P, double* unew) {
+int download_level_host(rg_ctx* c, Plan& P, double* unew, const double* src_dev) {
+    if (P.targ_runs.size() <= kMaxRuns) {
+        if (int rc = copy_runs(c, P.targ_runs, unew, src_dev ? src_dev : c->d_unew, cudaMemcpyDeviceToHost)) return rc;
+        return check_cuda(c, cudaStreamSynchronize(c->stream), "level download sync");
+    }
     const int nv = c->nvar, ntarg = (int)P.h_targ.size();
     const size_t ncell = (size_t)c->ncell;
     const size_t n = (size_t)nv * ntarg;
     if (n == 0) return check_cuda(c, cudaStreamSynchronize(c->stream), "level download sync");
     if (int rc = grow_stage(c, n)) return rc;
-    k_gather_targets<<<blocks(c, ntarg), 256, 0, c->stream>>>(P.targ_ids, ntarg, nv, ncell, c->d_unew, c->d_stage);
+    k_gather_targets<<<blocks(c, ntarg), 256, 0, c->stream>>>(P.targ_ids, ntarg, nv, ncell, src_dev ? src_dev : c->d_unew,
+                                                              c->d_stage);
     if (int rc = check_cuda(c, cudaMemcpyAsync(c->h_stage, c->d_stage, n * sizeof(double), cudaMemcpyDeviceToHost,
                                                c->stream),
                             "level download"))

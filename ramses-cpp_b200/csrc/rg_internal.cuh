@@ -26,6 +26,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/rgpu.h"
@@ -121,6 +122,9 @@ struct Plan {
     int* read_ids = nullptr;   // [ncells + nextra_prim] then targ_ids [ntarg] (one allocation)
     int* targ_ids = nullptr;
     std::vector<int> h_read, h_targ;
+    // the same cells as runs of consecutive cell ids (first id, count): few on
+    // a uniform level (one per child slot), so transfers are plain copies
+    std::vector<std::pair<int, int>> read_runs, targ_runs;
     int nbox = 0;              // ensemble level: number of boxes (0: one grid)
     int* obox = nullptr;       // [noct]
     BoxStep* boxes = nullptr;  // [nbox]
@@ -230,8 +234,10 @@ void remember_shape(rg_ctx* c, const Plan& P);
 int build_lattice(rg_ctx* c, Plan& P);
 int launch_level_output(rg_ctx* c, const Plan& P, double* out_dev);
 int set_box_lattices(rg_ctx* c, Plan& P, const int* ext, const int* lat_id, const int* lat_p);
+// unew may be null (only uold's read cells are uploaded)
 int upload_level_host(rg_ctx* c, Plan& P, const double* uold, const double* unew);
-int download_level_host(rg_ctx* c, Plan& P, double* unew);
+// the level's targets of src_dev (default: the device unew) into host array dst
+int download_level_host(rg_ctx* c, Plan& P, double* dst, const double* src_dev = nullptr);
 int mlp_ensure(rg_ctx* c);
 int mlp_train(rg_ctx* c, int nsamples, int epochs, int batch, float lr, unsigned long long seed, float* loss_out);
 int mlp_grad(rg_ctx* c, int n, const float* x_host, const float* t_host, float* grad_host, float* loss_host);

@@ -118,6 +118,7 @@ def lib():
     IP = C.POINTER(C.c_int)
     L.rg_set_level_lattices.argtypes = [VP, C.c_int, C.c_int, IP, IP, IP]
     L.rg_level_output.argtypes = [VP, C.c_int, C.POINTER(C.c_double), C.c_int64]
+    L.rg_level_substep_host.argtypes = [VP, C.c_int, C.c_double, C.c_int, VP, VP, C.POINTER(C.c_double)]
     _lib = L
     return L
 
@@ -198,6 +199,14 @@ class Context:
         uo = np.ascontiguousarray(uold)
         self._chk(self.L.rg_godunov_level_host(self.h, il, dt, dx, uo.ctypes.data_as(C.POINTER(C.c_double)),
                                                unew.ctypes.data_as(C.POINTER(C.c_double))))
+
+    def level_substep_host_ptr(self, il, dx, uold_ptr, unew_ptr=None, pressure_cap=False, want_dt=True):
+        """Substep on host state at raw addresses (e.g. pinned torch tensors): uold is
+        read and then updated in place at the level's targets."""
+        dt = C.c_double(0)
+        self._chk(self.L.rg_level_substep_host(self.h, il, dx, 1 if pressure_cap else 0, uold_ptr, unew_ptr,
+                                               C.byref(dt) if want_dt else None))
+        return dt.value if want_dt else None
 
     def godunov_level_noalloc(self, il, dt, dx, uold_dev_ptr, unew_dev_ptr):
         """Allocation-free level step on caller-owned device buffers (raw addresses)."""

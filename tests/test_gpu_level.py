@@ -457,3 +457,33 @@ def test_substep_on_amr_levels(ctx_factory, oracle, golden, key):
     a, b = np.empty_like(uold), np.empty_like(unew)
     ctx.download_state(uold=a, unew=b)
     assert bits_equal(a, uold) and bits_equal(b, unew)
+
+
+def test_host_substeps_move_only_the_level(ctx_factory, oracle):
+    """rg_level_substep_host on a host array: oracle bits and dt each substep,
+    and cells outside the level (the coarse levels) keep their host values."""
+    L = 5
+    g = rg_tree.build_uniform(3, L)
+    ga = ga_of(g)
+    params = make_params(3, slope_type=2, riemann="hllc")
+    ctx = ctx_factory(params)
+    ctx.sync_topology(g)
+    uold = rg_tree.sedov_state(g, L)
+    unew = uold.copy()
+    host = uold.copy()
+    host_unew = np.full_like(uold, 7.0)
+    outside = np.setdiff1d(np.arange(1, g.ncell + 1), g.cell_ids(L))
+    before = host.reshape(5, -1)[:, outside - 1].copy()
+    dx = 1.0 / 2 ** L
+    for step in range(3):
+        dt = oracle.courant(ga, 3, 5, L, dx, 1.4, 0.8, uold, pressure_cap=False)
+        oracle.set_unew(ga, 3, 5, L, uold, unew)
+        oracle.godunov_fine(ga, params, L, dt, dx, uold, unew)
+        oracle.set_uold(ga, 3, 5, L, uold, unew)
+        dt_gpu = ctx.level_substep_host_ptr(L, dx, host.ctypes.data, host_unew.ctypes.data)
+        assert dt_gpu == dt, step
+        ids = g.cell_ids(L)
+        assert bits_equal(host.reshape(5, -1)[:, ids - 1], uold.reshape(5, -1)[:, ids - 1]), step
+        assert bits_equal(host_unew.reshape(5, -1)[:, ids - 1], unew.reshape(5, -1)[:, ids - 1]), step
+    assert bits_equal(host.reshape(5, -1)[:, outside - 1], before)
+    assert np.all(host_unew.reshape(5, -1)[:, outside - 1] == 7.0)
