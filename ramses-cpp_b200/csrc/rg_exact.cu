@@ -67,8 +67,10 @@ __global__ void k_stress_states(int n, unsigned long long seed, double* ql, doub
     }
 }
 
-template <int NDIM>
-__global__ void k_exact_batch(int n, const double* __restrict__ ql, const double* __restrict__ qr,
+// LEARNED: the network may be evaluated (out of line; it needs registers), so
+// fewer resident blocks; the plain start keeps more warps in flight.
+template <int NDIM, bool LEARNED>
+__global__ void __launch_bounds__(256, LEARNED ? 2 : 4) k_exact_batch(int n, const double* __restrict__ ql, const double* __restrict__ qr,
                               const double* __restrict__ gam, double gamma0, double* flux, double* pstar, int* iters,
                               const float* __restrict__ mlp, int niter, double tol, DevStatus* st) {
     constexpr int NV = NDIM + 2;
@@ -82,7 +84,7 @@ __global__ void k_exact_batch(int n, const double* __restrict__ ql, const double
         }
         double gamma = gam ? gam[i] : gamma0;
         double smallp = 1e-10 * 1e-10 / gamma;
-        double guess = mlp_guess<NDIM>(mlp, a, b, gamma, smallp);
+        double guess = LEARNED ? mlp_guess<NDIM>(mlp, a, b, gamma, smallp) : -1.0;
         double ps;
         int it = solve_exact_p<NDIM>(a, b, f, gamma, smallp, niter, tol, guess, &ps);
         if (flux) {
@@ -143,11 +145,19 @@ int launch_stress_states(rg_ctx* c, int n, unsigned long long seed, double* ql, 
 int launch_exact_batch(rg_ctx* c, int n, const double* ql, const double* qr, const double* gam, double* flux,
                        double* pstar, int* iters, const float* mlp, int niter, double tol) {
     if (c->params.ndim == 1)
-        k_exact_batch<1><<<blocks_for(c, n), 256, 0, c->stream>>>(n, ql, qr, gam, c->params.gamma, flux, pstar, iters,
-                                                                  mlp, niter, tol, c->d_status);
+        if (mlp)
+            k_exact_batch<1, true><<<blocks_for(c, n), 256, 0, c->stream>>>(n, ql, qr, gam, c->params.gamma, flux,
+                                                                            pstar, iters, mlp, niter, tol, c->d_status);
+        else
+            k_exact_batch<1, false><<<blocks_for(c, n), 256, 0, c->stream>>>(n, ql, qr, gam, c->params.gamma, flux,
+                                                                             pstar, iters, mlp, niter, tol, c->d_status);
     else
-        k_exact_batch<3><<<blocks_for(c, n), 256, 0, c->stream>>>(n, ql, qr, gam, c->params.gamma, flux, pstar, iters,
-                                                                  mlp, niter, tol, c->d_status);
+        if (mlp)
+            k_exact_batch<3, true><<<blocks_for(c, n), 256, 0, c->stream>>>(n, ql, qr, gam, c->params.gamma, flux,
+                                                                            pstar, iters, mlp, niter, tol, c->d_status);
+        else
+            k_exact_batch<3, false><<<blocks_for(c, n), 256, 0, c->stream>>>(n, ql, qr, gam, c->params.gamma, flux,
+                                                                             pstar, iters, mlp, niter, tol, c->d_status);
     return check_cuda(c, cudaGetLastError(), "exact batch");
 }
 
