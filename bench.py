@@ -17,8 +17,9 @@ The line also carries the other workloads of the path, each measured on the
 same box:
 - "newton": the exact Riemann solver on the stress workload (256^3
   independent interface pairs), plain two-shock Newton start against the
-  learned start (network trained on the GPU first), and the Sedov step run
-  with the exact solver under both starts;
+  learned start (network trained on the GPU first), the Sedov step run with
+  the exact solver under both starts, and (N = 1) the sub-cycled Sedov AMR
+  run with the exact solver under both starts;
 - "ensemble": 512 independent uneven boxes stepped together (sharded over
   the ranks when N > 1);
 - "amr": the sub-cycled Sedov AMR run through the reference's own
@@ -521,6 +522,60 @@ def amr_sample(variant, steps, lmin=7, lmax=10, ngridmax=400000):
     return out
 
 
+def amr_exact_sample(guess, steps, lmin=7, lmax=10, ngridmax=400000):
+    """Config 5's AMR part: the sub-cycled Sedov AMR run (tree maintenance by
+    the reference's own TreeUpdater) with every godunov_fine on the GPU through
+    rg_godunov_level_host, exact solver in converged mode (|dp|/p < 1e-14),
+    plain or learned Newton start; runs in its own process (the reference
+    prints a line per flagged cell)."""
+    import hashlib
+
+    import numpy as np
+    sys.path.insert(0, str(ROOT / "tests"))
+    import rgpu
+    from refsupport import AmrRun, RefHarness, namelist, sedov_ic
+    learned = guess == "learned"
+    nml = namelist(slope_type=2, riemann="exact", levelmin=lmin, levelmax=lmax, err_grad_d=0.1, err_grad_p=0.1)
+    h = RefHarness(3).create(nml, ngridmax=ngridmax, levelmin=lmin, nlevelmax=lmax, gamma=1.4)
+    ctx = rgpu.Context(rgpu.make_params(3, slope_type=2, riemann="exact", exact_niter=100, exact_tol=1e-14,
+                                        exact_guess=1 if learned else 0), 0)
+    ctx.set_autotune(False)  # same face kernel shape for both starts, no tuning inside the timed steps
+    if learned:
+        ctx.mlp_train()
+    sent = {}
+    hyd = [0.0]
+
+    def on_g(run, il, dt, dx):
+        t = time.perf_counter()
+        a = run.h.arrays()
+        if any(k not in sent or not np.array_equal(sent[k], a[k]) for k in ("son", "father", "nbor", "next", "headl")):
+            ctx.sync_topology(run.h.grid())
+            for k in ("son", "father", "nbor", "next", "headl"):
+                sent[k] = a[k].copy()
+        ctx.godunov_level_host(il, dt, dx, a["uold"], a["unew"])
+        hyd[0] += time.perf_counter() - t
+
+    r = AmrRun(h, lmin, lmax, 1.4, ed=0.1, ep=0.1, on_godunov=on_g)
+    r.initialize(sedov_ic(3, lmin))
+    r.coarse_step()  # warm-up step (plans, autotuner)
+    ctx.exact_stats(reset=True)
+    hyd[0] = 0.0
+    cu0 = r.cell_updates
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        r.coarse_step()
+    wall = time.perf_counter() - t0
+    iters, calls = ctx.exact_stats()
+    a = h.arrays()
+    out = {"guess": guess, "coarse_steps": steps, "wall_s": wall, "hydro_s": hyd[0],
+           "cell_updates": r.cell_updates - cu0, "hydro_cell_updates_per_s": (r.cell_updates - cu0) / hyd[0],
+           "iters_per_interface": iters / max(calls, 1), "interfaces": calls,
+           "digest": hashlib.sha1(a["uold"].tobytes()).hexdigest()}
+    ctx.close()
+    h.close()
+    return out
+
+
 def sod_sample(variant):
     """Config 1: 1D Sod, 1024 cells (reference levelmin=levelmax=11), MinMod +
     HLLC, reference CFL (courant 0.8; p <= 100 rho holds), to t = 0.245."""
@@ -626,6 +681,16 @@ def amr_report(steps):
                     "includes the level-sparse host<->device copies of every godunov_fine call"}
 
 
+def amr_exact_report(steps):
+    plain = run_sample("--amr-exact-sample", "plain", steps)
+    learned = run_sample("--amr-exact-sample", "learned", steps)
+    return {"workload": "3D Sedov AMR (levelmin 7, levelmax 10) with the exact solver in converged mode, tree "
+                        "maintenance by the reference, every godunov_fine on the GPU (rg_godunov_level_host)",
+            "plain": plain, "learned": learned,
+            "iteration_ratio": plain["iters_per_interface"] / max(learned["iters_per_interface"], 1e-30),
+            "same_state_bits": plain["digest"] == learned["digest"]}
+
+
 def sod_report():
     ref = run_sample("--sod-sample", "cpu")
     gpu = run_sample("--sod-sample", "gpu")
@@ -648,6 +713,7 @@ def main():
     ap.add_argument("--cpu-sample", nargs=2, type=int, metavar=("LEVEL", "STEPS"), help=argparse.SUPPRESS)
     ap.add_argument("--amr-sample", nargs=2, metavar=("VARIANT", "STEPS"), help=argparse.SUPPRESS)
     ap.add_argument("--sod-sample", metavar="VARIANT", help=argparse.SUPPRESS)
+    ap.add_argument("--amr-exact-sample", nargs=2, metavar=("GUESS", "STEPS"), help=argparse.SUPPRESS)
     ap.add_argument("--profile-case", choices=["learned"], help="small run for ncu captures (no timing output)")
     args = ap.parse_args()
     if args.cpu_sample:
@@ -658,6 +724,9 @@ def main():
         return
     if args.sod_sample:
         print(json.dumps(sod_sample(args.sod_sample)))
+        return
+    if args.amr_exact_sample:
+        print(json.dumps(amr_exact_sample(args.amr_exact_sample[0], int(args.amr_exact_sample[1]))))
         return
     if args.profile_case == "learned":
         profile_case_learned()
@@ -695,6 +764,8 @@ def main():
             out["ensemble"] = ens_out
             if world == 1:
                 out["amr"] = amr_report(3)
+                if "newton" in out:
+                    out["newton"]["amr_exact"] = amr_exact_report(3)
                 out["sod1d"] = sod_report()
     if world > 1:
         import torch.distributed as dist

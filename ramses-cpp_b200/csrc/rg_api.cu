@@ -71,12 +71,11 @@ namespace {
 template <typename T>
 int grow(rg_ctx* c, T** p, size_t* cap, size_t n, const char* what) {
     if (*cap >= n && *p) return RG_OK;
-    cudaFree(*p);
+    dev_free(c, *p);
     *p = nullptr;
     *cap = 0;
-    if (cudaMalloc((void**)p, sizeof(T) * (n ? n : 1)) != cudaSuccess) {
-        cudaGetLastError();
-        return set_error(c, RG_ERR_NOMEM, std::string("cudaMalloc failed: ") + what);
+    if (dev_alloc(c, (void**)p, sizeof(T) * (n ? n : 1)) != cudaSuccess) {
+        return set_error(c, RG_ERR_NOMEM, std::string("device allocation failed: ") + what);
     }
     *cap = n;
     return RG_OK;
@@ -102,7 +101,7 @@ int validate_params(rg_ctx* c, const rg_params* p) {
     } while (0)
 
 void invalidate_plans(rg_ctx* c) {
-    for (auto& p : c->plans) free_plan(p);
+    for (auto& p : c->plans) free_plan(c, p);
 }
 
 // dt of every box of an ensemble level (synchronises the stream)
@@ -124,11 +123,11 @@ int get_plan(rg_ctx* c, int ilevel, Plan** out) {
     Plan& p = c->plans[ilevel];
     if (!p.valid) {
         if (int rc = build_plan(c, ilevel, p)) {
-            free_plan(p);
+            free_plan(c, p);
             return rc;
         }
         if (int rc = build_lattice(c, p)) {
-            free_plan(p);
+            free_plan(c, p);
             return rc;
         }
         if ((int)c->tuned.size() > ilevel) {
@@ -166,6 +165,31 @@ void record_updates(rg_ctx* c, int ilevel, const Plan& P) {
 }  // namespace
 
 namespace rg {
+int create_pool(rg_ctx* c) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = c->device;
+    if (int rc = check_cuda(c, cudaMemPoolCreate(&c->pool, &props), "device memory pool")) return rc;
+    unsigned long long keep = ~0ULL;  // freed memory stays in the pool for the next plan
+    return check_cuda(c, cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep), "memory pool");
+}
+
+cudaError_t dev_alloc(rg_ctx* c, void** p, size_t bytes) {
+    *p = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, c->pool, c->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+    }
+    return e;
+}
+
+void dev_free(rg_ctx* c, void* p) {
+    if (p) cudaFreeAsync(p, c->stream);
+}
+
 void remember_shape(rg_ctx* c, const Plan& P) {
     if (P.ilevel < 0) return;
     if ((int)c->tuned.size() <= P.ilevel) c->tuned.resize((size_t)P.ilevel + 1);
@@ -209,13 +233,18 @@ rg_ctx* rg_create(const rg_params* params, int device) {
     if (check_cuda(c, cudaSetDevice(device), "cudaSetDevice") ||
         check_cuda(c, cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device), "SM count") ||
         check_cuda(c, cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking), "stream") ||
-        check_cuda(c, cudaMalloc(&c->d_status, sizeof(DevStatus)), "status") ||
-        check_cuda(c, cudaMallocHost(&c->h_status, sizeof(DevStatus)), "pinned status") ||
-        check_cuda(c, cudaMemset(c->d_status, 0, sizeof(DevStatus)), "status init")) {
+        create_pool(c)) {
         c->broken = true;
         return c;
     }
     c->stream = c->own_stream;
+    if (check_cuda(c, dev_alloc(c, &c->d_status, sizeof(DevStatus)), "status") ||
+        check_cuda(c, cudaMallocHost(&c->h_status, sizeof(DevStatus)), "pinned status") ||
+        check_cuda(c, cudaMemsetAsync(c->d_status, 0, sizeof(DevStatus), c->stream), "status init") ||
+        check_cuda(c, cudaStreamSynchronize(c->stream), "status init")) {
+        c->broken = true;
+        return c;
+    }
     for (auto& e : c->ev) cudaEventCreate(&e);
     const char* t = getenv("RG_TIMING");
     c->timing = t && t[0] == '1';
@@ -231,14 +260,16 @@ void rg_destroy(rg_ctx* c) {
         if (e) cudaEventDestroy(e);
     int* ip[] = {c->d_son, c->d_father, c->d_nbor, c->d_next, c->d_bound, c->d_jump, c->d_dist, c->d_jump2,
                  c->d_dist2, c->d_cell_level, c->d_cpos, c->d_tmap, c->d_pmark, c->d_scan};
-    for (int* p : ip) cudaFree(p);
-    cudaFree(c->d_uold);
-    cudaFree(c->d_unew);
-    cudaFree(c->d_prim);
-    cudaFree(c->d_flux);
-    cudaFree(c->d_mlp);
-    cudaFree(c->d_stage);
-    cudaFree(c->d_status);
+    for (int* p : ip) dev_free(c, p);
+    dev_free(c, c->d_uold);
+    dev_free(c, c->d_unew);
+    dev_free(c, c->d_prim);
+    dev_free(c, c->d_flux);
+    dev_free(c, c->d_mlp);
+    dev_free(c, c->d_stage);
+    dev_free(c, c->d_status);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->pool) cudaMemPoolDestroy(c->pool);
     if (c->h_status) cudaFreeHost(c->h_status);
     if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -325,10 +356,10 @@ int rg_sync_topology(rg_ctx* c, const rg_grid_view* g) {
     cap = c->cap_grid * 6;
     if (int rc = grow(c, &c->d_nbor, &cap, 6 * ngm, "nbor")) return rc;
     c->cap_grid = std::max(c->cap_grid, ngm);
-    cudaFree(c->d_bound);
+    dev_free(c, c->d_bound);
     c->d_bound = nullptr;
     if (c->nbound_type) {
-        if (check_cuda(c, cudaMalloc(&c->d_bound, sizeof(int) * c->nbound_type), "bound_type")) return RG_ERR_NOMEM;
+        if (check_cuda(c, dev_alloc(c, &c->d_bound, sizeof(int) * c->nbound_type), "bound_type")) return RG_ERR_NOMEM;
         cudaMemcpyAsync(c->d_bound, g->bound_type, sizeof(int) * c->nbound_type, cudaMemcpyHostToDevice, c->stream);
     }
     size_t nheadl = (size_t)(c->ncpu + c->nboundary) * (c->nlevelmax + 1);
@@ -582,9 +613,11 @@ int rg_level_substep_host(rg_ctx* c, int ilevel, double dx, int pressure_cap, do
         if (int rc = download_level_host(c, *P, unew, c->d_unew)) return rc;
     if (int rc = download_level_host(c, *P, uold, c->d_uold)) return rc;
     if (dt_used) {
-        if (int rc = check_cuda(c, cudaMemcpy(c->h_status, c->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost),
+        if (int rc = check_cuda(c, cudaMemcpyAsync(c->h_status, c->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                                                   c->stream),
                                 "dt copy"))
             return rc;
+        if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "dt copy")) return rc;
         *dt_used = c->h_status->dt;
     }
     return RG_OK;
@@ -610,20 +643,22 @@ int rg_set_level_boxes(rg_ctx* c, int ilevel, int nbox, const int* first_oct, co
         boxes[(size_t)b] = BoxStep{0ULL, 0.0, dx[b], 0.0, 0.0, 0, 0};
     }
     if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "boxes sync")) return rc;
-    cudaFree(P->obox);
-    cudaFree(P->boxes);
+    dev_free(c, P->obox);
+    dev_free(c, P->boxes);
     P->obox = nullptr;
     P->boxes = nullptr;
     P->nbox = 0;
-    if (int rc = check_cuda(c, cudaMalloc(&P->obox, obox.size() * sizeof(int)), "cudaMalloc(boxes)")) return rc;
-    if (int rc = check_cuda(c, cudaMalloc(&P->boxes, boxes.size() * sizeof(BoxStep)), "cudaMalloc(boxes)")) return rc;
-    if (int rc = check_cuda(c, cudaMemcpy(P->obox, obox.data(), obox.size() * sizeof(int), cudaMemcpyHostToDevice),
+    if (int rc = check_cuda(c, dev_alloc(c, &P->obox, obox.size() * sizeof(int)), "dev_alloc(c, boxes)")) return rc;
+    if (int rc = check_cuda(c, dev_alloc(c, &P->boxes, boxes.size() * sizeof(BoxStep)), "dev_alloc(c, boxes)")) return rc;
+    if (int rc = check_cuda(c, cudaMemcpyAsync(P->obox, obox.data(), obox.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                               c->stream),
                             "boxes upload"))
         return rc;
-    if (int rc = check_cuda(c, cudaMemcpy(P->boxes, boxes.data(), boxes.size() * sizeof(BoxStep),
-                                          cudaMemcpyHostToDevice),
+    if (int rc = check_cuda(c, cudaMemcpyAsync(P->boxes, boxes.data(), boxes.size() * sizeof(BoxStep),
+                                               cudaMemcpyHostToDevice, c->stream),
                             "boxes upload"))
         return rc;
+    if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "boxes upload")) return rc;
     P->nbox = nbox;
     if (P->graph) {
         cudaGraphExecDestroy(P->graph);

@@ -10,11 +10,17 @@
 // at its update targets (the level's cells and the coarser cells that
 // receive refluxes), and writes unew only at those targets.  So instead of
 // the whole state (2 x nvar x ncell doubles up, nvar x ncell down) a call
-// moves exactly those cells: as plain copies of their runs of consecutive
-// cell ids when there are few (a uniform level: one run per child slot), else
-// gathered on the host into pinned staging, one copy each way, scattered on
-// the device.
+// moves exactly those cells.  From page-locked host arrays whose level cells
+// form few runs of consecutive ids (a uniform level: one run per child slot)
+// each run is one DMA straight between the caller's array and the device
+// state.  Otherwise (pageable arrays, as AmrGrid's std::vectors are, or a
+// fragmented level) the cells are gathered on the host into pinned staging,
+// run by run where runs are long, moved in one copy each way and scattered on
+// the device: the driver stages a pageable copy through its own buffers with
+// a wait per row, so many small pageable copies would cost far more than the
+// host gather.
 #include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "rg_internal.cuh"
@@ -81,10 +87,10 @@ int grow_stage(rg_ctx* c, size_t doubles) {
         c->cap_hstage = doubles;
     }
     if (c->cap_dstage < doubles) {
-        cudaFree(c->d_stage);
+        dev_free(c, c->d_stage);
         c->d_stage = nullptr;
         c->cap_dstage = 0;
-        if (int rc = check_cuda(c, cudaMalloc(&c->d_stage, doubles * sizeof(double)), "device level staging"))
+        if (int rc = check_cuda(c, dev_alloc(c, &c->d_stage, doubles * sizeof(double)), "device level staging"))
             return rc;
         c->cap_dstage = doubles;
     }
@@ -98,9 +104,9 @@ int grow_stage(rg_ctx* c, size_t doubles) {
 int level_ids(rg_ctx* c, Plan& P) {
     if (P.ids_ready) return RG_OK;
     const int nread = P.ncells + P.nextra_prim;
-    cudaFree(P.read_ids);
+    dev_free(c, P.read_ids);
     P.read_ids = nullptr;
-    if (int rc = check_cuda(c, cudaMalloc(&P.read_ids, sizeof(int) * ((size_t)nread + P.ntarg + 1)), "level ids"))
+    if (int rc = check_cuda(c, dev_alloc(c, &P.read_ids, sizeof(int) * ((size_t)nread + P.ntarg + 1)), "level ids"))
         return rc;
     P.targ_ids = P.read_ids + nread;
     k_level_ids<<<blocks(c, std::max(nread, P.ntarg)), 256, 0, c->stream>>>(tree_view(c), P.view(), P.read_ids,
@@ -149,11 +155,66 @@ int copy_runs(rg_ctx* c, const std::vector<std::pair<int, int>>& runs, double* d
     }
     return RG_OK;
 }
+
+// true when the whole state array [nvar][ncell] at p is page-locked host memory
+bool state_pinned(rg_ctx* c, const double* p) {
+    const size_t n = (size_t)c->nvar * (size_t)c->ncell;
+    if (n == 0) return false;
+    for (const double* q : {p, p + (n - 1)}) {
+        cudaPointerAttributes a{};
+        if (cudaPointerGetAttributes(&a, q) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        if (a.type != cudaMemoryTypeHost) return false;
+    }
+    return true;
+}
+
+// dst[iv][t] = src[iv][ids[t] - 1] for the level's ids, by runs when they are
+// long on average, else cell by cell
+void gather_host(const std::vector<int>& ids, const std::vector<std::pair<int, int>>& runs, const double* src,
+                 size_t ncell, int nv, double* dst) {
+    const size_t n = ids.size();
+    const bool by_runs = runs.size() * 8 <= n;
+    for (int iv = 0; iv < nv; ++iv) {
+        const double* s = src + (size_t)iv * ncell;
+        double* d = dst + (size_t)iv * n;
+        if (by_runs) {
+            for (const auto& r : runs) {
+                std::memcpy(d, s + ((size_t)r.first - 1), sizeof(double) * (size_t)r.second);
+                d += r.second;
+            }
+        } else {
+            for (size_t t = 0; t < n; ++t) d[t] = s[ids[t] - 1];
+        }
+    }
+}
+
+// dst[iv][ids[t] - 1] = src[iv][t], the inverse of gather_host
+void scatter_host(const std::vector<int>& ids, const std::vector<std::pair<int, int>>& runs, const double* src,
+                  size_t ncell, int nv, double* dst) {
+    const size_t n = ids.size();
+    const bool by_runs = runs.size() * 8 <= n;
+    for (int iv = 0; iv < nv; ++iv) {
+        const double* s = src + (size_t)iv * n;
+        double* d = dst + (size_t)iv * ncell;
+        if (by_runs) {
+            for (const auto& r : runs) {
+                std::memcpy(d + ((size_t)r.first - 1), s, sizeof(double) * (size_t)r.second);
+                s += r.second;
+            }
+        } else {
+            for (size_t t = 0; t < n; ++t) d[ids[t] - 1] = s[t];
+        }
+    }
+}
 }  // namespace
 
 int upload_level_host(rg_ctx* c, Plan& P, const double* uold, const double* unew) {
     if (int rc = level_ids(c, P)) return rc;
-    if (P.read_runs.size() <= kMaxRuns && (!unew || P.targ_runs.size() <= kMaxRuns)) {
+    if (P.read_runs.size() <= kMaxRuns && (!unew || P.targ_runs.size() <= kMaxRuns) && state_pinned(c, uold) &&
+        (!unew || state_pinned(c, unew))) {
         if (int rc = copy_runs(c, P.read_runs, c->d_uold, uold, cudaMemcpyHostToDevice)) return rc;
         if (unew) return copy_runs(c, P.targ_runs, c->d_unew, unew, cudaMemcpyHostToDevice);
         return RG_OK;
@@ -166,17 +227,8 @@ int upload_level_host(rg_ctx* c, Plan& P, const double* uold, const double* unew
     // the previous call's download has completed (it synchronised), so the
     // pinned buffer is free to refill
     double* s = c->h_stage;
-    for (int iv = 0; iv < nv; ++iv) {
-        const double* src = uold + (size_t)iv * ncell;
-        double* dst = s + (size_t)iv * nread;
-        for (int t = 0; t < nread; ++t) dst[t] = src[P.h_read[(size_t)t] - 1];
-    }
-    double* sn = s + (size_t)nv * nread;
-    for (int iv = 0; iv < nv; ++iv) {
-        const double* src = unew + (size_t)iv * ncell;
-        double* dst = sn + (size_t)iv * ntarg;
-        for (int t = 0; t < ntarg; ++t) dst[t] = src[P.h_targ[(size_t)t] - 1];
-    }
+    gather_host(P.h_read, P.read_runs, uold, ncell, nv, s);
+    if (unew) gather_host(P.h_targ, P.targ_runs, unew, ncell, nv, s + (size_t)nv * nread);
     if (int rc = check_cuda(c, cudaMemcpyAsync(c->d_stage, s, n * sizeof(double), cudaMemcpyHostToDevice, c->stream),
                             "level upload"))
         return rc;
@@ -186,7 +238,7 @@ int upload_level_host(rg_ctx* c, Plan& P, const double* uold, const double* unew
 }
 
 int download_level_host(rg_ctx* c, Plan& P, double* unew, const double* src_dev) {
-    if (P.targ_runs.size() <= kMaxRuns) {
+    if (P.targ_runs.size() <= kMaxRuns && state_pinned(c, unew)) {
         if (int rc = copy_runs(c, P.targ_runs, unew, src_dev ? src_dev : c->d_unew, cudaMemcpyDeviceToHost)) return rc;
         return check_cuda(c, cudaStreamSynchronize(c->stream), "level download sync");
     }
@@ -202,11 +254,7 @@ int download_level_host(rg_ctx* c, Plan& P, double* unew, const double* src_dev)
                             "level download"))
         return rc;
     if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "level download sync")) return rc;
-    for (int iv = 0; iv < nv; ++iv) {
-        double* dst = unew + (size_t)iv * ncell;
-        const double* src = c->h_stage + (size_t)iv * ntarg;
-        for (int t = 0; t < ntarg; ++t) dst[P.h_targ[(size_t)t] - 1] = src[t];
-    }
+    scatter_host(P.h_targ, P.targ_runs, c->h_stage, ncell, nv, unew);
     return RG_OK;
 }
 

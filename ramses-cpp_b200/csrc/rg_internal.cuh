@@ -156,6 +156,7 @@ struct rg_ctx {
     int sm_count = 0;
     cudaStream_t stream = nullptr;      // stream in use
     cudaStream_t own_stream = nullptr;  // created by rg_create
+    cudaMemPool_t pool = nullptr;       // every device array of the context (dev_alloc)
     std::string err;
     bool broken = false;
 
@@ -212,7 +213,20 @@ int set_error(rg_ctx* c, int code, const std::string& msg);
 int check_cuda(rg_ctx* c, cudaError_t e, const char* what);
 int check_device_status(rg_ctx* c);  // synchronises
 int build_plan(rg_ctx* c, int ilevel, Plan& plan);
-void free_plan(Plan& plan);
+void free_plan(rg_ctx* c, Plan& plan);
+// Device arrays of a context come from its own stream-ordered memory pool:
+// allocated and freed in order on the context's stream, freed memory kept by
+// the pool for reuse.  Plans are rebuilt after every tree change; plain
+// cudaMalloc / cudaFree cost milliseconds per call (a free waits for the whole
+// device) with stalls of hundreds of milliseconds under that churn, the pool
+// microseconds.
+int create_pool(rg_ctx* c);
+cudaError_t dev_alloc(rg_ctx* c, void** p, size_t bytes);
+template <class T>
+cudaError_t dev_alloc(rg_ctx* c, T** p, size_t bytes) {
+    return dev_alloc(c, (void**)p, bytes);
+}
+void dev_free(rg_ctx* c, void* p);
 int rank_lists(rg_ctx* c);
 Plan* existing_plan(rg_ctx* c, int ilevel);  // built plan or nullptr; never builds
 int compute_cell_levels(rg_ctx* c);

@@ -171,17 +171,17 @@ int build_lattice(rg_ctx* c, Plan& P) {
     if (int rc = check_cuda(c, cudaMemcpyAsync(&kind0, P.kind, 1, cudaMemcpyDeviceToHost, c->stream), "lattice kind"))
         return rc;
     int* d_bad = nullptr;
-    if (int rc = check_cuda(c, cudaMalloc(&d_bad, sizeof(int)), "lattice flag")) return rc;
-    if (int rc = check_cuda(c, cudaMalloc(&P.lat_id, sizeof(int) * (size_t)P.ncells), "lattice ids")) return rc;
-    if (int rc = check_cuda(c, cudaMalloc(&P.lat_p, sizeof(int) * (size_t)P.ncells), "lattice positions")) return rc;
+    if (int rc = check_cuda(c, dev_alloc(c, &d_bad, sizeof(int)), "lattice flag")) return rc;
+    if (int rc = check_cuda(c, dev_alloc(c, &P.lat_id, sizeof(int) * (size_t)P.ncells), "lattice ids")) return rc;
+    if (int rc = check_cuda(c, dev_alloc(c, &P.lat_p, sizeof(int) * (size_t)P.ncells), "lattice positions")) return rc;
     cudaMemsetAsync(P.lat_p, 0xff, sizeof(int) * (size_t)P.ncells, c->stream);
     cudaMemsetAsync(d_bad, 0, sizeof(int), c->stream);
     if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "lattice kind sync")) return rc;
     const int kd = kind0;
     if ((kd & KIND_MASK) != K_GHOST && (kd & KIND_MASK) != K_SAME) {
-        cudaFree(d_bad);
-        cudaFree(P.lat_id);
-        cudaFree(P.lat_p);
+        dev_free(c, d_bad);
+        dev_free(c, P.lat_id);
+        dev_free(c, P.lat_p);
         P.lat_id = P.lat_p = nullptr;
         return RG_OK;
     }
@@ -193,11 +193,11 @@ int build_lattice(rg_ctx* c, Plan& P) {
     int bad = 1;
     cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
     const cudaError_t e = cudaStreamSynchronize(c->stream);
-    cudaFree(d_bad);
+    dev_free(c, d_bad);
     if (int rc = check_cuda(c, e, "lattice check")) return rc;
     if (bad) {
-        cudaFree(P.lat_id);
-        cudaFree(P.lat_p);
+        dev_free(c, P.lat_id);
+        dev_free(c, P.lat_p);
         P.lat_id = P.lat_p = nullptr;
         return RG_OK;
     }
@@ -228,26 +228,26 @@ int set_box_lattices(rg_ctx* c, Plan& P, const int* ext, const int* lat_id, cons
     int* d_bad = nullptr;
     int* d_seen = nullptr;
     auto fail = [&](int rc) {
-        cudaFree(d_bad);
-        cudaFree(d_seen);
-        cudaFree(P.lat_id);
-        cudaFree(P.lat_p);
-        cudaFree(P.bl_ext);
-        cudaFree(P.bl_off);
-        cudaFree(P.bl_brick_off);
+        dev_free(c, d_bad);
+        dev_free(c, d_seen);
+        dev_free(c, P.lat_id);
+        dev_free(c, P.lat_p);
+        dev_free(c, P.bl_ext);
+        dev_free(c, P.bl_off);
+        dev_free(c, P.bl_brick_off);
         P.lat_id = P.lat_p = P.bl_ext = P.bl_off = P.bl_brick_off = nullptr;
         P.box_lattice = 0;
         return rc;
     };
     fail(RG_OK);
     const size_t n = (size_t)P.ncells;
-    if (check_cuda(c, cudaMalloc(&d_bad, sizeof(int)), "box lattice flag") ||
-        check_cuda(c, cudaMalloc(&d_seen, sizeof(int) * n), "box lattice marks") ||
-        check_cuda(c, cudaMalloc(&P.lat_id, sizeof(int) * n), "box lattice ids") ||
-        check_cuda(c, cudaMalloc(&P.lat_p, sizeof(int) * n), "box lattice positions") ||
-        check_cuda(c, cudaMalloc(&P.bl_ext, sizeof(int) * hext.size()), "box lattice extents") ||
-        check_cuda(c, cudaMalloc(&P.bl_off, sizeof(int) * hoff.size()), "box lattice offsets") ||
-        check_cuda(c, cudaMalloc(&P.bl_brick_off, sizeof(int) * hbrick.size()), "box lattice bricks"))
+    if (check_cuda(c, dev_alloc(c, &d_bad, sizeof(int)), "box lattice flag") ||
+        check_cuda(c, dev_alloc(c, &d_seen, sizeof(int) * n), "box lattice marks") ||
+        check_cuda(c, dev_alloc(c, &P.lat_id, sizeof(int) * n), "box lattice ids") ||
+        check_cuda(c, dev_alloc(c, &P.lat_p, sizeof(int) * n), "box lattice positions") ||
+        check_cuda(c, dev_alloc(c, &P.bl_ext, sizeof(int) * hext.size()), "box lattice extents") ||
+        check_cuda(c, dev_alloc(c, &P.bl_off, sizeof(int) * hoff.size()), "box lattice offsets") ||
+        check_cuda(c, dev_alloc(c, &P.bl_brick_off, sizeof(int) * hbrick.size()), "box lattice bricks"))
         return fail(RG_ERR_NOMEM);
     cudaStream_t s = c->stream;
     cudaMemcpyAsync(&kind0, P.kind, 1, cudaMemcpyDeviceToHost, s);
@@ -266,8 +266,8 @@ int set_box_lattices(rg_ctx* c, Plan& P, const int* ext, const int* lat_id, cons
     int bad = 1;
     cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (int rc = check_cuda(c, cudaStreamSynchronize(s), "box lattice check")) return fail(rc);
-    cudaFree(d_bad);
-    cudaFree(d_seen);
+    dev_free(c, d_bad);
+    dev_free(c, d_seen);
     d_bad = d_seen = nullptr;
     if (bad) return fail(set_error(c, RG_ERR_ARG, "box lattices do not match the level's neighbours"));
     P.box_lattice = 1;

@@ -308,7 +308,7 @@ int launch_features(rg_ctx* c, int n, const double* ql, const double* qr, const 
 int mlp_ensure(rg_ctx* c) {
     if (c->d_mlp) return RG_OK;
     size_t bytes = sizeof(float) * (MLP_NPARAM + 3 * MLP_NTRAIN + 2);
-    if (cudaMalloc(&c->d_mlp, bytes) != cudaSuccess) {
+    if (dev_alloc(c, &c->d_mlp, bytes) != cudaSuccess) {
         cudaGetLastError();
         c->d_mlp = nullptr;
         return set_error(c, RG_ERR_NOMEM, "MLP parameters");
@@ -339,11 +339,11 @@ int mlp_train(rg_ctx* c, int nsamples, int epochs, int batch, float lr, unsigned
     float *X = nullptr, *T = nullptr;
     size_t n = (size_t)nsamples;
     auto cleanup = [&]() {
-        cudaFree(ql); cudaFree(qr); cudaFree(gam); cudaFree(ps); cudaFree(X); cudaFree(T);
+        dev_free(c, ql); dev_free(c, qr); dev_free(c, gam); dev_free(c, ps); dev_free(c, X); dev_free(c, T);
     };
-    if (cudaMalloc(&ql, sizeof(double) * nv * n) != cudaSuccess || cudaMalloc(&qr, sizeof(double) * nv * n) != cudaSuccess ||
-        cudaMalloc(&gam, sizeof(double) * n) != cudaSuccess || cudaMalloc(&ps, sizeof(double) * n) != cudaSuccess ||
-        cudaMalloc(&X, sizeof(float) * MLP_IN * n) != cudaSuccess || cudaMalloc(&T, sizeof(float) * n) != cudaSuccess) {
+    if (dev_alloc(c, &ql, sizeof(double) * nv * n) != cudaSuccess || dev_alloc(c, &qr, sizeof(double) * nv * n) != cudaSuccess ||
+        dev_alloc(c, &gam, sizeof(double) * n) != cudaSuccess || dev_alloc(c, &ps, sizeof(double) * n) != cudaSuccess ||
+        dev_alloc(c, &X, sizeof(float) * MLP_IN * n) != cudaSuccess || dev_alloc(c, &T, sizeof(float) * n) != cudaSuccess) {
         cudaGetLastError();
         cleanup();
         return set_error(c, RG_ERR_NOMEM, "training data");
@@ -421,10 +421,10 @@ int mlp_train(rg_ctx* c, int nsamples, int epochs, int batch, float lr, unsigned
 int mlp_grad(rg_ctx* c, int n, const float* x_host, const float* t_host, float* grad_host, float* loss_host) {
     if (int rc = mlp_ensure(c)) return rc;
     float *X = nullptr, *T = nullptr, *G = nullptr;
-    if (cudaMalloc(&X, sizeof(float) * MLP_IN * n) != cudaSuccess || cudaMalloc(&T, sizeof(float) * n) != cudaSuccess ||
-        cudaMalloc(&G, sizeof(float) * (MLP_NTRAIN + 1)) != cudaSuccess) {
+    if (dev_alloc(c, &X, sizeof(float) * MLP_IN * n) != cudaSuccess || dev_alloc(c, &T, sizeof(float) * n) != cudaSuccess ||
+        dev_alloc(c, &G, sizeof(float) * (MLP_NTRAIN + 1)) != cudaSuccess) {
         cudaGetLastError();
-        cudaFree(X); cudaFree(T); cudaFree(G);
+        dev_free(c, X); dev_free(c, T); dev_free(c, G);
         return set_error(c, RG_ERR_NOMEM, "gradient check buffers");
     }
     cudaMemcpyAsync(X, x_host, sizeof(float) * MLP_IN * n, cudaMemcpyHostToDevice, c->stream);
@@ -436,7 +436,7 @@ int mlp_grad(rg_ctx* c, int n, const float* x_host, const float* t_host, float* 
         cudaMemcpyAsync(loss_host, G + MLP_NTRAIN, sizeof(float), cudaMemcpyDeviceToHost, c->stream);
         rc = check_cuda(c, cudaStreamSynchronize(c->stream), "gradient check");
     }
-    cudaFree(X); cudaFree(T); cudaFree(G);
+    dev_free(c, X); dev_free(c, T); dev_free(c, G);
     return rc;
 }
 

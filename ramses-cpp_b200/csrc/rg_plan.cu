@@ -352,24 +352,24 @@ TreeView tree_view(const rg_ctx* c) {
                     c->d_son, c->d_father, c->d_nbor, c->d_bound, c->d_cell_level};
 }
 
-void free_plan(Plan& p) {
+void free_plan(rg_ctx* c, Plan& p) {
     if (p.graph) cudaGraphExecDestroy(p.graph);
-    cudaFree(p.octs);
-    cudaFree(p.icn);
-    cudaFree(p.stc);
-    cudaFree(p.kind);
-    cudaFree(p.toff);
-    cudaFree(p.tev);
-    cudaFree(p.textra);
-    cudaFree(p.xprim);
-    cudaFree(p.obox);
-    cudaFree(p.boxes);
-    cudaFree(p.read_ids);
-    cudaFree(p.lat_id);
-    cudaFree(p.lat_p);
-    cudaFree(p.bl_ext);
-    cudaFree(p.bl_off);
-    cudaFree(p.bl_brick_off);
+    dev_free(c, p.octs);
+    dev_free(c, p.icn);
+    dev_free(c, p.stc);
+    dev_free(c, p.kind);
+    dev_free(c, p.toff);
+    dev_free(c, p.tev);
+    dev_free(c, p.textra);
+    dev_free(c, p.xprim);
+    dev_free(c, p.obox);
+    dev_free(c, p.boxes);
+    dev_free(c, p.read_ids);
+    dev_free(c, p.lat_id);
+    dev_free(c, p.lat_p);
+    dev_free(c, p.bl_ext);
+    dev_free(c, p.bl_off);
+    dev_free(c, p.bl_brick_off);
     p = Plan();
 }
 
@@ -408,9 +408,9 @@ int exclusive_scan(rg_ctx* c, const int* in, int* out, int n, int* total) {
     if (nb < 1) nb = 1;
     size_t need = (size_t)nb + 1;
     if (c->cap_scan < need) {
-        cudaFree(c->d_scan);
+        dev_free(c, c->d_scan);
         c->d_scan = nullptr;
-        if (cudaMalloc(&c->d_scan, sizeof(int) * need) != cudaSuccess) return set_error(c, RG_ERR_NOMEM, "scan scratch");
+        if (dev_alloc(c, &c->d_scan, sizeof(int) * need) != cudaSuccess) return set_error(c, RG_ERR_NOMEM, "scan scratch");
         c->cap_scan = need;
     }
     k_scan_blocks<<<nb, SCAN_TPB, 0, c->stream>>>(in, out, n, c->d_scan);
@@ -425,9 +425,8 @@ int exclusive_scan(rg_ctx* c, const int* in, int* out, int n, int* total) {
 
 template <typename T>
 int dalloc(rg_ctx* c, T** p, size_t n, const char* what) {
-    if (cudaMalloc((void**)p, sizeof(T) * (n ? n : 1)) != cudaSuccess) {
-        cudaGetLastError();
-        return set_error(c, RG_ERR_NOMEM, std::string("cudaMalloc failed: ") + what);
+    if (dev_alloc(c, (void**)p, sizeof(T) * (n ? n : 1)) != cudaSuccess) {
+        return set_error(c, RG_ERR_NOMEM, std::string("device allocation failed: ") + what);
     }
     return RG_OK;
 }
@@ -437,7 +436,7 @@ int build_plan_t(rg_ctx* c, int ilevel, Plan& P) {
     constexpr int NS = 2 * NDIM, TTD = 1 << NDIM;
     cudaStream_t s = c->stream;
     TreeView T = tree_view(c);
-    free_plan(P);
+    free_plan(c, P);
     P.ilevel = ilevel;
     P.level0 = (ilevel == 0);
     int hv[4] = {0, 0, 0, 0};
@@ -462,7 +461,7 @@ int build_plan_t(rg_ctx* c, int ilevel, Plan& P) {
         if (int rc = dalloc(c, &P.octs, P.noct, "octs")) return rc;
         int* d_count = c->d_scan;  // reuse scan scratch as a counter
         if (c->cap_scan < 4) {
-            cudaFree(c->d_scan);
+            dev_free(c, c->d_scan);
             if (int rc = dalloc(c, &c->d_scan, 1024, "scan scratch")) return rc;
             c->cap_scan = 1024;
             d_count = c->d_scan;
@@ -498,7 +497,7 @@ int build_plan_t(rg_ctx* c, int ilevel, Plan& P) {
     int* d_nx = nullptr;  // [0] extra-prim count, [1] extra-target count
     int* d_xp = nullptr;
     int* d_textra = nullptr;
-    auto cleanup = [&]() { cudaFree(d_nx); cudaFree(d_xp); cudaFree(d_textra); };
+    auto cleanup = [&]() { dev_free(c, d_nx); dev_free(c, d_xp); dev_free(c, d_textra); };
     if (int rc = dalloc(c, &d_nx, 8, "plan counters")) return rc;
     if (int rc = dalloc(c, &d_xp, (size_t)c->ncell + 1, "xprim")) { cleanup(); return rc; }
     if (int rc = dalloc(c, &d_textra, (size_t)c->ncell + 1, "textra")) { cleanup(); return rc; }
