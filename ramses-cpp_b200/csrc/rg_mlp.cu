@@ -70,10 +70,12 @@ __device__ __forceinline__ float group_sum(float v) {  // over the 8 row groups 
 }
 
 // Loss and gradients of the batch [n0, n0+nb) (standardised X [IN][N] and T
-// [N]); gradients are summed into grad[NTRAIN], the squared error into *loss.
+// [N]).  Block b writes the sums over its samples to its own row
+// part[b][NTRAIN + 1] (gradients, then the squared error); k_grad_sum adds the
+// rows in block order.  No atomics: the gradient, hence the trained network
+// and every p* guess it makes, is the same bits on every run.
 __global__ void __launch_bounds__(TB) k_mlp_grad(const float* __restrict__ X, const float* __restrict__ T, int N,
-                                                 int n0, int nb, const float* __restrict__ w, float* grad,
-                                                 float* loss) {
+                                                 int n0, int nb, const float* __restrict__ w, float* part) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TrainSmem& S = *reinterpret_cast<TrainSmem*>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
@@ -245,14 +247,19 @@ __global__ void __launch_bounds__(TB) k_mlp_grad(const float* __restrict__ X, co
         }
         __syncthreads();
     }
-    // ---- flush
+    // ---- flush to this block's row: W1 / W2 entries belong to one thread each;
+    //      the per-warp sums of b1, b2, w3, b3 and the loss meet in shared
+    //      memory (free after the loop's last barrier) and are added in warp order
+    constexpr int NW = TB / 32;
+    float* row = part + (size_t)blockIdx.x * (MLP_NTRAIN + 1);
     {
         const int o = tid >> 1, half = tid & 1;
 #pragma unroll
-        for (int j = 0; j < 32; ++j) atomicAdd(&grad[MLP_W2 + o * MLP_H + half * 32 + j], acc_w2[j]);
+        for (int j = 0; j < 32; ++j) row[MLP_W2 + o * MLP_H + half * 32 + j] = acc_w2[j];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) atomicAdd(&grad[MLP_W1 + o * MLP_IN + half * 4 + k], acc_w1[k]);
+        for (int k = 0; k < 4; ++k) row[MLP_W1 + o * MLP_IN + half * 4 + k] = acc_w1[k];
     }
+    float* red = &S.dz2[0][0];  // [NW][3][H] column sums, then [NW][2] (loss, b3)
 #pragma unroll
     for (int nt = 0; nt < 8; ++nt)
 #pragma unroll
@@ -260,9 +267,9 @@ __global__ void __launch_bounds__(TB) k_mlp_grad(const float* __restrict__ X, co
             float a = group_sum(acc_db1[nt][e]), b = group_sum(acc_db2[nt][e]), c = group_sum(acc_dw3[nt][e]);
             if (g == 0) {
                 const int col = nt * 8 + 2 * t + e;
-                atomicAdd(&grad[MLP_B1 + col], a);
-                atomicAdd(&grad[MLP_B2 + col], b);
-                atomicAdd(&grad[MLP_W3 + col], c);
+                red[(warp * 3 + 0) * MLP_H + col] = a;
+                red[(warp * 3 + 1) * MLP_H + col] = b;
+                red[(warp * 3 + 2) * MLP_H + col] = c;
             }
         }
     float l = acc_loss, d3 = acc_db3;
@@ -271,8 +278,36 @@ __global__ void __launch_bounds__(TB) k_mlp_grad(const float* __restrict__ X, co
         d3 += __shfl_xor_sync(0xffffffffu, d3, off);
     }
     if (lane == 0) {
-        atomicAdd(loss, l);
-        atomicAdd(&grad[MLP_B3], d3);
+        red[NW * 3 * MLP_H + 2 * warp] = l;
+        red[NW * 3 * MLP_H + 2 * warp + 1] = d3;
+    }
+    __syncthreads();
+    for (int i = tid; i < 3 * MLP_H; i += TB) {
+        const int q = i / MLP_H, col = i % MLP_H;
+        float sum = 0.f;
+#pragma unroll
+        for (int wp = 0; wp < NW; ++wp) sum += red[(wp * 3 + q) * MLP_H + col];
+        row[(q == 0 ? MLP_B1 : (q == 1 ? MLP_B2 : MLP_W3)) + col] = sum;
+    }
+    if (tid == 0) {
+        float ls = 0.f, bs = 0.f;
+#pragma unroll
+        for (int wp = 0; wp < NW; ++wp) {
+            ls += red[NW * 3 * MLP_H + 2 * wp];
+            bs += red[NW * 3 * MLP_H + 2 * wp + 1];
+        }
+        row[MLP_B3] = bs;
+        row[MLP_NTRAIN] = ls;
+    }
+}
+
+// grad[p] += the blocks' rows summed in block order; column NTRAIN into *loss
+__global__ void k_grad_sum(const float* __restrict__ part, int nblk, float* grad, float* loss) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p <= MLP_NTRAIN; p += gridDim.x * blockDim.x) {
+        float sum = 0.f;
+        for (int b = 0; b < nblk; ++b) sum += part[(size_t)b * (MLP_NTRAIN + 1) + p];
+        if (p < MLP_NTRAIN) grad[p] += sum;
+        else *loss += sum;
     }
 }
 
@@ -305,9 +340,14 @@ int launch_stress_states(rg_ctx* c, int n, unsigned long long seed, double* ql, 
 int launch_features(rg_ctx* c, int n, const double* ql, const double* qr, const double* gam, const double* pstar,
                     float* X, float* T);
 
+// d_mlp: parameters [NPARAM], Adam moments m, v and the gradient [NTRAIN] each,
+// the loss, one spare float, then the gradient kernel's per-block rows
+// [sm_count][NTRAIN + 1]
+constexpr size_t kPartOffset = MLP_NPARAM + 3 * MLP_NTRAIN + 2;
+
 int mlp_ensure(rg_ctx* c) {
     if (c->d_mlp) return RG_OK;
-    size_t bytes = sizeof(float) * (MLP_NPARAM + 3 * MLP_NTRAIN + 2);
+    size_t bytes = sizeof(float) * (kPartOffset + (size_t)c->sm_count * (MLP_NTRAIN + 1));
     if (dev_alloc(c, &c->d_mlp, bytes) != cudaSuccess) {
         cudaGetLastError();
         c->d_mlp = nullptr;
@@ -325,7 +365,9 @@ static int grad_launch(rg_ctx* c, const float* X, const float* T, int N, int n0,
     }
     int tiles = (nb + SPB - 1) / SPB;
     int grid = tiles < c->sm_count ? tiles : c->sm_count;
-    k_mlp_grad<<<grid, TB, sizeof(TrainSmem), c->stream>>>(X, T, N, n0, nb, c->d_mlp, grad, loss);
+    float* part = c->d_mlp + kPartOffset;
+    k_mlp_grad<<<grid, TB, sizeof(TrainSmem), c->stream>>>(X, T, N, n0, nb, c->d_mlp, part);
+    k_grad_sum<<<(MLP_NTRAIN + 256) / 256, 256, 0, c->stream>>>(part, grid, grad, loss);
     return check_cuda(c, cudaGetLastError(), "MLP gradient kernel");
 }
 

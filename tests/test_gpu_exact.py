@@ -4,6 +4,8 @@
   workload: fluxes within 3e-12 (pow() differs by ulps between libm and CUDA);
 - the tensor-core training kernel's gradients against an FP64 CPU mirror of
   the same network with the same BF16 roundings;
+- training is reproducible: two contexts trained with the same seed hold the
+  same parameter bits (the gradient is reduced in a fixed order);
 - the learned start reaches the same converged root (|dp|/p <= 1e-13) with
   fewer Newton updates on the stress workload, and does not add updates
   where the two-shock start is already exact (the level step on Sedov).
@@ -122,6 +124,18 @@ def test_training_gradients_match_fp64_cpu(ctx):
         err = np.linalg.norm(gg - gc) / max(np.linalg.norm(gc), 1e-30)
         cos = gg @ gc / max(np.linalg.norm(gg) * np.linalg.norm(gc), 1e-30)
         assert err < 2e-2 and cos > 0.9995, f"{name}: rel err {err:.2e}, cosine {cos:.6f}"
+
+
+def test_training_is_reproducible(ctx):
+    ws = []
+    for _ in range(2):
+        c = rgpu.Context(rgpu.make_params(3, riemann="exact"), 0)
+        try:
+            c.mlp_train(nsamples=1 << 20, epochs=2, seed=9)
+            ws.append(c.mlp_get())
+        finally:
+            c.close()
+    assert np.array_equal(ws[0].view(np.int32), ws[1].view(np.int32))
 
 
 def test_learned_start_same_root_fewer_iterations(ctx):
