@@ -242,6 +242,8 @@ def gpu_arm(args, rank, world, local_rank):
     ctx.set_stream(stream.cuda_stream)
     ctx.sync_topology(g)
     ctx.upload_state(u0, u0)
+    if args.face_variant is not None:  # a fixed face-kernel shape instead of the autotuner's pick
+        ctx.set_face_config(L, args.face_variant, 1)
     dx = 1.0 / 2 ** L
     for _ in range(args.warmup):
         ctx.level_substep(L, dx, pressure_cap=False, use_graph=True)
@@ -708,6 +710,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--face-variant", type=int, default=None,
+                    help="face-kernel shape for the headline level (0-10) instead of the autotuner's pick; "
+                         "for profiler runs, whose serialised launches would skew the autotuner's timings")
     ap.add_argument("--no-newton", action="store_true", help="skip the exact-solver plain/learned report")
     ap.add_argument("--no-extra", action="store_true", help="skip the ensemble, AMR and Sod reports")
     ap.add_argument("--cpu-sample", nargs=2, type=int, metavar=("LEVEL", "STEPS"), help=argparse.SUPPRESS)
