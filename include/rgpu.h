@@ -304,6 +304,62 @@ int rg_face_config(rg_ctx* ctx, int ilevel, int* variant, int* batch, float* ms)
  * lattice; elsewhere those ids run the default shape). */
 int rg_set_face_config(rg_ctx* ctx, int ilevel, int variant, int batch);
 
+/* ---- device-resident tree maintenance (TreeUpdater on the GPU) -------------
+ * The reference rebuilds its AMR tree on the host between hydro steps
+ * (TreeUpdater, src/core/TreeUpdater.cpp:27-636).  After rg_tree_attach the
+ * tree lives on the device and these calls replace the TreeUpdater methods
+ * of the same names with the same arguments and the same results, bit for
+ * bit (flags, oct ids from the FIFO free list, level and free-list links,
+ * coordinates, prolonged and restricted states), so a whole coarse step
+ * (Simulation::amr_step, src/core/Simulation.cpp:522-635) runs without the
+ * host touching the tree.  Scope: 3D hydro (nvar 5), ncpu 1, no boundary
+ * patches, levels above the coarse level (ilevel >= 2; the coarse level is
+ * refined at initialisation, on the host); the free list does not grow
+ * (the reference doubles ngridmax when it runs out: RG_ERR_UNSUPPORTED
+ * here, attach with room to spare).  Not reproduced: the debug printf of
+ * each flagged cell (TreeUpdater.cpp:519). */
+typedef struct rg_tree_arrays {
+    int* son;      /* [ncell]      (rg_tree_fetch writes; attach reads the grid view's) */
+    int* father;   /* [ngridmax]                                                      */
+    int* nbor;     /* [6*ngridmax]                                                    */
+    int* next;     /* [ngridmax]                                                      */
+    int* prev;     /* [ngridmax]   AmrGrid::prev                                      */
+    int* headl;    /* [(ncpu+nboundary)*(nlevelmax+1)] headl_vec                      */
+    int* taill;    /* same shape: taill_vec                                           */
+    int* numbl;    /* same shape: numbl_vec                                           */
+    int* flag1;    /* [ncell]                                                         */
+    int* flag2;    /* [ncell]                                                         */
+    int* cpu_map;  /* [ncell]                                                         */
+    double* xg;    /* [3*ngridmax] oct centres                                        */
+    double* uold;  /* [nvar*ncell]                                                    */
+    double* unew;  /* [nvar*ncell]                                                    */
+    int headf, tailf, numbf; /* AmrGrid free list                                     */
+} rg_tree_arrays;
+/* Take over the tree: rg_sync_topology(g) plus the state and every other
+ * tree array of t (its son/father/nbor/next/headl are not read: the view's
+ * are).  levelmin: amr_params/levelmin, read by flag_fine.  A later
+ * rg_sync_topology hands the tree back to the host. */
+int rg_tree_attach(rg_ctx* ctx, const rg_grid_view* g, const rg_tree_arrays* t, int levelmin);
+/* Copy the device-resident tree and state back into t (NULL arrays are
+ * skipped); headf/tailf/numbf are filled in. */
+int rg_tree_fetch(rg_ctx* ctx, rg_tree_arrays* t);
+/* TreeUpdater::flag_fine (TreeUpdater.cpp:327-575) with its smooth_fine,
+ * test_flag and ensure_ref_rules; err_grad_b2 > 0 is RG_ERR_UNSUPPORTED
+ * (MHD only). */
+int rg_flag_fine(rg_ctx* ctx, int ilevel, double err_grad_d, double err_grad_p, double err_grad_u,
+                 double err_grad_b2, int nexpand, int icount, int nsubcycle);
+/* TreeUpdater::make_grid_fine (TreeUpdater.cpp:27-149): new octs for
+ * flagged unrefined cells of level ilevel, state prolonged by interpol_hydro
+ * (HydroSolver.cpp:734-876, params.interpol_var / interpol_type). */
+int rg_make_grid_fine(rg_ctx* ctx, int ilevel);
+/* TreeUpdater::remove_grid_fine (TreeUpdater.cpp:151-186). */
+int rg_remove_grid_fine(rg_ctx* ctx, int ilevel);
+/* TreeUpdater::restrict_fine (TreeUpdater.cpp:188-207): uold of level
+ * ilevel's refined cells from their children. */
+int rg_restrict_fine(rg_ctx* ctx, int ilevel);
+/* AmrGrid::count_grids_at_level (AmrGrid.cpp:304-308) of the resident tree. */
+int rg_count_grids(rg_ctx* ctx, int ilevel, int* n);
+
 #ifdef __cplusplus
 }
 #endif

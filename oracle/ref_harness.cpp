@@ -100,6 +100,8 @@ long long rh_get(void* hp, const char* name) {
     if (n == "nboundary") return g.nboundary;
     if (n == "nlevelmax") return g.nlevelmax;
     if (n == "numbf") return g.numbf;
+    if (n == "headf") return g.headf;
+    if (n == "tailf") return g.tailf;
     if (n == "headl_size") return (long long)g.headl_vec.size();
     return -1;
 }
@@ -116,6 +118,10 @@ void* rh_ptr(void* hp, const char* name) {
     if (n == "prev") return g.prev.data();
     if (n == "headl") return g.headl_vec.data();
     if (n == "flag1") return g.flag1.data();
+    if (n == "flag2") return g.flag2.data();
+    if (n == "cpu_map") return g.cpu_map.data();
+    if (n == "taill") return g.taill_vec.data();
+    if (n == "numbl") return g.numbl_vec.data();
     if (n == "xg") return g.xg.data();
     return nullptr;
 }

@@ -118,6 +118,7 @@ int box_dts(rg_ctx* c, const Plan& P, double* out) {
 
 int get_plan(rg_ctx* c, int ilevel, Plan** out) {
     if (!c->have_topology) return set_error(c, RG_ERR_STATE, "rg_sync_topology has not been called");
+    if (int rc = refresh_tree(c)) return rc;
     if (ilevel < 0 || ilevel > c->nlevelmax) return set_error(c, RG_ERR_ARG, "ilevel outside 0..nlevelmax");
     if ((int)c->plans.size() < c->nlevelmax + 1) c->plans.resize(c->nlevelmax + 1);
     Plan& p = c->plans[ilevel];
@@ -196,6 +197,17 @@ void remember_shape(rg_ctx* c, const Plan& P) {
     c->tuned[(size_t)P.ilevel] = TunedShape{P.face_variant, P.face_batch, P.ncells, P.face_ms};
 }
 
+int refresh_tree(rg_ctx* c) {
+    if (!c->tree_dirty) return RG_OK;
+    c->tree_dirty = false;
+    if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "tree refresh")) return rc;
+    invalidate_plans(c);
+    c->topo_version++;
+    if (int rc = rank_lists(c)) return rc;
+    if (int rc = compute_cell_levels(c)) return rc;
+    return check_device_status(c);
+}
+
 Plan* existing_plan(rg_ctx* c, int ilevel) {
     if (!c->have_topology || ilevel < 0 || ilevel >= (int)c->plans.size()) return nullptr;
     Plan& p = c->plans[ilevel];
@@ -268,6 +280,9 @@ void rg_destroy(rg_ctx* c) {
     dev_free(c, c->d_mlp);
     dev_free(c, c->d_stage);
     dev_free(c, c->d_status);
+    int* tp[] = {c->d_prev, c->d_flag1, c->d_flag2, c->d_cpu_map, c->d_fq, c->d_tscr};
+    for (int* p : tp) dev_free(c, p);
+    dev_free(c, c->d_xg);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->pool) cudaMemPoolDestroy(c->pool);
     if (c->h_status) cudaFreeHost(c->h_status);
@@ -303,6 +318,8 @@ int rg_set_params(rg_ctx* c, const rg_params* params) {
 int rg_sync_topology(rg_ctx* c, const rg_grid_view* g) {
     CTX_GUARD(c);
     c->next_level = -1;  // the state or the CFL word may change
+    c->tree_resident = false;  // the host's tree is the one in use from now on
+    c->tree_dirty = false;
     if (!g || !g->son || !g->father || !g->nbor || !g->next || !g->headl) return set_error(c, RG_ERR_ARG, "null grid array");
     if (g->ngridmax < 1 || g->ncoarse < 1 || g->nx < 1 || g->ny < 1 || g->nz < 1 || g->ncpu < 1 || g->nlevelmax < 1)
         return set_error(c, RG_ERR_ARG, "bad grid sizes");
@@ -896,6 +913,121 @@ int rg_last_kernel_ms(rg_ctx* c, float* out, int n) {
     CTX_GUARD(c);
     for (int i = 0; i < n && i < 3; ++i) out[i] = c->last_ms[i];
     return c->timing ? RG_OK : set_error(c, RG_ERR_STATE, "timing disabled (set RG_TIMING=1)");
+}
+
+/* ---- device-resident tree ---------------------------------------------- */
+int rg_tree_attach(rg_ctx* c, const rg_grid_view* g, const rg_tree_arrays* t, int levelmin) {
+    CTX_GUARD(c);
+    if (!g || !t) return set_error(c, RG_ERR_ARG, "grid view and tree arrays required");
+    if (c->params.ndim != 3 || c->params.nvar != 5)
+        return set_error(c, RG_ERR_UNSUPPORTED, "device tree operations need ndim 3 and nvar 5");
+    if (!t->prev || !t->taill || !t->numbl || !t->flag1 || !t->flag2 || !t->cpu_map || !t->xg || !t->uold || !t->unew)
+        return set_error(c, RG_ERR_ARG, "null tree array");
+    if (int rc = rg_sync_topology(c, g)) return rc;
+    if (int rc = rg_upload_state(c, t->uold, t->unew)) return rc;
+    const size_t ngm = (size_t)c->ngridmax, nc = (size_t)c->ncell, nh = c->h_headl.size();
+    int** ip[] = {&c->d_prev, &c->d_fq, &c->d_flag1, &c->d_flag2, &c->d_cpu_map};
+    const size_t isz[] = {ngm, ngm, nc, nc, nc};
+    for (int i = 0; i < 5; ++i) {
+        dev_free(c, *ip[i]);
+        *ip[i] = nullptr;
+        if (int rc = check_cuda(c, dev_alloc(c, ip[i], sizeof(int) * isz[i]), "tree arrays")) return rc;
+    }
+    dev_free(c, c->d_xg);
+    c->d_xg = nullptr;
+    if (int rc = check_cuda(c, dev_alloc(c, &c->d_xg, sizeof(double) * 3 * ngm), "tree coordinates")) return rc;
+    // the free list, walked from its head, becomes the ring's initial content
+    if (t->numbf < 0 || (size_t)t->numbf > ngm) return set_error(c, RG_ERR_TOPOLOGY, "numbf out of range");
+    c->h_fq.assign(ngm, 0);
+    int g_at = t->headf, n = 0, last = 0;
+    while (g_at > 0 && n < t->numbf) {
+        if ((size_t)g_at > ngm) return set_error(c, RG_ERR_TOPOLOGY, "free list entry out of range");
+        c->h_fq[(size_t)n++] = g_at;
+        last = g_at;
+        g_at = g->next[g_at - 1];
+    }
+    if (n != t->numbf || g_at != 0 || last != t->tailf)
+        return set_error(c, RG_ERR_TOPOLOGY, "free list (headf, next, tailf, numbf) is inconsistent");
+    c->fq_head = 0;
+    c->numbf = n;
+    c->h_taill.assign(t->taill, t->taill + nh);
+    c->h_numbl.assign(t->numbl, t->numbl + nh);
+    c->levelmin = levelmin;
+    cudaStream_t s = c->stream;
+    cudaMemcpyAsync(c->d_prev, t->prev, sizeof(int) * ngm, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(c->d_fq, c->h_fq.data(), sizeof(int) * ngm, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(c->d_flag1, t->flag1, sizeof(int) * nc, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(c->d_flag2, t->flag2, sizeof(int) * nc, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(c->d_cpu_map, t->cpu_map, sizeof(int) * nc, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(c->d_xg, t->xg, sizeof(double) * 3 * ngm, cudaMemcpyHostToDevice, s);
+    if (int rc = check_cuda(c, cudaStreamSynchronize(s), "tree upload")) return rc;
+    c->tree_resident = true;
+    c->tree_dirty = false;
+    return RG_OK;
+}
+
+int rg_tree_fetch(rg_ctx* c, rg_tree_arrays* t) {
+    CTX_GUARD(c);
+    if (!c->tree_resident) return set_error(c, RG_ERR_STATE, "no device-resident tree");
+    if (!t) return set_error(c, RG_ERR_ARG, "tree arrays required");
+    const size_t ngm = (size_t)c->ngridmax, nc = (size_t)c->ncell, nh = c->h_headl.size();
+    const size_t ns = (size_t)c->nvar * nc;
+    cudaStream_t s = c->stream;
+    struct {
+        void* dst;
+        const void* src;
+        size_t bytes;
+    } cp[] = {{t->son, c->d_son, sizeof(int) * nc},        {t->father, c->d_father, sizeof(int) * ngm},
+              {t->nbor, c->d_nbor, sizeof(int) * 6 * ngm}, {t->next, c->d_next, sizeof(int) * ngm},
+              {t->prev, c->d_prev, sizeof(int) * ngm},     {t->flag1, c->d_flag1, sizeof(int) * nc},
+              {t->flag2, c->d_flag2, sizeof(int) * nc},    {t->cpu_map, c->d_cpu_map, sizeof(int) * nc},
+              {t->xg, c->d_xg, sizeof(double) * 3 * ngm},  {t->uold, c->d_uold, sizeof(double) * ns},
+              {t->unew, c->d_unew, sizeof(double) * ns}};
+    for (auto& e : cp)
+        if (e.dst)
+            if (int rc = check_cuda(c, cudaMemcpyAsync(e.dst, e.src, e.bytes, cudaMemcpyDeviceToHost, s), "tree fetch"))
+                return rc;
+    if (int rc = check_cuda(c, cudaStreamSynchronize(s), "tree fetch")) return rc;
+    if (t->headl) std::copy(c->h_headl.begin(), c->h_headl.end(), t->headl);
+    if (t->taill) std::copy(c->h_taill.begin(), c->h_taill.end(), t->taill);
+    if (t->numbl) std::copy(c->h_numbl.begin(), c->h_numbl.end(), t->numbl);
+    (void)nh;
+    const int ngmi = c->ngridmax;
+    t->numbf = c->numbf;
+    t->headf = c->numbf > 0 ? c->h_fq[(size_t)c->fq_head] : 0;
+    t->tailf = c->numbf > 0 ? c->h_fq[(size_t)((c->fq_head + c->numbf - 1) % ngmi)] : 0;
+    return RG_OK;
+}
+
+int rg_flag_fine(rg_ctx* c, int ilevel, double err_grad_d, double err_grad_p, double err_grad_u, double err_grad_b2,
+                 int nexpand, int icount, int nsubcycle) {
+    CTX_GUARD(c);
+    return tree_flag_fine(c, ilevel, err_grad_d, err_grad_p, err_grad_u, err_grad_b2, nexpand, icount, nsubcycle);
+}
+
+int rg_make_grid_fine(rg_ctx* c, int ilevel) {
+    CTX_GUARD(c);
+    return tree_make_grid_fine(c, ilevel);
+}
+
+int rg_remove_grid_fine(rg_ctx* c, int ilevel) {
+    CTX_GUARD(c);
+    return tree_remove_grid_fine(c, ilevel);
+}
+
+int rg_restrict_fine(rg_ctx* c, int ilevel) {
+    CTX_GUARD(c);
+    return tree_restrict_fine(c, ilevel);
+}
+
+int rg_count_grids(rg_ctx* c, int ilevel, int* n) {
+    CTX_GUARD(c);
+    if (!n) return set_error(c, RG_ERR_ARG, "n is NULL");
+    if (!c->tree_resident) return set_error(c, RG_ERR_STATE, "no device-resident tree");
+    *n = 0;
+    if (ilevel < 0 || ilevel > c->nlevelmax) return RG_OK;  // AmrGrid::numbl returns 0 out of range
+    *n = c->h_numbl[(size_t)ilevel * (c->ncpu + c->nboundary)];
+    return RG_OK;
 }
 
 }  // extern "C"

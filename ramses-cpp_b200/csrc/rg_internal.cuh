@@ -205,6 +205,19 @@ struct rg_ctx {
     float* d_mlp = nullptr;  // learned Newton start: parameters + Adam state
     bool mlp_valid = false;
     std::vector<long long> cell_updates;
+
+    // device-resident tree (rg_tree_attach, rg_tree.cu): the arrays only the
+    // tree operations need, the free list as a FIFO ring of oct ids (device
+    // d_fq, host mirror h_fq, entries fq_head .. fq_head + numbf - 1 modulo
+    // ngridmax) and the level lists' tails and counts (heads: h_headl)
+    int *d_prev = nullptr, *d_flag1 = nullptr, *d_flag2 = nullptr, *d_cpu_map = nullptr, *d_fq = nullptr;
+    double* d_xg = nullptr;
+    int* d_tscr = nullptr;  // tree-operation scratch
+    size_t cap_tscr = 0;
+    std::vector<int> h_taill, h_numbl, h_fq;
+    int fq_head = 0, numbf = 0, levelmin = 1;
+    bool tree_resident = false;
+    bool tree_dirty = false;  // links changed on the device: ranks, cell levels and plans are stale
 };
 
 namespace rg {
@@ -228,6 +241,20 @@ cudaError_t dev_alloc(rg_ctx* c, T** p, size_t bytes) {
 }
 void dev_free(rg_ctx* c, void* p);
 int rank_lists(rg_ctx* c);
+// Exclusive scan of n ints on the context stream; *total gets the sum (synchronises).
+int exclusive_scan(rg_ctx* c, const int* in, int* out, int n, int* total);
+// Octs of level list `ilevel` in linked-list order, from the list ranks, into the
+// device array out[cap]; *noct gets the count (synchronises).
+int level_oct_list(rg_ctx* c, int ilevel, int* out, int cap, int* noct);
+// after device tree operations changed links: drop plans, re-rank the lists,
+// recompute cell levels (no-op when nothing changed)
+int refresh_tree(rg_ctx* c);
+// TreeUpdater operations on the device-resident tree (rg_tree.cu)
+int tree_flag_fine(rg_ctx* c, int ilevel, double ed, double ep, double ev, double eb2, int nexp, int icount,
+                   int nsub);
+int tree_make_grid_fine(rg_ctx* c, int ilevel);
+int tree_remove_grid_fine(rg_ctx* c, int ilevel);
+int tree_restrict_fine(rg_ctx* c, int ilevel);
 Plan* existing_plan(rg_ctx* c, int ilevel);  // built plan or nullptr; never builds
 int compute_cell_levels(rg_ctx* c);
 // step launchers (enqueue only)

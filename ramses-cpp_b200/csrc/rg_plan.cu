@@ -11,6 +11,7 @@
 #include <cstdio>
 
 #include "rg_internal.cuh"
+#include "rg_nav.cuh"
 
 namespace rg {
 
@@ -18,53 +19,6 @@ namespace {
 
 constexpr int TPB = 256;
 inline int nblk(long long n, int tpb = TPB) { return (int)std::max(1LL, std::min((n + tpb - 1) / tpb, 1LL << 30)); }
-
-__device__ __forceinline__ void raise_err(DevStatus* st, int code, int info) {
-    if (atomicCAS(&st->err, 0, code) == 0) st->info = info;
-}
-
-__device__ __forceinline__ int coarse_nbor(const TreeView& T, int icell, int idim, int side) {
-    if (icell <= 0 || icell > T.ncoarse) return 0;
-    int nx = T.nx, ny = T.ny, nz = T.nz;
-    int idx = icell - 1;
-    int iz = idx / (nx * ny), rem = idx % (nx * ny);
-    int iy = rem / nx, ix = rem % nx;
-    int c0 = ix, c1 = iy, c2 = iz;
-    int d = (side == 0) ? -1 : 1;
-    if (idim == 0) c0 = (c0 + d + nx) % nx;
-    else if (idim == 1) c1 = (c1 + d + ny) % ny;
-    else c2 = (c2 + d + nz) % nz;
-    return c2 * nx * ny + c1 * nx + c0 + 1;
-}
-
-// AmrGrid::get_nbor_cells for one direction; the recursion through the father
-// oct (AmrGrid.cpp:429-440) becomes a bounded loop.
-__device__ int nbor_cell_dir(const TreeView& T, int igrid, int ic, int idim, int side, DevStatus* st) {
-    for (int depth = 0; depth < 64; ++depth) {
-        int bit = ((ic - 1) >> idim) & 1;
-        int ig_idx = (side == 0) ? (bit ? 0 : 2 * idim + 1) : (bit ? 2 * idim + 2 : 0);
-        int ic_pos = ((ic - 1) ^ (1 << idim)) + 1;
-        int ig;
-        if (ig_idx == 0) {
-            ig = igrid;
-        } else {
-            int v = T.nbor[(size_t)(ig_idx - 1) * T.ngridmax + igrid - 1];
-            ig = (v > T.ncell) ? 0 : v;
-        }
-        if (ig > 0) {
-            if (ig_idx == 0) return T.ncoarse + (ic_pos - 1) * T.ngridmax + ig;
-            int ch = (ig <= T.ncell) ? T.son[ig - 1] : 0;
-            return (ch > 0) ? T.ncoarse + (ic_pos - 1) * T.ngridmax + ch : ig;
-        }
-        if (ig < 0) return ig;
-        int ifather = T.father[igrid - 1];
-        if (ifather <= T.ncoarse) return coarse_nbor(T, ifather, idim, side);
-        igrid = ((ifather - T.ncoarse - 1) % T.ngridmax) + 1;
-        ic = ((ifather - T.ncoarse - 1) / T.ngridmax) + 1;
-    }
-    raise_err(st, DE_NBOR_DEPTH, igrid);
-    return 0;
-}
 
 // Neighbour of an arbitrary cell id, as the ghost branch looks it up
 // (HydroSolver.cpp:179-187).
@@ -402,26 +356,6 @@ int compute_cell_levels(rg_ctx* c) {
 
 namespace {
 
-// Exclusive scan of n ints on the context stream; returns the grand total.
-int exclusive_scan(rg_ctx* c, const int* in, int* out, int n, int* total) {
-    int nb = (n + SCAN_ITEMS - 1) / SCAN_ITEMS;
-    if (nb < 1) nb = 1;
-    size_t need = (size_t)nb + 1;
-    if (c->cap_scan < need) {
-        dev_free(c, c->d_scan);
-        c->d_scan = nullptr;
-        if (dev_alloc(c, &c->d_scan, sizeof(int) * need) != cudaSuccess) return set_error(c, RG_ERR_NOMEM, "scan scratch");
-        c->cap_scan = need;
-    }
-    k_scan_blocks<<<nb, SCAN_TPB, 0, c->stream>>>(in, out, n, c->d_scan);
-    k_scan_sums<<<1, SCAN_TPB, 0, c->stream>>>(c->d_scan, nb, c->d_scan + nb);
-    k_scan_add<<<nb, SCAN_TPB, 0, c->stream>>>(out, n, c->d_scan);
-    if (int rc = check_cuda(c, cudaGetLastError(), "scan")) return rc;
-    if (int rc = check_cuda(c, cudaMemcpyAsync(total, c->d_scan + nb, sizeof(int), cudaMemcpyDeviceToHost, c->stream),
-                            "scan total"))
-        return rc;
-    return check_cuda(c, cudaStreamSynchronize(c->stream), "scan sync");
-}
 
 template <typename T>
 int dalloc(rg_ctx* c, T** p, size_t n, const char* what) {
@@ -546,6 +480,56 @@ int build_plan(rg_ctx* c, int ilevel, Plan& plan) {
         case 3: return build_plan_t<3>(c, ilevel, plan);
         default: return set_error(c, RG_ERR_UNSUPPORTED, "ndim must be 1 or 3");
     }
+}
+
+// Exclusive scan of n ints on the context stream; returns the grand total.
+int exclusive_scan(rg_ctx* c, const int* in, int* out, int n, int* total) {
+    int nb = (n + SCAN_ITEMS - 1) / SCAN_ITEMS;
+    if (nb < 1) nb = 1;
+    size_t need = (size_t)nb + 1;
+    if (c->cap_scan < need) {
+        dev_free(c, c->d_scan);
+        c->d_scan = nullptr;
+        if (dev_alloc(c, &c->d_scan, sizeof(int) * need) != cudaSuccess) return set_error(c, RG_ERR_NOMEM, "scan scratch");
+        c->cap_scan = need;
+    }
+    k_scan_blocks<<<nb, SCAN_TPB, 0, c->stream>>>(in, out, n, c->d_scan);
+    k_scan_sums<<<1, SCAN_TPB, 0, c->stream>>>(c->d_scan, nb, c->d_scan + nb);
+    k_scan_add<<<nb, SCAN_TPB, 0, c->stream>>>(out, n, c->d_scan);
+    if (int rc = check_cuda(c, cudaGetLastError(), "scan")) return rc;
+    if (int rc = check_cuda(c, cudaMemcpyAsync(total, c->d_scan + nb, sizeof(int), cudaMemcpyDeviceToHost, c->stream),
+                            "scan total"))
+        return rc;
+    return check_cuda(c, cudaStreamSynchronize(c->stream), "scan sync");
+}
+
+int level_oct_list(rg_ctx* c, int ilevel, int* out, int cap, int* noct) {
+    *noct = 0;
+    if (ilevel < 1 || ilevel > c->nlevelmax) return set_error(c, RG_ERR_ARG, "level outside 1..nlevelmax");
+    const int head = c->h_headl[(size_t)ilevel * (c->ncpu + c->nboundary)];
+    if (head > c->ngridmax || head < 0) return set_error(c, RG_ERR_TOPOLOGY, "headl entry out of range");
+    if (head == 0) return RG_OK;
+    cudaStream_t s = c->stream;
+    int dh = 0, count = 0;
+    if (int rc = check_cuda(c, cudaMemcpyAsync(&dh, c->d_dist + head - 1, sizeof(int), cudaMemcpyDeviceToHost, s),
+                            "list length"))
+        return rc;
+    if (int rc = check_cuda(c, cudaStreamSynchronize(s), "list length sync")) return rc;
+    const int n = dh + 1;
+    if (n > cap) return set_error(c, RG_ERR_TOPOLOGY, "level list longer than ngridmax");
+    if (c->cap_scan < 4) {
+        dev_free(c, c->d_scan);
+        if (int rc = dalloc(c, &c->d_scan, 1024, "scan scratch")) return rc;
+        c->cap_scan = 1024;
+    }
+    cudaMemsetAsync(c->d_scan, 0, sizeof(int), s);
+    k_level_octs<<<nblk(c->ngridmax), TPB, 0, s>>>(c->ngridmax, c->d_jump, c->d_dist, head - 1, n, out, c->d_scan,
+                                                   c->d_status);
+    cudaMemcpyAsync(&count, c->d_scan, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (int rc = check_cuda(c, cudaStreamSynchronize(s), "level octs")) return rc;
+    if (count != n) return set_error(c, RG_ERR_TOPOLOGY, "level linked list merges with another chain");
+    *noct = n;
+    return RG_OK;
 }
 
 }  // namespace rg

@@ -1,0 +1,751 @@
+// rg_tree.cu -- AMR tree maintenance on the device (TreeUpdater on the GPU).
+//
+// The reference (RAMSES-CPP) rebuilds its tree on the host between hydro
+// steps: TreeUpdater::flag_fine, smooth_fine, test_flag, ensure_ref_rules,
+// make_grid_fine, remove_grid_fine and restrict_fine
+// (src/core/TreeUpdater.cpp:27-636), with the oct free list and level lists of
+// AmrGrid (src/core/AmrGrid.cpp:259-302), the coordinate lookups of
+// get_27_cell_neighbors (:474-511) and the prolongation interpol_hydro
+// (src/solvers/hydro/HydroSolver.cpp:734-876).  Here the tree stays in device
+// memory for a whole run and every one of those operations is a few kernels
+// over the level's octs; the host keeps only the list heads, tails and counts
+// and a mirror of the free list's order.
+//
+// Every loop of the reference that looks sequential is one of two kinds:
+//   - per cell or per oct with disjoint writes (flags, gradients, restriction,
+//     nesting rules, the new octs' neighbours and interpolated states): the
+//     writes of one iteration never feed a later iteration's reads, so one
+//     thread per cell or oct gives the same bits;
+//   - order-carrying (which oct id a refined cell gets, the level and free
+//     lists' links): the reference walks cells in list order, pops ids from
+//     the head of the FIFO free list and appends to list tails, so the k-th
+//     refined cell in list order gets the k-th free id and the lists end up
+//     as the compacted sequences; an exclusive scan over the list order
+//     reproduces both.
+// Scope: refinement of levels above the coarse level (the coarse level,
+// ilevel 1 in the reference's numbering, is refined at initialisation on the
+// host; below levelmin its flags are all set, which is handled), ncpu == 1,
+// nvar == ndim + 2 = 5 and no boundary patches, as on the rest of this path;
+// the free list never grows (the reference doubles ngridmax when it runs
+// out, here that is an error).
+// The per-flagged-cell printf of flag_fine (TreeUpdater.cpp:519) is not
+// reproduced: it writes to stdout and changes no state.
+#include <algorithm>
+#include <vector>
+
+#include "rg_face.cuh"
+#include "rg_nav.cuh"
+
+namespace rg {
+
+namespace {
+
+constexpr int TPB = 256;
+inline int nblk(long long n) { return (int)std::max(1LL, std::min((n + TPB - 1) / TPB, 1LL << 30)); }
+
+struct TreeMut {
+    int ncoarse, ngridmax, ncell;
+    int* son;
+    int* father;
+    int* nbor;
+    int* next;
+    int* prev;
+    int* flag1;
+    int* flag2;
+    int* cpu_map;
+    double* xg;
+    double* uold;
+    double* unew;
+};
+
+TreeMut tree_mut(rg_ctx* c) {
+    return TreeMut{c->ncoarse, c->ngridmax, c->ncell, c->d_son, c->d_father, c->d_nbor, c->d_next, c->d_prev,
+                   c->d_flag1, c->d_flag2, c->d_cpu_map, c->d_xg, c->d_uold, c->d_unew};
+}
+
+// cell id (1-based) of position p = icx * noct + k of a level's cells
+__device__ __forceinline__ int lvl_cell(const TreeMut& M, const int* octs, int noct, int p) {
+    const int icx = p / noct, k = p - icx * noct;
+    return M.ncoarse + icx * M.ngridmax + octs[k];
+}
+
+// AmrGrid::get_nbor_cells_exact (AmrGrid.cpp:449-472) for one direction: the
+// neighbour cell at the same level, or 0 when that oct does not exist
+__device__ __forceinline__ int nbor_exact_dir(const TreeMut& M, int igrid, int ic, int idim, int side) {
+    const int bit = ((ic - 1) >> idim) & 1;
+    const int ig_idx = (side == 0) ? (bit ? 0 : 2 * idim + 1) : (bit ? 2 * idim + 2 : 0);
+    const int ic_pos = ((ic - 1) ^ (1 << idim)) + 1;
+    if (ig_idx == 0) return M.ncoarse + (ic_pos - 1) * M.ngridmax + igrid;
+    int ig = M.nbor[(size_t)(ig_idx - 1) * M.ngridmax + igrid - 1];
+    if (ig > M.ncell) ig = 0;  // get_nbor_grids (AmrGrid.cpp:389-400)
+    if (ig <= 0) return 0;
+    const int ch = M.son[ig - 1];
+    return ch > 0 ? M.ncoarse + (ic_pos - 1) * M.ngridmax + ch : 0;
+}
+
+// ---------------------------------------------------------------- flag_fine
+// TreeUpdater.cpp:414-446: reset, then keep cells whose son oct has a
+// refined or flagged cell (always flag below levelmin)
+__global__ void k_flag_init(TreeMut M, const int* __restrict__ octs, int noct, int below_min) {
+    const int n = 8 * noct;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const int idc = lvl_cell(M, octs, noct, p) - 1;
+        int f = 0;
+        if (below_min) {
+            f = 1;
+        } else {
+            const int ch = M.son[idc];
+            if (ch > 0)
+                for (int s = 0; s < 8; ++s) {
+                    const int ids = M.ncoarse + s * M.ngridmax + ch - 1;
+                    if (M.son[ids] > 0 || M.flag1[ids] == 1) {
+                        f = 1;
+                        break;
+                    }
+                }
+        }
+        M.flag1[idc] = f;
+    }
+}
+
+// smooth_fine (TreeUpdater.cpp:211-259): unflagged cells with a flagged
+// same-level neighbour; marks first, then applied (the reference's ok_flag)
+__global__ void k_smooth_mark(TreeMut M, const int* __restrict__ octs, int noct, int* ok) {
+    const int n = 8 * noct;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const int icx = p / noct, k = p - icx * noct, ig = octs[k], ic = icx + 1;
+        const int idc = M.ncoarse + icx * M.ngridmax + ig - 1;
+        int o = 0;
+        if (M.flag1[idc] == 0) {
+            int nf = 0;
+            for (int s = 0; s < 6; ++s) {
+                const int nc = nbor_exact_dir(M, ig, ic, s >> 1, s & 1);
+                if (nc > 0 && nc <= M.ncell && M.flag1[nc - 1] == 1) ++nf;
+            }
+            o = nf > 0;
+        }
+        ok[p] = o;
+    }
+}
+
+__global__ void k_smooth_apply(TreeMut M, const int* __restrict__ octs, int noct, const int* __restrict__ ok) {
+    const int n = 8 * noct;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+        if (ok[p] == 1) M.flag1[lvl_cell(M, octs, noct, p) - 1] = 1;
+}
+
+struct CellState {
+    double d, v[3], p;
+};
+
+// get_cell_state of flag_fine (TreeUpdater.cpp:346-385), hydro variables, no
+// non-thermal energies
+__device__ __forceinline__ CellState cell_state(const TreeMut& M, int cell, double gamma) {
+    CellState s{};
+    const size_t nc = (size_t)M.ncell, i = (size_t)cell - 1;
+    s.d = smax(M.uold[i], 1e-10);
+    double v2 = 0.0;
+#pragma unroll
+    for (int idim = 0; idim < 3; ++idim) {
+        s.v[idim] = M.uold[(size_t)(2 + idim - 1) * nc + i] / s.d;
+        v2 = v2 + s.v[idim] * s.v[idim];
+    }
+    const double ek = 0.5 * s.d * v2;
+    const double em = 0.0, e_nonthermal = 0.0;
+    const double e_tot = M.uold[(size_t)4 * nc + i];
+    s.p = smax((e_tot - ek - em - e_nonthermal) * (gamma - 1.0), s.d * 1e-10);
+    return s;
+}
+
+__device__ __forceinline__ double err_grad(double l, double c, double r, double floor_val) {
+    return 2.0 * smax(fabs(r - c) / (r + c + floor_val), fabs(c - l) / (c + l + floor_val));
+}
+
+__device__ __forceinline__ double err_grad_u(double vl, double vc, double vr, double pl, double pc, double pr,
+                                             double dl, double dc, double dr, double gamma) {
+    const double floor_val = 1e-10;
+    const double cg = sqrt(smax(gamma * pl / dl, floor_val * floor_val));
+    const double cm = sqrt(smax(gamma * pc / dc, floor_val * floor_val));
+    const double cd = sqrt(smax(gamma * pr / dr, floor_val * floor_val));
+    return 2.0 * smax(fabs(vr - vc) / (cd + cm + fabs(vr) + fabs(vc) + floor_val),
+                      fabs(vc - vl) / (cm + cg + fabs(vc) + fabs(vl) + floor_val));
+}
+
+// gradient criteria (TreeUpdater.cpp:491-535), 3D hydro: density, pressure,
+// velocity (no magnetic energy on the hydro path)
+__global__ void k_flag_grad(TreeMut M, const int* __restrict__ octs, int noct, double ed, double ep, double ev,
+                            double gamma) {
+    const int n = 8 * noct;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const int icx = p / noct, k = p - icx * noct, ig = octs[k], ic = icx + 1;
+        const int idc = M.ncoarse + icx * M.ngridmax + ig - 1;
+        if (M.flag1[idc] != 0) continue;
+        const CellState sc = cell_state(M, idc + 1, gamma);
+        bool ok = false;
+        for (int idim = 0; idim < 3 && !ok; ++idim) {
+            int id_l = nbor_exact_dir(M, ig, ic, idim, 0);
+            if (id_l == 0) id_l = M.nbor[(size_t)(2 * idim) * M.ngridmax + ig - 1];
+            int id_r = nbor_exact_dir(M, ig, ic, idim, 1);
+            if (id_r == 0) id_r = M.nbor[(size_t)(2 * idim + 1) * M.ngridmax + ig - 1];
+            const CellState sl = (id_l > 0 && id_l <= M.ncell) ? cell_state(M, id_l, gamma) : sc;
+            const CellState sr = (id_r > 0 && id_r <= M.ncell) ? cell_state(M, id_r, gamma) : sc;
+            if (ed > 0.0 && err_grad(sl.d, sc.d, sr.d, 1e-10) > ed) ok = true;
+            else if (ep > 0.0 && err_grad(sl.p, sc.p, sr.p, 1e-10) > ep) ok = true;
+            else if (ev > 0.0 && err_grad_u(sl.v[idim], sc.v[idim], sr.v[idim], sl.p, sc.p, sr.p, sl.d, sc.d, sr.d,
+                                            gamma) > ev)
+                ok = true;
+        }
+        if (ok) M.flag1[idc] = 1;
+    }
+}
+
+// test_flag (TreeUpdater.cpp:263-307): cells whose son oct has a refined or
+// flagged cell stay flagged
+__global__ void k_test_flag(TreeMut M, const int* __restrict__ octs, int noct) {
+    const int n = 8 * noct;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const int idc = lvl_cell(M, octs, noct, p) - 1;
+        const int ch = M.son[idc];
+        if (ch <= 0) continue;
+        for (int s = 0; s < 8; ++s) {
+            const int ids = M.ncoarse + s * M.ngridmax + ch - 1;
+            if (M.son[ids] > 0 || M.flag1[ids] == 1) {
+                M.flag1[idc] = 1;
+                break;
+            }
+        }
+    }
+}
+
+// AmrGrid::get_cell_level (AmrGrid.hpp:69-80)
+__device__ __forceinline__ int cell_level(const TreeMut& M, int icell) {
+    if (icell <= M.ncoarse) return 0;
+    int cur = ((icell - M.ncoarse - 1) % M.ngridmax) + 1;
+    int level = 1;
+    for (int guard = 0; guard < 64 && cur > 0; ++guard) {
+        const int fc = M.father[cur - 1];
+        if (fc <= M.ncoarse) break;
+        cur = ((fc - M.ncoarse - 1) % M.ngridmax) + 1;
+        ++level;
+    }
+    return level;
+}
+
+struct Geo {
+    int nx, ny, nz;
+    double boxlen;
+};
+
+// AmrGrid::get_cell_center (AmrGrid.cpp:331-365), 3D
+__device__ void cell_center(const TreeMut& M, const Geo& G, int icell, double* xc) {
+    xc[0] = 0.5 * G.boxlen;
+    xc[1] = 0.5 * G.boxlen;
+    xc[2] = 0.5 * G.boxlen;
+    if (icell <= M.ncoarse) {
+        int idx = icell - 1;
+        const int iz = idx / (G.nx * G.ny);
+        idx %= (G.nx * G.ny);
+        const int iy = idx / G.nx, ix = idx % G.nx;
+        const double dxc = G.boxlen / (double)max(G.nx, max(G.ny, G.nz));
+        xc[0] = (ix + 0.5) * dxc;
+        xc[1] = (iy + 0.5) * dxc;
+        xc[2] = (iz + 0.5) * dxc;
+        return;
+    }
+    const int ig = ((icell - M.ncoarse - 1) % M.ngridmax) + 1;
+    const int idc = (icell - M.ncoarse - 1) / M.ngridmax;
+    const int ixyz[3] = {idc & 1, (idc & 2) >> 1, (idc & 4) >> 2};
+    const int level = cell_level(M, icell);
+    const double dx = G.boxlen / (double)(G.nx * (1 << level));
+    const double scale = G.boxlen / (double)G.nx;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) xc[d] = M.xg[(size_t)d * M.ngridmax + ig - 1] * scale + (double)(ixyz[d] - 0.5) * dx;
+}
+
+// AmrGrid::find_cell_by_coords (AmrGrid.cpp:367-387), 3D
+__device__ int cell_at(const TreeMut& M, const Geo& G, const double* x, int level) {
+    const double dxc = G.boxlen / (double)max(G.nx, max(G.ny, G.nz));
+    const int ix = min(max((int)(x[0] / dxc), 0), G.nx - 1);
+    const int iy = min(max((int)(x[1] / dxc), 0), G.ny - 1);
+    const int iz = min(max((int)(x[2] / dxc), 0), G.nz - 1);
+    int cur = iz * G.nx * G.ny + iy * G.nx + ix + 1;
+    const double scale = G.boxlen / (double)G.nx;
+    for (int lev = 1; lev <= level && M.son[cur - 1] > 0; ++lev) {
+        const int ig = M.son[cur - 1];
+        const int ixc = x[0] > M.xg[ig - 1] * scale ? 1 : 0;
+        const int iyc = x[1] > M.xg[(size_t)M.ngridmax + ig - 1] * scale ? 1 : 0;
+        const int izc = x[2] > M.xg[(size_t)2 * M.ngridmax + ig - 1] * scale ? 1 : 0;
+        const int ic = izc * 4 + iyc * 2 + ixc + 1;
+        cur = M.ncoarse + (ic - 1) * M.ngridmax + ig;
+    }
+    return cur;
+}
+
+// ensure_ref_rules (TreeUpdater.cpp:578-634): an oct stays flagged only when
+// all 27 cells around its father exist at the father's level and are refined
+// (get_27_cell_neighbors, AmrGrid.cpp:474-511, by coordinates)
+__global__ void k_ensure_ref_rules(TreeMut M, Geo G, const int* __restrict__ octs, int noct) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < noct; k += gridDim.x * blockDim.x) {
+        const int ig = octs[k];
+        const int fc = M.father[ig - 1];
+        bool ok = fc > 0;
+        if (ok && fc > M.ncell) ok = false;  // get_27_cell_neighbors returns no neighbours
+        if (ok) {
+            const int level = cell_level(M, fc);
+            double xc[3];
+            cell_center(M, G, fc, xc);
+            const double dxl = G.boxlen / (double)(G.nx * (1 << level));
+            for (int dz = -1; dz <= 1 && ok; ++dz)
+                for (int dy = -1; dy <= 1 && ok; ++dy)
+                    for (int dx = -1; dx <= 1 && ok; ++dx) {
+                        double x[3] = {xc[0], xc[1], xc[2]};
+                        x[0] += dx * dxl;
+                        x[1] += dy * dxl;
+                        x[2] += dz * dxl;
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) {
+                            if (x[d] < 0.0) x[d] += G.boxlen;
+                            else if (x[d] >= G.boxlen) x[d] -= G.boxlen;
+                        }
+                        const int nb = cell_at(M, G, x, level);
+                        if (cell_level(M, nb) != level || M.son[nb - 1] == 0) ok = false;
+                    }
+        }
+        if (!ok)
+            for (int s = 0; s < 8; ++s) M.flag1[M.ncoarse + s * M.ngridmax + ig - 1] = 0;
+    }
+}
+
+// flag_fine on the coarse level below levelmin (TreeUpdater.cpp:396-413): every
+// coarse cell flagged and owned by this process
+__global__ void k_flag_coarse_below_min(TreeMut M) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M.ncoarse; i += gridDim.x * blockDim.x) {
+        M.cpu_map[i] = 1;
+        M.flag1[i] = 1;
+    }
+}
+
+// make_grid_fine(1) candidates (TreeUpdater.cpp:33-41): counted only; refining
+// the coarse level is left to the host
+__global__ void k_coarse_candidates(TreeMut M, int* count) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M.ncoarse; i += gridDim.x * blockDim.x)
+        if (M.flag1[i] == 1 && M.flag2[i] == 1 && M.son[i] == 0) atomicAdd(count, 1);
+}
+
+// ---------------------------------------------------------------- make_grid_fine
+__global__ void k_authorize(TreeMut M) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M.ncell; i += gridDim.x * blockDim.x)
+        M.flag2[i] = (M.cpu_map[i] == 1) ? 1 : 0;
+}
+
+// candidates in the reference's order: octs in list order, child slots inside
+__global__ void k_refine_mark(TreeMut M, const int* __restrict__ octs, int noct, int* mark) {
+    const int n = 8 * noct;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const int k = q >> 3, icx = q & 7;
+        const int idc = M.ncoarse + icx * M.ngridmax + octs[k] - 1;
+        mark[q] = (M.flag1[idc] == 1 && M.flag2[idc] == 1 && M.son[idc] == 0) ? 1 : 0;
+    }
+}
+
+// interpol_hydro (HydroSolver.cpp:734-876), 3D, no non-thermal energies or
+// passive scalars, no barotropic EOS
+__device__ void interpol_3d(const double u1[7][5], double u2[8][5], int interpol_var, int interpol_type, double gam,
+                            double smalle) {
+    constexpr int NV = 5;
+    double q1[7][NV], q2[8][NV];
+    if (interpol_var == 0) {
+        for (int i = 0; i < 7; ++i)
+            for (int iv = 0; iv < NV; ++iv) q1[i][iv] = u1[i][iv];
+    } else if (interpol_var == 1) {
+        for (int i = 0; i < 7; ++i) {
+            const double d = smax(u1[i][0], 1e-10);
+            q1[i][0] = u1[i][0];
+            double e_kin = 0.0;
+            for (int idim = 1; idim <= 3; ++idim) {
+                q1[i][idim] = u1[i][idim];
+                e_kin = e_kin + 0.5 * u1[i][idim] * u1[i][idim] / d;
+            }
+            const double e_nonthermal = 0.0;
+            q1[i][4] = u1[i][4] - e_kin - e_nonthermal;
+        }
+    } else {
+        for (int i = 0; i < 7; ++i) ctoprim<3>(u1[i], q1[i], gam, smalle);
+    }
+    for (int iv = 0; iv < NV; ++iv) {
+        double slopes[3] = {0.0, 0.0, 0.0};
+        for (int idim = 0; idim < 3; ++idim) {
+            const double dlft = q1[0][iv] - q1[2 * idim + 1][iv];
+            const double drgt = q1[2 * idim + 2][iv] - q1[0][iv];
+            if (dlft * drgt > 0.0) {
+                const double sgn = (dlft >= 0.0) ? 1.0 : -1.0;
+                int itype = interpol_type;
+                if (interpol_type == 4) itype = (interpol_var == 2 && iv >= 1 && iv <= 3) ? 3 : 2;
+                if (itype == 1) slopes[idim] = sgn * 0.5 * smin(fabs(dlft), fabs(drgt));
+                else if (itype == 2) slopes[idim] = sgn * smin3(fabs(dlft), fabs(drgt), 0.25 * fabs(dlft + drgt));
+                else if (itype == 3) slopes[idim] = 0.25 * (dlft + drgt);
+                else slopes[idim] = 0.0;
+            }
+        }
+        for (int i = 0; i < 8; ++i) {
+            const int ix = i & 1, iy = (i & 2) >> 1, iz = (i & 4) >> 2;
+            q2[i][iv] = q1[0][iv] + (ix - 0.5) * slopes[0] + (iy - 0.5) * slopes[1] + (iz - 0.5) * slopes[2];
+        }
+    }
+    if (interpol_var == 0) {
+        for (int i = 0; i < 8; ++i)
+            for (int iv = 0; iv < NV; ++iv) u2[i][iv] = q2[i][iv];
+    } else if (interpol_var == 1) {
+        for (int i = 0; i < 8; ++i) {
+            const double d = smax(q2[i][0], 1e-10);
+            u2[i][0] = d;
+            double e_kin = 0.0;
+            for (int idim = 1; idim <= 3; ++idim) {
+                u2[i][idim] = q2[i][idim];
+                e_kin = e_kin + 0.5 * q2[i][idim] * q2[i][idim] / d;
+            }
+            const double e_nonthermal = 0.0;
+            u2[i][4] = q2[i][4] + e_kin + e_nonthermal;
+        }
+    } else {
+        const double oneover_n2d = 1.0 / 8;
+        for (int di = 1; di <= 3; ++di) {
+            double mom_sum = 0.0;
+            for (int i = 0; i < 8; ++i) mom_sum = mom_sum + q2[i][0] * q2[i][di] * oneover_n2d;
+            const double mom_err = mom_sum - u1[0][di];
+            for (int i = 0; i < 8; ++i) {
+                const double d = smax(q2[i][0], 1e-10);
+                q2[i][di] = (d * q2[i][di] - mom_err) / d;
+            }
+        }
+        for (int i = 0; i < 8; ++i) {
+            const double d = smax(q2[i][0], 1e-10);
+            const double p = smax(q2[i][4], 1e-20);
+            u2[i][0] = d;
+            double v2 = 0.0;
+            for (int di = 1; di <= 3; ++di) {
+                u2[i][di] = d * q2[i][di];
+                v2 = v2 + q2[i][di] * q2[i][di];
+            }
+            const double e_thermal = p / (gam - 1.0), e_kinetic = 0.5 * d * v2, e_nonthermal = 0.0;
+            u2[i][4] = e_thermal + e_kinetic + e_nonthermal;
+        }
+    }
+}
+
+// one refined cell: its new oct (the j-th free id), links to father and
+// neighbours, coordinates, prolonged state (TreeUpdater.cpp:76-149)
+__global__ void k_refine(TreeMut M, TreeView T, Geo G, const int* __restrict__ octs, int noct,
+                         const int* __restrict__ mark, const int* __restrict__ rank, const int* __restrict__ fq,
+                         int fq_head, int ilevel, int interpol_var, int interpol_type, double gamma, double smalle,
+                         const int* __restrict__ bound_type, int nbound_type, int* newlist, DevStatus* st) {
+    const int n = 8 * noct;
+    const size_t nc = (size_t)M.ncell;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        if (!mark[q]) continue;
+        const int k = q >> 3, icx = q & 7, ig = octs[k], ic = icx + 1;
+        const int idc = M.ncoarse + icx * M.ngridmax + ig - 1;
+        const int j = rank[q];
+        const int new_ig = fq[(int)(((long long)fq_head + j) % M.ngridmax)];
+        newlist[j] = new_ig;
+        M.son[idc] = new_ig;
+        M.father[new_ig - 1] = idc + 1;
+        int icn[6];
+#pragma unroll
+        for (int s = 0; s < 6; ++s) {
+            icn[s] = nbor_cell_dir(T, ig, ic, s >> 1, s & 1, st);
+            M.nbor[(size_t)s * M.ngridmax + new_ig - 1] = icn[s];
+        }
+        const double dx_level = 1.0 / (double)(1 << (ilevel - 1));
+        const int ixyz[3] = {icx & 1, (icx & 2) >> 1, (icx & 4) >> 2};
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            M.xg[(size_t)d * M.ngridmax + new_ig - 1] =
+                M.xg[(size_t)d * M.ngridmax + ig - 1] + (double)(ixyz[d] - 0.5) * dx_level;
+        double u1[7][5], u2[8][5];
+        for (int iv = 0; iv < 5; ++iv) u1[0][iv] = M.uold[(size_t)iv * nc + idc];
+        for (int i = 1; i <= 6; ++i) {
+            const int id_n = icn[i - 1];
+            if (id_n > 0) {
+                for (int iv = 0; iv < 5; ++iv) u1[i][iv] = M.uold[(size_t)iv * nc + id_n - 1];
+            } else {
+                for (int iv = 0; iv < 5; ++iv) u1[i][iv] = u1[0][iv];
+                const int ib = -id_n;
+                if (ib > 0 && ib <= nbound_type && bound_type[ib - 1] == 1) {
+                    const int idim = (i - 1) / 2;
+                    u1[i][1 + idim] *= -1.0;
+                }
+            }
+        }
+        interpol_3d(u1, u2, interpol_var, interpol_type, gamma, smalle);
+        for (int isc = 0; isc < 8; ++isc) {
+            const size_t child = (size_t)M.ncoarse + (size_t)isc * M.ngridmax + new_ig - 1;
+            for (int iv = 0; iv < 5; ++iv) {
+                M.uold[(size_t)iv * nc + child] = u2[isc][iv];
+                M.unew[(size_t)iv * nc + child] = u2[isc][iv];
+            }
+            M.cpu_map[child] = 1;
+        }
+    }
+}
+
+// links of list[0..n) chained in order after `before` (0: a list of its own):
+// add_to_level_list (AmrGrid.cpp:289-302) and the free list's tail pushes
+// (free_grid, :282-284)
+__global__ void k_link_chain(int* next, int* prev, const int* __restrict__ list, int n, int before) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const int g = list[j];
+        prev[g - 1] = j > 0 ? list[j - 1] : before;
+        next[g - 1] = j + 1 < n ? list[j + 1] : 0;
+        if (j == 0 && before > 0) next[before - 1] = g;
+    }
+}
+
+// ---------------------------------------------------------------- remove_grid_fine
+__global__ void k_kill_mark(TreeMut M, const int* __restrict__ octs, int noct, int* mark) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < noct; k += gridDim.x * blockDim.x) {
+        const int ig = octs[k];
+        const int fc = M.father[ig - 1];
+        int rm = 0;
+        if (fc > 0 && M.flag1[fc - 1] == 0) {
+            rm = 1;
+            for (int s = 0; s < 8; ++s)
+                if (M.son[M.ncoarse + s * M.ngridmax + ig - 1] > 0) {
+                    rm = 0;
+                    break;
+                }
+        }
+        mark[k] = rm;
+    }
+}
+
+// unlink and free the marked octs (TreeUpdater.cpp:164-181, free_grid
+// AmrGrid.cpp:270-287): compacted kept list, freed ids in list order, the
+// freed ids appended to the free-list ring
+__global__ void k_kill(TreeMut M, const int* __restrict__ octs, int noct, const int* __restrict__ mark,
+                       const int* __restrict__ rank, int* kept, int* freed, int* fq, int fq_tail) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < noct; k += gridDim.x * blockDim.x) {
+        const int ig = octs[k];
+        const int r = rank[k];
+        if (!mark[k]) {
+            kept[k - r] = ig;
+            continue;
+        }
+        freed[r] = ig;
+        fq[(int)(((long long)fq_tail + r) % M.ngridmax)] = ig;
+        for (int s = 0; s < 6; ++s) M.nbor[(size_t)s * M.ngridmax + ig - 1] = 0;
+        const int fc = M.father[ig - 1];
+        if (fc > 0) M.son[fc - 1] = 0;
+        M.father[ig - 1] = 0;
+        for (int s = 0; s < 8; ++s) {
+            const int idc = M.ncoarse + s * M.ngridmax + ig - 1;
+            M.son[idc] = 0;
+            M.flag1[idc] = 0;
+            M.flag2[idc] = 0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- restrict_fine
+// father = mean of its 8 children, summed in child order (TreeUpdater.cpp:188-207)
+__global__ void k_restrict(TreeMut M, const int* __restrict__ octs, int noct) {
+    const size_t nc = (size_t)M.ncell;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < noct; k += gridDim.x * blockDim.x) {
+        const int ig = octs[k];
+        const int fc = M.father[ig - 1];
+        if (fc <= 0) continue;
+        for (int iv = 0; iv < 5; ++iv) {
+            double sum = 0;
+            for (int s = 0; s < 8; ++s) sum += M.uold[(size_t)iv * nc + M.ncoarse + (size_t)s * M.ngridmax + ig - 1];
+            M.uold[(size_t)iv * nc + fc - 1] = sum / 8;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- host side
+int hidx(const rg_ctx* c, int ilevel) { return ilevel * (c->ncpu + c->nboundary); }
+
+// RG_OK to go on, a negative value when the call is a no-op (ilevel >= nlevelmax,
+// where the reference returns at once), else an error code
+int check_tree(rg_ctx* c, int ilevel) {
+    if (!c->tree_resident) return set_error(c, RG_ERR_STATE, "no device-resident tree: call rg_tree_attach first");
+    if (ilevel >= c->nlevelmax) return -1;
+    if (ilevel < 1) return set_error(c, RG_ERR_ARG, "level below 1");
+    c->next_level = -1;  // the state or the topology may change
+    return refresh_tree(c);
+}
+
+// scratch carved from one pool allocation: [octs ngm][mark 8ngm+1][rank 8ngm+1][list ngm][list2 ngm]
+struct TreeScratch {
+    int *octs, *mark, *rank, *list, *list2;
+};
+
+int tree_scratch(rg_ctx* c, TreeScratch* s) {
+    const size_t ngm = (size_t)c->ngridmax, need = 20 * ngm + 16;
+    if (c->cap_tscr < need) {
+        dev_free(c, c->d_tscr);
+        c->d_tscr = nullptr;
+        c->cap_tscr = 0;
+        if (int rc = check_cuda(c, dev_alloc(c, &c->d_tscr, need * sizeof(int)), "tree scratch")) return rc;
+        c->cap_tscr = need;
+    }
+    s->octs = c->d_tscr;
+    s->mark = s->octs + ngm;
+    s->rank = s->mark + 8 * ngm + 1;
+    s->list = s->rank + 8 * ngm + 1;
+    s->list2 = s->list + ngm;
+    return RG_OK;
+}
+
+int set_dev_int(rg_ctx* c, int* dst, int v) {
+    // synchronous: the value lives on this stack frame
+    if (int rc = check_cuda(c, cudaMemcpyAsync(dst, &v, sizeof(int), cudaMemcpyHostToDevice, c->stream), "tree link"))
+        return rc;
+    return check_cuda(c, cudaStreamSynchronize(c->stream), "tree link");
+}
+
+}  // namespace
+
+int tree_flag_fine(rg_ctx* c, int ilevel, double ed, double ep, double ev, double eb2, int nexp, int icount,
+                   int nsub) {
+    if (int rc = check_tree(c, ilevel)) return rc < 0 ? RG_OK : rc;  // no-op at and above nlevelmax (TreeUpdater.cpp:329)
+    if (eb2 > 0.0) return set_error(c, RG_ERR_UNSUPPORTED, "err_grad_b2 needs MHD variables");
+    TreeMut M = tree_mut(c);
+    cudaStream_t s = c->stream;
+    const int lmin = c->levelmin;
+    if (ilevel == 1) {
+        // below levelmin every coarse cell ends flagged, and smoothing a fully
+        // flagged level changes nothing; refinement criteria on the coarse
+        // level itself are not covered here
+        if (ilevel >= lmin)
+            return set_error(c, RG_ERR_UNSUPPORTED, "coarse-level refinement criteria (levelmin 1) stay on the host");
+        k_flag_coarse_below_min<<<nblk(c->ncoarse), TPB, 0, s>>>(M);
+        return check_cuda(c, cudaGetLastError(), "coarse flags");
+    }
+    TreeScratch S;
+    if (int rc = tree_scratch(c, &S)) return rc;
+    int noct = 0;
+    if (int rc = level_oct_list(c, ilevel, S.octs, c->ngridmax, &noct)) return rc;
+    if (noct == 0) return RG_OK;
+    const int n = 8 * noct;
+    auto smooth = [&]() {
+        k_smooth_mark<<<nblk(n), TPB, 0, s>>>(M, S.octs, noct, S.mark);
+        k_smooth_apply<<<nblk(n), TPB, 0, s>>>(M, S.octs, noct, S.mark);
+    };
+    k_flag_init<<<nblk(n), TPB, 0, s>>>(M, S.octs, noct, ilevel < lmin ? 1 : 0);
+    if (ilevel >= lmin) smooth();
+    if (ilevel >= lmin && (ed > 0.0 || ep > 0.0 || ev > 0.0))
+        k_flag_grad<<<nblk(n), TPB, 0, s>>>(M, S.octs, noct, ed, ep, ev, c->params.gamma);
+    if (ilevel > lmin && icount < nsub) k_test_flag<<<nblk(n), TPB, 0, s>>>(M, S.octs, noct);
+    for (int i = 0; i < nexp; ++i) smooth();
+    if (ilevel > lmin && icount < nsub)
+        k_ensure_ref_rules<<<nblk(noct), TPB, 0, s>>>(M, Geo{c->nx, c->ny, c->nz, c->params.boxlen}, S.octs, noct);
+    if (int rc = check_cuda(c, cudaGetLastError(), "flag_fine kernels")) return rc;
+    return check_device_status(c);
+}
+
+int tree_make_grid_fine(rg_ctx* c, int ilevel) {
+    if (int rc = check_tree(c, ilevel)) return rc < 0 ? RG_OK : rc;  // no-op at and above nlevelmax (TreeUpdater.cpp:28)
+    TreeScratch S;
+    if (int rc = tree_scratch(c, &S)) return rc;
+    TreeMut M = tree_mut(c);
+    cudaStream_t s = c->stream;
+    k_authorize<<<nblk(c->ncell), TPB, 0, s>>>(M);
+    if (ilevel == 1) {
+        int* d_count = S.mark;
+        int count = 0;
+        cudaMemsetAsync(d_count, 0, sizeof(int), s);
+        k_coarse_candidates<<<nblk(c->ncoarse), TPB, 0, s>>>(M, d_count);
+        cudaMemcpyAsync(&count, d_count, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (int rc = check_cuda(c, cudaStreamSynchronize(s), "coarse candidates")) return rc;
+        if (count > 0) return set_error(c, RG_ERR_UNSUPPORTED, "refining coarse cells stays on the host");
+        return RG_OK;
+    }
+    int noct = 0;
+    if (int rc = level_oct_list(c, ilevel, S.octs, c->ngridmax, &noct)) return rc;
+    if (noct == 0) return check_cuda(c, cudaStreamSynchronize(s), "authorize");
+    const int n8 = 8 * noct;
+    k_refine_mark<<<nblk(n8), TPB, 0, s>>>(M, S.octs, noct, S.mark);
+    int n = 0;
+    if (int rc = exclusive_scan(c, S.mark, S.rank, n8, &n)) return rc;
+    if (n == 0) return RG_OK;
+    if (n > c->numbf)
+        return set_error(c, RG_ERR_UNSUPPORTED, "free oct list exhausted (" + std::to_string(n) + " needed, " +
+                                                    std::to_string(c->numbf) + " free): attach with a larger ngridmax");
+    const StepK K = step_consts(c);
+    k_refine<<<nblk(n8), TPB, 0, s>>>(M, tree_view(c), Geo{c->nx, c->ny, c->nz, c->params.boxlen}, S.octs, noct,
+                                      S.mark, S.rank, c->d_fq, c->fq_head, ilevel, c->params.interpol_var,
+                                      c->params.interpol_type, c->params.gamma, K.smalle, c->d_bound, c->nbound_type,
+                                      S.list, c->d_status);
+    // the new octs, in order, are the next n entries of the free-list ring
+    const int ngm = c->ngridmax, L = ilevel + 1;
+    const int first = c->h_fq[(size_t)c->fq_head], last = c->h_fq[(size_t)((c->fq_head + n - 1) % ngm)];
+    const int old_tail = c->h_taill[(size_t)hidx(c, L)];
+    k_link_chain<<<nblk(n), TPB, 0, s>>>(c->d_next, c->d_prev, S.list, n, old_tail);
+    if (old_tail == 0) c->h_headl[(size_t)hidx(c, L)] = first;
+    c->h_taill[(size_t)hidx(c, L)] = last;
+    c->h_numbl[(size_t)hidx(c, L)] += n;
+    c->fq_head = (c->fq_head + n) % ngm;
+    c->numbf -= n;
+    if (c->numbf > 0)
+        if (int rc = set_dev_int(c, c->d_prev + c->h_fq[(size_t)c->fq_head] - 1, 0)) return rc;
+    c->tree_dirty = true;
+    if (int rc = check_cuda(c, cudaGetLastError(), "make_grid_fine kernels")) return rc;
+    return check_device_status(c);
+}
+
+int tree_remove_grid_fine(rg_ctx* c, int ilevel) {
+    if (int rc = check_tree(c, ilevel)) return rc < 0 ? RG_OK : rc;  // no-op at and above nlevelmax (TreeUpdater.cpp:152)
+    TreeScratch S;
+    if (int rc = tree_scratch(c, &S)) return rc;
+    int noct = 0;
+    if (int rc = level_oct_list(c, ilevel, S.octs, c->ngridmax, &noct)) return rc;
+    if (noct == 0) return RG_OK;
+    TreeMut M = tree_mut(c);
+    cudaStream_t s = c->stream;
+    k_kill_mark<<<nblk(noct), TPB, 0, s>>>(M, S.octs, noct, S.mark);
+    int nkill = 0;
+    if (int rc = exclusive_scan(c, S.mark, S.rank, noct, &nkill)) return rc;
+    if (nkill == 0) return RG_OK;
+    const int ngm = c->ngridmax, m = noct - nkill;
+    const int fq_tail = (c->fq_head + c->numbf) % ngm;
+    const int old_tailf = c->numbf > 0 ? c->h_fq[(size_t)((fq_tail - 1 + ngm) % ngm)] : 0;
+    k_kill<<<nblk(noct), TPB, 0, s>>>(M, S.octs, noct, S.mark, S.rank, S.list, S.list2, c->d_fq, fq_tail);
+    k_link_chain<<<nblk(std::max(m, 1)), TPB, 0, s>>>(c->d_next, c->d_prev, S.list, m, 0);
+    k_link_chain<<<nblk(nkill), TPB, 0, s>>>(c->d_next, c->d_prev, S.list2, nkill, old_tailf);
+    std::vector<int> freed((size_t)nkill);
+    int ends[2] = {0, 0};
+    cudaMemcpyAsync(freed.data(), S.list2, sizeof(int) * nkill, cudaMemcpyDeviceToHost, s);
+    if (m > 0) {
+        cudaMemcpyAsync(&ends[0], S.list, sizeof(int), cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&ends[1], S.list + m - 1, sizeof(int), cudaMemcpyDeviceToHost, s);
+    }
+    if (int rc = check_cuda(c, cudaStreamSynchronize(s), "remove_grid_fine")) return rc;
+    for (int j = 0; j < nkill; ++j) c->h_fq[(size_t)((fq_tail + j) % ngm)] = freed[(size_t)j];
+    c->numbf += nkill;
+    c->h_headl[(size_t)hidx(c, ilevel)] = ends[0];
+    c->h_taill[(size_t)hidx(c, ilevel)] = ends[1];
+    c->h_numbl[(size_t)hidx(c, ilevel)] -= nkill;
+    c->tree_dirty = true;
+    if (int rc = check_cuda(c, cudaGetLastError(), "remove_grid_fine kernels")) return rc;
+    return check_device_status(c);
+}
+
+int tree_restrict_fine(rg_ctx* c, int ilevel) {
+    // restrict_fine(ilevel) reads level ilevel + 1; the reference walks an
+    // empty list when ilevel + 1 > nlevelmax
+    if (!c->tree_resident) return set_error(c, RG_ERR_STATE, "no device-resident tree: call rg_tree_attach first");
+    if (ilevel < 0 || ilevel > c->nlevelmax) return set_error(c, RG_ERR_ARG, "level outside 0..nlevelmax");
+    c->next_level = -1;
+    if (ilevel + 1 > c->nlevelmax) return RG_OK;
+    if (int rc = refresh_tree(c)) return rc;
+    TreeScratch S;
+    if (int rc = tree_scratch(c, &S)) return rc;
+    int noct = 0;
+    if (int rc = level_oct_list(c, ilevel + 1, S.octs, c->ngridmax, &noct)) return rc;
+    if (noct == 0) return RG_OK;
+    k_restrict<<<nblk(noct), TPB, 0, c->stream>>>(tree_mut(c), S.octs, noct);
+    return check_cuda(c, cudaGetLastError(), "restrict_fine kernel");
+}
+
+}  // namespace rg

@@ -37,6 +37,35 @@ class rg_grid_view(C.Structure):
                 ("bound_type", I32P), ("nbound_type", C.c_int)]
 
 
+class rg_tree_arrays(C.Structure):
+    _fields_ = [(k, I32P) for k in ("son", "father", "nbor", "next", "prev", "headl", "taill", "numbl", "flag1",
+                                    "flag2", "cpu_map")] + \
+               [("xg", C.POINTER(C.c_double)), ("uold", C.POINTER(C.c_double)), ("unew", C.POINTER(C.c_double)),
+                ("headf", C.c_int), ("tailf", C.c_int), ("numbf", C.c_int)]
+
+
+TREE_INT_ARRAYS = ("son", "father", "nbor", "next", "prev", "headl", "taill", "numbl", "flag1", "flag2", "cpu_map")
+TREE_F64_ARRAYS = ("xg", "uold", "unew")
+
+
+def tree_arrays(d):
+    """rg_tree_arrays over a dict of contiguous numpy arrays (int32 / float64)
+    and the scalars headf, tailf, numbf; the arrays are written in place by
+    rg_tree_fetch."""
+    t = rg_tree_arrays()
+    for k in TREE_INT_ARRAYS:
+        a = d[k]
+        assert a.dtype == np.int32 and a.flags.c_contiguous
+        setattr(t, k, a.ctypes.data_as(I32P))
+    for k in TREE_F64_ARRAYS:
+        a = d[k]
+        assert a.dtype == np.float64 and a.flags.c_contiguous
+        setattr(t, k, a.ctypes.data_as(C.POINTER(C.c_double)))
+    t.headf, t.tailf, t.numbf = int(d["headf"]), int(d["tailf"]), int(d["numbf"])
+    t._keep = d
+    return t
+
+
 def make_params(ndim, nvar=None, slope_type=1, riemann="hllc", interpol_type=1, interpol_var=0, gamma=1.4,
                 courant_factor=0.8, exact_niter=10, exact_tol=1e-6, exact_guess=0, boxlen=1.0):
     r = RIEMANN.get(riemann, 0) if isinstance(riemann, str) else int(riemann)
@@ -119,6 +148,14 @@ def lib():
     L.rg_set_level_lattices.argtypes = [VP, C.c_int, C.c_int, IP, IP, IP]
     L.rg_level_output.argtypes = [VP, C.c_int, C.POINTER(C.c_double), C.c_int64]
     L.rg_level_substep_host.argtypes = [VP, C.c_int, C.c_double, C.c_int, VP, VP, C.POINTER(C.c_double)]
+    TP = C.POINTER(rg_tree_arrays)
+    L.rg_tree_attach.argtypes = [VP, C.POINTER(rg_grid_view), TP, C.c_int]
+    L.rg_tree_fetch.argtypes = [VP, TP]
+    L.rg_flag_fine.argtypes = [VP, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int]
+    L.rg_make_grid_fine.argtypes = [VP, C.c_int]
+    L.rg_remove_grid_fine.argtypes = [VP, C.c_int]
+    L.rg_restrict_fine.argtypes = [VP, C.c_int]
+    L.rg_count_grids.argtypes = [VP, C.c_int, IP]
     _lib = L
     return L
 
@@ -170,6 +207,45 @@ class Context:
         self._view = grid_view(g)
         self.ncell = int(g.ncell)
         self._chk(self.L.rg_sync_topology(self.h, C.byref(self._view)))
+
+    # -- device-resident tree (TreeUpdater on the GPU) ---------------------------
+    def tree_attach(self, g, arrays, levelmin):
+        """Take over the tree: g gives sizes and son/father/nbor/next/headl,
+        arrays (a dict like RefHarness.tree_arrays) the rest and the state."""
+        self._view = grid_view(g)
+        self.ncell = int(g.ncell)
+        d = {k: np.ascontiguousarray(arrays[k], dtype=np.int32) for k in TREE_INT_ARRAYS}
+        d.update({k: np.ascontiguousarray(arrays[k], dtype=np.float64) for k in TREE_F64_ARRAYS})
+        d.update(headf=arrays["headf"], tailf=arrays["tailf"], numbf=arrays["numbf"])
+        self._tree = tree_arrays(d)
+        self._chk(self.L.rg_tree_attach(self.h, C.byref(self._view), C.byref(self._tree), int(levelmin)))
+
+    def tree_fetch(self, like):
+        """Fresh numpy copies of every tree array and the state (shapes from `like`)."""
+        d = {k: np.zeros(np.shape(like[k]), dtype=np.int32) for k in TREE_INT_ARRAYS}
+        d.update({k: np.zeros(np.shape(like[k]), dtype=np.float64) for k in TREE_F64_ARRAYS})
+        d.update(headf=0, tailf=0, numbf=0)
+        t = tree_arrays(d)
+        self._chk(self.L.rg_tree_fetch(self.h, C.byref(t)))
+        d.update(headf=t.headf, tailf=t.tailf, numbf=t.numbf)
+        return d
+
+    def flag_fine(self, il, ed=-1.0, ep=-1.0, ev=-1.0, eb2=-1.0, nexp=1, icount=1, nsub=2):
+        self._chk(self.L.rg_flag_fine(self.h, il, ed, ep, ev, eb2, nexp, icount, nsub))
+
+    def make_grid_fine(self, il):
+        self._chk(self.L.rg_make_grid_fine(self.h, il))
+
+    def remove_grid_fine(self, il):
+        self._chk(self.L.rg_remove_grid_fine(self.h, il))
+
+    def restrict_fine(self, il):
+        self._chk(self.L.rg_restrict_fine(self.h, il))
+
+    def count_grids(self, il):
+        n = C.c_int(0)
+        self._chk(self.L.rg_count_grids(self.h, il, C.byref(n)))
+        return n.value
 
     def upload_state(self, uold=None, unew=None):
         self._chk(self.L.rg_upload_state(self.h, _f64(uold), _f64(unew)))

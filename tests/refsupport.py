@@ -150,6 +150,18 @@ class RefHarness:
                     headl=self._arr("headl", self.get("headl_size"), np.int32),
                     xg=self._arr("xg", 3 * ngm, np.float64), flag1=self._arr("flag1", ncell, np.int32))
 
+    def tree_arrays(self):
+        """Every array and scalar of the reference's tree (AmrGrid.hpp:26-30): the
+        hydro arrays plus prev, flag2, cpu_map, the level-list tails and counts
+        and the free list (headf, tailf, numbf)."""
+        a = self.arrays()
+        ncell, ngm, nh = self.get("ncell"), self.get("ngridmax"), self.get("headl_size")
+        a.update(prev=self._arr("prev", ngm, np.int32), flag2=self._arr("flag2", ncell, np.int32),
+                 cpu_map=self._arr("cpu_map", ncell, np.int32), taill=self._arr("taill", nh, np.int32),
+                 numbl=self._arr("numbl", nh, np.int32))
+        a.update(headf=self.get("headf"), tailf=self.get("tailf"), numbf=self.get("numbf"))
+        return a
+
     def grid(self):
         a = self.arrays()
         return GridArrays(ncoarse=self.get("ncoarse"), ngridmax=self.get("ngridmax"), ncell=self.get("ncell"),

@@ -1,0 +1,117 @@
+"""AMR tree maintenance on the GPU (rg_tree.cu) against the reference's own
+TreeUpdater (src/core/TreeUpdater.cpp), run through the compiled reference
+harness on the same tree.
+
+- every operation, level by level, on a sub-cycled Sedov tree after a coarse
+  step: flag_fine (with smooth_fine, test_flag and ensure_ref_rules),
+  make_grid_fine (oct ids from the FIFO free list, neighbours, coordinates,
+  interpol_hydro for each interpol_var), remove_grid_fine (unlinking, freed
+  ids appended to the free list) and restrict_fine: every tree array, the
+  list heads / tails / counts, the free list and the state equal bit for bit;
+- whole coarse steps with the tree resident on the device (rg_amr.DeviceAmrRun)
+  against the reference's run (refsupport.AmrRun): same tree, same state,
+  same time, same cell-update count after each step.
+"""
+import numpy as np
+import pytest
+
+import rgpu
+from rg_amr import DeviceAmrRun
+from refsupport import AmrRun, RefHarness, namelist, sedov_ic
+
+pytestmark = pytest.mark.gpu
+
+LMIN, LMAX, GAMMA, ED, EP = 4, 7, 1.4, 0.1, 0.1
+
+
+def bits_equal(a, b):
+    return np.array_equal(np.ascontiguousarray(a).view(np.int64), np.ascontiguousarray(b).view(np.int64))
+
+
+def reference_run(steps, interpol_var=0, interpol_type=1):
+    nml = namelist(slope_type=2, riemann="hllc", interpol_type=interpol_type, interpol_var=interpol_var,
+                   levelmin=LMIN, levelmax=LMAX, err_grad_d=ED, err_grad_p=EP)
+    h = RefHarness(3).create(nml, ngridmax=30000, levelmin=LMIN, nlevelmax=LMAX, gamma=GAMMA)
+    r = AmrRun(h, LMIN, LMAX, GAMMA, ed=ED, ep=EP)
+    r.initialize(sedov_ic(3, LMIN))
+    for _ in range(steps):
+        r.coarse_step()
+    return h, r
+
+
+def device_ctx(h, interpol_var=0, interpol_type=1):
+    params = rgpu.make_params(3, slope_type=2, riemann="hllc", interpol_type=interpol_type,
+                              interpol_var=interpol_var, gamma=GAMMA)
+    ctx = rgpu.Context(params, 0)
+    ctx.tree_attach(h.grid(), h.tree_arrays(), LMIN)
+    return ctx
+
+
+def assert_same_tree(h, ctx, what):
+    want = h.tree_arrays()
+    got = ctx.tree_fetch(want)
+    for k in rgpu.TREE_INT_ARRAYS:
+        bad = np.flatnonzero(got[k] != want[k])
+        assert bad.size == 0, f"{what}: {k} differs at {bad[:5]} (got {got[k][bad[:5]]}, want {want[k][bad[:5]]})"
+    for k in rgpu.TREE_F64_ARRAYS:
+        assert bits_equal(got[k], want[k]), f"{what}: {k} differs"
+    for k in ("headf", "tailf", "numbf"):
+        assert got[k] == want[k], f"{what}: {k} {got[k]} != {want[k]}"
+
+
+@pytest.mark.parametrize("interpol_var", [0, 1, 2])
+def test_each_tree_operation_matches_reference(rgpu_lib, interpol_var):
+    itype = 4 if interpol_var == 2 else 1  # type 4 mixes central and moncen slopes
+    h, _ = reference_run(1, interpol_var, itype)
+    ctx = device_ctx(h, interpol_var, itype)
+    try:
+        assert_same_tree(h, ctx, "attach")
+        made = killed = 0
+        for il in range(LMAX, LMIN - 1, -1):
+            for icount in (1, 2):
+                h.flag_fine(il, ED, EP, -1.0, -1.0, 1, icount, 2)
+                ctx.flag_fine(il, ED, EP, -1.0, -1.0, 1, icount, 2)
+                assert_same_tree(h, ctx, f"flag_fine({il}, icount={icount})")
+        for il in range(LMIN, LMAX + 1):
+            n0 = h.count_grids(il + 1)
+            h.make_grid_fine(il)
+            ctx.make_grid_fine(il)
+            made += h.count_grids(il + 1) - n0
+            assert_same_tree(h, ctx, f"make_grid_fine({il})")
+            assert ctx.count_grids(il + 1) == h.count_grids(il + 1)
+        # re-flag each level with thresholds nothing exceeds and without the
+        # sub-cycle rules: only fathers of refined octs keep their flags, so the
+        # finest octs are removed
+        for il in range(LMAX, LMIN, -1):
+            h.flag_fine(il - 1, 1e30, 1e30, -1.0, -1.0, 0, 2, 2)
+            ctx.flag_fine(il - 1, 1e30, 1e30, -1.0, -1.0, 0, 2, 2)
+            n0 = h.count_grids(il)
+            h.remove_grid_fine(il)
+            ctx.remove_grid_fine(il)
+            killed += n0 - h.count_grids(il)
+            assert_same_tree(h, ctx, f"remove_grid_fine({il})")
+        for il in range(LMAX, -1, -1):
+            h.restrict_fine(il)
+            ctx.restrict_fine(il)
+        assert_same_tree(h, ctx, "restrict_fine")
+        assert made > 0, "the sequence refined nothing"
+        assert killed > 0, "the sequence removed nothing"
+    finally:
+        ctx.close()
+
+
+def test_device_resident_amr_run_matches_reference(rgpu_lib):
+    h, r = reference_run(0)
+    ctx = device_ctx(h)
+    try:
+        d = DeviceAmrRun(ctx, nx=1, levelmin=LMIN, nlevelmax=LMAX, ed=ED, ep=EP)
+        headf0 = h.tree_arrays()["headf"]
+        for step in range(3):
+            r.coarse_step()
+            d.coarse_step()
+            assert_same_tree(h, ctx, f"coarse step {step}")
+            assert d.t == r.t and d.cell_updates == r.cell_updates
+        assert sum(h.count_grids(il) for il in range(LMIN + 1, LMAX + 1)) > 0
+        assert h.tree_arrays()["headf"] != headf0, "no oct was allocated during the run"
+    finally:
+        ctx.close()
