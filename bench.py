@@ -23,7 +23,8 @@ same box:
 - "ensemble": 512 independent uneven boxes stepped together (sharded over
   the ranks when N > 1);
 - "amr": the sub-cycled Sedov AMR run through the reference's own
-  AmrGrid/TreeUpdater step, CPU reference against the GPU drop-in (N = 1);
+  AmrGrid/TreeUpdater step, CPU reference against the GPU drop-in, and the
+  same run with the tree resident on the GPU (N = 1);
 - "sod1d": the 1D Sod run to t = 0.245, CPU reference against the GPU (N = 1).
 """
 import argparse
@@ -524,6 +525,44 @@ def amr_sample(variant, steps, lmin=7, lmax=10, ngridmax=400000):
     return out
 
 
+def amr_device_sample(steps, lmin=7, lmax=10, ngridmax=400000):
+    """Config 3 with the tree resident on the GPU: initialisation by the
+    reference on the host (as in the other arms), then rg_tree_attach and every
+    coarse step (tree maintenance, CFL, hydro) on the device through
+    rg_amr.DeviceAmrRun; the digest covers the same arrays as amr_sample's."""
+    import hashlib
+    sys.path.insert(0, str(ROOT / "tests"))
+    import rgpu
+    from rg_amr import DeviceAmrRun
+    from refsupport import AmrRun, RefHarness, namelist, sedov_ic
+    nml = namelist(slope_type=2, riemann="hllc", levelmin=lmin, levelmax=lmax, err_grad_d=0.1, err_grad_p=0.1)
+    h = RefHarness(3).create(nml, ngridmax=ngridmax, levelmin=lmin, nlevelmax=lmax, gamma=1.4)
+    r = AmrRun(h, lmin, lmax, 1.4, ed=0.1, ep=0.1)
+    r.initialize(sedov_ic(3, lmin))
+    ctx = rgpu.Context(rgpu.make_params(3, slope_type=2, riemann="hllc", interpol_type=1, interpol_var=0, gamma=1.4),
+                       0)
+    t0 = time.perf_counter()
+    ctx.tree_attach(h.grid(), h.tree_arrays(), lmin)
+    attach_s = time.perf_counter() - t0
+    d = DeviceAmrRun(ctx, nx=1, levelmin=lmin, nlevelmax=lmax, ed=0.1, ep=0.1)
+    d.coarse_step()  # warm-up step (plans, autotuner), as in the other arms
+    ctx.synchronize()
+    cu0 = d.cell_updates
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        d.coarse_step()
+    ctx.synchronize()
+    wall = time.perf_counter() - t0
+    got = ctx.tree_fetch(h.tree_arrays())
+    out = {"variant": "gpu_resident", "coarse_steps": steps, "wall_s": wall, "attach_s": attach_s,
+           "cell_updates": d.cell_updates - cu0, "t": d.t,
+           "octs_per_level": [ctx.count_grids(il) for il in range(lmin, lmax + 1)],
+           "digest": hashlib.sha1(got["uold"].tobytes() + got["son"].tobytes()).hexdigest()}
+    ctx.close()
+    h.close()
+    return out
+
+
 def amr_exact_sample(guess, steps, lmin=7, lmax=10, ngridmax=400000):
     """Config 5's AMR part: the sub-cycled Sedov AMR run (tree maintenance by
     the reference's own TreeUpdater) with every godunov_fine on the GPU through
@@ -672,6 +711,7 @@ def run_sample(flag, *args, timeout=900):
 def amr_report(steps):
     ref = run_sample("--amr-sample", "cpu", steps)
     gpu = run_sample("--amr-sample", "gpu", steps)
+    res = run_sample("--amr-device-sample", steps)
     return {"workload": "3D Sedov AMR, reference levelmin 7, levelmax 10 (64^3 base, 512^3 effective), "
                         "err_grad_d = err_grad_p = 0.1, sub-cycled, MonCen + HLLC, through the reference's own "
                         "AmrGrid/TreeUpdater/Simulation step with the hydro solver swapped by create_hydro_solver",
@@ -679,8 +719,13 @@ def amr_report(steps):
             "reference_cpu": ref, "gpu_dropin": gpu, "bit_identical": ref["digest"] == gpu["digest"],
             "wall_speedup": ref["wall_s"] / gpu["wall_s"], "hydro_speedup": ref["hydro_s"] / gpu["hydro_s"],
             "gpu_hydro_cell_updates_per_s": gpu["cell_updates"] / gpu["hydro_s"],
-            "note": "tree maintenance (flag/refine/restrict) stays on the host in both arms; GPU hydro time "
-                    "includes the level-sparse host<->device copies of every godunov_fine call"}
+            "gpu_resident": res, "resident_bit_identical": ref["digest"] == res["digest"],
+            "resident_wall_speedup": ref["wall_s"] / res["wall_s"],
+            "resident_cell_updates_per_s": res["cell_updates"] / res["wall_s"],
+            "note": "gpu_dropin: tree maintenance (flag/refine/restrict) on the host as in the reference, GPU hydro "
+                    "time includes the level-sparse host<->device copies of every godunov_fine call; "
+                    "gpu_resident: the tree on the device too (rg_tree_attach + DeviceAmrRun), the host reads "
+                    "back level counts and one dt per level step"}
 
 
 def amr_exact_report(steps):
@@ -719,6 +764,7 @@ def main():
     ap.add_argument("--amr-sample", nargs=2, metavar=("VARIANT", "STEPS"), help=argparse.SUPPRESS)
     ap.add_argument("--sod-sample", metavar="VARIANT", help=argparse.SUPPRESS)
     ap.add_argument("--amr-exact-sample", nargs=2, metavar=("GUESS", "STEPS"), help=argparse.SUPPRESS)
+    ap.add_argument("--amr-device-sample", type=int, metavar="STEPS", help=argparse.SUPPRESS)
     ap.add_argument("--profile-case", choices=["learned"], help="small run for ncu captures (no timing output)")
     args = ap.parse_args()
     if args.cpu_sample:
@@ -729,6 +775,9 @@ def main():
         return
     if args.sod_sample:
         print(json.dumps(sod_sample(args.sod_sample)))
+        return
+    if args.amr_device_sample:
+        print(json.dumps(amr_device_sample(args.amr_device_sample)))
         return
     if args.amr_exact_sample:
         print(json.dumps(amr_exact_sample(args.amr_exact_sample[0], int(args.amr_exact_sample[1]))))
