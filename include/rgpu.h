@@ -360,6 +360,30 @@ int rg_restrict_fine(rg_ctx* ctx, int ilevel);
 /* AmrGrid::count_grids_at_level (AmrGrid.cpp:304-308) of the resident tree. */
 int rg_count_grids(rg_ctx* ctx, int ilevel, int* n);
 
+/* One coarse step of the resident run: Simulation::run's step
+ * (Simulation.cpp:366-397) with Simulation::amr_step (:522-635), every grid
+ * and hydro call on the device, sub-cycling 2 from levelmin on.  The clock
+ * carries Simulation's dtnew_/dtold_, time, step count and the hydro cell
+ * updates from one call to the next (zero it before the first). */
+typedef struct rg_amr_config {
+    int levelmin;          /* amr_params/levelmin                                   */
+    int nexpand;           /* amr_params/nexpand                                    */
+    double courant_factor; /* hydro_params/courant_factor                           */
+    double err_grad_d;     /* refine_params; <= 0 switches a criterion off          */
+    double err_grad_p;
+    double err_grad_u;
+    int pressure_cap;      /* 1: compute_courant_step as the reference (p <= 100 rho
+                              cap); 0: the same formula without the cap             */
+    double boxlen;         /* amr_params/boxlen                                     */
+} rg_amr_config;
+typedef struct rg_amr_clock {
+    double dtnew[33], dtold[33]; /* per level                                          */
+    double t;
+    int64_t nstep;
+    int64_t cell_updates;        /* son == 0 cells processed by godunov_fine           */
+} rg_amr_clock;
+int rg_amr_coarse_step(rg_ctx* ctx, const rg_amr_config* cfg, rg_amr_clock* clock);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,6 +1,6 @@
 """A whole AMR run with the tree and the state resident on the GPU.
 
-`DeviceAmrRun` replays Simulation::amr_step and the coarse step around it
+`DeviceAmrRun` runs Simulation::amr_step and the coarse step around it
 (RAMSES-CPP src/core/Simulation.cpp:366-397, 522-635) on one rgpu.Context
 after `Context.tree_attach`: the tree operations (flag_fine, make_grid_fine,
 remove_grid_fine, restrict_fine; rg_tree.cu), the CFL step
@@ -10,16 +10,26 @@ counts and one dt per level step.  Same call sequence as the reference's
 step, so the tree, every oct id and the state come out bit for bit as the
 reference's own run leaves them.
 
+By default a coarse step is one native call (rg_amr_coarse_step, rg_amr.cu);
+`native=False` issues the same sequence call by call from Python through the
+per-operation entry points, which the tests use to check both paths.
+
 The CFL step takes the reference formula with or without its p <= 100 rho
 cap (`pressure_cap`); the sub-cycled Sedov runs use it without the cap, which
 makes the blast unstable at these resolutions.
 """
 
 
+import rgpu
+
+
 class DeviceAmrRun:
     def __init__(self, ctx, nx, levelmin, nlevelmax, cfl=0.8, ed=-1.0, ep=-1.0, ev=-1.0, nexpand=1,
-                 pressure_cap=False, boxlen=1.0):
+                 pressure_cap=False, boxlen=1.0, native=True):
         self.ctx, self.nx, self.lmin, self.lmax = ctx, nx, levelmin, nlevelmax
+        self.native = native
+        self.cfg = rgpu.rg_amr_config(levelmin, nexpand, cfl, ed, ep, ev, 1 if pressure_cap else 0, boxlen)
+        self.clock = rgpu.rg_amr_clock()
         self.cfl, self.ed, self.ep, self.ev, self.nexp = cfl, ed, ep, ev, nexpand
         self.pressure_cap, self.boxlen = pressure_cap, boxlen
         self.nsub = [1] * 33
@@ -72,6 +82,10 @@ class DeviceAmrRun:
                     self.nsub[il - 1] if il > 0 else 1)
 
     def coarse_step(self):
+        if self.native:
+            self.ctx.amr_coarse_step(self.cfg, self.clock)
+            self.t, self.nstep, self.cell_updates = self.clock.t, self.clock.nstep, self.clock.cell_updates
+            return
         c = self.ctx
         if self.lmin < self.lmax:
             for il in range(1, self.lmin):

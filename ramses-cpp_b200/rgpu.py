@@ -44,6 +44,17 @@ class rg_tree_arrays(C.Structure):
                 ("headf", C.c_int), ("tailf", C.c_int), ("numbf", C.c_int)]
 
 
+class rg_amr_config(C.Structure):
+    _fields_ = [("levelmin", C.c_int), ("nexpand", C.c_int), ("courant_factor", C.c_double),
+                ("err_grad_d", C.c_double), ("err_grad_p", C.c_double), ("err_grad_u", C.c_double),
+                ("pressure_cap", C.c_int), ("boxlen", C.c_double)]
+
+
+class rg_amr_clock(C.Structure):
+    _fields_ = [("dtnew", C.c_double * 33), ("dtold", C.c_double * 33), ("t", C.c_double), ("nstep", C.c_int64),
+                ("cell_updates", C.c_int64)]
+
+
 TREE_INT_ARRAYS = ("son", "father", "nbor", "next", "prev", "headl", "taill", "numbl", "flag1", "flag2", "cpu_map")
 TREE_F64_ARRAYS = ("xg", "uold", "unew")
 
@@ -156,6 +167,7 @@ def lib():
     L.rg_remove_grid_fine.argtypes = [VP, C.c_int]
     L.rg_restrict_fine.argtypes = [VP, C.c_int]
     L.rg_count_grids.argtypes = [VP, C.c_int, IP]
+    L.rg_amr_coarse_step.argtypes = [VP, C.POINTER(rg_amr_config), C.POINTER(rg_amr_clock)]
     _lib = L
     return L
 
@@ -241,6 +253,10 @@ class Context:
 
     def restrict_fine(self, il):
         self._chk(self.L.rg_restrict_fine(self.h, il))
+
+    def amr_coarse_step(self, cfg, clock):
+        """rg_amr_coarse_step: one coarse step of the resident run (clock updated in place)."""
+        self._chk(self.L.rg_amr_coarse_step(self.h, C.byref(cfg), C.byref(clock)))
 
     def count_grids(self, il):
         n = C.c_int(0)

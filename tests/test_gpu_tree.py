@@ -8,9 +8,10 @@ harness on the same tree.
   interpol_hydro for each interpol_var), remove_grid_fine (unlinking, freed
   ids appended to the free list) and restrict_fine: every tree array, the
   list heads / tails / counts, the free list and the state equal bit for bit;
-- whole coarse steps with the tree resident on the device (rg_amr.DeviceAmrRun)
-  against the reference's run (refsupport.AmrRun): same tree, same state,
-  same time, same cell-update count after each step.
+- whole coarse steps with the tree resident on the device (rg_amr.DeviceAmrRun,
+  through the native rg_amr_coarse_step and call by call) against the
+  reference's run (refsupport.AmrRun): same tree, same state, same time, same
+  cell-update count after each step.
 """
 import numpy as np
 import pytest
@@ -100,11 +101,13 @@ def test_each_tree_operation_matches_reference(rgpu_lib, interpol_var):
         ctx.close()
 
 
-def test_device_resident_amr_run_matches_reference(rgpu_lib):
+@pytest.mark.parametrize("native", [True, False])
+def test_device_resident_amr_run_matches_reference(rgpu_lib, native):
+    """native: rg_amr_coarse_step; else the same sequence call by call."""
     h, r = reference_run(0)
     ctx = device_ctx(h)
     try:
-        d = DeviceAmrRun(ctx, nx=1, levelmin=LMIN, nlevelmax=LMAX, ed=ED, ep=EP)
+        d = DeviceAmrRun(ctx, nx=1, levelmin=LMIN, nlevelmax=LMAX, ed=ED, ep=EP, native=native)
         headf0 = h.tree_arrays()["headf"]
         for step in range(3):
             r.coarse_step()
