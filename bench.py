@@ -13,6 +13,12 @@ Prints one JSON line (rank 0).  N > 1 runs one independent replica per GPU
 (weak scaling): the single-grid step of this workload is not partitioned, so
 the ranks exchange nothing but the final timing maximum.
 
+Besides the HBM `roofline` of the face kernel (the contract's), the line
+carries `roofline_fp64`: the same kernel against the FP64 pipe, its actual
+bound (executed FP64 FLOPs per cell update from the committed ncu summary,
+over its CUDA-event time, against the FP64 throughput measured on this GPU
+by rg_measure_fp64_peak).
+
 The line also carries the other workloads of the path, each measured on the
 same box:
 - "newton": the exact Riemann solver on the stress workload (256^3
@@ -59,18 +65,23 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic(kernel):
-    """dram bytes per launch of the face kernel from the committed ncu summary."""
+def profile_value(kernel, key):
+    """A `key: value` figure of the face kernel's committed ncu summary."""
     f = ROOT / "profiles" / f"{kernel}_sedov128.md"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
-        if line.startswith("traffic_bytes_per_launch:"):
+        if line.startswith(key + ":"):
             try:
                 return int(float(line.split(":", 1)[1].strip()))
             except ValueError:
                 return None
     return None
+
+
+def profile_traffic(kernel):
+    """dram bytes per launch of the face kernel from the committed ncu summary."""
+    return profile_value(kernel, "traffic_bytes_per_launch")
 
 
 # ---------------------------------------------------------------- clocks
@@ -312,6 +323,7 @@ def gpu_arm(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_e2e = float(t.item())
     e2e_value = world * cells * ne / (ms_e2e / 1e3)
+    fp64_peak = ctx.measure_fp64_peak() if rank == 0 else None
     ctx.close()
     if rank != 0:
         return None
@@ -332,6 +344,7 @@ def gpu_arm(args, rank, world, local_rank):
                      "traffic": profile_traffic(face_kernel), "kernel": face_kernel, "variant": variant,
                      "algorithmic_bytes_per_launch": alg_bytes, "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
                      "step_hbm_frac": (BYTES_PER_CELL_UPDATE * value / world / 1e9) / peak},
+        "roofline_fp64": fp64_roofline(face_kernel, cells, face_s, fp64_peak),
         "kernel_ms": {"prim": kms[0], "face": kms[1], "fold": kms[2]},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * g.nvar * cells,
                 "d2h_bytes_per_step": 8 * g.nvar * cells, "ms_per_step": ms_e2e / ne,
@@ -340,6 +353,25 @@ def gpu_arm(args, rank, world, local_rank):
         "clocks": clocks,
     }
     return out
+
+
+def fp64_roofline(face_kernel, cells, face_s, peak_tflops):
+    """The face kernel against the FP64 pipe, its real bound: executed FP64
+    FLOPs per cell update (ncu instruction counts, a DFMA counted as 2) over
+    its CUDA-event time, against the FP64 throughput measured on this GPU."""
+    fpc = profile_value(face_kernel, "fp64_flops_per_cell_update")
+    if fpc is None or not peak_tflops:
+        return None
+    achieved = fpc * cells / face_s / 1e12
+    opc = profile_value(face_kernel, "fp64_ops_per_cell_update")
+    # instruction throughput: DMUL and DADD take an issue slot of the FP64 pipe
+    # like a DFMA but carry one FLOP, so the FLOP fraction understates it
+    op_frac = (opc * cells / face_s / 1e12) / (peak_tflops / 2) if opc else None
+    return {"bound": "fp64", "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
+            "frac": achieved / peak_tflops, "op_frac": op_frac, "flops_per_cell_update": fpc,
+            "ops_per_cell_update": opc, "kernel": face_kernel,
+            "peak_source": "rg_measure_fp64_peak: independent DFMA chains on every SM, best of 5 (measured here)",
+            "flops_source": f"profiles/{face_kernel}_sedov128.md (ncu executed DFMA/DMUL/DADD per cell update)"}
 
 
 def newton_report(local_rank, stream, steps):

@@ -296,6 +296,12 @@ int rg_set_level_lattices(rg_ctx* ctx, int ilevel, int nbox, const int* extent, 
  * rg_level_substep's dt_used reports the smallest of them. */
 int rg_level_box_dt(rg_ctx* ctx, int ilevel, double* dt_out, int nbox);
 
+/* No reference counterpart, measurement only: the device's FP64 throughput
+ * in TFLOP/s (independent fused multiply-add chains on every SM, best of 5
+ * timed launches), the peak the face kernel's compute roofline is reported
+ * against. */
+int rg_measure_fp64_peak(rg_ctx* ctx, double* tflops);
+
 /* Shape chosen for a level: variant index, batch, and its timed ms. */
 int rg_face_config(rg_ctx* ctx, int ilevel, int* variant, int* batch, float* ms);
 /* Pin the face-kernel shape of a level (variant 0..10, batch >= 1; 7 and 8

@@ -25,7 +25,7 @@ FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "
                 "--expt-relaxed-constexpr", f"-I{ROOT / 'include'}"]
 SOURCES = ["rg_api.cu", "rg_plan.cu", "rg_step.cu", "rg_face.cu", "rg_face_1d.cu", "rg_face_3d.cu",
            "rg_noalloc.cu", "rg_exact.cu", "rg_mlp.cu", "rg_host_level.cu",
-           "rg_lattice.cu", "rg_output.cu", "rg_tree.cu", "rg_amr.cu"]
+           "rg_lattice.cu", "rg_output.cu", "rg_tree.cu", "rg_amr.cu", "rg_measure.cu"]
 
 
 def _newer(target: Path, deps) -> bool:

@@ -168,6 +168,7 @@ def lib():
     L.rg_restrict_fine.argtypes = [VP, C.c_int]
     L.rg_count_grids.argtypes = [VP, C.c_int, IP]
     L.rg_amr_coarse_step.argtypes = [VP, C.POINTER(rg_amr_config), C.POINTER(rg_amr_clock)]
+    L.rg_measure_fp64_peak.argtypes = [VP, C.POINTER(C.c_double)]
     _lib = L
     return L
 
@@ -257,6 +258,12 @@ class Context:
     def amr_coarse_step(self, cfg, clock):
         """rg_amr_coarse_step: one coarse step of the resident run (clock updated in place)."""
         self._chk(self.L.rg_amr_coarse_step(self.h, C.byref(cfg), C.byref(clock)))
+
+    def measure_fp64_peak(self):
+        """Device FP64 throughput in TFLOP/s (rg_measure_fp64_peak)."""
+        v = C.c_double(0)
+        self._chk(self.L.rg_measure_fp64_peak(self.h, C.byref(v)))
+        return v.value
 
     def count_grids(self, il):
         n = C.c_int(0)
