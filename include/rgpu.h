@@ -157,6 +157,18 @@ int rg_synchronize(rg_ctx* ctx);
 int rg_set_stream(rg_ctx* ctx, void* stream);
 int rg_get_stream(rg_ctx* ctx, void** stream);
 
+/* A single-level run: the host loop
+ *     t = t_start; n = 0;
+ *     while (t < t_end && n < max_steps) { rg_level_substep(.., &dt); t += dt; ++n; }
+ * (Simulation's time loop when levelmin == levelmax, Simulation.cpp:366-430)
+ * as ONE CUDA graph launch: a WHILE conditional node repeats the substep and
+ * a clock kernel that adds dt on the device and sets the loop condition, so
+ * no dt travels to the host between substeps.  Same state bits, t and step
+ * count as the host loop.  Levels without refined cells whose stencils stay
+ * inside them (uniform periodic grids), one box; max_steps bounds the loop. */
+int rg_level_run(rg_ctx* ctx, int ilevel, double dx, int pressure_cap, double t_start, double t_end,
+                 int64_t max_steps, double* t_out, int64_t* steps_out);
+
 /* ---- exact solver and its learned Newton start ----------------------------- */
 /* Exact two-shock Newton solves (RiemannSolver::solve_godunov_nr,
  * RiemannSolver.cpp:194-307) of n independent interfaces.  Device arrays:

@@ -158,6 +158,19 @@ int ensure_flux(rg_ctx* c, const Plan& P) {
     return grow(c, &c->d_flux, &c->cap_flux, need, "flux scratch");
 }
 
+// rg_level_run's clock: start values, then after each substep t += dt, one
+// more step, and the WHILE node's condition for the next iteration
+__global__ void k_run_init(DevStatus* st, double t, long long steps) {
+    st->run_t = t;
+    st->run_steps = steps;
+}
+
+__global__ void k_run_advance(DevStatus* st, cudaGraphConditionalHandle h, double t_end, long long max_steps) {
+    st->run_t = st->run_t + st->dt;
+    st->run_steps += 1;
+    cudaGraphSetConditional(h, (st->run_t < t_end && st->run_steps < max_steps) ? 1u : 0u);
+}
+
 void record_updates(rg_ctx* c, int ilevel, const Plan& P) {
     if ((int)c->cell_updates.size() < c->nlevelmax + 1) c->cell_updates.resize(c->nlevelmax + 1, 0);
     c->cell_updates[ilevel] = P.nactive;
@@ -638,6 +651,97 @@ int rg_level_substep_host(rg_ctx* c, int ilevel, double dx, int pressure_cap, do
         *dt_used = c->h_status->dt;
     }
     return RG_OK;
+}
+
+int rg_level_run(rg_ctx* c, int ilevel, double dx, int pressure_cap, double t_start, double t_end, int64_t max_steps,
+                 double* t_out, int64_t* steps_out) {
+    CTX_GUARD(c);
+    if (!t_out || !steps_out) return set_error(c, RG_ERR_ARG, "t_out and steps_out required");
+    *t_out = t_start;
+    *steps_out = 0;
+    if (max_steps < 1 || !(t_start < t_end)) return RG_OK;  // the host loop would not enter
+    if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state uploaded");
+    if (int rc = check_learned(c)) return rc;
+    Plan* P;
+    if (int rc = get_plan(c, ilevel, &P)) return rc;
+    if (P->ncells == 0 || P->nactive != P->ncells || !leaf_fusable(*P) || P->nbox > 0)
+        return set_error(c, RG_ERR_UNSUPPORTED,
+                         "rg_level_run needs a level without refined cells whose stencils stay inside it (one box)");
+    double t = t_start;
+    long long n = 0;
+    if (P->face_variant < 0) {
+        // the first substep of a plan runs eagerly and chooses the face shape
+        double dt = 0.0;
+        if (int rc = rg_level_substep(c, ilevel, dx, pressure_cap, 0, &dt)) return rc;
+        t = t + dt;
+        n = 1;
+        if (int rc = get_plan(c, ilevel, &P)) return rc;
+        if (!(t < t_end) || n >= max_steps) {
+            *t_out = t;
+            *steps_out = n;
+            return RG_OK;
+        }
+    }
+    record_updates(c, ilevel, *P);
+    if (int rc = ensure_flux(c, *P)) return rc;
+    const double cfl = c->params.courant_factor;
+    const int cap_key = pressure_cap ? 1 : 0;
+    const bool ready = c->next_level == ilevel && c->next_cap == cap_key && c->next_dx == dx && c->next_cfl == cfl;
+    c->next_level = -1;
+    if (!ready)
+        if (int rc = launch_leaf_prefix(c, *P, dx, pressure_cap, cfl)) return rc;
+    k_run_init<<<1, 1, 0, c->stream>>>(c->d_status, t, n);
+    // one graph: a WHILE node whose body is the substep (dt finalize, face,
+    // fold with the next CFL word and primitives) and the clock advance
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    auto fail = [&](int rc) {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    };
+    if (int rc = check_cuda(c, cudaGraphCreate(&g, 0), "run graph")) return rc;
+    cudaGraphConditionalHandle h;
+    if (int rc = check_cuda(c, cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault), "run handle"))
+        return fail(rc);
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (int rc = check_cuda(c, cudaGraphAddNode(&node, g, nullptr, 0, &np), "run loop node")) return fail(rc);
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    const bool timing = c->timing;
+    c->timing = false;
+    if (int rc = check_cuda(c, cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0,
+                                                             cudaStreamCaptureModeThreadLocal),
+                            "run capture")) {
+        c->timing = timing;
+        return fail(rc);
+    }
+    int rc_enq = launch_leaf_core(c, *P, dx, pressure_cap, cfl);
+    k_run_advance<<<1, 1, 0, c->stream>>>(c->d_status, h, t_end, max_steps);
+    cudaGraph_t captured = nullptr;
+    cudaError_t ec = cudaStreamEndCapture(c->stream, &captured);
+    c->timing = timing;
+    if (rc_enq) return fail(rc_enq);
+    if (int rc = check_cuda(c, ec, "run capture end")) return fail(rc);
+    if (int rc = check_cuda(c, cudaGraphInstantiate(&exec, g, 0), "run graph instantiate")) return fail(rc);
+    if (int rc = check_cuda(c, cudaGraphLaunch(exec, c->stream), "run graph launch")) return fail(rc);
+    if (int rc = check_cuda(c, cudaMemcpyAsync(c->h_status, c->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                                               c->stream),
+                            "run clock"))
+        return fail(rc);
+    if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "run")) return fail(rc);
+    fail(RG_OK);
+    c->next_level = ilevel;  // the last fold left the next substep's CFL word and primitives
+    c->next_cap = cap_key;
+    c->next_dx = dx;
+    c->next_cfl = cfl;
+    *t_out = c->h_status->run_t;
+    *steps_out = c->h_status->run_steps;
+    return check_device_status(c);
 }
 
 int rg_set_level_boxes(rg_ctx* c, int ilevel, int nbox, const int* first_oct, const double* dx) {

@@ -53,6 +53,8 @@ struct DevStatus {
     int dx_pow2;
     unsigned int face_next, face_done;  // persistent face-kernel work queue
     unsigned long long exact_iters, exact_calls;  // exact-solver Newton statistics
+    double run_t;                                 // rg_level_run: the level's time and
+    long long run_steps;                          // substeps, advanced on the device
 };
 
 // Step values of one box of an ensemble level (independent periodic boxes

@@ -169,6 +169,8 @@ def lib():
     L.rg_count_grids.argtypes = [VP, C.c_int, IP]
     L.rg_amr_coarse_step.argtypes = [VP, C.POINTER(rg_amr_config), C.POINTER(rg_amr_clock)]
     L.rg_measure_fp64_peak.argtypes = [VP, C.POINTER(C.c_double)]
+    L.rg_level_run.argtypes = [VP, C.c_int, C.c_double, C.c_int, C.c_double, C.c_double, C.c_int64,
+                               C.POINTER(C.c_double), C.POINTER(C.c_int64)]
     _lib = L
     return L
 
@@ -258,6 +260,13 @@ class Context:
     def amr_coarse_step(self, cfg, clock):
         """rg_amr_coarse_step: one coarse step of the resident run (clock updated in place)."""
         self._chk(self.L.rg_amr_coarse_step(self.h, C.byref(cfg), C.byref(clock)))
+
+    def level_run(self, il, dx, t_end, t_start=0.0, pressure_cap=False, max_steps=10**7):
+        """rg_level_run: substeps until t >= t_end in one graph launch; returns (t, steps)."""
+        t, n = C.c_double(0), C.c_int64(0)
+        self._chk(self.L.rg_level_run(self.h, il, dx, 1 if pressure_cap else 0, t_start, t_end, int(max_steps),
+                                      C.byref(t), C.byref(n)))
+        return t.value, n.value
 
     def measure_fp64_peak(self):
         """Device FP64 throughput in TFLOP/s (rg_measure_fp64_peak)."""

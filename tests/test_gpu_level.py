@@ -487,3 +487,51 @@ def test_host_substeps_move_only_the_level(ctx_factory, oracle):
         assert bits_equal(host_unew.reshape(5, -1)[:, ids - 1], unew.reshape(5, -1)[:, ids - 1]), step
     assert bits_equal(host.reshape(5, -1)[:, outside - 1], before)
     assert np.all(host_unew.reshape(5, -1)[:, outside - 1] == 7.0)
+
+
+@pytest.mark.parametrize("case", ["sod1d", "sedov3d"])
+def test_level_run_matches_host_loop(ctx_factory, case):
+    """rg_level_run (one graph launch with a device-side WHILE loop) against the
+    host loop `while t < t_end: t += level_substep()`: same state bits, same
+    time, same step count; the 1D case is the Sod run of config 1 to t = 0.245."""
+    if case == "sod1d":
+        ndim, L, params, cap, t_end = 1, 11, make_params(1, slope_type=1, riemann="hllc"), True, 0.245
+        g = rg_tree.build_uniform(1, L)
+        u0 = rg_tree.sod_state(g, L, 1.4)
+    else:
+        ndim, L, params, cap, t_end = 3, 5, make_params(3, slope_type=2, riemann="hllc"), False, 1.5e-2
+        g = rg_tree.build_uniform(3, L)
+        u0 = rg_tree.sedov_state(g, L)
+    dx = 1.0 / 2 ** L
+    out = []
+    for mode in ("host", "run"):
+        ctx = ctx_factory(params)
+        ctx.sync_topology(g)
+        ctx.upload_state(u0, u0)
+        if mode == "host":
+            t, n = 0.0, 0
+            while t < t_end:
+                t += ctx.level_substep(L, dx, pressure_cap=cap, use_graph=True, want_dt=True)
+                n += 1
+        else:
+            t, n = ctx.level_run(L, dx, t_end, pressure_cap=cap)
+        u = np.empty_like(u0)
+        ctx.download_state(uold=u)
+        out.append((t, n, u))
+    (t0, n0, u0h), (t1, n1, u1) = out
+    assert n0 > 10 and n1 == n0 and t1 == t0
+    assert bits_equal(u1, u0h)
+
+
+def test_level_run_stops_at_max_steps(ctx_factory):
+    L = 11
+    g = rg_tree.build_uniform(1, L)
+    u0 = rg_tree.sod_state(g, L, 1.4)
+    ctx = ctx_factory(make_params(1, slope_type=1, riemann="hllc"))
+    ctx.sync_topology(g)
+    ctx.upload_state(u0, u0)
+    t, n = ctx.level_run(L, 1.0 / 2 ** L, 10.0, pressure_cap=True, max_steps=37)
+    assert n == 37 and 0.0 < t < 10.0
+    t2, n2 = ctx.level_run(L, 1.0 / 2 ** L, 10.0, t_start=t, pressure_cap=True, max_steps=3)
+    assert n2 == 3 and t2 > t
+    assert ctx.level_run(L, 1.0 / 2 ** L, 0.0, t_start=1.0) == (1.0, 0)  # t_start >= t_end: no substep
