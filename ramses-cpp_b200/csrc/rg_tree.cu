@@ -565,11 +565,12 @@ __global__ void k_restrict(TreeMut M, const int* __restrict__ octs, int noct) {
 // ---------------------------------------------------------------- host side
 int hidx(const rg_ctx* c, int ilevel) { return ilevel * (c->ncpu + c->nboundary); }
 
-// RG_OK to go on, a negative value when the call is a no-op (ilevel >= nlevelmax,
-// where the reference returns at once), else an error code
+// RG_OK to go on, kNoOp when the call does nothing (ilevel >= nlevelmax, where
+// the reference returns at once), else an error code (error codes are negative)
+constexpr int kNoOp = 1;
 int check_tree(rg_ctx* c, int ilevel) {
     if (!c->tree_resident) return set_error(c, RG_ERR_STATE, "no device-resident tree: call rg_tree_attach first");
-    if (ilevel >= c->nlevelmax) return -1;
+    if (ilevel >= c->nlevelmax) return kNoOp;
     if (ilevel < 1) return set_error(c, RG_ERR_ARG, "level below 1");
     c->next_level = -1;  // the state or the topology may change
     return refresh_tree(c);
@@ -608,7 +609,7 @@ int set_dev_int(rg_ctx* c, int* dst, int v) {
 
 int tree_flag_fine(rg_ctx* c, int ilevel, double ed, double ep, double ev, double eb2, int nexp, int icount,
                    int nsub) {
-    if (int rc = check_tree(c, ilevel)) return rc < 0 ? RG_OK : rc;  // no-op at and above nlevelmax (TreeUpdater.cpp:329)
+    if (int rc = check_tree(c, ilevel)) return rc == kNoOp ? RG_OK : rc;  // no-op at and above nlevelmax (TreeUpdater.cpp:329)
     if (eb2 > 0.0) return set_error(c, RG_ERR_UNSUPPORTED, "err_grad_b2 needs MHD variables");
     TreeMut M = tree_mut(c);
     cudaStream_t s = c->stream;
@@ -645,7 +646,7 @@ int tree_flag_fine(rg_ctx* c, int ilevel, double ed, double ep, double ev, doubl
 }
 
 int tree_make_grid_fine(rg_ctx* c, int ilevel) {
-    if (int rc = check_tree(c, ilevel)) return rc < 0 ? RG_OK : rc;  // no-op at and above nlevelmax (TreeUpdater.cpp:28)
+    if (int rc = check_tree(c, ilevel)) return rc == kNoOp ? RG_OK : rc;  // no-op at and above nlevelmax (TreeUpdater.cpp:28)
     TreeScratch S;
     if (int rc = tree_scratch(c, &S)) return rc;
     TreeMut M = tree_mut(c);
@@ -695,7 +696,7 @@ int tree_make_grid_fine(rg_ctx* c, int ilevel) {
 }
 
 int tree_remove_grid_fine(rg_ctx* c, int ilevel) {
-    if (int rc = check_tree(c, ilevel)) return rc < 0 ? RG_OK : rc;  // no-op at and above nlevelmax (TreeUpdater.cpp:152)
+    if (int rc = check_tree(c, ilevel)) return rc == kNoOp ? RG_OK : rc;  // no-op at and above nlevelmax (TreeUpdater.cpp:152)
     TreeScratch S;
     if (int rc = tree_scratch(c, &S)) return rc;
     int noct = 0;

@@ -118,3 +118,63 @@ def test_device_resident_amr_run_matches_reference(rgpu_lib, native):
         assert h.tree_arrays()["headf"] != headf0, "no oct was allocated during the run"
     finally:
         ctx.close()
+
+
+def test_tree_calls_report_misuse(rgpu_lib):
+    """Errors instead of undefined behaviour: no attached tree, an inconsistent
+    free list, a refinement that needs more octs than the free list holds (the
+    reference would double ngridmax), and a single-level run on a level that
+    has refined cells."""
+    h, _ = reference_run(0)
+    params = rgpu.make_params(3, slope_type=2, riemann="hllc", gamma=GAMMA)
+    ctx = rgpu.Context(params, 0)
+    try:
+        with pytest.raises(rgpu.RGError) as e:
+            ctx.make_grid_fine(LMIN)
+        assert e.value.code == rgpu.RG_ERR_STATE
+        bad = dict(h.tree_arrays())
+        bad["numbf"] = int(bad["numbf"]) + 1
+        with pytest.raises(rgpu.RGError) as e:
+            ctx.tree_attach(h.grid(), bad, LMIN)
+        assert e.value.code == rgpu.RG_ERR_TOPOLOGY
+        ctx.tree_attach(h.grid(), h.tree_arrays(), LMIN)
+        with pytest.raises(rgpu.RGError) as e:
+            ctx.level_run(LMIN, 1.0 / 2 ** LMIN, 1.0)  # level LMIN has refined cells after initialisation
+        assert e.value.code == rgpu.RG_ERR_UNSUPPORTED
+        assert ctx.count_grids(LMAX + 5) == 0
+    finally:
+        ctx.close()
+
+
+def test_free_list_exhaustion_is_an_error(rgpu_lib):
+    """The device is handed an empty free list; a refinement that creates octs
+    on the reference (which would grow its arrays when it ran out) must fail
+    with RG_ERR_UNSUPPORTED instead."""
+    h, _ = reference_run(0)
+    t = {k: (v.copy() if hasattr(v, "copy") else v) for k, v in h.tree_arrays().items()}
+    t["headf"], t["tailf"], t["numbf"] = 0, 0, 0
+    ctx = device_ctx_from(h.grid(), t)
+    try:
+        for il in range(LMIN, LMAX):
+            args = (il, ED, EP, -1.0, -1.0, 3, 2, 2)  # wider smoothing than the run's: flags beyond the refined region
+            h.flag_fine(*args)
+            ctx.flag_fine(*args)
+            n0 = h.count_grids(il + 1)
+            h.make_grid_fine(il)
+            if h.count_grids(il + 1) == n0:
+                ctx.make_grid_fine(il)  # nothing to create on either side
+                continue
+            with pytest.raises(rgpu.RGError) as e:
+                ctx.make_grid_fine(il)
+            assert e.value.code == rgpu.RG_ERR_UNSUPPORTED
+            return
+        pytest.fail("the reference created no oct on any level: the case proves nothing")
+    finally:
+        ctx.close()
+
+
+def device_ctx_from(g, arrays):
+    params = rgpu.make_params(3, slope_type=2, riemann="hllc", gamma=GAMMA)
+    ctx = rgpu.Context(params, 0)
+    ctx.tree_attach(g, arrays, LMIN)
+    return ctx
