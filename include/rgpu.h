@@ -164,8 +164,11 @@ int rg_get_stream(rg_ctx* ctx, void** stream);
  * as ONE CUDA graph launch: a WHILE conditional node repeats the substep and
  * a clock kernel that adds dt on the device and sets the loop condition, so
  * no dt travels to the host between substeps.  Same state bits, t and step
- * count as the host loop.  Levels without refined cells whose stencils stay
- * inside them (uniform periodic grids), one box; max_steps bounds the loop. */
+ * count as the host loop.  Levels of at most 1024 cells run the whole loop
+ * in one single-block kernel instead (block barriers between the phases of
+ * a substep, no launch per substep).  Levels without refined cells whose
+ * stencils stay inside them (uniform periodic grids), one box; max_steps
+ * bounds the loop. */
 int rg_level_run(rg_ctx* ctx, int ilevel, double dx, int pressure_cap, double t_start, double t_end,
                  int64_t max_steps, double* t_out, int64_t* steps_out);
 

@@ -691,6 +691,22 @@ int rg_level_run(rg_ctx* c, int ilevel, double dx, int pressure_cap, double t_st
     if (!ready)
         if (int rc = launch_leaf_prefix(c, *P, dx, pressure_cap, cfl)) return rc;
     k_run_init<<<1, 1, 0, c->stream>>>(c->d_status, t, n);
+    if (P->ncells <= kRunBlockCells) {
+        // small level: the whole loop in one single-block kernel
+        if (int rc = launch_run_block(c, *P, dx, pressure_cap, t_end, max_steps)) return rc;
+        if (int rc = check_cuda(c, cudaMemcpyAsync(c->h_status, c->d_status, sizeof(DevStatus),
+                                                   cudaMemcpyDeviceToHost, c->stream),
+                                "run clock"))
+            return rc;
+        if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "run")) return rc;
+        c->next_level = ilevel;
+        c->next_cap = cap_key;
+        c->next_dx = dx;
+        c->next_cfl = cfl;
+        *t_out = c->h_status->run_t;
+        *steps_out = c->h_status->run_steps;
+        return check_device_status(c);
+    }
     // one graph: a WHILE node whose body is the substep (dt finalize, face,
     // fold with the next CFL word and primitives) and the clock advance
     cudaGraph_t g = nullptr;

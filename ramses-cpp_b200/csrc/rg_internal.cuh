@@ -251,6 +251,11 @@ int level_oct_list(rg_ctx* c, int ilevel, int* out, int cap, int* noct);
 // after device tree operations changed links: drop plans, re-rank the lists,
 // recompute cell levels (no-op when nothing changed)
 int refresh_tree(rg_ctx* c);
+// rg_level_run on a level of at most kRunBlockCells cells (two per thread of
+// the block): the whole loop in one single-block kernel (rg_step.cu); the clock
+// in DevStatus run_t/run_steps.  Larger levels are faster spread over the GPU.
+constexpr int kRunBlockCells = 1024;
+int launch_run_block(rg_ctx* c, const Plan& P, double dx, int pressure_cap, double t_end, long long max_steps);
 // TreeUpdater operations on the device-resident tree (rg_tree.cu)
 int tree_flag_fine(rg_ctx* c, int ilevel, double ed, double ep, double ev, double eb2, int nexp, int icount,
                    int nsub);

@@ -740,4 +740,162 @@ int launch_set_dt_host(rg_ctx* c, double dt, double dx) {
     return check_cuda(c, cudaGetLastError(), "dt set");
 }
 
+// ---------------------------------------------------------------- small-level runs
+// rg_level_run on a small level (at most kRunBlockCells cells): the whole
+// loop in ONE block of one kernel.  Each substep is the fused leaf substep of
+// the three kernels above with block barriers in place of kernel boundaries:
+// dt from the CFL word (re-armed), every cell's fluxes and own flux sum (the
+// per-(cell, direction) work of k_face_tiles, same functions, same order),
+// then every target's ordered fold with the next primitives and CFL
+// candidates (k_fold_next), then the clock.  Global writes of one phase are
+// visible to the whole block after the barrier, and only one block exists,
+// so nothing waits across blocks; max_steps bounds the loop.
+namespace {
+
+constexpr int kRunBlock = 512;
+
+template <int NDIM, int RS>
+__global__ void __launch_bounds__(kRunBlock) k_level_run_block(TreeView T, PlanView P, double* __restrict__ uold,
+                                                              double* __restrict__ unew, double* __restrict__ prim,
+                                                              double* __restrict__ flux, double* __restrict__ fsum,
+                                                              DevStatus* st, StepK K, double dx, double cfl,
+                                                              int pressure_cap, double dt_start, double t_end,
+                                                              long long max_steps) {
+    constexpr int NV = Dims<NDIM>::NV, NS = Dims<NDIM>::NS;
+    const size_t ncell = (size_t)T.ncell;
+    const int nc = P.ncells, nt = P.ntarg;
+    __shared__ int s_go;
+    __shared__ unsigned long long s_best;
+    unsigned long long iters = 0, calls = 0;
+    for (long long guard = 0; guard < max_steps; ++guard) {
+        if (threadIdx.x == 0) {
+            set_step_values(st, __longlong_as_double((long long)st->dtmin_bits), dx);
+            st->dtmin_bits = (unsigned long long)__double_as_longlong(dt_start);
+            s_best = ~0ULL;
+        }
+        __syncthreads();
+        const double dt = st->dt;
+        const DxDiv D{st->dx, st->inv_dx, st->dx_pow2 != 0};
+        // fluxes and own flux sums
+        for (int p = threadIdx.x; p < nc; p += blockDim.x) {
+            const int c = cell_of(T, P, p);
+            double fs[NV];
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) fs[iv] = 0.0;
+            bool any = false;
+#pragma unroll 1
+            for (int idim = 0; idim < NDIM; ++idim) {
+                const int s0 = 2 * idim;
+                const int kd0 = P.kind[(size_t)s0 * nc + p];
+                if (kd0 == K_NONE) continue;
+                any = true;
+                const int kd1 = P.kind[(size_t)(s0 + 1) * nc + p];
+                double qc[NV], qmo[NV], qpo[NV], ql[NV], qr[NV];
+                load_rot<NDIM>(prim, ncell, c, idim, qc);
+                const int l = P.icn[(size_t)s0 * nc + p], rr = P.icn[(size_t)(s0 + 1) * nc + p];
+                load_nb_rot<NDIM>(T, prim, ncell, l, idim, qc, ql);
+                load_nb_rot<NDIM>(T, prim, ncell, rr, idim, qc, qr);
+                own_trace<NDIM>(qc, ql, qr, dt, D, K, qmo, qpo);
+#pragma unroll
+                for (int side = 0; side < 2; ++side) {
+                    const int kd = side ? kd1 : kd0;
+                    const int s = s0 + side;
+                    double f[NV];
+                    if ((kd & KIND_MASK) == K_ZERO) {
+#pragma unroll
+                        for (int iv = 0; iv < NV; ++iv) f[iv] = 0.0;
+                    } else {
+                        const int n = P.icn[(size_t)s * nc + p];
+                        double qf[NV];
+                        neighbour_face<NDIM>(T, P, prim, uold, ncell, p, c, idim, side, kd, n, qc, nullptr, dt, D, K,
+                                             qf);
+                        if (side == 0) iters += riemann<NDIM, RS>(qf, qpo, f, K);
+                        else iters += riemann<NDIM, RS>(qmo, qf, f, K);
+                        ++calls;
+                        rot_swap<NDIM>(f, idim);
+                    }
+                    const double sign = side ? -1.0 : 1.0;
+#pragma unroll
+                    for (int iv = 0; iv < NV; ++iv) {
+                        flux[((size_t)s * NV + iv) * nc + p] = f[iv];
+                        fs[iv] = fs[iv] + sign * f[iv];
+                    }
+                }
+            }
+            if (any)
+#pragma unroll
+                for (int iv = 0; iv < NV; ++iv) fsum[(size_t)iv * nc + p] = fs[iv];
+        }
+        __syncthreads();
+        // ordered fold, next primitives and CFL candidates
+        unsigned long long best = ~0ULL;
+        for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+            const int a = P.toff[t], b = P.toff[t + 1];
+            const int cell = cell_of(T, P, t);
+            double u[NV], q[NV];
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) u[iv] = uold[(size_t)iv * ncell + cell - 1];
+            if (a < b) {
+                fold_events<NDIM, true, true>(P, a, b, flux, fsum, K.gamma, st->dtdx, u);
+#pragma unroll
+                for (int iv = 0; iv < NV; ++iv) {
+                    unew[(size_t)iv * ncell + cell - 1] = u[iv];
+                    uold[(size_t)iv * ncell + cell - 1] = u[iv];
+                }
+            }
+            ctoprim<NDIM>(u, q, K.gamma, K.smalle);
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) prim[(size_t)iv * ncell + cell - 1] = q[iv];
+            if (T.son[cell - 1] == 0) {
+                unsigned long long bits;
+                if (cfl_candidate<NDIM>(u, dx, K.gamma, cfl, pressure_cap, &bits) && bits < best) best = bits;
+            }
+        }
+        if (best != ~0ULL) atomicMin(&s_best, best);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            if (s_best != ~0ULL) atomicMin(&st->dtmin_bits, s_best);
+            st->run_t = st->run_t + dt;
+            st->run_steps += 1;
+            s_go = (st->run_t < t_end && st->run_steps < max_steps) ? 1 : 0;
+        }
+        __syncthreads();
+        if (!s_go) break;
+    }
+    if (RS == RG_RIEMANN_EXACT) {
+        if (calls) {
+            atomicAdd(&st->exact_iters, iters);
+            atomicAdd(&st->exact_calls, calls);
+        }
+    }
+}
+
+template <int NDIM>
+int launch_run_block_t(rg_ctx* c, const Plan& P, double dx, int pressure_cap, double t_end, long long max_steps) {
+    StepK K = step_consts(c);
+    const double start = c->params.boxlen / 1e-10, cfl = c->params.courant_factor;
+    double* fsum = c->d_flux + (size_t)(2 * NDIM) * (NDIM + 2) * P.ncells;
+#define RG_RUN_ARGS                                                                                                  \
+    tree_view(c), P.view(), c->d_uold, c->d_unew, c->d_prim, c->d_flux, fsum, c->d_status, K, dx, cfl, pressure_cap, \
+        start, t_end, max_steps
+    switch (c->params.riemann) {
+        case RG_RIEMANN_HLLC: k_level_run_block<NDIM, RG_RIEMANN_HLLC><<<1, kRunBlock, 0, c->stream>>>(RG_RUN_ARGS); break;
+        case RG_RIEMANN_HLL: k_level_run_block<NDIM, RG_RIEMANN_HLL><<<1, kRunBlock, 0, c->stream>>>(RG_RUN_ARGS); break;
+        case RG_RIEMANN_EXACT: k_level_run_block<NDIM, RG_RIEMANN_EXACT><<<1, kRunBlock, 0, c->stream>>>(RG_RUN_ARGS); break;
+        case RG_RIEMANN_ACOUSTIC:
+            k_level_run_block<NDIM, RG_RIEMANN_ACOUSTIC><<<1, kRunBlock, 0, c->stream>>>(RG_RUN_ARGS);
+            break;
+        default: k_level_run_block<NDIM, RG_RIEMANN_LLF><<<1, kRunBlock, 0, c->stream>>>(RG_RUN_ARGS); break;
+    }
+#undef RG_RUN_ARGS
+    return check_cuda(c, cudaGetLastError(), "small-level run kernel");
+}
+
+}  // namespace
+
+int launch_run_block(rg_ctx* c, const Plan& P, double dx, int pressure_cap, double t_end, long long max_steps) {
+    if (c->params.ndim == 1) return launch_run_block_t<1>(c, P, dx, pressure_cap, t_end, max_steps);
+    return launch_run_block_t<3>(c, P, dx, pressure_cap, t_end, max_steps);
+}
+
 }  // namespace rg

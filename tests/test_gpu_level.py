@@ -489,12 +489,17 @@ def test_host_substeps_move_only_the_level(ctx_factory, oracle):
     assert np.all(host_unew.reshape(5, -1)[:, outside - 1] == 7.0)
 
 
-@pytest.mark.parametrize("case", ["sod1d", "sedov3d"])
+@pytest.mark.parametrize("case", ["sod1d", "sedov3d_small", "sedov3d"])
 def test_level_run_matches_host_loop(ctx_factory, case):
-    """rg_level_run (one graph launch with a device-side WHILE loop) against the
-    host loop `while t < t_end: t += level_substep()`: same state bits, same
-    time, same step count; the 1D case is the Sod run of config 1 to t = 0.245."""
-    if case == "sod1d":
+    """rg_level_run against the host loop `while t < t_end: t += level_substep()`:
+    same state bits, same time, same step count.  sod1d (1024 cells, the Sod
+    run of config 1 to t = 0.245) and sedov3d_small (8^3 = 512 cells) take the
+    single-block kernel; sedov3d (32^3) the graph with a device-side WHILE loop."""
+    if case == "sedov3d_small":
+        ndim, L, params, cap, t_end = 3, 3, make_params(3, slope_type=2, riemann="hllc"), False, 0.3
+        g = rg_tree.build_uniform(3, L)
+        u0 = rg_tree.sedov_state(g, L)
+    elif case == "sod1d":
         ndim, L, params, cap, t_end = 1, 11, make_params(1, slope_type=1, riemann="hllc"), True, 0.245
         g = rg_tree.build_uniform(1, L)
         u0 = rg_tree.sod_state(g, L, 1.4)
