@@ -511,10 +511,18 @@ int level_oct_list(rg_ctx* c, int ilevel, int* out, int cap, int* noct) {
     if (head == 0) return RG_OK;
     cudaStream_t s = c->stream;
     int dh = 0, count = 0;
-    if (int rc = check_cuda(c, cudaMemcpyAsync(&dh, c->d_dist + head - 1, sizeof(int), cudaMemcpyDeviceToHost, s),
-                            "list length"))
-        return rc;
-    if (int rc = check_cuda(c, cudaStreamSynchronize(s), "list length sync")) return rc;
+    if (c->tree_resident) {
+        // the resident tree keeps every level's count on the host: no read of
+        // the list length (a longer list raises DE_LIST in k_level_octs, a
+        // shorter one fails the count check below)
+        dh = c->h_numbl[(size_t)ilevel * (c->ncpu + c->nboundary)] - 1;
+        if (dh < 0) return set_error(c, RG_ERR_TOPOLOGY, "level count and head disagree");
+    } else {
+        if (int rc = check_cuda(c, cudaMemcpyAsync(&dh, c->d_dist + head - 1, sizeof(int), cudaMemcpyDeviceToHost, s),
+                                "list length"))
+            return rc;
+        if (int rc = check_cuda(c, cudaStreamSynchronize(s), "list length sync")) return rc;
+    }
     const int n = dh + 1;
     if (n > cap) return set_error(c, RG_ERR_TOPOLOGY, "level list longer than ngridmax");
     if (c->cap_scan < 4) {

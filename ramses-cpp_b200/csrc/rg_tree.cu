@@ -598,11 +598,12 @@ int tree_scratch(rg_ctx* c, TreeScratch* s) {
     return RG_OK;
 }
 
+__global__ void k_set_int(int* dst, int v) { *dst = v; }
+
+// one link write in stream order (a kernel argument, so nothing waits)
 int set_dev_int(rg_ctx* c, int* dst, int v) {
-    // synchronous: the value lives on this stack frame
-    if (int rc = check_cuda(c, cudaMemcpyAsync(dst, &v, sizeof(int), cudaMemcpyHostToDevice, c->stream), "tree link"))
-        return rc;
-    return check_cuda(c, cudaStreamSynchronize(c->stream), "tree link");
+    k_set_int<<<1, 1, 0, c->stream>>>(dst, v);
+    return check_cuda(c, cudaGetLastError(), "tree link");
 }
 
 }  // namespace
