@@ -168,7 +168,8 @@ int rg_get_stream(rg_ctx* ctx, void** stream);
  * in one single-block kernel instead (block barriers between the phases of
  * a substep, no launch per substep).  Levels without refined cells whose
  * stencils stay inside them (uniform periodic grids), one box; max_steps
- * bounds the loop. */
+ * bounds the loop, and each launch runs at most 65,536 substeps (the host
+ * relaunches until t_end or max_steps), so no launch runs for long. */
 int rg_level_run(rg_ctx* ctx, int ilevel, double dx, int pressure_cap, double t_start, double t_end,
                  int64_t max_steps, double* t_out, int64_t* steps_out);
 

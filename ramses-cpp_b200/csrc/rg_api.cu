@@ -165,11 +165,17 @@ __global__ void k_run_init(DevStatus* st, double t, long long steps) {
     st->run_steps = steps;
 }
 
-__global__ void k_run_advance(DevStatus* st, cudaGraphConditionalHandle h, double t_end, long long max_steps) {
+__global__ void k_run_limit(DevStatus* st, long long limit) { st->run_limit = limit; }
+
+__global__ void k_run_advance(DevStatus* st, cudaGraphConditionalHandle h, double t_end) {
     st->run_t = st->run_t + st->dt;
     st->run_steps += 1;
-    cudaGraphSetConditional(h, (st->run_t < t_end && st->run_steps < max_steps) ? 1u : 0u);
+    cudaGraphSetConditional(h, (st->run_t < t_end && st->run_steps < st->run_limit) ? 1u : 0u);
 }
+
+// substeps per launch of the run kernel or graph: bounds how long one launch
+// runs (tens of milliseconds to seconds) whatever max_steps the caller asks
+constexpr long long kRunChunk = 65536;
 
 void record_updates(rg_ctx* c, int ilevel, const Plan& P) {
     if ((int)c->cell_updates.size() < c->nlevelmax + 1) c->cell_updates.resize(c->nlevelmax + 1, 0);
@@ -691,20 +697,30 @@ int rg_level_run(rg_ctx* c, int ilevel, double dx, int pressure_cap, double t_st
     if (!ready)
         if (int rc = launch_leaf_prefix(c, *P, dx, pressure_cap, cfl)) return rc;
     k_run_init<<<1, 1, 0, c->stream>>>(c->d_status, t, n);
-    if (P->ncells <= kRunBlockCells) {
-        // small level: the whole loop in one single-block kernel
-        if (int rc = launch_run_block(c, *P, dx, pressure_cap, t_end, max_steps)) return rc;
+    // launches of at most kRunChunk substeps until t_end or max_steps
+    auto read_clock = [&]() -> int {
         if (int rc = check_cuda(c, cudaMemcpyAsync(c->h_status, c->d_status, sizeof(DevStatus),
                                                    cudaMemcpyDeviceToHost, c->stream),
                                 "run clock"))
             return rc;
         if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "run")) return rc;
+        t = c->h_status->run_t;
+        n = c->h_status->run_steps;
+        return c->h_status->err ? check_device_status(c) : RG_OK;
+    };
+    if (P->ncells <= kRunBlockCells) {
+        // small level: the loop in a single-block kernel
+        while (t < t_end && n < max_steps) {
+            const long long limit = std::min<long long>(max_steps, n + kRunChunk);
+            if (int rc = launch_run_block(c, *P, dx, pressure_cap, t_end, limit)) return rc;
+            if (int rc = read_clock()) return rc;
+        }
         c->next_level = ilevel;
         c->next_cap = cap_key;
         c->next_dx = dx;
         c->next_cfl = cfl;
-        *t_out = c->h_status->run_t;
-        *steps_out = c->h_status->run_steps;
+        *t_out = t;
+        *steps_out = n;
         return check_device_status(c);
     }
     // one graph: a WHILE node whose body is the substep (dt finalize, face,
@@ -737,26 +753,25 @@ int rg_level_run(rg_ctx* c, int ilevel, double dx, int pressure_cap, double t_st
         return fail(rc);
     }
     int rc_enq = launch_leaf_core(c, *P, dx, pressure_cap, cfl);
-    k_run_advance<<<1, 1, 0, c->stream>>>(c->d_status, h, t_end, max_steps);
+    k_run_advance<<<1, 1, 0, c->stream>>>(c->d_status, h, t_end);
     cudaGraph_t captured = nullptr;
     cudaError_t ec = cudaStreamEndCapture(c->stream, &captured);
     c->timing = timing;
     if (rc_enq) return fail(rc_enq);
     if (int rc = check_cuda(c, ec, "run capture end")) return fail(rc);
     if (int rc = check_cuda(c, cudaGraphInstantiate(&exec, g, 0), "run graph instantiate")) return fail(rc);
-    if (int rc = check_cuda(c, cudaGraphLaunch(exec, c->stream), "run graph launch")) return fail(rc);
-    if (int rc = check_cuda(c, cudaMemcpyAsync(c->h_status, c->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
-                                               c->stream),
-                            "run clock"))
-        return fail(rc);
-    if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "run")) return fail(rc);
+    while (t < t_end && n < max_steps) {
+        k_run_limit<<<1, 1, 0, c->stream>>>(c->d_status, std::min<long long>(max_steps, n + kRunChunk));
+        if (int rc = check_cuda(c, cudaGraphLaunch(exec, c->stream), "run graph launch")) return fail(rc);
+        if (int rc = read_clock()) return fail(rc);
+    }
     fail(RG_OK);
     c->next_level = ilevel;  // the last fold left the next substep's CFL word and primitives
     c->next_cap = cap_key;
     c->next_dx = dx;
     c->next_cfl = cfl;
-    *t_out = c->h_status->run_t;
-    *steps_out = c->h_status->run_steps;
+    *t_out = t;
+    *steps_out = n;
     return check_device_status(c);
 }
 

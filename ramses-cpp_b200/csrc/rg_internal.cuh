@@ -54,7 +54,8 @@ struct DevStatus {
     unsigned int face_next, face_done;  // persistent face-kernel work queue
     unsigned long long exact_iters, exact_calls;  // exact-solver Newton statistics
     double run_t;                                 // rg_level_run: the level's time and
-    long long run_steps;                          // substeps, advanced on the device
+    long long run_steps;                          // substeps, advanced on the device,
+    long long run_limit;                          // and the step count this launch stops at
 };
 
 // Step values of one box of an ensemble level (independent periodic boxes
