@@ -43,24 +43,28 @@ struct BrickGeom {
     const int* brick_off;
 };
 
-template <int RS, int MINB, bool BOXED>
-__global__ void __launch_bounds__(BRICK_THREADS, MINB)
-    k_face_brick(PlanView P, BrickGeom G, const int* __restrict__ lat_id, const int* __restrict__ lat_p, int kind,
-                 const double* __restrict__ prim, size_t ncell, double* __restrict__ flux,
-                 double* __restrict__ fsum, DevStatus* st, StepK K) {
+// The face work of one brick (index `brick` in the level's brick order), by
+// the whole block: stage the brick and its halo in sq (shared, [NV][BSITES]),
+// then every cell's fluxes and own flux sum.  Newton statistics of the exact
+// solver are added to iters / calls.
+template <int RS, bool BOXED>
+__device__ __forceinline__ void brick_face(const PlanView& P, const BrickGeom& G, const int* __restrict__ lat_id,
+                                           const int* __restrict__ lat_p, int kind, const double* __restrict__ prim,
+                                           size_t ncell, double* __restrict__ flux, double* __restrict__ fsum,
+                                           const DevStatus* st, const StepK& K, int brick, double* sq,
+                                           unsigned long long& iters, unsigned long long& calls) {
     constexpr int NV = 5;
-    extern __shared__ __align__(16) double sq[];  // [NV][BSITES]
-    int ex = G.ex, ey = G.ey, ez = G.ez, local = blockIdx.x;
+    int ex = G.ex, ey = G.ey, ez = G.ez, local = brick;
     double dt = st->dt;
     DxDiv D{st->dx, st->inv_dx, st->dx_pow2 != 0};
     if constexpr (BOXED) {
         int lo = 0, hi = G.nbox - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (G.brick_off[mid] <= (int)blockIdx.x) lo = mid;
+            if (G.brick_off[mid] <= brick) lo = mid;
             else hi = mid - 1;
         }
-        local = blockIdx.x - G.brick_off[lo];
+        local = brick - G.brick_off[lo];
         ex = G.ext[3 * lo];
         ey = G.ext[3 * lo + 1];
         ez = G.ext[3 * lo + 2];
@@ -86,7 +90,6 @@ __global__ void __launch_bounds__(BRICK_THREADS, MINB)
     __syncthreads();
     const int nc = P.ncells;
     const bool ghost = (kind & KIND_MASK) == K_GHOST;
-    unsigned long long iters = 0, calls = 0;
     for (int u = threadIdx.x; u < BRICK * BRICK * BRICK; u += blockDim.x) {
         const int x = u % BRICK, y = (u / BRICK) % BRICK, z = u / (BRICK * BRICK);
         const int site = (x + BHALO) + BSIDE * ((y + BHALO) + BSIDE * (z + BHALO));
@@ -128,6 +131,17 @@ __global__ void __launch_bounds__(BRICK_THREADS, MINB)
 #pragma unroll
         for (int iv = 0; iv < NV; ++iv) fsum[(size_t)iv * nc + p] = fs[iv];
     }
+}
+
+template <int RS, int MINB, bool BOXED>
+__global__ void __launch_bounds__(BRICK_THREADS, MINB)
+    k_face_brick(PlanView P, BrickGeom G, const int* __restrict__ lat_id, const int* __restrict__ lat_p, int kind,
+                 const double* __restrict__ prim, size_t ncell, double* __restrict__ flux,
+                 double* __restrict__ fsum, DevStatus* st, StepK K) {
+    extern __shared__ __align__(16) double sq[];  // [NV][BSITES]
+    unsigned long long iters = 0, calls = 0;
+    brick_face<RS, BOXED>(P, G, lat_id, lat_p, kind, prim, ncell, flux, fsum, st, K, (int)blockIdx.x, sq, iters,
+                          calls);
     if (RS == RG_RIEMANN_EXACT) {
         for (int o = 16; o > 0; o >>= 1) {
             iters += __shfl_xor_sync(0xffffffffu, iters, o);
