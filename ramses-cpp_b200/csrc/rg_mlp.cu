@@ -358,10 +358,14 @@ int mlp_ensure(rg_ctx* c) {
 }
 
 static int grad_launch(rg_ctx* c, const float* X, const float* T, int N, int n0, int nb, float* grad, float* loss) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrainSmem));
-        attr = true;
+    static bool attr_set[64] = {};  // per device: the shared-memory opt-in is a function attribute
+    const int dev = c->device & 63;
+    if (!attr_set[dev]) {
+        if (int rc = check_cuda(c, cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                        (int)sizeof(TrainSmem)),
+                                "MLP gradient kernel shared memory"))
+            return rc;
+        attr_set[dev] = true;
     }
     int tiles = (nb + SPB - 1) / SPB;
     int grid = tiles < c->sm_count ? tiles : c->sm_count;
