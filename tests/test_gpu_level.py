@@ -540,3 +540,11 @@ def test_level_run_stops_at_max_steps(ctx_factory):
     t2, n2 = ctx.level_run(L, 1.0 / 2 ** L, 10.0, t_start=t, pressure_cap=True, max_steps=3)
     assert n2 == 3 and t2 > t
     assert ctx.level_run(L, 1.0 / 2 ** L, 0.0, t_start=1.0) == (1.0, 0)  # t_start >= t_end: no substep
+
+
+def test_fp64_peak_probe(ctx_factory):
+    """rg_measure_fp64_peak: the FP64 throughput the face kernel's compute
+    roofline is reported against; a B200 lands in the tens of TFLOP/s."""
+    ctx = ctx_factory(make_params(3))
+    v = ctx.measure_fp64_peak()
+    assert 5.0 < v < 200.0, v
