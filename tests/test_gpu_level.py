@@ -459,9 +459,12 @@ def test_substep_on_amr_levels(ctx_factory, oracle, golden, key):
     assert bits_equal(a, uold) and bits_equal(b, unew)
 
 
-def test_host_substeps_move_only_the_level(ctx_factory, oracle):
+@pytest.mark.parametrize("memory", ["pageable", "pinned"])
+def test_host_substeps_move_only_the_level(ctx_factory, oracle, memory):
     """rg_level_substep_host on a host array: oracle bits and dt each substep,
-    and cells outside the level (the coarse levels) keep their host values."""
+    and cells outside the level (the coarse levels) keep their host values.
+    pageable: numpy arrays (gathered run by run into pinned staging); pinned:
+    page-locked arrays (one DMA per run of consecutive cell ids)."""
     L = 5
     g = rg_tree.build_uniform(3, L)
     ga = ga_of(g)
@@ -470,8 +473,14 @@ def test_host_substeps_move_only_the_level(ctx_factory, oracle):
     ctx.sync_topology(g)
     uold = rg_tree.sedov_state(g, L)
     unew = uold.copy()
-    host = uold.copy()
-    host_unew = np.full_like(uold, 7.0)
+    if memory == "pinned":
+        torch = pytest.importorskip("torch")
+        t_host = torch.from_numpy(uold.copy()).pin_memory()
+        t_unew = torch.full((uold.size,), 7.0, dtype=torch.float64).pin_memory()
+        host, host_unew = t_host.numpy(), t_unew.numpy()  # views of the page-locked buffers
+    else:
+        host = uold.copy()
+        host_unew = np.full_like(uold, 7.0)
     outside = np.setdiff1d(np.arange(1, g.ncell + 1), g.cell_ids(L))
     before = host.reshape(5, -1)[:, outside - 1].copy()
     dx = 1.0 / 2 ** L
