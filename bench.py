@@ -13,6 +13,11 @@ Prints one JSON line (rank 0).  N > 1 runs one independent replica per GPU
 (weak scaling): the single-grid step of this workload is not partitioned, so
 the ranks exchange nothing but the final timing maximum.
 
+`e2e.bound` puts the end-to-end step against this box's own link: the level's
+cells up and down at the pinned copy bandwidth measured in the same run, plus
+the device step (the two cannot overlap: a step's input is the previous
+step's output).
+
 Besides the HBM `roofline` of the face kernel (the contract's), the line
 carries `roofline_fp64`: the same kernel against the FP64 pipe, its actual
 bound (executed FP64 FLOPs per cell update from the committed ncu summary,
@@ -324,6 +329,7 @@ def gpu_arm(args, rank, world, local_rank):
         ms_e2e = float(t.item())
     e2e_value = world * cells * ne / (ms_e2e / 1e3)
     fp64_peak = ctx.measure_fp64_peak() if rank == 0 else None
+    link = pinned_copy_gbs(torch, stream, 8 * g.nvar * cells) if rank == 0 else None
     ctx.close()
     if rank != 0:
         return None
@@ -348,11 +354,46 @@ def gpu_arm(args, rank, world, local_rank):
         "kernel_ms": {"prim": kms[0], "face": kms[1], "fold": kms[2]},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * g.nvar * cells,
                 "d2h_bytes_per_step": 8 * g.nvar * cells, "ms_per_step": ms_e2e / ne,
-                "path": "rg_level_substep_host on pinned host memory: the level's cells up, substep, its cells down"},
+                "path": "rg_level_substep_host on pinned host memory: the level's cells up, substep, its cells down",
+                "bound": e2e_bound(link, 8 * g.nvar * cells, ms / args.steps, ms_e2e / ne)},
         "gpu_launches": GPU_KERNELS_PER_STEP * args.steps,
         "clocks": clocks,
     }
     return out
+
+
+def pinned_copy_gbs(torch, stream, nbytes, reps=5):
+    """This box's host<->device copy bandwidth for one level's state: a
+    page-locked buffer of the e2e step's size copied up and down, best of
+    `reps`, CUDA events on the bench stream."""
+    n = nbytes // 8
+    h = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    d = torch.empty(n, dtype=torch.float64, device="cuda")
+    out = {}
+    for name, (dst, src) in (("h2d_gbs", (d, h)), ("d2h_gbs", (h, d))):
+        best = 1e30
+        with torch.cuda.stream(stream):
+            for _ in range(reps):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                dst.copy_(src, non_blocking=True)
+                b.record(stream)
+                b.synchronize()
+                best = min(best, a.elapsed_time(b))
+        out[name] = nbytes / (best / 1e3) / 1e9
+    return out
+
+
+def e2e_bound(link, nbytes, ms_device, ms_e2e):
+    """Lower bound of the e2e step on this box: the level's cells up and down
+    at the measured copy bandwidths, plus the device-resident step."""
+    if not link:
+        return None
+    ms_copy = nbytes / (link["h2d_gbs"] * 1e9) * 1e3 + nbytes / (link["d2h_gbs"] * 1e9) * 1e3
+    return {"h2d_gbs": link["h2d_gbs"], "d2h_gbs": link["d2h_gbs"], "copy_ms": ms_copy,
+            "bound_ms": ms_copy + ms_device, "frac": (ms_copy + ms_device) / ms_e2e,
+            "note": "copies at the measured pinned bandwidth plus the device step, serial (a step's input is the "
+                    "previous step's output)"}
 
 
 def fp64_roofline(face_kernel, cells, face_s, peak_tflops):
