@@ -336,9 +336,12 @@ int rg_set_face_config(rg_ctx* ctx, int ilevel, int variant, int batch);
  * (Simulation::amr_step, src/core/Simulation.cpp:522-635) runs without the
  * host touching the tree.  Scope: 3D hydro (nvar 5), ncpu 1, no boundary
  * patches, levels above the coarse level (ilevel >= 2; the coarse level is
- * refined at initialisation, on the host); the free list does not grow
- * (the reference doubles ngridmax when it runs out: RG_ERR_UNSUPPORTED
- * here, attach with room to spare).  Not reproduced: the debug printf of
+ * refined at initialisation, on the host).  When make_grid_fine needs more
+ * octs than the free list holds, ngridmax doubles (as often as needed) with
+ * the reference's relayout of every array (AmrGrid::resize_grids,
+ * AmrGrid.cpp:117-248, called from get_free_grid, :259-261): ncell and the
+ * cell ids change, so size the host arrays by rg_tree_sizes before
+ * rg_tree_fetch or rg_download_state.  Not reproduced: the debug printf of
  * each flagged cell (TreeUpdater.cpp:519). */
 typedef struct rg_tree_arrays {
     int* son;      /* [ncell]      (rg_tree_fetch writes; attach reads the grid view's) */
@@ -381,6 +384,9 @@ int rg_remove_grid_fine(rg_ctx* ctx, int ilevel);
 int rg_restrict_fine(rg_ctx* ctx, int ilevel);
 /* AmrGrid::count_grids_at_level (AmrGrid.cpp:304-308) of the resident tree. */
 int rg_count_grids(rg_ctx* ctx, int ilevel, int* n);
+/* AmrGrid::ngridmax and ::ncell of the context's tree (they grow when
+ * rg_make_grid_fine runs out of free octs).  Either pointer may be NULL. */
+int rg_tree_sizes(rg_ctx* ctx, int* ngridmax, int* ncell);
 
 /* One coarse step of the resident run: Simulation::run's step
  * (Simulation.cpp:366-397) with Simulation::amr_step (:522-635), every grid

@@ -1165,4 +1165,12 @@ int rg_count_grids(rg_ctx* c, int ilevel, int* n) {
     return RG_OK;
 }
 
+int rg_tree_sizes(rg_ctx* c, int* ngridmax, int* ncell) {
+    CTX_GUARD(c);
+    if (!c->have_topology) return set_error(c, RG_ERR_STATE, "rg_sync_topology has not been called");
+    if (ngridmax) *ngridmax = c->ngridmax;
+    if (ncell) *ncell = c->ncell;
+    return RG_OK;
+}
+
 }  // extern "C"

@@ -25,12 +25,14 @@
 // Scope: refinement of levels above the coarse level (the coarse level,
 // ilevel 1 in the reference's numbering, is refined at initialisation on the
 // host; below levelmin its flags are all set, which is handled), ncpu == 1,
-// nvar == ndim + 2 = 5 and no boundary patches, as on the rest of this path;
-// the free list never grows (the reference doubles ngridmax when it runs
-// out, here that is an error).
+// nvar == ndim + 2 = 5 and no boundary patches, as on the rest of this path.
+// A free list too short for a refinement grows the arrays as the reference's
+// resize_grids does (tree_grow).
 // The per-flagged-cell printf of flag_fine (TreeUpdater.cpp:519) is not
 // reproduced: it writes to stdout and changes no state.
 #include <algorithm>
+#include <cstdint>
+#include <string>
 #include <vector>
 
 #include "rg_face.cuh"
@@ -606,6 +608,156 @@ int set_dev_int(rg_ctx* c, int* dst, int v) {
     return check_cuda(c, cudaGetLastError(), "tree link");
 }
 
+// ---------------------------------------------------------------- growing the oct arrays
+// AmrGrid::resize_grids (AmrGrid.cpp:117-248): cell ncoarse + (ic-1)*ngridmax
+// + ig keeps its (ic, ig) under the new ngridmax, so per-cell planes move
+// slot by slot; per-oct planes keep their first ngm0 entries; everything new
+// is zero; cell ids stored in father and nbor (values above ncoarse) are
+// relabelled the same way.
+__device__ __forceinline__ int relabel_cell(int id, int ncoarse, int ngm0, int ngm1) {
+    if (id <= ncoarse) return id;
+    const int r = id - 1 - ncoarse;
+    return ncoarse + (r / ngm0) * ngm1 + r % ngm0 + 1;
+}
+
+template <class T>
+__global__ void k_relocate_cells(const T* __restrict__ src, T* __restrict__ dst, int nplanes, size_t plane0,
+                                 size_t plane1, int ncoarse, int ngm0, int ngm1) {
+    const size_t n = (size_t)nplanes * plane1, ncell1 = (size_t)ncoarse + 8 * (size_t)ngm1;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t v = i / plane1, j = i - v * plane1;
+        T x = T(0);
+        if (j < (size_t)ncoarse) {
+            x = src[v * plane0 + j];
+        } else if (j < ncell1) {
+            const size_t r = j - ncoarse, ic = r / ngm1, ig = r - ic * ngm1;
+            if (ig < (size_t)ngm0) x = src[v * plane0 + ncoarse + ic * ngm0 + ig];
+        }
+        dst[i] = x;
+    }
+}
+
+template <class T>
+__global__ void k_relocate_octs(const T* __restrict__ src, T* __restrict__ dst, int nplanes, int ncoarse, int ngm0,
+                                int ngm1, bool relabel) {
+    const size_t n = (size_t)nplanes * ngm1;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t v = i / ngm1, ig = i - v * ngm1;
+        T x = T(0);
+        if (ig < (size_t)ngm0) x = src[v * ngm0 + ig];
+        if constexpr (sizeof(T) == sizeof(int))
+            if (relabel) x = relabel_cell(x, ncoarse, ngm0, ngm1);
+        dst[i] = x;
+    }
+}
+
+// the new octs first..last appended to the free list after `before` (its
+// old tail, 0 when it was empty), as resize_grids links them
+__global__ void k_link_new_octs(int* next, int* prev, int first, int last, int before) {
+    for (int g = first + blockIdx.x * blockDim.x + threadIdx.x; g <= last; g += gridDim.x * blockDim.x) {
+        prev[g - 1] = g > first ? g - 1 : before;
+        next[g - 1] = g < last ? g + 1 : 0;
+        if (g == first && before > 0) next[before - 1] = first;
+    }
+}
+
+// *p (nplanes planes of plane0 entries) replaced by a relocated copy with
+// planes of plane1 entries; cells: per-cell layout, else per-oct
+template <class T>
+int relocate(rg_ctx* c, T** p, bool cells, int nplanes, size_t plane0, size_t plane1, int ngm0, int ngm1,
+             bool relabel, const char* what) {
+    T* dst = nullptr;
+    const size_t n = (size_t)nplanes * plane1;
+    if (dev_alloc(c, &dst, sizeof(T) * n) != cudaSuccess)
+        return set_error(c, RG_ERR_NOMEM, std::string("device allocation failed while growing the tree: ") + what);
+    if (cells)
+        k_relocate_cells<T><<<nblk((long long)n), TPB, 0, c->stream>>>(*p, dst, nplanes, plane0, plane1, c->ncoarse,
+                                                                     ngm0, ngm1);
+    else
+        k_relocate_octs<T><<<nblk((long long)n), TPB, 0, c->stream>>>(*p, dst, nplanes, c->ncoarse, ngm0, ngm1,
+                                                                    relabel);
+    dev_free(c, *p);
+    *p = dst;
+    return check_cuda(c, cudaGetLastError(), what);
+}
+
+// *p replaced by an uninitialised array of n entries (scratch whose content is rebuilt)
+template <class T>
+int renew(rg_ctx* c, T** p, size_t n, const char* what) {
+    dev_free(c, *p);
+    *p = nullptr;
+    if (dev_alloc(c, p, sizeof(T) * (n ? n : 1)) != cudaSuccess)
+        return set_error(c, RG_ERR_NOMEM, std::string("device allocation failed while growing the tree: ") + what);
+    return RG_OK;
+}
+
+// Doubles ngridmax until the free list holds `need` octs, as get_free_grid's
+// resize_grids(2 * ngridmax) does each time the list runs dry
+// (AmrGrid.cpp:259-261).  Growing before the refinement instead of in the
+// middle of it gives the same arrays: make_grid_fine recomputes every cell id
+// it still holds under the new ngridmax (TreeUpdater.cpp:62-75), the octs it
+// takes from the free list are the old entries first and then ngm0+1, ngm0+2,
+// ... in both cases, and a taken oct's free-list links are reset either way.
+int tree_grow(rg_ctx* c, int need) {
+    const int ngm0 = c->ngridmax, nc0 = c->ncell, nv = c->nvar;
+    long long ngm1 = ngm0, avail = c->numbf;
+    while (avail < need) {
+        avail += ngm1;
+        ngm1 *= 2;
+    }
+    const long long nc1 = (long long)c->ncoarse + 8 * ngm1;
+    if (nc1 + 1 > (long long)INT32_MAX)
+        return set_error(c, RG_ERR_UNSUPPORTED, "growing ngridmax to " + std::to_string(ngm1) +
+                                                    " would overflow 32-bit cell ids");
+    const int g1 = (int)ngm1, n1 = (int)nc1;
+    // per-cell state and flags, moved slot by slot
+    if (int rc = relocate(c, &c->d_uold, true, nv, nc0, n1, ngm0, g1, false, "uold")) return rc;
+    if (int rc = relocate(c, &c->d_unew, true, nv, nc0, n1, ngm0, g1, false, "unew")) return rc;
+    if (int rc = relocate(c, &c->d_son, true, 1, (size_t)nc0 + 1, (size_t)n1 + 1, ngm0, g1, false, "son")) return rc;
+    if (int rc = relocate(c, &c->d_flag1, true, 1, nc0, n1, ngm0, g1, false, "flag1")) return rc;
+    if (int rc = relocate(c, &c->d_flag2, true, 1, nc0, n1, ngm0, g1, false, "flag2")) return rc;
+    if (int rc = relocate(c, &c->d_cpu_map, true, 1, nc0, n1, ngm0, g1, false, "cpu_map")) return rc;
+    // per-oct links, neighbours and coordinates
+    if (int rc = relocate(c, &c->d_father, false, 1, ngm0, g1, ngm0, g1, true, "father")) return rc;
+    if (int rc = relocate(c, &c->d_nbor, false, 6, ngm0, g1, ngm0, g1, true, "nbor")) return rc;
+    if (int rc = relocate(c, &c->d_next, false, 1, ngm0, g1, ngm0, g1, false, "next")) return rc;
+    if (int rc = relocate(c, &c->d_prev, false, 1, ngm0, g1, ngm0, g1, false, "prev")) return rc;
+    if (int rc = relocate(c, &c->d_xg, false, 3, ngm0, g1, ngm0, g1, false, "xg")) return rc;
+    // scratch sized by the tree, rebuilt by the next refresh or step
+    const size_t cell1 = (size_t)n1 + 1;
+    int** cell_scr[] = {&c->d_cell_level, &c->d_cpos, &c->d_tmap, &c->d_pmark};
+    for (int** p : cell_scr)
+        if (int rc = renew(c, p, cell1, "cell scratch")) return rc;
+    int** oct_scr[] = {&c->d_jump, &c->d_dist, &c->d_jump2, &c->d_dist2};
+    for (int** p : oct_scr)
+        if (int rc = renew(c, p, (size_t)g1, "oct scratch")) return rc;
+    if (int rc = renew(c, &c->d_prim, (size_t)nv * n1, "primitives")) return rc;
+    c->cap_cell = cell1;
+    c->cap_grid = (size_t)g1;
+    c->cap_state = (size_t)nv * n1;
+    // the free list: its old entries in order, then ngm0+1 .. ngm1
+    std::vector<int> fq((size_t)g1, 0);
+    for (int j = 0; j < c->numbf; ++j) fq[(size_t)j] = c->h_fq[(size_t)((c->fq_head + j) % ngm0)];
+    const int before = c->numbf > 0 ? fq[(size_t)c->numbf - 1] : 0;
+    for (int g = ngm0 + 1; g <= g1; ++g) fq[(size_t)(c->numbf + g - ngm0 - 1)] = g;
+    c->h_fq.swap(fq);
+    if (int rc = renew(c, &c->d_fq, (size_t)g1, "free list")) return rc;
+    if (int rc = check_cuda(c, cudaMemcpyAsync(c->d_fq, c->h_fq.data(), sizeof(int) * (size_t)g1,
+                                               cudaMemcpyHostToDevice, c->stream),
+                            "free list upload"))
+        return rc;
+    k_link_new_octs<<<nblk(g1 - ngm0), TPB, 0, c->stream>>>(c->d_next, c->d_prev, ngm0 + 1, g1, before);
+    c->fq_head = 0;
+    c->numbf += g1 - ngm0;
+    c->ngridmax = g1;
+    c->ncell = n1;
+    c->next_level = -1;
+    c->tree_dirty = true;  // cell ids moved: plans, ranks and cell levels are stale
+    if (int rc = check_cuda(c, cudaGetLastError(), "tree growth kernels")) return rc;
+    // the upload above reads the host ring: keep it alive until the copy is done
+    return check_cuda(c, cudaStreamSynchronize(c->stream), "tree growth");
+}
+
 }  // namespace
 
 int tree_flag_fine(rg_ctx* c, int ilevel, double ed, double ep, double ev, double eb2, int nexp, int icount,
@@ -671,9 +823,12 @@ int tree_make_grid_fine(rg_ctx* c, int ilevel) {
     int n = 0;
     if (int rc = exclusive_scan(c, S.mark, S.rank, n8, &n)) return rc;
     if (n == 0) return RG_OK;
-    if (n > c->numbf)
-        return set_error(c, RG_ERR_UNSUPPORTED, "free oct list exhausted (" + std::to_string(n) + " needed, " +
-                                                    std::to_string(c->numbf) + " free): attach with a larger ngridmax");
+    if (n > c->numbf) {
+        // the free list is too short: grow the arrays as the reference does,
+        // then start over on the relabelled tree (authorisation is idempotent)
+        if (int rc = tree_grow(c, n)) return rc;
+        return tree_make_grid_fine(c, ilevel);
+    }
     const StepK K = step_consts(c);
     k_refine<<<nblk(n8), TPB, 0, s>>>(M, tree_view(c), Geo{c->nx, c->ny, c->nz, c->params.boxlen}, S.octs, noct,
                                       S.mark, S.rank, c->d_fq, c->fq_head, ilevel, c->params.interpol_var,

@@ -167,6 +167,7 @@ def lib():
     L.rg_remove_grid_fine.argtypes = [VP, C.c_int]
     L.rg_restrict_fine.argtypes = [VP, C.c_int]
     L.rg_count_grids.argtypes = [VP, C.c_int, IP]
+    L.rg_tree_sizes.argtypes = [VP, IP, IP]
     L.rg_amr_coarse_step.argtypes = [VP, C.POINTER(rg_amr_config), C.POINTER(rg_amr_clock)]
     L.rg_measure_fp64_peak.argtypes = [VP, C.POINTER(C.c_double)]
     L.rg_level_run.argtypes = [VP, C.c_int, C.c_double, C.c_int, C.c_double, C.c_double, C.c_int64,
@@ -235,10 +236,21 @@ class Context:
         self._tree = tree_arrays(d)
         self._chk(self.L.rg_tree_attach(self.h, C.byref(self._view), C.byref(self._tree), int(levelmin)))
 
+    def tree_sizes(self):
+        """(ngridmax, ncell) of the context's tree: both grow when make_grid_fine runs out of free octs."""
+        g, n = C.c_int(0), C.c_int(0)
+        self._chk(self.L.rg_tree_sizes(self.h, C.byref(g), C.byref(n)))
+        return g.value, n.value
+
     def tree_fetch(self, like):
-        """Fresh numpy copies of every tree array and the state (shapes from `like`)."""
-        d = {k: np.zeros(np.shape(like[k]), dtype=np.int32) for k in TREE_INT_ARRAYS}
-        d.update({k: np.zeros(np.shape(like[k]), dtype=np.float64) for k in TREE_F64_ARRAYS})
+        """Fresh numpy copies of every tree array and the state, sized by the
+        device tree (the level-list arrays by `like`)."""
+        ngm, ncell = self.tree_sizes()
+        nv = self.nvar
+        per = {"son": ncell, "father": ngm, "nbor": 6 * ngm, "next": ngm, "prev": ngm, "flag1": ncell,
+               "flag2": ncell, "cpu_map": ncell, "xg": 3 * ngm, "uold": nv * ncell, "unew": nv * ncell}
+        d = {k: np.zeros(per.get(k, len(like[k])), dtype=np.int32) for k in TREE_INT_ARRAYS}
+        d.update({k: np.zeros(per[k], dtype=np.float64) for k in TREE_F64_ARRAYS})
         d.update(headf=0, tailf=0, numbf=0)
         t = tree_arrays(d)
         self._chk(self.L.rg_tree_fetch(self.h, C.byref(t)))

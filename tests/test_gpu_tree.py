@@ -8,6 +8,8 @@ harness on the same tree.
   interpol_hydro for each interpol_var), remove_grid_fine (unlinking, freed
   ids appended to the free list) and restrict_fine: every tree array, the
   list heads / tails / counts, the free list and the state equal bit for bit;
+- a run that outgrows its free list: ngridmax doubled and every array
+  relabelled as the reference's resize_grids does;
 - whole coarse steps with the tree resident on the device (rg_amr.DeviceAmrRun,
   through the native rg_amr_coarse_step and call by call) against the
   reference's run (refsupport.AmrRun): same tree, same state, same time, same
@@ -122,9 +124,7 @@ def test_device_resident_amr_run_matches_reference(rgpu_lib, native):
 
 def test_tree_calls_report_misuse(rgpu_lib):
     """Errors instead of undefined behaviour: no attached tree, an inconsistent
-    free list, a refinement that needs more octs than the free list holds (the
-    reference would double ngridmax), and a single-level run on a level that
-    has refined cells."""
+    free list, and a single-level run on a level that has refined cells."""
     h, _ = reference_run(0)
     params = rgpu.make_params(3, slope_type=2, riemann="hllc", gamma=GAMMA)
     ctx = rgpu.Context(params, 0)
@@ -146,35 +146,32 @@ def test_tree_calls_report_misuse(rgpu_lib):
         ctx.close()
 
 
-def test_free_list_exhaustion_is_an_error(rgpu_lib):
-    """The device is handed an empty free list; a refinement that creates octs
-    on the reference (which would grow its arrays when it ran out) must fail
-    with RG_ERR_UNSUPPORTED instead."""
-    h, _ = reference_run(0)
-    t = {k: (v.copy() if hasattr(v, "copy") else v) for k, v in h.tree_arrays().items()}
-    t["headf"], t["tailf"], t["numbf"] = 0, 0, 0
-    ctx = device_ctx_from(h.grid(), t)
+def test_free_list_growth_matches_reference(rgpu_lib):
+    """A run whose refinements outgrow the free list.  The reference doubles
+    ngridmax in get_free_grid whenever the list runs dry (AmrGrid.cpp:259-261,
+    resize_grids :117-248), relabelling every cell id, several times within
+    one make_grid_fine here; the device grows the same way, and after each
+    coarse step the sizes, every tree array, the free list and the state are
+    equal."""
+    nml = namelist(slope_type=2, riemann="hllc", levelmin=LMIN, levelmax=LMAX, err_grad_d=ED, err_grad_p=EP)
+    probe = RefHarness(3).create(nml, ngridmax=30000, levelmin=LMIN, nlevelmax=LMAX, gamma=GAMMA)
+    AmrRun(probe, LMIN, LMAX, GAMMA, ed=ED, ep=EP).initialize(sedov_ic(3, LMIN))
+    ngm0 = probe.get("ngridmax") - probe.get("numbf") + 8  # the initialised tree plus 8 free octs
+    probe.close()
+    h = RefHarness(3).create(nml, ngridmax=ngm0, levelmin=LMIN, nlevelmax=LMAX, gamma=GAMMA)
+    r = AmrRun(h, LMIN, LMAX, GAMMA, ed=ED, ep=EP)
+    r.initialize(sedov_ic(3, LMIN))
+    assert h.get("ngridmax") == ngm0, "the reference grew during initialisation: the case tests nothing"
+    ctx = device_ctx(h)
     try:
-        for il in range(LMIN, LMAX):
-            args = (il, ED, EP, -1.0, -1.0, 3, 2, 2)  # wider smoothing than the run's: flags beyond the refined region
-            h.flag_fine(*args)
-            ctx.flag_fine(*args)
-            n0 = h.count_grids(il + 1)
-            h.make_grid_fine(il)
-            if h.count_grids(il + 1) == n0:
-                ctx.make_grid_fine(il)  # nothing to create on either side
-                continue
-            with pytest.raises(rgpu.RGError) as e:
-                ctx.make_grid_fine(il)
-            assert e.value.code == rgpu.RG_ERR_UNSUPPORTED
-            return
-        pytest.fail("the reference created no oct on any level: the case proves nothing")
+        d = DeviceAmrRun(ctx, nx=1, levelmin=LMIN, nlevelmax=LMAX, ed=ED, ep=EP)
+        for step in range(3):
+            r.coarse_step()
+            d.coarse_step()
+            assert ctx.tree_sizes() == (h.get("ngridmax"), h.get("ncell")), f"coarse step {step}"
+            assert_same_tree(h, ctx, f"coarse step {step}")
+            assert d.t == r.t and d.cell_updates == r.cell_updates
+        assert h.get("ngridmax") >= 4 * ngm0, "the run did not outgrow the free list twice"
     finally:
         ctx.close()
-
-
-def device_ctx_from(g, arrays):
-    params = rgpu.make_params(3, slope_type=2, riemann="hllc", gamma=GAMMA)
-    ctx = rgpu.Context(params, 0)
-    ctx.tree_attach(g, arrays, LMIN)
-    return ctx
+        h.close()
