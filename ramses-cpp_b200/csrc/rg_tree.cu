@@ -698,7 +698,23 @@ int renew(rg_ctx* c, T** p, size_t n, const char* what) {
 // it still holds under the new ngridmax (TreeUpdater.cpp:62-75), the octs it
 // takes from the free list are the old entries first and then ngm0+1, ngm0+2,
 // ... in both cases, and a taken oct's free-list links are reset either way.
+int tree_grow_arrays(rg_ctx* c, int need);
+
 int tree_grow(rg_ctx* c, int need) {
+    const int rc = tree_grow_arrays(c, need);
+    if (rc != RG_OK && rc != RG_ERR_UNSUPPORTED) {
+        // some arrays may already have the new layout and others not: the
+        // tree and the state are lost, and every later call says so
+        c->tree_resident = false;
+        c->have_topology = false;
+        c->have_state = false;
+        c->tree_dirty = false;
+        for (auto& p : c->plans) free_plan(c, p);
+    }
+    return rc;
+}
+
+int tree_grow_arrays(rg_ctx* c, int need) {
     const int ngm0 = c->ngridmax, nc0 = c->ncell, nv = c->nvar;
     long long ngm1 = ngm0, avail = c->numbf;
     while (avail < need) {
