@@ -265,6 +265,15 @@ int rg_level_octs(rg_ctx* ctx, int ilevel, int* octs_out, int cap, int* n_out);
 /* Neighbour cell ids per level cell, the result of AmrGrid::get_nbor_cells
  * (AmrGrid.cpp:402-444): out[(k*2^ndim + ic-1)*6 + j], j = 2*idim+side. */
 int rg_level_nbor_cells(rg_ctx* ctx, int ilevel, int* out, int cap);
+/* Sizes of a level's step plan (built on demand): the level's cells, the
+ * update targets (those cells plus the coarser cells that receive
+ * refluxes, HydroSolver.cpp:476-482), the ordered update events, the coarser
+ * cells read by ghost stencils, and the targets with more than 16 updates,
+ * which the fold hands one warp each. */
+typedef struct rg_plan_info {
+    int ncells, ntarg, nevents, nextra_prim, nlong;
+} rg_plan_info;
+int rg_level_plan_info(rg_ctx* ctx, int ilevel, rg_plan_info* out);
 /* Number of cell updates (son==0 cells) the last rg_godunov_level or
  * rg_level_substep of this level processed. */
 int64_t rg_level_cell_updates(rg_ctx* ctx, int ilevel);

@@ -909,6 +909,15 @@ int rg_level_octs(rg_ctx* c, int ilevel, int* octs_out, int cap, int* n_out) {
     return RG_OK;
 }
 
+int rg_level_plan_info(rg_ctx* c, int ilevel, rg_plan_info* out) {
+    CTX_GUARD(c);
+    if (!out) return set_error(c, RG_ERR_ARG, "out is NULL");
+    Plan* P;
+    if (int rc = get_plan(c, ilevel, &P)) return rc;
+    *out = rg_plan_info{P->ncells, P->ntarg, P->nevents, P->nextra_prim, P->nlong};
+    return RG_OK;
+}
+
 int rg_level_nbor_cells(rg_ctx* c, int ilevel, int* out, int cap) {
     CTX_GUARD(c);
     Plan* P;

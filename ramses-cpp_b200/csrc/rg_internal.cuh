@@ -96,6 +96,9 @@ struct PlanView {
 // Box of level cell p (ensemble levels only).
 __device__ __forceinline__ int box_of(const PlanView& P, int p) { return P.obox[p % P.noct]; }
 
+// A target with more updates than this is folded by a whole warp (k_fold_long).
+constexpr int kLongEvents = 16;
+
 struct Plan {
     bool valid = false;
     int ilevel = -1, level0 = 0, noct = 0, ncells = 0, ntarg = 0, nextra_prim = 0, nevents = 0;
@@ -128,6 +131,11 @@ struct Plan {
     // the same cells as runs of consecutive cell ids (first id, count): few on
     // a uniform level (one per child slot), so transfers are plain copies
     std::vector<std::pair<int, int>> read_runs, targ_runs;
+    // targets with more than kLongEvents updates (coarse cells taking the
+    // refluxes of many finer faces), folded one warp each by k_fold_long and
+    // skipped by k_fold
+    int nlong = 0;
+    int* tlong = nullptr;      // [nlong] target indices
     int nbox = 0;              // ensemble level: number of boxes (0: one grid)
     int* obox = nullptr;       // [noct]
     BoxStep* boxes = nullptr;  // [nbox]

@@ -228,6 +228,12 @@ __global__ void k_ev_fill(int ncells, int level0, int noct, const int* __restric
     }
 }
 
+// targets whose event count exceeds `limit`, appended to out (count in *n)
+__global__ void k_long_targets(int ntarg, const int* __restrict__ off, int limit, int* out, int* n) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntarg; t += gridDim.x * blockDim.x)
+        if (off[t + 1] - off[t] > limit) out[atomicAdd(n, 1)] = t;
+}
+
 __global__ void k_ev_sort(int ntarg, const int* __restrict__ off, int* ev) {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntarg; t += gridDim.x * blockDim.x) {
         int a = off[t], b = off[t + 1];
@@ -324,6 +330,7 @@ void free_plan(rg_ctx* c, Plan& p) {
     dev_free(c, p.bl_ext);
     dev_free(c, p.bl_off);
     dev_free(c, p.bl_brick_off);
+    dev_free(c, p.tlong);
     p = Plan();
 }
 
@@ -464,7 +471,20 @@ int build_plan_t(rg_ctx* c, int ilevel, Plan& P) {
     k_ev_fill<NDIM><<<nblk(nc), TPB, 0, s>>>(nc, P.level0, P.noct, c->d_cpos, c->d_tmap, P.icn, P.kind, P.toff, cnt,
                                              P.tev);
     k_ev_sort<<<nblk(P.ntarg), TPB, 0, s>>>(P.ntarg, P.toff, P.tev);
+    // long targets, compacted into d_textra's space (its content was copied out above)
+    int* d_nlong = d_nx + 2;
+    k_long_targets<<<nblk(P.ntarg), TPB, 0, s>>>(P.ntarg, P.toff, kLongEvents, d_textra, d_nlong);
+    cudaMemcpyAsync(&hv[2], d_nlong, sizeof(int), cudaMemcpyDeviceToHost, s);
     int rc_ev = check_cuda(c, cudaStreamSynchronize(s), "plan events");
+    if (!rc_ev && hv[2] > 0) {
+        P.nlong = hv[2];
+        rc_ev = dalloc(c, &P.tlong, (size_t)P.nlong, "long targets");
+        if (!rc_ev) {
+            // in atomic order: targets are independent, so the order changes no result
+            cudaMemcpyAsync(P.tlong, d_textra, sizeof(int) * P.nlong, cudaMemcpyDeviceToDevice, s);
+            rc_ev = check_cuda(c, cudaStreamSynchronize(s), "long targets");
+        }
+    }
     cleanup();
     if (rc_ev) return rc_ev;
     if (int rc = check_device_status(c)) return rc;

@@ -128,7 +128,7 @@ __global__ void k_fold(TreeView T, PlanView P, const double* __restrict__ flux, 
     const double dtdx0 = st->dtdx;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < P.ntarg; t += gridDim.x * blockDim.x) {
         int a = P.toff[t], b = P.toff[t + 1];
-        if (a == b) continue;
+        if (a == b || b - a > kLongEvents) continue;  // long targets: k_fold_long
         const double dtdx = P.obox ? box_dtdx<NDIM>(P, a) : dtdx0;
         int cell = (t < nc) ? cell_of(T, P, t) : P.textra[t - nc];
         const bool from_old = LEAF && t < nc;
@@ -145,6 +145,138 @@ __global__ void k_fold(TreeView T, PlanView P, const double* __restrict__ flux, 
             for (int iv = 0; iv < NV; ++iv) uold[(size_t)iv * ncell + cell - 1] = u[iv];
         }
     }
+}
+
+// The targets k_fold skips, those with more than kLongEvents updates (in AMR
+// runs, coarse cells that take the refluxes of many finer faces: 192 at the
+// edge of the finest level of the 64^3-base Sedov run), one warp each.  A
+// thread walking such a chain waits on its loads event after event, and the
+// few long chains set the whole fold's duration.  Here the lanes fetch 32
+// events at a time and form each one's term -- dtdx * sign * flux * factor
+// for a reflux, the own flux sum for the own update, the expressions of
+// fold_events -- and the terms are then applied in event order:
+//   - a coarser target takes refluxes only, whose subtractions act on each
+//     variable separately, so lane iv walks variable iv's terms in order
+//     from shared memory;
+//   - a level cell (whose own update mixes the variables through its clamps)
+//     applies them on values broadcast from the lane that formed them, every
+//     lane computing the whole state.
+// Either way the result is the sequential fold's arithmetic, bit for bit.
+constexpr int kLongThreads = 256, kLongChunk = 32, kLongPad = kLongChunk + 1;
+
+template <int NDIM, bool LEAF = false, bool FSUM = false>
+__global__ void __launch_bounds__(kLongThreads)
+    k_fold_long(TreeView T, PlanView P, const int* __restrict__ tlong, int nlong, const double* __restrict__ flux,
+                double* __restrict__ unew, const DevStatus* __restrict__ st, double gamma,
+                double* __restrict__ uold = nullptr, const double* __restrict__ fsum = nullptr) {
+    constexpr int NV = Dims<NDIM>::NV, NS = Dims<NDIM>::NS, TTD = Dims<NDIM>::TTD;
+    // per warp: the terms of one chunk, variable-major, rows padded so the
+    // NV walking lanes read from different banks
+    __shared__ double terms[kLongThreads / 32][NV * kLongPad];
+    double* my = terms[threadIdx.x >> 5];
+    const size_t ncell = (size_t)T.ncell;
+    const int nc = P.ncells, lane = threadIdx.x & 31;
+    const int nwarp = (int)(((size_t)gridDim.x * blockDim.x) >> 5);
+    const double factor = 1.0 / (1 << NDIM);
+    for (int w = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5); w < nlong; w += nwarp) {
+        const int t = tlong[w];
+        const int a = P.toff[t], b = P.toff[t + 1];
+        const double dtdx = P.obox ? box_dtdx<NDIM>(P, a) : st->dtdx;
+        if (t >= nc) {
+            const int cell = P.textra[t - nc];
+            double u = lane < NV ? unew[(size_t)lane * ncell + cell - 1] : 0.0;
+            for (int e0 = a; e0 < b; e0 += kLongChunk) {
+                const int e = e0 + lane;
+                if (e < b) {
+                    const int key = P.tev[e];
+                    const int slot = key & 7, cp = key >> 3;
+                    const int ps = P.level0 ? cp : (cp % TTD) * P.noct + cp / TTD;
+                    const double sign = (slot & 1) ? -1.0 : 1.0;
+#pragma unroll
+                    for (int iv = 0; iv < NV; ++iv)
+                        my[iv * kLongPad + lane] = dtdx * sign * flux[((size_t)slot * NV + iv) * nc + ps] * factor;
+                }
+                __syncwarp();
+                const int m = (b - e0 < kLongChunk) ? b - e0 : kLongChunk;
+                if (lane < NV) {
+                    const double* s = my + lane * kLongPad;
+#pragma unroll 8
+                    for (int j = 0; j < m; ++j) u = u - s[j];
+                }
+                __syncwarp();
+            }
+            if (lane < NV) unew[(size_t)lane * ncell + cell - 1] = u;
+            continue;
+        }
+        const int cell = cell_of(T, P, t);
+        const bool from_old = LEAF;
+        const double* src = from_old ? uold : unew;
+        double u[NV];
+#pragma unroll
+        for (int iv = 0; iv < NV; ++iv) u[iv] = src[(size_t)iv * ncell + cell - 1];
+        for (int e0 = a; e0 < b; e0 += 32) {
+            const int e = e0 + lane;
+            int own = 0;
+            double val[NV];
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) val[iv] = 0.0;
+            if (e < b) {
+                const int key = P.tev[e];
+                const int slot = key & 7, cp = key >> 3;
+                const int ps = P.level0 ? cp : (cp % TTD) * P.noct + cp / TTD;
+                if (slot == OWN_SLOT) {
+                    own = 1;
+                    if constexpr (FSUM) {
+#pragma unroll
+                        for (int iv = 0; iv < NV; ++iv) val[iv] = fsum[(size_t)iv * nc + ps];
+                    } else {
+#pragma unroll
+                        for (int sl = 0; sl < NS; ++sl) {
+                            const double sign = (sl & 1) ? -1.0 : 1.0;
+#pragma unroll
+                            for (int iv = 0; iv < NV; ++iv)
+                                val[iv] = val[iv] + sign * flux[((size_t)sl * NV + iv) * nc + ps];
+                        }
+                    }
+                } else {
+                    const double sign = (slot & 1) ? -1.0 : 1.0;
+#pragma unroll
+                    for (int iv = 0; iv < NV; ++iv) val[iv] = dtdx * sign * flux[((size_t)slot * NV + iv) * nc + ps] * factor;
+                }
+            }
+            const int m = (b - e0 < 32) ? b - e0 : 32;
+            for (int j = 0; j < m; ++j) {
+                const int oj = __shfl_sync(0xffffffffu, own, j);
+                double vj[NV];
+#pragma unroll
+                for (int iv = 0; iv < NV; ++iv) vj[iv] = __shfl_sync(0xffffffffu, val[iv], j);
+                if (oj) {
+                    own_update<NDIM>(vj, gamma, dtdx, u);
+                } else {
+#pragma unroll
+                    for (int iv = 0; iv < NV; ++iv) u[iv] = u[iv] - vj[iv];
+                }
+            }
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) unew[(size_t)iv * ncell + cell - 1] = u[iv];
+            if (from_old) {
+#pragma unroll
+                for (int iv = 0; iv < NV; ++iv) uold[(size_t)iv * ncell + cell - 1] = u[iv];
+            }
+        }
+    }
+}
+
+// k_fold_long over a plan's long targets (nothing when it has none)
+template <int NDIM, bool LEAF = false, bool FSUM = false>
+void launch_fold_long(rg_ctx* c, const Plan& P, const TreeView& T, const PlanView& V, const double* flux,
+                      double* unew, double gamma, double* uold = nullptr, const double* fsum = nullptr) {
+    if (P.nlong == 0) return;
+    const int blocks = (int)std::min<long long>(((long long)P.nlong * 32 + kLongThreads - 1) / kLongThreads, 65535);
+    k_fold_long<NDIM, LEAF, FSUM><<<blocks, kLongThreads, 0, c->stream>>>(T, V, P.tlong, P.nlong, flux, unew,
+                                                                          c->d_status, gamma, uold, fsum);
 }
 
 // Leaf-level fold that also prepares the next substep: on a level whose
@@ -442,6 +574,7 @@ int launch_godunov_t(rg_ctx* c, const Plan& P) {
     if (c->timing) cudaEventRecord(c->ev[2], c->stream);
     k_fold<NDIM, false, true><<<grid_for(c, P.ntarg, 256), 256, 0, c->stream>>>(T, V, c->d_flux, c->d_unew,
                                                                                c->d_status, K.gamma, nullptr, fsum);
+    launch_fold_long<NDIM, false, true>(c, P, T, V, c->d_flux, c->d_unew, K.gamma, nullptr, fsum);
     if (c->timing) cudaEventRecord(c->ev[3], c->stream);
     return check_cuda(c, cudaGetLastError(), "godunov kernels");
 }
@@ -472,6 +605,7 @@ int launch_godunov_ext_t(rg_ctx* c, const Plan& P, const double* uold, double* u
         default: launch_face_ext_t<NDIM, RG_RIEMANN_LLF>(c, P, K, uold, prim, flux); break;
     }
     k_fold<NDIM><<<grid_for(c, P.ntarg, 256), 256, 0, c->stream>>>(T, V, flux, unew, c->d_status, K.gamma);
+    launch_fold_long<NDIM>(c, P, T, V, flux, unew, K.gamma);
     return check_cuda(c, cudaGetLastError(), "godunov kernels (caller buffers)");
 }
 
@@ -538,6 +672,7 @@ int launch_leaf_core_t(rg_ctx* c, const Plan& P, double dx, int pressure_cap, do
     } else {
         k_fold<NDIM, true, true><<<g, 256, 0, c->stream>>>(T, V, c->d_flux, c->d_unew, c->d_status, K.gamma,
                                                            c->d_uold, fsum);
+        launch_fold_long<NDIM, true, true>(c, P, T, V, c->d_flux, c->d_unew, K.gamma, c->d_uold, fsum);
     }
     if (c->timing) cudaEventRecord(c->ev[3], c->stream);
     return check_cuda(c, cudaGetLastError(), "leaf substep kernels");

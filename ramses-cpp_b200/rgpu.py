@@ -55,6 +55,10 @@ class rg_amr_clock(C.Structure):
                 ("cell_updates", C.c_int64)]
 
 
+class rg_plan_info(C.Structure):
+    _fields_ = [(k, C.c_int) for k in ("ncells", "ntarg", "nevents", "nextra_prim", "nlong")]
+
+
 TREE_INT_ARRAYS = ("son", "father", "nbor", "next", "prev", "headl", "taill", "numbl", "flag1", "flag2", "cpu_map")
 TREE_F64_ARRAYS = ("xg", "uold", "unew")
 
@@ -168,6 +172,7 @@ def lib():
     L.rg_restrict_fine.argtypes = [VP, C.c_int]
     L.rg_count_grids.argtypes = [VP, C.c_int, IP]
     L.rg_tree_sizes.argtypes = [VP, IP, IP]
+    L.rg_level_plan_info.argtypes = [VP, C.c_int, C.POINTER(rg_plan_info)]
     L.rg_amr_coarse_step.argtypes = [VP, C.POINTER(rg_amr_config), C.POINTER(rg_amr_clock)]
     L.rg_measure_fp64_peak.argtypes = [VP, C.POINTER(C.c_double)]
     L.rg_level_run.argtypes = [VP, C.c_int, C.c_double, C.c_int, C.c_double, C.c_double, C.c_int64,
@@ -363,6 +368,12 @@ class Context:
 
     def synchronize(self):
         self._chk(self.L.rg_synchronize(self.h))
+
+    def plan_info(self, il):
+        """rg_level_plan_info as a dict: ncells, ntarg, nevents, nextra_prim, nlong."""
+        i = rg_plan_info()
+        self._chk(self.L.rg_level_plan_info(self.h, il, C.byref(i)))
+        return {k: getattr(i, k) for k, _ in rg_plan_info._fields_}
 
     def level_octs(self, il):
         n = C.c_int(0)
