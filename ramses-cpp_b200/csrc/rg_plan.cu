@@ -86,6 +86,12 @@ __global__ void k_level_octs(int n, const int* __restrict__ jump, const int* __r
     }
 }
 
+// the count k_level_octs found must be the list's length (a shorter chain
+// than the level count says)
+__global__ void k_check_count(const int* count, int noct, DevStatus* st) {
+    if (*count != noct) raise_err(st, DE_LIST, noct);
+}
+
 // ---------------------------------------------------------------- plan cells
 __device__ __forceinline__ int plan_cell_id(const TreeView& T, const int* octs, int level0, int noct, int p) {
     if (level0) return p + 1;
@@ -387,7 +393,10 @@ int build_plan_t(rg_ctx* c, int ilevel, Plan& P) {
         int head = 0;
         if (ilevel >= 0 && ilevel <= c->nlevelmax) head = c->h_headl[(size_t)ilevel * (c->ncpu + c->nboundary)];
         if (head > c->ngridmax || head < 0) return set_error(c, RG_ERR_TOPOLOGY, "headl entry out of range");
-        if (head > 0) {
+        if (head > 0 && c->tree_resident) {
+            P.noct = c->h_numbl[(size_t)ilevel * (c->ncpu + c->nboundary)];  // checked by the count below
+            if (P.noct < 1) return set_error(c, RG_ERR_TOPOLOGY, "level count and head disagree");
+        } else if (head > 0) {
             int dh = 0;
             if (int rc = check_cuda(c, cudaMemcpyAsync(&dh, c->d_dist + head - 1, sizeof(int), cudaMemcpyDeviceToHost, s),
                                     "list length"))
@@ -553,6 +562,13 @@ int level_oct_list(rg_ctx* c, int ilevel, int* out, int cap, int* noct) {
     cudaMemsetAsync(c->d_scan, 0, sizeof(int), s);
     k_level_octs<<<nblk(c->ngridmax), TPB, 0, s>>>(c->ngridmax, c->d_jump, c->d_dist, head - 1, n, out, c->d_scan,
                                                    c->d_status);
+    if (c->tree_resident) {
+        // the count is the host's own: check the chain on the device and do
+        // not wait (a mismatch is reported by the next call that synchronises)
+        k_check_count<<<1, 1, 0, s>>>(c->d_scan, n, c->d_status);
+        *noct = n;
+        return check_cuda(c, cudaGetLastError(), "level octs");
+    }
     cudaMemcpyAsync(&count, c->d_scan, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (int rc = check_cuda(c, cudaStreamSynchronize(s), "level octs")) return rc;
     if (count != n) return set_error(c, RG_ERR_TOPOLOGY, "level linked list merges with another chain");

@@ -810,8 +810,9 @@ int tree_flag_fine(rg_ctx* c, int ilevel, double ed, double ep, double ev, doubl
     for (int i = 0; i < nexp; ++i) smooth();
     if (ilevel > lmin && icount < nsub)
         k_ensure_ref_rules<<<nblk(noct), TPB, 0, s>>>(M, Geo{c->nx, c->ny, c->nz, c->params.boxlen}, S.octs, noct);
-    if (int rc = check_cuda(c, cudaGetLastError(), "flag_fine kernels")) return rc;
-    return check_device_status(c);
+    // nothing to read back: the host does not wait here, and a check the
+    // kernels failed is reported by the next call that synchronises
+    return check_cuda(c, cudaGetLastError(), "flag_fine kernels");
 }
 
 int tree_make_grid_fine(rg_ctx* c, int ilevel) {
