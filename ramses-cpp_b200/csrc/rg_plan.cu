@@ -8,6 +8,7 @@
 //   interface branches       HydroSolver.cpp:118-162, reflux test :476
 //   CPU update order         HydroSolver.cpp:565-572 (octs, ic, idim, side)
 #include <algorithm>
+#include <climits>
 #include <cstdio>
 
 #include "rg_internal.cuh"
@@ -240,9 +241,13 @@ __global__ void k_long_targets(int ntarg, const int* __restrict__ off, int limit
         if (off[t + 1] - off[t] > limit) out[atomicAdd(n, 1)] = t;
 }
 
-__global__ void k_ev_sort(int ntarg, const int* __restrict__ off, int* ev) {
+// each target's events into ascending key order (the CPU order), one thread
+// per target; targets with more than `skip_above` events are left to
+// k_ev_sort_long
+__global__ void k_ev_sort(int ntarg, const int* __restrict__ off, int* ev, int skip_above) {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntarg; t += gridDim.x * blockDim.x) {
         int a = off[t], b = off[t + 1];
+        if (b - a > skip_above) continue;
         for (int i = a + 1; i < b; ++i) {
             int v = ev[i], j = i - 1;
             while (j >= a && ev[j] > v) {
@@ -251,6 +256,52 @@ __global__ void k_ev_sort(int ntarg, const int* __restrict__ off, int* ev) {
             }
             ev[j + 1] = v;
         }
+    }
+}
+
+// The long targets' events (list and count from k_long_targets), one block
+// per target: a bitonic network in shared memory.  Keys are distinct (one per
+// source cell and slot), so any correct sort gives k_ev_sort's order; a
+// target with more than kSortMax events falls back to one thread's
+// insertion sort.
+constexpr int kSortMax = 2048, kSortThreads = 256;
+__global__ void __launch_bounds__(kSortThreads)
+    k_ev_sort_long(const int* __restrict__ tlong, const int* __restrict__ nlong, const int* __restrict__ off, int* ev) {
+    __shared__ int sh[kSortMax];
+    const int n_long = *nlong;
+    for (int w = blockIdx.x; w < n_long; w += gridDim.x) {
+        const int t = tlong[w], a = off[t], n = off[t + 1] - a;
+        if (n > kSortMax) {
+            if (threadIdx.x == 0)
+                for (int i = a + 1; i < a + n; ++i) {
+                    const int v = ev[i];
+                    int j = i - 1;
+                    for (; j >= a && ev[j] > v; --j) ev[j + 1] = ev[j];
+                    ev[j + 1] = v;
+                }
+            __syncthreads();
+            continue;
+        }
+        int m = 1;
+        while (m < n) m <<= 1;
+        for (int i = threadIdx.x; i < m; i += blockDim.x) sh[i] = i < n ? ev[a + i] : INT_MAX;
+        __syncthreads();
+        for (int k = 2; k <= m; k <<= 1)
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = threadIdx.x; i < m; i += blockDim.x) {
+                    const int ixj = i ^ j;
+                    if (ixj > i) {
+                        const int x = sh[i], y = sh[ixj];
+                        if ((x > y) == ((i & k) == 0)) {
+                            sh[i] = y;
+                            sh[ixj] = x;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        for (int i = threadIdx.x; i < n; i += blockDim.x) ev[a + i] = sh[i];
+        __syncthreads();
     }
 }
 
@@ -479,10 +530,12 @@ int build_plan_t(rg_ctx* c, int ilevel, Plan& P) {
     cudaMemsetAsync(cnt, 0, sizeof(int) * ((size_t)P.ntarg + 1), s);
     k_ev_fill<NDIM><<<nblk(nc), TPB, 0, s>>>(nc, P.level0, P.noct, c->d_cpos, c->d_tmap, P.icn, P.kind, P.toff, cnt,
                                              P.tev);
-    k_ev_sort<<<nblk(P.ntarg), TPB, 0, s>>>(P.ntarg, P.toff, P.tev);
-    // long targets, compacted into d_textra's space (its content was copied out above)
+    // long targets, compacted into d_textra's space (its content was copied
+    // out above); their events are sorted a block each, the rest a thread each
     int* d_nlong = d_nx + 2;
     k_long_targets<<<nblk(P.ntarg), TPB, 0, s>>>(P.ntarg, P.toff, kLongEvents, d_textra, d_nlong);
+    k_ev_sort<<<nblk(P.ntarg), TPB, 0, s>>>(P.ntarg, P.toff, P.tev, kLongEvents);
+    k_ev_sort_long<<<2 * c->sm_count, kSortThreads, 0, s>>>(d_textra, d_nlong, P.toff, P.tev);
     cudaMemcpyAsync(&hv[2], d_nlong, sizeof(int), cudaMemcpyDeviceToHost, s);
     int rc_ev = check_cuda(c, cudaStreamSynchronize(s), "plan events");
     if (!rc_ev && hv[2] > 0) {
