@@ -1107,6 +1107,7 @@ int rg_tree_attach(rg_ctx* c, const rg_grid_view* g, const rg_tree_arrays* t, in
     if (int rc = check_cuda(c, cudaStreamSynchronize(s), "tree upload")) return rc;
     c->tree_resident = true;
     c->tree_dirty = false;
+    c->auth_dirty = true;
     return RG_OK;
 }
 

@@ -229,6 +229,11 @@ struct rg_ctx {
     int fq_head = 0, numbf = 0, levelmin = 1;
     bool tree_resident = false;
     bool tree_dirty = false;  // links changed on the device: ranks, cell levels and plans are stale
+    // authorize_fine (flag2 = cpu_map == myid over every cell) has an effect:
+    // false while flag2 == (cpu_map == 1) holds everywhere, which only
+    // attaching, refining (new cells' cpu_map), removing (freed cells' flag2)
+    // and the coarse flags below levelmin (coarse cpu_map) can break
+    bool auth_dirty = true;
 };
 
 namespace rg {

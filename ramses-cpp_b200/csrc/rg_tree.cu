@@ -790,6 +790,7 @@ int tree_flag_fine(rg_ctx* c, int ilevel, double ed, double ep, double ev, doubl
         if (ilevel >= lmin)
             return set_error(c, RG_ERR_UNSUPPORTED, "coarse-level refinement criteria (levelmin 1) stay on the host");
         k_flag_coarse_below_min<<<nblk(c->ncoarse), TPB, 0, s>>>(M);
+        c->auth_dirty = true;
         return check_cuda(c, cudaGetLastError(), "coarse flags");
     }
     TreeScratch S;
@@ -821,7 +822,10 @@ int tree_make_grid_fine(rg_ctx* c, int ilevel) {
     if (int rc = tree_scratch(c, &S)) return rc;
     TreeMut M = tree_mut(c);
     cudaStream_t s = c->stream;
-    k_authorize<<<nblk(c->ncell), TPB, 0, s>>>(M);
+    if (c->auth_dirty) {
+        k_authorize<<<nblk(c->ncell), TPB, 0, s>>>(M);
+        c->auth_dirty = false;
+    }
     if (ilevel == 1) {
         int* d_count = S.mark;
         int count = 0;
@@ -861,6 +865,7 @@ int tree_make_grid_fine(rg_ctx* c, int ilevel) {
     c->h_numbl[(size_t)hidx(c, L)] += n;
     c->fq_head = (c->fq_head + n) % ngm;
     c->numbf -= n;
+    c->auth_dirty = true;  // the new cells have cpu_map 1 and flag2 0
     if (c->numbf > 0)
         if (int rc = set_dev_int(c, c->d_prev + c->h_fq[(size_t)c->fq_head] - 1, 0)) return rc;
     c->tree_dirty = true;
@@ -885,6 +890,7 @@ int tree_remove_grid_fine(rg_ctx* c, int ilevel) {
     const int fq_tail = (c->fq_head + c->numbf) % ngm;
     const int old_tailf = c->numbf > 0 ? c->h_fq[(size_t)((fq_tail - 1 + ngm) % ngm)] : 0;
     k_kill<<<nblk(noct), TPB, 0, s>>>(M, S.octs, noct, S.mark, S.rank, S.list, S.list2, c->d_fq, fq_tail);
+    c->auth_dirty = true;  // the freed cells have cpu_map 1 and flag2 0
     k_link_chain<<<nblk(std::max(m, 1)), TPB, 0, s>>>(c->d_next, c->d_prev, S.list, m, 0);
     k_link_chain<<<nblk(nkill), TPB, 0, s>>>(c->d_next, c->d_prev, S.list2, nkill, old_tailf);
     std::vector<int> freed((size_t)nkill);
