@@ -379,7 +379,10 @@ int rg_tree_attach(rg_ctx* ctx, const rg_grid_view* g, const rg_tree_arrays* t, 
 int rg_tree_fetch(rg_ctx* ctx, rg_tree_arrays* t);
 /* TreeUpdater::flag_fine (TreeUpdater.cpp:327-575) with its smooth_fine,
  * test_flag and ensure_ref_rules; err_grad_b2 > 0 is RG_ERR_UNSUPPORTED
- * (MHD only). */
+ * (MHD only).  Neither this call nor rg_restrict_fine waits for the device:
+ * a consistency check their kernels fail is returned by the next call that
+ * synchronises (rg_make_grid_fine, rg_remove_grid_fine, rg_courant_step,
+ * rg_synchronize, ...). */
 int rg_flag_fine(rg_ctx* ctx, int ilevel, double err_grad_d, double err_grad_p, double err_grad_u,
                  double err_grad_b2, int nexpand, int icount, int nsubcycle);
 /* TreeUpdater::make_grid_fine (TreeUpdater.cpp:27-149): new octs for

@@ -285,9 +285,15 @@ __device__ int cell_at(const TreeMut& M, const Geo& G, const double* x, int leve
 
 // ensure_ref_rules (TreeUpdater.cpp:578-634): an oct stays flagged only when
 // all 27 cells around its father exist at the father's level and are refined
-// (get_27_cell_neighbors, AmrGrid.cpp:474-511, by coordinates)
+// (get_27_cell_neighbors, AmrGrid.cpp:474-511, by coordinates).  One thread
+// per (oct, neighbour): each lookup is a descent of the tree through
+// dependent loads, so the 27 of an oct run side by side instead of one after
+// another.  A failing neighbour clears the oct's flags; the reference stops
+// at the first failure, which writes the same zeros.
 __global__ void k_ensure_ref_rules(TreeMut M, Geo G, const int* __restrict__ octs, int noct) {
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < noct; k += gridDim.x * blockDim.x) {
+    const long long n = 27LL * noct;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(q / 27), j = (int)(q % 27);
         const int ig = octs[k];
         const int fc = M.father[ig - 1];
         bool ok = fc > 0;
@@ -297,21 +303,18 @@ __global__ void k_ensure_ref_rules(TreeMut M, Geo G, const int* __restrict__ oct
             double xc[3];
             cell_center(M, G, fc, xc);
             const double dxl = G.boxlen / (double)(G.nx * (1 << level));
-            for (int dz = -1; dz <= 1 && ok; ++dz)
-                for (int dy = -1; dy <= 1 && ok; ++dy)
-                    for (int dx = -1; dx <= 1 && ok; ++dx) {
-                        double x[3] = {xc[0], xc[1], xc[2]};
-                        x[0] += dx * dxl;
-                        x[1] += dy * dxl;
-                        x[2] += dz * dxl;
+            const int dz = j / 9 - 1, dy = (j / 3) % 3 - 1, dx = j % 3 - 1;
+            double x[3] = {xc[0], xc[1], xc[2]};
+            x[0] += dx * dxl;
+            x[1] += dy * dxl;
+            x[2] += dz * dxl;
 #pragma unroll
-                        for (int d = 0; d < 3; ++d) {
-                            if (x[d] < 0.0) x[d] += G.boxlen;
-                            else if (x[d] >= G.boxlen) x[d] -= G.boxlen;
-                        }
-                        const int nb = cell_at(M, G, x, level);
-                        if (cell_level(M, nb) != level || M.son[nb - 1] == 0) ok = false;
-                    }
+            for (int d = 0; d < 3; ++d) {
+                if (x[d] < 0.0) x[d] += G.boxlen;
+                else if (x[d] >= G.boxlen) x[d] -= G.boxlen;
+            }
+            const int nb = cell_at(M, G, x, level);
+            if (cell_level(M, nb) != level || M.son[nb - 1] == 0) ok = false;
         }
         if (!ok)
             for (int s = 0; s < 8; ++s) M.flag1[M.ncoarse + s * M.ngridmax + ig - 1] = 0;
@@ -810,7 +813,8 @@ int tree_flag_fine(rg_ctx* c, int ilevel, double ed, double ep, double ev, doubl
     if (ilevel > lmin && icount < nsub) k_test_flag<<<nblk(n), TPB, 0, s>>>(M, S.octs, noct);
     for (int i = 0; i < nexp; ++i) smooth();
     if (ilevel > lmin && icount < nsub)
-        k_ensure_ref_rules<<<nblk(noct), TPB, 0, s>>>(M, Geo{c->nx, c->ny, c->nz, c->params.boxlen}, S.octs, noct);
+        k_ensure_ref_rules<<<nblk(27LL * noct), TPB, 0, s>>>(M, Geo{c->nx, c->ny, c->nz, c->params.boxlen}, S.octs,
+                                                              noct);
     // nothing to read back: the host does not wait here, and a check the
     // kernels failed is reported by the next call that synchronises
     return check_cuda(c, cudaGetLastError(), "flag_fine kernels");
