@@ -745,7 +745,8 @@ def profile_case_learned():
     """A small run of the learned part for ncu captures: training on 1e6 stress
     states for 2 epochs (launches: one k_exact_batch for the labels, then
     k_mlp_grad + k_adam per batch), then the exact solver on 4M stress pairs
-    with the plain start (k_exact_batch #1) and the learned start (#2)."""
+    with the plain start (k_exact_batch #1) and the learned start (the
+    tensor-core starts, k_mlp_guess_tc, then k_exact_batch #2 from them)."""
     import torch
     import rgpu
     ctx = rgpu.Context(rgpu.make_params(3, riemann="exact"), 0)

@@ -28,13 +28,11 @@ namespace {
 
 constexpr int TB = 128;       // threads per block: 4 warps
 constexpr int SPB = 64;       // samples per block iteration (16 per warp)
-constexpr int W1P = 24;       // padded row stride (bf16) of W1 [64][16 used]
-constexpr int W2P = 72;       // padded row stride (bf16) of W2 / W2^T [64][64]
 
 struct TrainSmem {
-    __nv_bfloat16 w1[MLP_H][W1P];
-    __nv_bfloat16 w2[MLP_H][W2P];   // [out][in]
-    __nv_bfloat16 w2t[MLP_H][W2P];  // [in][out]
+    __nv_bfloat16 w1[MLP_H][MLP_W1P];
+    __nv_bfloat16 w2[MLP_H][MLP_W2P];   // [out][in]
+    __nv_bfloat16 w2t[MLP_H][MLP_W2P];  // [in][out]
     float b1[MLP_H], b2[MLP_H], w3[MLP_H];
     float h1b[SPB][MLP_H + 1];      // BF16-rounded H1 per sample
     float dz2[SPB][MLP_H + 1];
@@ -42,26 +40,6 @@ struct TrainSmem {
     float xb[SPB][MLP_IN + 1];
 };
 
-__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
-    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
-    return *reinterpret_cast<uint32_t*>(&v);
-}
-__device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
-
-__device__ __forceinline__ void mma16816(float* d, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
-                                         uint32_t b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};\n"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-}
-
-__device__ __forceinline__ float quad_sum(float v) {
-    v += __shfl_xor_sync(0xffffffffu, v, 1);
-    v += __shfl_xor_sync(0xffffffffu, v, 2);
-    return v;
-}
 __device__ __forceinline__ float group_sum(float v) {  // over the 8 row groups of a warp
     v += __shfl_xor_sync(0xffffffffu, v, 4);
     v += __shfl_xor_sync(0xffffffffu, v, 8);

@@ -26,8 +26,10 @@
 // Target: log(max(p*, 1e-30 pref) / b); the guess is b * exp(prediction).
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stdint.h>
 
 #include "rg_physics.cuh"
 
@@ -55,6 +57,32 @@ constexpr float MLP_GATE_DEFAULT = 0.05f;
 constexpr double MLP_WEAK_P = 1.3, MLP_WEAK_U = 0.3;
 constexpr float MLP_LOG_FLOOR = 1e-30f;
 
+constexpr int MLP_W1P = 24;  // padded row stride (bf16) of W1 in shared memory [64][16 used]
+constexpr int MLP_W2P = 72;  // padded row stride (bf16) of W2 / W2^T in shared memory [64][64]
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+__device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+
+// d += A B on the tensor cores: one m16n8k16 tile, BF16 operands, FP32 accumulation
+__device__ __forceinline__ void mma16816(float* d, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                         uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// sum over the 4 threads of an mma row group
+__device__ __forceinline__ float quad_sum(float v) {
+    v += __shfl_xor_sync(0xffffffffu, v, 1);
+    v += __shfl_xor_sync(0xffffffffu, v, 2);
+    return v;
+}
+
 __device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
 __device__ __forceinline__ float silu_grad(float z) {
     float s = 1.0f / (1.0f + __expf(-z));
@@ -66,7 +94,18 @@ __device__ __forceinline__ float silu_grad(float z) {
 // in units of pref, densities of rref = max(rl, rr), velocities of
 // sqrt(pref/rref) -- so that every intermediate stays in FP32 range whatever
 // the states' scale; the features are ratios and do not depend on the units.
-template <int NDIM>
+// FAST: hardware approximations of log, asinh and the FP32 divides (the
+// batched tensor-core guess, where the features only seed Newton); the
+// training data and the in-solver guess use the accurate functions.
+__device__ __forceinline__ float feat_div(float a, float b, bool fast) { return fast ? __fdividef(a, b) : a / b; }
+__device__ __forceinline__ float feat_log(float a, bool fast) { return fast ? __logf(a) : logf(a); }
+__device__ __forceinline__ float feat_asinh(float a, bool fast) {
+    if (!fast) return asinhf(a);
+    const float m = fabsf(a);
+    return copysignf(__logf(m + sqrtf(fmaf(m, m, 1.0f))), a);
+}
+
+template <int NDIM, bool FAST = false>
 __device__ __forceinline__ void mlp_features(const double* ql, const double* qr, double gamma, double smallp,
                                              float* x, double* pref_out, double* base_out,
                                              double* p2s_out = nullptr) {
@@ -79,25 +118,25 @@ __device__ __forceinline__ void mlp_features(const double* ql, const double* qr,
     const float al = (float)(rl * ir), ar = (float)(rr * ir);
     const float bl = (float)(pl * ip), br = (float)(pr * ip);
     const float vl = (float)(ql[1] * iv), vr = (float)(qr[1] * iv);
-    float cl = sqrtf(g * bl / al), cr = sqrtf(g * br / ar);
+    float cl = sqrtf(feat_div(g * bl, al, FAST)), cr = sqrtf(feat_div(g * br, ar, FAST));
     float wl = sqrtf(g * bl * al), wr = sqrtf(g * br * ar);
-    float p2s = fmaxf((wr * bl + wl * br + wl * wr * (vl - vr)) / (wl + wr + 1e-30f), 0.f);
+    float p2s = fmaxf(feat_div(wr * bl + wl * br + wl * wr * (vl - vr), wl + wr + 1e-30f, FAST), 0.f);
     // Toro's two-shock estimate: the linearised formula above with each wave's
     // mass flux W_k(p) = sqrt(gamma p_k rho_k (1 + (gamma+1)/(2 gamma) (p-p_k)/p_k))
     // -- the function the solver's Newton iteration works on -- taken at the
     // plain guess instead of at p_k
     const float g6 = (g + 1.f) / (2.f * g);
-    const float wl0 = sqrtf(fmaxf(wl * wl * (1.f + g6 * (p2s - bl) / bl), 0.f));
-    const float wr0 = sqrtf(fmaxf(wr * wr * (1.f + g6 * (p2s - br) / br), 0.f));
-    const float pts = fmaxf((wr0 * bl + wl0 * br + wl0 * wr0 * (vl - vr)) / (wl0 + wr0 + 1e-30f), 0.f);
-    x[0] = logf(al / ar);
-    x[1] = logf(bl / br);
-    x[2] = asinhf((vl - vr) / (cl + cr));
-    x[3] = asinhf(vl / cl);
-    x[4] = asinhf(vr / cr);
+    const float wl0 = sqrtf(fmaxf(wl * wl * (1.f + feat_div(g6 * (p2s - bl), bl, FAST)), 0.f));
+    const float wr0 = sqrtf(fmaxf(wr * wr * (1.f + feat_div(g6 * (p2s - br), br, FAST)), 0.f));
+    const float pts = fmaxf(feat_div(wr0 * bl + wl0 * br + wl0 * wr0 * (vl - vr), wl0 + wr0 + 1e-30f, FAST), 0.f);
+    x[0] = feat_log(feat_div(al, ar, FAST), FAST);
+    x[1] = feat_log(feat_div(bl, br, FAST), FAST);
+    x[2] = feat_asinh(feat_div(vl - vr, cl + cr, FAST), FAST);
+    x[3] = feat_asinh(feat_div(vl, cl, FAST), FAST);
+    x[4] = feat_asinh(feat_div(vr, cr, FAST), FAST);
     x[5] = g;
-    x[6] = logf(fmaxf(p2s, MLP_LOG_FLOOR));
-    x[7] = logf(fmaxf(pts, MLP_LOG_FLOOR));
+    x[6] = feat_log(fmaxf(p2s, MLP_LOG_FLOOR), FAST);
+    x[7] = feat_log(fmaxf(pts, MLP_LOG_FLOOR), FAST);
     *pref_out = pref;
     *base_out = pref * (double)fmaxf(pts, MLP_LOG_FLOOR);
     if (p2s_out) *p2s_out = pref * (double)p2s;
