@@ -2,7 +2,7 @@
 //
 // The reference routes its log output through spdlog (ramses/utils/Logger.hpp,
 // macros RAMSES_INFO and friends).  spdlog is fetched by CMake over the network,
-// which this build does not have, and logging does no arithmetic on the hydro
+// which is not reachable here, and logging does no arithmetic on the hydro
 // path, so every macro here expands to nothing.  This header replaces the
 // reference's Logger.hpp only inside the oracle build (oracle/_ref).
 #ifndef RAMSES_LOGGER_HPP

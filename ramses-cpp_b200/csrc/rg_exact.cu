@@ -4,7 +4,7 @@
 // The exact solver is RiemannSolver::solve_godunov_nr of RAMSES-CPP
 // (src/solvers/hydro/RiemannSolver.cpp:194-307), in rg_physics.cuh.  Two modes:
 // the reference's (10 iterations, |dp/(p+1e-10)| < 1e-6) and a converged one
-// (tolerance 1e-14, larger iteration cap) in which the learned guess is judged:
+// (tolerance 1e-14, larger iteration cap) in which the learned guess is evaluated:
 // it must reach the same root with fewer Newton updates.
 #include <algorithm>
 #include <cstdint>

@@ -16,7 +16,7 @@
 // state.  Otherwise (pageable arrays, as AmrGrid's std::vectors are, or a
 // fragmented level) the cells are gathered on the host into pinned staging,
 // run by run where runs are long, moved in one copy each way and scattered on
-// the device: the driver stages a pageable copy through its own buffers with
+// the device: the CUDA driver stages a pageable copy through its own buffers with
 // a wait per row, so many small pageable copies would cost far more than the
 // host gather.
 #include <algorithm>

@@ -4,7 +4,7 @@ forwards every call to the reference harness (the reference's own
 TreeUpdater and HydroSolver, compiled here) must leave the same tree, state,
 time and cell-update count as refsupport.AmrRun, the replay of
 Simulation::run / amr_step (src/core/Simulation.cpp:366-397, 522-635).  This
-checks the driver's control flow (which level steps, in which order, with
+checks the coarse-step loop's control flow (which level steps, in which order, with
 which icount / nsubcycle arguments) without a GPU; the device operations
 themselves are checked against the reference in tests/test_gpu_tree.py."""
 import numpy as np

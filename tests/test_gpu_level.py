@@ -1,7 +1,7 @@
 """GPU level step (librgpu.so through its C ABI) against the oracle and the
 reference's golden vectors.  Bit-exact for integer work and for the
 HLLC/HLL/LLF/acoustic solvers; the exact solver differs only through pow()
-(CUDA vs glibc) and is held to 3e-12 relative."""
+(CUDA vs glibc) and is held to 3e-12 relative (the path's stated tolerance)."""
 import numpy as np
 import pytest
 
