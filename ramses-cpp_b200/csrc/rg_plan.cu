@@ -71,8 +71,12 @@ __global__ void k_cell_levels(TreeView T, int* cell_level, int ttd, DevStatus* s
     }
 }
 
+// count[0]: octs found; check_on_device: the block that finishes last
+// (count[1] counts finished blocks) compares count[0] with noct itself -- a
+// shorter chain than the level count says raises DE_LIST -- so the host
+// need not read it back
 __global__ void k_level_octs(int n, const int* __restrict__ jump, const int* __restrict__ dist, int head0, int noct,
-                             int* octs, int* count, DevStatus* st) {
+                             int* octs, int* count, DevStatus* st, bool check_on_device) {
     int tail = jump[head0];
     int dh = dist[head0];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -85,12 +89,12 @@ __global__ void k_level_octs(int n, const int* __restrict__ jump, const int* __r
         octs[pos] = i + 1;
         atomicAdd(count, 1);
     }
-}
-
-// the count k_level_octs found must be the list's length (a shorter chain
-// than the level count says)
-__global__ void k_check_count(const int* count, int noct, DevStatus* st) {
-    if (*count != noct) raise_err(st, DE_LIST, noct);
+    if (!check_on_device) return;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(count + 1, 1) == (int)gridDim.x - 1 && atomicAdd(count, 0) != noct) raise_err(st, DE_LIST, noct);
+    }
 }
 
 // ---------------------------------------------------------------- plan cells
@@ -469,7 +473,7 @@ int build_plan_t(rg_ctx* c, int ilevel, Plan& P) {
         }
         cudaMemsetAsync(d_count, 0, sizeof(int), s);
         k_level_octs<<<nblk(c->ngridmax), TPB, 0, s>>>(c->ngridmax, c->d_jump, c->d_dist, head - 1, P.noct, P.octs,
-                                                       d_count, c->d_status);
+                                                       d_count, c->d_status, false);
         cudaMemcpyAsync(&hv[0], d_count, sizeof(int), cudaMemcpyDeviceToHost, s);
         if (int rc = check_cuda(c, cudaStreamSynchronize(s), "level octs")) return rc;
         if (hv[0] != P.noct) return set_error(c, RG_ERR_TOPOLOGY, "level linked list merges with another chain");
@@ -612,13 +616,13 @@ int level_oct_list(rg_ctx* c, int ilevel, int* out, int cap, int* noct) {
         if (int rc = dalloc(c, &c->d_scan, 1024, "scan scratch")) return rc;
         c->cap_scan = 1024;
     }
-    cudaMemsetAsync(c->d_scan, 0, sizeof(int), s);
+    cudaMemsetAsync(c->d_scan, 0, 2 * sizeof(int), s);
+    // with the tree resident the count is the host's own: the chain is
+    // checked on the device and the host does not wait (a mismatch is
+    // reported by the next call that synchronises)
     k_level_octs<<<nblk(c->ngridmax), TPB, 0, s>>>(c->ngridmax, c->d_jump, c->d_dist, head - 1, n, out, c->d_scan,
-                                                   c->d_status);
+                                                   c->d_status, c->tree_resident);
     if (c->tree_resident) {
-        // the count is the host's own: check the chain on the device and do
-        // not wait (a mismatch is reported by the next call that synchronises)
-        k_check_count<<<1, 1, 0, s>>>(c->d_scan, n, c->d_status);
         *noct = n;
         return check_cuda(c, cudaGetLastError(), "level octs");
     }
