@@ -51,3 +51,23 @@ def test_invalid_params_are_reported_not_raised(rgpu_lib):
         assert rgpu_lib.rg_godunov_level(None, 1, 0.1, 0.1) == rgpu.RG_ERR_ARG
     finally:
         rgpu_lib.rg_destroy(h)
+
+
+def test_tree_and_plan_queries_report_misuse(rgpu_lib):
+    """rg_tree_sizes and rg_level_plan_info: a null context is RG_ERR_ARG, a
+    context without a tree or without a usable device an error status, a null
+    output RG_ERR_ARG -- never a crash."""
+    g, n = C.c_int(-7), C.c_int(-7)
+    info = rgpu.rg_plan_info()
+    assert rgpu_lib.rg_tree_sizes(None, C.byref(g), C.byref(n)) == rgpu.RG_ERR_ARG
+    assert rgpu_lib.rg_level_plan_info(None, 1, C.byref(info)) == rgpu.RG_ERR_ARG
+    p = rgpu.make_params(3)
+    h = rgpu_lib.rg_create(C.byref(p), 0)
+    assert h
+    try:
+        assert rgpu_lib.rg_tree_sizes(h, C.byref(g), C.byref(n)) != rgpu.RG_OK
+        assert (g.value, n.value) == (-7, -7)
+        assert rgpu_lib.rg_level_plan_info(h, 1, None) != rgpu.RG_OK
+        assert rgpu_lib.rg_level_plan_info(h, 1, C.byref(info)) != rgpu.RG_OK
+    finally:
+        rgpu_lib.rg_destroy(h)
