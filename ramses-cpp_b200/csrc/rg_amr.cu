@@ -7,8 +7,12 @@
 // refine / remove the finer levels, CFL step capped by the coarser level's dt
 // over its sub-cycles, set_unew, the finer sub-steps, godunov_fine, set_uold,
 // restrict_fine, flag_fine of the next finer level) with every grid and hydro
-// call on the device: the host only reads the level counts (kept on the host)
-// and one dt per level step.  Sub-cycling 2 from levelmin on, 1 below, as
+// call on the device.  The clock (each level's dtnew / dtold and the time)
+// lives in device memory for the step: the CFL step, its cap by the coarser
+// level's dt over its sub-cycles and the time updates are single-thread
+// kernels with the host's arithmetic, since the control flow depends only on
+// the level counts, which the host keeps; so the host reads no dt back.
+// Sub-cycling 2 from levelmin on, 1 below, as
 // Simulation's nsubcycle_ default.  Physics modules the hydro configs switch
 // off (turbulence, sinks, stars, cooling, RT) are not called.
 #include <algorithm>
@@ -19,12 +23,37 @@ namespace rg {
 namespace {
 
 constexpr int kMaxLevel = 32;
+// device clock: dtnew[0..32], dtold[0..32], t
+constexpr int kDtOld = kMaxLevel + 1, kClockT = 2 * (kMaxLevel + 1), kClockN = kClockT + 1;
 
 struct AmrRunState {
-    double dtnew[kMaxLevel + 1] = {}, dtold[kMaxLevel + 1] = {};
-    double t = 0.0;
+    double* ck = nullptr;  // device clock
     long long nstep = 0, cell_updates = 0;
 };
+
+// Simulation.cpp:552-554: dtold = dtnew; dtnew = the CFL step (the CFL
+// word), capped by the coarser level's dtnew over its sub-cycles
+// (nsub_coarser > 0 above levelmin)
+__global__ void k_amr_dt(double* ck, const DevStatus* st, int il, int nsub_coarser) {
+    ck[kDtOld + il] = ck[il];
+    double d = __longlong_as_double((long long)st->dtmin_bits);
+    if (nsub_coarser > 0) {
+        const double cand = ck[il - 1] / (double)nsub_coarser;
+        d = cand < d ? cand : d;  // std::min(d, cand)
+    }
+    ck[il] = d;
+}
+
+// a level without finer octs (Simulation.cpp:600-603): the finer level's
+// steps are this one's over its sub-cycles, and the time advances
+__global__ void k_amr_no_finer(double* ck, int il, int nsub) {
+    const double v = ck[il] / (double)nsub;
+    ck[kDtOld + il + 1] = v;
+    ck[il + 1] = v;
+    ck[kClockT] += ck[il];
+}
+
+__global__ void k_amr_advance(double* ck, int il) { ck[kClockT] += ck[il]; }
 
 int count_grids(const rg_ctx* c, int il) {
     if (il < 0 || il > c->nlevelmax) return 0;
@@ -44,13 +73,8 @@ int amr_step(rg_ctx* c, const rg_amr_config& cfg, AmrRunState& S, int il, int ic
             if (int rc = tree_remove_grid_fine(c, i + 1)) return rc;
     }
     const double dx = cfg.boxlen / (double)(c->nx * (1 << il));
-    S.dtold[il] = S.dtnew[il];
-    if (int rc = rg_courant_step(c, il, dx, cfg.courant_factor, cfg.pressure_cap, &S.dtnew[il])) return rc;
-    if (il > lmin) {
-        const double cand = S.dtnew[il - 1] / (double)nsubcycle(cfg, il - 1);
-        S.dtnew[il] = std::min(S.dtnew[il], cand);
-    }
-    const double dt = S.dtnew[il];
+    if (int rc = courant_step_device(c, il, dx, cfg.courant_factor, cfg.pressure_cap)) return rc;
+    k_amr_dt<<<1, 1, 0, c->stream>>>(S.ck, c->d_status, il, il > lmin ? nsubcycle(cfg, il - 1) : 0);
     if (int rc = rg_set_unew(c, il)) return rc;
     const int nsub = nsubcycle(cfg, il);
     if (il < lmax) {
@@ -58,22 +82,38 @@ int amr_step(rg_ctx* c, const rg_amr_config& cfg, AmrRunState& S, int il, int ic
             for (int i = 1; i <= nsub; ++i)
                 if (int rc = amr_step(c, cfg, S, il + 1, i)) return rc;
         } else {
-            S.dtold[il + 1] = S.dtnew[il] / (double)nsub;
-            S.dtnew[il + 1] = S.dtnew[il] / (double)nsub;
-            S.t += dt;
+            k_amr_no_finer<<<1, 1, 0, c->stream>>>(S.ck, il, nsub);
             S.nstep++;
         }
     } else {
-        S.t += dt;
+        k_amr_advance<<<1, 1, 0, c->stream>>>(S.ck, il);
         S.nstep++;
     }
-    if (int rc = rg_godunov_level(c, il, dt, dx)) return rc;
+    // this level's dtnew is still the one set above: the finer steps only
+    // change the finer levels' entries
+    if (int rc = godunov_level_device_dt(c, il, S.ck + il, dx)) return rc;
     S.cell_updates += rg_level_cell_updates(c, il);
     if (int rc = rg_set_uold(c, il)) return rc;
     if (il < lmax)
         if (int rc = tree_restrict_fine(c, il)) return rc;
     return tree_flag_fine(c, il + 1, cfg.err_grad_d, cfg.err_grad_p, cfg.err_grad_u, -1.0, cfg.nexpand, icount,
                           il > 0 ? nsubcycle(cfg, il - 1) : 1);
+}
+
+int coarse_step(rg_ctx* c, const rg_amr_config& cfgr, AmrRunState& S) {
+    const rg_amr_config* cfg = &cfgr;
+    const int lmin = cfg->levelmin, lmax = c->nlevelmax;
+    if (lmin < lmax)
+        for (int il = 1; il <= lmin - 1; ++il)
+            if (int rc = tree_make_grid_fine(c, il)) return rc;
+    if (int rc = amr_step(c, *cfg, S, lmin, 1)) return rc;
+    for (int il = lmin; il >= 1; --il)
+        if (int rc = tree_flag_fine(c, il, cfg->err_grad_d, cfg->err_grad_p, cfg->err_grad_u, -1.0, cfg->nexpand, 2, 2))
+            return rc;
+    if (lmin < lmax)
+        for (int il = lmin - 1; il >= 0; --il)
+            if (int rc = tree_restrict_fine(c, il)) return rc;
+    return check_cuda(c, cudaGetLastError(), "coarse-step clock kernels");
 }
 
 }  // namespace
@@ -91,26 +131,30 @@ extern "C" int rg_amr_coarse_step(rg_ctx* c, const rg_amr_config* cfg, rg_amr_cl
     if (!(cfg->boxlen > 0.0)) return set_error(c, RG_ERR_ARG, "boxlen must be positive");
     cudaSetDevice(c->device);
     AmrRunState S;
-    std::copy(clock->dtnew, clock->dtnew + kMaxLevel + 1, S.dtnew);
-    std::copy(clock->dtold, clock->dtold + kMaxLevel + 1, S.dtold);
-    S.t = clock->t;
+    double h[kClockN];
+    std::copy(clock->dtnew, clock->dtnew + kMaxLevel + 1, h);
+    std::copy(clock->dtold, clock->dtold + kMaxLevel + 1, h + kDtOld);
+    h[kClockT] = clock->t;
+    if (int rc = check_cuda(c, dev_alloc(c, &S.ck, sizeof(h)), "coarse-step clock")) return rc;
+    if (int rc = check_cuda(c, cudaMemcpyAsync(S.ck, h, sizeof(h), cudaMemcpyHostToDevice, c->stream), "clock upload")) {
+        dev_free(c, S.ck);
+        return rc;
+    }
     S.nstep = clock->nstep;
     S.cell_updates = clock->cell_updates;
-    const int lmin = cfg->levelmin, lmax = c->nlevelmax;
-    if (lmin < lmax)
-        for (int il = 1; il <= lmin - 1; ++il)
-            if (int rc = tree_make_grid_fine(c, il)) return rc;
-    if (int rc = amr_step(c, *cfg, S, lmin, 1)) return rc;
-    for (int il = lmin; il >= 1; --il)
-        if (int rc = tree_flag_fine(c, il, cfg->err_grad_d, cfg->err_grad_p, cfg->err_grad_u, -1.0, cfg->nexpand, 2, 2))
-            return rc;
-    if (lmin < lmax)
-        for (int il = lmin - 1; il >= 0; --il)
-            if (int rc = tree_restrict_fine(c, il)) return rc;
-    std::copy(S.dtnew, S.dtnew + kMaxLevel + 1, clock->dtnew);
-    std::copy(S.dtold, S.dtold + kMaxLevel + 1, clock->dtold);
-    clock->t = S.t;
+    const int rc_step = coarse_step(c, *cfg, S);
+    // the clock comes back with the step (the copy waits for it); on an error
+    // the caller's clock is left as it was
+    const int rc_copy = check_cuda(c, cudaMemcpyAsync(h, S.ck, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "clock");
+    const int rc_sync = check_cuda(c, cudaStreamSynchronize(c->stream), "coarse step");
+    dev_free(c, S.ck);
+    if (rc_step) return rc_step;
+    if (rc_copy) return rc_copy;
+    if (rc_sync) return rc_sync;
+    std::copy(h, h + kMaxLevel + 1, clock->dtnew);
+    std::copy(h + kDtOld, h + kDtOld + kMaxLevel + 1, clock->dtold);
+    clock->t = h[kClockT];
     clock->nstep = S.nstep;
     clock->cell_updates = S.cell_updates;
-    return check_cuda(c, cudaStreamSynchronize(c->stream), "coarse step");
+    return RG_OK;
 }

@@ -541,6 +541,39 @@ int rg_courant_step(rg_ctx* c, int ilevel, double dx, double courant_factor, int
     return RG_OK;
 }
 
+}  // extern "C"
+
+namespace rg {
+int courant_step_device(rg_ctx* c, int ilevel, double dx, double courant_factor, int pressure_cap) {
+    CTX_GUARD(c);
+    c->next_level = -1;  // the state or the CFL word may change
+    if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state uploaded");
+    Plan* P;
+    if (int rc = get_plan(c, ilevel, &P)) return rc;
+    if (P->nbox > 0) return set_error(c, RG_ERR_STATE, "ensemble level: read the per-box steps with rg_level_box_dt");
+    return launch_courant(c, *P, dx, pressure_cap, courant_factor);
+}
+
+int godunov_level_device_dt(rg_ctx* c, int ilevel, const double* dt_dev, double dx) {
+    CTX_GUARD(c);
+    c->next_level = -1;  // the state or the CFL word may change
+    if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state uploaded");
+    if (int rc = check_learned(c)) return rc;
+    Plan* P;
+    if (int rc = get_plan(c, ilevel, &P)) return rc;
+    if (P->nbox > 0) return set_error(c, RG_ERR_STATE, "ensemble level: every box has its own dt, use rg_level_substep");
+    record_updates(c, ilevel, *P);
+    if (P->ncells == 0) return RG_OK;
+    if (int rc = ensure_flux(c, *P)) return rc;
+    if (int rc = launch_set_dt_device(c, dt_dev, dx)) return rc;
+    if (int rc = launch_godunov(c, *P)) return rc;
+    if (P->face_variant < 0 && ++P->substeps_run >= 1) return autotune_face(c, *P, step_consts(c));
+    return RG_OK;
+}
+}  // namespace rg
+
+extern "C" {
+
 int rg_level_substep(rg_ctx* c, int ilevel, double dx, int pressure_cap, int use_graph, double* dt_used) {
     CTX_GUARD(c);
     if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state uploaded");

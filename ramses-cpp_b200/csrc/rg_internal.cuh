@@ -282,6 +282,12 @@ int compute_cell_levels(rg_ctx* c);
 int launch_set_unew(rg_ctx* c, const Plan& p);
 int launch_set_uold(rg_ctx* c, const Plan& p);
 int launch_courant(rg_ctx* c, const Plan& p, double dx, int pressure_cap, double courant_factor);
+// the step values (dt, dt/dx, 1/dx) from a dt in device memory
+int launch_set_dt_device(rg_ctx* c, const double* dt, double dx);
+// rg_courant_step without reading the step back: the CFL word holds it
+int courant_step_device(rg_ctx* c, int ilevel, double dx, double courant_factor, int pressure_cap);
+// rg_godunov_level with its dt read by the device from dt_dev
+int godunov_level_device_dt(rg_ctx* c, int ilevel, const double* dt_dev, double dx);
 int launch_set_dt_host(rg_ctx* c, double dt, double dx);
 int launch_finalize_dt(rg_ctx* c, double dx);
 int launch_godunov(rg_ctx* c, const Plan& p);

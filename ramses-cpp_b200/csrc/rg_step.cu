@@ -447,6 +447,7 @@ __global__ void k_dt_finalize(DevStatus* st, double dx, double dt_start) {
     st->dtmin_bits = (unsigned long long)__double_as_longlong(dt_start);
 }
 __global__ void k_dt_set(DevStatus* st, double dt, double dx) { set_step_values(st, dt, dx); }
+__global__ void k_dt_set_dev(DevStatus* st, const double* dt, double dx) { set_step_values(st, *dt, dx); }
 
 // ---- ensemble levels: one CFL step per box
 __global__ void k_box_courant_init(BoxStep* boxes, int nbox, double dt_start) {
@@ -737,6 +738,11 @@ int launch_finalize_dt(rg_ctx* c, double dx) {
 int launch_set_dt_host(rg_ctx* c, double dt, double dx) {
     k_dt_set<<<1, 1, 0, c->stream>>>(c->d_status, dt, dx);
     return check_cuda(c, cudaGetLastError(), "dt set");
+}
+
+int launch_set_dt_device(rg_ctx* c, const double* dt, double dx) {
+    k_dt_set_dev<<<1, 1, 0, c->stream>>>(c->d_status, dt, dx);
+    return check_cuda(c, cudaGetLastError(), "dt set (device)");
 }
 
 // ---------------------------------------------------------------- small-level runs
