@@ -5,14 +5,17 @@
 after `Context.tree_attach`: the tree operations (flag_fine, make_grid_fine,
 remove_grid_fine, restrict_fine; rg_tree.cu), the CFL step
 (compute_courant_step, HydroSolver.cpp:878-977), set_unew / godunov_fine /
-set_uold all run on the device, and the host reads back only the level
-counts and one dt per level step.  Same call sequence as the reference's
+set_uold all run on the device.  Same call sequence as the reference's
 step, so the tree, every oct id and the state come out bit for bit as the
-reference's own run leaves them.
+reference's own run leaves them; when a refinement needs more octs than the
+free list holds, ngridmax doubles as in the reference (Context.tree_sizes
+gives the new sizes).
 
-By default a coarse step is one native call (rg_amr_coarse_step, rg_amr.cu);
-`native=False` issues the same sequence call by call from Python through the
-per-operation entry points, which the tests use to check both paths.
+By default a coarse step is one native call (rg_amr_coarse_step, rg_amr.cu),
+whose clock (each level's dt and the time) stays on the device until the
+step ends; `native=False` issues the same sequence call by call from Python
+through the per-operation entry points, reading each level's dt back, which
+the tests use to check both paths.
 
 The CFL step takes the reference formula with or without its p <= 100 rho
 cap (`pressure_cap`); the sub-cycled Sedov runs use it without the cap, which
