@@ -26,11 +26,25 @@ constexpr int BRICK = 8, BHALO = 2, BSIDE = BRICK + 2 * BHALO, BSITES = BSIDE * 
 constexpr int BRICK_THREADS = 256;
 constexpr size_t BRICK_SMEM = sizeof(double) * 5 * BSITES;  // 69,120 bytes (3D: nvar 5)
 
-// Rotated primitive state of shared-memory site `site` for direction idim.
-__device__ __forceinline__ void brick_state(const double* __restrict__ sq, int site, int idim, double* q) {
-#pragma unroll
-    for (int iv = 0; iv < 5; ++iv) q[iv] = sq[iv * BSITES + site];
-    rot_swap<3>(q, idim);
+// Rotated primitive state of shared-memory site `site`: the normal velocity
+// read from plane o1 into slot 1, the tangential ones from o2 and o3 (planes
+// of the direction, set once per direction by brick_planes), so the rotation
+// costs no data movement after the loads.
+__device__ __forceinline__ void brick_state(const double* __restrict__ sq, int site, int o1, int o2, int o3,
+                                            double* q) {
+    q[0] = sq[site];
+    q[1] = sq[o1 + site];
+    q[2] = sq[o2 + site];
+    q[3] = sq[o3 + site];
+    q[4] = sq[4 * BSITES + site];
+}
+
+// Planes of slots 1..3 for direction idim: rot_swap<3>'s exchange of slot 1
+// with slot 1 + idim, applied to where the values are read from.
+__device__ __forceinline__ void brick_planes(int idim, int& o1, int& o2, int& o3) {
+    o1 = (1 + idim) * BSITES;
+    o2 = (idim == 1 ? 1 : 2) * BSITES;
+    o3 = (idim == 2 ? 1 : 3) * BSITES;
 }
 
 // Lattice geometry of a level: one lattice (nbox == 0: extents ex, ey, ez) or
@@ -100,17 +114,19 @@ __device__ __forceinline__ void brick_face(const PlanView& P, const BrickGeom& G
 #pragma unroll 1
         for (int idim = 0; idim < 3; ++idim) {
             const int stride = idim == 0 ? 1 : (idim == 1 ? BSIDE : BSIDE * BSIDE);
+            int o1, o2, o3;
+            brick_planes(idim, o1, o2, o3);
             double qc[NV], ql[NV], qr[NV], qmo[NV], qpo[NV];
-            brick_state(sq, site, idim, qc);
-            brick_state(sq, site - stride, idim, ql);
-            brick_state(sq, site + stride, idim, qr);
+            brick_state(sq, site, o1, o2, o3, qc);
+            brick_state(sq, site - stride, o1, o2, o3, ql);
+            brick_state(sq, site + stride, o1, o2, o3, qr);
             own_trace<3>(qc, ql, qr, dt, D, K, qmo, qpo);
 #pragma unroll
             for (int side = 0; side < 2; ++side) {
                 // neighbour n = c -/+ e, its stencil (n - e, n + e) = (c - 2e, c) / (c, c + 2e)
                 double qn[NV], qfar[NV], qm[NV], qp[NV], f[NV];
-                brick_state(sq, side ? site + stride : site - stride, idim, qn);
-                brick_state(sq, side ? site + 2 * stride : site - 2 * stride, idim, qfar);
+                brick_state(sq, side ? site + stride : site - stride, o1, o2, o3, qn);
+                brick_state(sq, side ? site + 2 * stride : site - 2 * stride, o1, o2, o3, qfar);
                 const double* qnl = side ? qc : qfar;
                 const double* qnr = side ? qfar : qc;
                 if (ghost) ghost_trace<3>(qn, qnl, qnr, dt, D, K, qm, qp);
