@@ -18,7 +18,19 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parents[1]
 ORACLE_DIR = ROOT / "oracle"
-REF_SRC = Path(os.environ.get("RG_REFERENCE_DIR", "/root/reference"))
+
+
+def reference_dir():
+    """Where the RAMSES-CPP sources are: RG_REFERENCE_DIR, else the default of
+    the oracle's build recipe (``make -C oracle refdir``)."""
+    env = os.environ.get("RG_REFERENCE_DIR")
+    if env:
+        return Path(env)
+    r = subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), "refdir"], capture_output=True, text=True)
+    return Path(r.stdout.strip()) if r.returncode == 0 and r.stdout.strip() else Path("reference-not-configured")
+
+
+REF_SRC = reference_dir()
 
 I32P = C.POINTER(C.c_int)
 F64P = C.POINTER(C.c_double)
