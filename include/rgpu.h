@@ -244,13 +244,19 @@ int rg_level_substep_host(rg_ctx* ctx, int ilevel, double dx, int pressure_cap, 
  * device-memory budget committed at start-up, a framework allocator that owns
  * the free memory, a time loop that may not call cudaMalloc/cudaFree because
  * they synchronise): it calls no allocating routine.  State comes from the
- * caller's device buffers, [nvar][ncell] like the grid: uold_dev is read,
- * unew_dev is updated in place.  The flux scratch is a 64 MiB static device
+ * caller's device buffers, [nvar][ncell] like the grid, on the context's
+ * device and at least nvar*ncell doubles long (checked; RG_ERR_ARG otherwise):
+ * uold_dev is read; unew_dev must already hold the level's starting unew --
+ * normally a copy of uold_dev, as rg_set_unew makes it -- since the fold adds
+ * the flux updates to it, and only the level's update targets (its cells and
+ * the coarser cells that take refluxes) are written.  The flux scratch is a 64 MiB static device
  * array inside the library (levels of at most 279,620 cells in 3D, 1,398,101
  * in 1D; larger levels return RG_ERR_ARG); every GPU that loads the library
  * keeps those 64 MiB until exit.  The level's plan must already exist (one
  * earlier rg_godunov_level or rg_set_unew call for the level after
- * rg_sync_topology builds it), else RG_ERR_STATE.  The first call on each
+ * rg_sync_topology, or after a change of the device-resident tree, builds
+ * it), else RG_ERR_STATE; RG_ERR_STATE too for the learned Newton start
+ * without a network, as rg_godunov_level.  The first call on each
  * device resolves the scratch address with cudaGetSymbolAddress, so make that
  * first call before any stream capture.  All calls share the one scratch
  * array: calls whose kernels overlap on the GPU race and must be ordered by
@@ -281,6 +287,10 @@ int64_t rg_level_cell_updates(rg_ctx* ctx, int ilevel);
  * context stream); per-kernel breakdown in out[0..n) (prim, face, fold; in a
  * fused leaf substep "prim" covers the CFL + primitive pass). */
 int rg_last_kernel_ms(rg_ctx* ctx, float* out, int n);
+/* Device memory of the context's stream-ordered pool, which every device
+ * array of the context comes from: bytes the pool holds from the driver
+ * (reserved) and bytes handed out (used).  No reference counterpart. */
+int rg_pool_usage(rg_ctx* ctx, uint64_t* reserved, uint64_t* used);
 /* Enable (on != 0) or disable the per-kernel CUDA events read by
  * rg_last_kernel_ms; they are recorded by rg_godunov_level and by eager
  * (use_graph == 0) rg_level_substep calls (captured graphs carry no events).  The RG_TIMING=1 environment variable sets the

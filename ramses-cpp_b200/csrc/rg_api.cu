@@ -1092,6 +1092,21 @@ int rg_last_kernel_ms(rg_ctx* c, float* out, int n) {
     return c->timing ? RG_OK : set_error(c, RG_ERR_STATE, "timing disabled (set RG_TIMING=1)");
 }
 
+int rg_pool_usage(rg_ctx* c, uint64_t* reserved, uint64_t* used) {
+    CTX_GUARD(c);
+    if (!reserved || !used) return set_error(c, RG_ERR_ARG, "reserved and used must be non-null");
+    unsigned long long r = 0, u = 0;  // the attributes are 64-bit values
+    if (int rc = check_cuda(c, cudaMemPoolGetAttribute(c->pool, cudaMemPoolAttrReservedMemCurrent, &r),
+                            "cudaMemPoolGetAttribute"))
+        return rc;
+    if (int rc = check_cuda(c, cudaMemPoolGetAttribute(c->pool, cudaMemPoolAttrUsedMemCurrent, &u),
+                            "cudaMemPoolGetAttribute"))
+        return rc;
+    *reserved = r;
+    *used = u;
+    return RG_OK;
+}
+
 /* ---- device-resident tree ---------------------------------------------- */
 int rg_tree_attach(rg_ctx* c, const rg_grid_view* g, const rg_tree_arrays* t, int levelmin) {
     CTX_GUARD(c);

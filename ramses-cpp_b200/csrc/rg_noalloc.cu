@@ -20,6 +20,14 @@
 //     flux slot the fold kernel reads is written by the face kernel of the same
 //     call.  Calls whose kernels overlap on the GPU race on the array; the
 //     caller must order them (one stream, or events between streams).
+//
+// What the caller hands over: uold_dev and unew_dev are device memory of the
+// context's device, each at least nvar*ncell doubles from the pointer on
+// (checked with cudaPointerGetAttributes and the driver's address-range
+// query; neither allocates).  unew_dev must already hold the level's starting
+// unew -- normally a copy of uold_dev, as rg_set_unew makes it -- because the
+// fold adds the flux updates to it; only the level's update targets (its
+// cells and the coarser cells that take refluxes) are written.
 #include <mutex>
 #include <string>
 
@@ -53,6 +61,55 @@ int scratch_address(rg_ctx* c, double** out) {
     return RG_OK;
 }
 
+// cuMemGetAddressRange through the runtime's driver entry point (librgpu.so
+// links the runtime only): the base and size of the allocation holding a
+// device pointer.  Null when the driver does not offer it.
+using AddressRangeFn = int (*)(unsigned long long* base, size_t* size, unsigned long long ptr);
+
+AddressRangeFn address_range_fn() {
+    static AddressRangeFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuMemGetAddressRange", &f, 12000, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return static_cast<AddressRangeFn>(nullptr);
+        }
+        return reinterpret_cast<AddressRangeFn>(f);
+    }();
+    return fn;
+}
+
+// A caller's state buffer: device memory of this context's device with room
+// for nvar*ncell doubles from p on.
+int check_state_buffer(rg_ctx* c, const void* p, const char* name) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return rg::set_error(c, RG_ERR_ARG, std::string(name) + " is not a pointer the CUDA runtime knows");
+    }
+    if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged)
+        return rg::set_error(c, RG_ERR_ARG, std::string(name) + " is not device memory");
+    if (a.type == cudaMemoryTypeDevice && a.device != c->device)
+        return rg::set_error(c, RG_ERR_ARG, std::string(name) + " belongs to device " + std::to_string(a.device) +
+                                                ", the context runs on device " + std::to_string(c->device));
+    const size_t need = sizeof(double) * (size_t)c->nvar * (size_t)c->ncell;
+    if (AddressRangeFn range = address_range_fn()) {
+        unsigned long long base = 0;
+        size_t size = 0;
+        const unsigned long long addr = reinterpret_cast<unsigned long long>(p);
+        // memory the driver cannot size (an allocation of another allocator
+        // mapped by hand) passes unchecked; the pointer attributes above hold
+        if (range(&base, &size, addr) == 0 && addr + need > base + size)
+            return rg::set_error(c, RG_ERR_ARG,
+                                 std::string(name) + " holds " + std::to_string((base + size - addr) / sizeof(double)) +
+                                     " doubles from the pointer on; the grid needs nvar*ncell = " +
+                                     std::to_string(need / sizeof(double)));
+    }
+    return RG_OK;
+}
+
 }  // namespace
 
 extern "C" int rg_godunov_level_noalloc(rg_ctx* c, int ilevel, double dt, double dx, const double* uold_dev,
@@ -62,6 +119,18 @@ extern "C" int rg_godunov_level_noalloc(rg_ctx* c, int ilevel, double dt, double
     if (!uold_dev || !unew_dev) return rg::set_error(c, RG_ERR_ARG, "uold_dev and unew_dev must be device pointers");
     c->next_level = -1;  // this call uses the context's CFL word and primitive array
     if (int rc = rg::check_cuda(c, cudaSetDevice(c->device), "cudaSetDevice")) return rc;
+    if (!c->have_topology) return rg::set_error(c, RG_ERR_STATE, "rg_sync_topology has not been called");
+    // a resident tree whose links changed since the last plan build: the
+    // plans' oct lists and neighbour ids follow the old tree, and rebuilding
+    // them allocates
+    if (c->tree_dirty)
+        return rg::set_error(c, RG_ERR_STATE,
+                             "the resident tree changed since the level plans were built; make one allocating call "
+                             "for the level (rg_godunov_level or rg_set_unew) first");
+    if (c->params.riemann == RG_RIEMANN_EXACT && c->params.exact_guess == RG_GUESS_LEARNED && !c->mlp_valid)
+        return rg::set_error(c, RG_ERR_STATE, "exact_guess is RG_GUESS_LEARNED but no network was trained or set");
+    if (int rc = check_state_buffer(c, uold_dev, "uold_dev")) return rc;
+    if (int rc = check_state_buffer(c, unew_dev, "unew_dev")) return rc;
     rg::Plan* P = rg::existing_plan(c, ilevel);
     if (P && P->nbox > 0) return rg::set_error(c, RG_ERR_STATE, "ensemble level: every box has its own dt");
     if (!P)

@@ -139,6 +139,7 @@ def lib():
     L.rg_level_cell_updates.restype = C.c_int64
     L.rg_level_cell_updates.argtypes = [C.c_void_p, C.c_int]
     L.rg_last_kernel_ms.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_int]
+    L.rg_pool_usage.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.rg_set_stream.argtypes = [C.c_void_p, C.c_void_p]
     L.rg_set_timing.argtypes = [C.c_void_p, C.c_int]
     L.rg_exact_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_int]
@@ -471,6 +472,12 @@ class Context:
 
     def set_timing(self, on):
         self._chk(self.L.rg_set_timing(self.h, 1 if on else 0))
+
+    def pool_usage(self):
+        """(reserved, used) bytes of the context's device memory pool."""
+        r, u = C.c_uint64(0), C.c_uint64(0)
+        self._chk(self.L.rg_pool_usage(self.h, C.byref(r), C.byref(u)))
+        return r.value, u.value
 
     def kernel_ms(self):
         out = (C.c_float * 3)()
