@@ -296,6 +296,13 @@ int rg_pool_usage(rg_ctx* ctx, uint64_t* reserved, uint64_t* used);
  * (use_graph == 0) rg_level_substep calls (captured graphs carry no events).  The RG_TIMING=1 environment variable sets the
  * initial value. */
 int rg_set_timing(rg_ctx* ctx, int on);
+/* With rg_set_timing(ctx, 2) every level step (rg_godunov_level and the level
+ * steps inside rg_amr_coarse_step) records its own events: this returns the
+ * summed device milliseconds of its three phases (ms[0] primitives, ms[1]
+ * face kernel, ms[2] fold), the cells the face kernels processed and the
+ * number of level steps since the last reset (reset != 0 clears them).
+ * Synchronises the context stream.  No reference counterpart. */
+int rg_kernel_ms_totals(rg_ctx* ctx, double* ms, int64_t* cells, int64_t* steps, int reset);
 /* Exact-solver statistics accumulated by the face kernels: Newton updates
  * and Riemann solves since the last reset (reset != 0 clears them). */
 int rg_exact_stats(rg_ctx* ctx, int64_t* iters, int64_t* calls, int reset);

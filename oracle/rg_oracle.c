@@ -410,6 +410,15 @@ void orc_solve_exact(const double* ql, const double* qr, double* flux, double ga
     if (p0 > 0.0) pstar = p0;
     double pold = pstar;
     int it = 0;
+    /* Converged mode (tol below the reference's 1e-6), this library's own
+     * addition: g(p) = usl - usr is strictly decreasing and convex in p >= 0,
+     * so the signs of the evaluated g bracket the root; a Newton step that
+     * leaves the bracket is replaced by its midpoint (bracketed Newton-
+     * bisection, Numerical Recipes 3rd ed. sec. 9.4), and the loop also ends
+     * when the bracket has closed to tol relative.  Reference mode runs
+     * RiemannSolver.cpp:220-235 as written. */
+    const int safe = tol < 1e-6;
+    double lo = 0.0, hi = INFINITY;
     for (int iter = 0; iter < niter; ++iter) {
         double wwl_sq = cl_sq * (1.0 + gamma6 * (pold - pl) / (pl + 1e-20));
         double wwr_sq = cr_sq * (1.0 + gamma6 * (pold - pr) / (pr + 1e-20));
@@ -421,9 +430,39 @@ void orc_solve_exact(const double* ql, const double* qr, double* flux, double ga
         double usr = ur + (pold - pr) / (wwr + 1e-20);
         double delp = (qr_nr * ql_nr / (qr_nr + ql_nr + 1e-20)) * (usl - usr);
         delp = smax(delp, -pold);
-        pold = pold + delp;
         it++;
+        if (safe) {
+            double gv = usl - usr, pn;
+            if (gv > 0.0) lo = smax(lo, pold);
+            else if (gv < 0.0) hi = smin(hi, pold);
+            else break;
+            pn = pold + delp;
+            if (fabs(delp / (pn + 1e-10)) < tol) { pold = pn; break; }
+            if (!((pn > lo || pn == 0.0) && pn < hi)) pn = hi < INFINITY ? 0.5 * (lo + hi) : 2.0 * lo + 1e-300;
+            pold = pn;
+            if (hi - lo <= tol * (lo + 1e-10)) break;
+            continue;
+        }
+        pold = pold + delp;
         if (fabs(delp / (pold + 1e-10)) < tol) break;
+    }
+    if (safe) {
+        /* polish: the root truncated to 30 significant bits, then two plain
+         * Newton updates, so the result no longer depends on the start */
+        union { double d; unsigned long long u; } b;
+        b.d = pold;
+        b.u &= ~((1ULL << 22) - 1);
+        pold = b.d;
+        for (int k = 0; k < 2; ++k) {
+            double wwl = sqrt(smax(cl_sq * (1.0 + gamma6 * (pold - pl) / (pl + 1e-20)), 0.0));
+            double wwr = sqrt(smax(cr_sq * (1.0 + gamma6 * (pold - pr) / (pr + 1e-20)), 0.0));
+            double ql_nr = (2.0 * pow(wwl, 3)) / (wwl * wwl + cl_sq + 1e-20);
+            double qr_nr = (2.0 * pow(wwr, 3)) / (wwr * wwr + cr_sq + 1e-20);
+            double usl = ul - (pold - pl) / (wwl + 1e-20);
+            double usr = ur + (pold - pr) / (wwr + 1e-20);
+            double delp = (qr_nr * ql_nr / (qr_nr + ql_nr + 1e-20)) * (usl - usr);
+            pold = pold + smax(delp, -pold);
+        }
     }
     pstar = pold;
     if (iters) *iters = it;

@@ -289,6 +289,8 @@ void rg_destroy(rg_ctx* c) {
     invalidate_plans(c);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
+    for (auto& set : c->acc_ev)
+        for (auto& e : set) cudaEventDestroy(e);
     int* ip[] = {c->d_son, c->d_father, c->d_nbor, c->d_next, c->d_bound, c->d_jump, c->d_dist, c->d_jump2,
                  c->d_dist2, c->d_cell_level, c->d_cpos, c->d_tmap, c->d_pmark, c->d_scan};
     for (int* p : ip) dev_free(c, p);
@@ -1083,6 +1085,29 @@ int rg_mlp_grad(rg_ctx* c, int n, const float* x, const float* t, float* grad, f
 int rg_set_timing(rg_ctx* c, int on) {
     CTX_GUARD(c);
     c->timing = on != 0;
+    c->timing_acc = on == 2;
+    c->acc_n = 0;
+    return RG_OK;
+}
+
+int rg_kernel_ms_totals(rg_ctx* c, double* ms, int64_t* cells, int64_t* steps, int reset) {
+    CTX_GUARD(c);
+    if (!ms || !cells || !steps) return set_error(c, RG_ERR_ARG, "ms[3], cells and steps must be non-null");
+    if (!c->timing_acc) return set_error(c, RG_ERR_STATE, "accumulating timing is off (rg_set_timing(ctx, 2))");
+    if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "kernel timing")) return rc;
+    ms[0] = ms[1] = ms[2] = 0.0;
+    long long n = 0;
+    for (size_t i = 0; i < c->acc_n; ++i) {
+        for (int k = 0; k < 3; ++k) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, c->acc_ev[i][k], c->acc_ev[i][k + 1]) == cudaSuccess) ms[k] += t;
+        }
+        n += c->acc_cells[i];
+    }
+    cudaGetLastError();
+    *cells = n;
+    *steps = (int64_t)c->acc_n;
+    if (reset) c->acc_n = 0;
     return RG_OK;
 }
 

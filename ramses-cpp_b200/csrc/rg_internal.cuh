@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <array>
 #include <string>
 #include <utility>
 #include <vector>
@@ -208,6 +209,13 @@ struct rg_ctx {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     float last_ms[3] = {0, 0, 0};
     bool timing = false;
+    // rg_set_timing(ctx, 2): every level step (launch_godunov) records its
+    // own four events from this pool and its cell count, summed by
+    // rg_kernel_ms_totals, so a whole AMR coarse step can be timed per kernel
+    bool timing_acc = false;
+    std::vector<std::array<cudaEvent_t, 4>> acc_ev;
+    std::vector<long long> acc_cells;
+    size_t acc_n = 0;
     bool no_autotune = false;
     double* h_stage = nullptr;  // pinned staging of level-sparse host transfers
     size_t cap_hstage = 0;
@@ -291,6 +299,9 @@ int godunov_level_device_dt(rg_ctx* c, int ilevel, const double* dt_dev, double 
 int launch_set_dt_host(rg_ctx* c, double dt, double dx);
 int launch_finalize_dt(rg_ctx* c, double dx);
 int launch_godunov(rg_ctx* c, const Plan& p);
+// the four events a level step records its kernel boundaries into: the
+// context's last-call set, or in accumulating mode the next set of the pool
+cudaEvent_t* step_events(rg_ctx* c, long long ncells);
 int launch_leaf_prefix(rg_ctx* c, const Plan& p, double dx, int pressure_cap, double courant_factor);
 int launch_leaf_core(rg_ctx* c, const Plan& p, double dx, int pressure_cap, double courant_factor);
 // a leaf level whose stencils and updates stay inside it: its fold can prepare

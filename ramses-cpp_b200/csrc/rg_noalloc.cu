@@ -136,7 +136,8 @@ extern "C" int rg_godunov_level_noalloc(rg_ctx* c, int ilevel, double dt, double
     if (!P)
         return rg::set_error(c, RG_ERR_STATE,
                              "no level plan: building one allocates, so call rg_godunov_level (or rg_set_unew) "
-                             "for this level once after rg_sync_topology, before the allocation-free calls");
+                             "for this level once after rg_sync_topology or a change of the resident tree, "
+                             "before the allocation-free calls");
     const size_t need = (size_t)(2 * c->params.ndim) * (c->params.ndim + 2) * (size_t)P->ncells;
     if (need > RG_NOALLOC_SCRATCH_DOUBLES)
         return rg::set_error(c, RG_ERR_ARG,

@@ -16,6 +16,8 @@
 // (exact solver) differs by at most a few ulp between libm and CUDA.
 #pragma once
 
+#include <math_constants.h>
+
 #include <cuda_runtime.h>
 
 namespace rg {
@@ -350,6 +352,23 @@ __device__ __forceinline__ void solve_acoustic(const double* ql, const double* q
 // Exact solver (two-shock Newton iteration, RiemannSolver.cpp:194-307).
 // niter/tol default to the reference's 10 and 1e-6; p_guess > 0 replaces the
 // initial guess of :215 (learned mode).  Returns the Newton update count.
+//
+// Converged mode (tol below the reference's 1e-6) safeguards the iteration:
+// the function the update zeroes, g(p) = u_L*(p) - u_R*(p) with the
+// two-shock mass fluxes W_k(p) = sqrt(gamma p_k rho_k (1 + (gamma+1)/(2 gamma)
+// (p - p_k)/p_k)), is continuous, strictly decreasing and convex on p >= 0,
+// so every evaluated p tells on which side of the root it lies.  The solver
+// keeps that bracket [lo, hi] and replaces a Newton step that leaves it by
+// its midpoint (a bracketed Newton-bisection hybrid, the safeguarded Newton
+// method of Numerical Recipes, 3rd ed., sec. 9.4 "rtsafe"); it stops as soon
+// as a Newton update is below tol relative (the reference's test, taken
+// before the bracket so that an update below one ulp still ends the loop) or
+// the bracket has closed to tol relative.  Newton is monotone from the left of
+// the root, so the bracket only acts after an overshoot from the right and
+// where rounding noise in g near an ill-conditioned (near-vacuum) root makes
+// the steps wander; then the bracket halves each step and the iteration ends
+// well inside the cap.  Reference mode (tol >= 1e-6) runs the reference's
+// loop unchanged.
 template <int NDIM>
 __device__ __forceinline__ int solve_exact_p(const double* ql, const double* qr, double* flux, double gamma,
                                              double smallp, int niter, double tol, double p_guess,
@@ -367,6 +386,8 @@ __device__ __forceinline__ int solve_exact_p(const double* ql, const double* qr,
     if (p_guess > 0.0) pstar = p_guess;
     double pold = pstar;
     int it = 0;
+    const bool safe = tol < 1e-6;
+    double lo = 0.0, hi = CUDART_INF;  // converged mode: g(lo) > 0 > g(hi)
     for (int iter = 0; iter < niter; ++iter) {
         double wwl_sq = cl_sq * (1.0 + gamma6 * (pold - pl) / (pl + 1e-20));
         double wwr_sq = cr_sq * (1.0 + gamma6 * (pold - pr) / (pr + 1e-20));
@@ -381,9 +402,49 @@ __device__ __forceinline__ int solve_exact_p(const double* ql, const double* qr,
         double usr = ur + (pold - pr) / (wwr + 1e-20);
         double delp = (qr_nr * ql_nr / (qr_nr + ql_nr + 1e-20)) * (usl - usr);
         delp = smax(delp, -pold);
-        pold = pold + delp;
         ++it;
+        if (safe) {
+            const double gv = usl - usr;
+            if (gv > 0.0) lo = smax(lo, pold);
+            else if (gv < 0.0) hi = smin(hi, pold);
+            else break;  // g(pold) == 0: the root itself
+            // the next point: Newton's (clamped at 0 like the reference's
+            // update, which is how a vacuum root p* = 0 is reached) while it
+            // stays inside the bracket, else the bracket's midpoint
+            double pn = pold + delp;
+            if (fabs(delp / (pn + 1e-10)) < tol) {  // the reference's test, on the Newton update
+                pold = pn;
+                break;
+            }
+            if (!((pn > lo || pn == 0.0) && pn < hi))
+                pn = hi < CUDART_INF ? 0.5 * (lo + hi) : 2.0 * lo + 1e-300;
+            pold = pn;
+            if (hi - lo <= tol * (lo + 1e-10)) break;
+            continue;
+        }
+        pold = pold + delp;
         if (fabs(delp / (pold + 1e-10)) < tol) break;
+    }
+    if (safe) {
+        // Polish: the converged root truncated to its 30 leading significant
+        // bits, then two plain Newton updates from there.  Where the root is
+        // ill-conditioned, where it ends inside the search depends on the start
+        // by a few ulp, and a flux sampled through a nearly stationary contact
+        // magnifies that; from the truncated value the arithmetic no longer
+        // depends on the start, so any two starts that converged to within
+        // 2^-30 of each other give the same bits.  From 2^-30 the two updates
+        // are back at the root's own rounding level.
+        pold = __longlong_as_double(__double_as_longlong(pold) & ~((1LL << 22) - 1));
+        for (int k = 0; k < 2; ++k) {
+            double wwl = sqrt(smax(cl_sq * (1.0 + gamma6 * (pold - pl) / (pl + 1e-20)), 0.0));
+            double wwr = sqrt(smax(cr_sq * (1.0 + gamma6 * (pold - pr) / (pr + 1e-20)), 0.0));
+            double ql_nr = (2.0 * (wwl * wwl * wwl)) / (wwl * wwl + cl_sq + 1e-20);
+            double qr_nr = (2.0 * (wwr * wwr * wwr)) / (wwr * wwr + cr_sq + 1e-20);
+            double usl = ul - (pold - pl) / (wwl + 1e-20);
+            double usr = ur + (pold - pr) / (wwr + 1e-20);
+            double delp = (qr_nr * ql_nr / (qr_nr + ql_nr + 1e-20)) * (usl - usr);
+            pold = pold + smax(delp, -pold);
+        }
     }
     pstar = pold;
     if (pstar_out) *pstar_out = pstar;

@@ -567,16 +567,17 @@ int launch_godunov_t(rg_ctx* c, const Plan& P) {
     TreeView T = tree_view(c);
     PlanView V = P.view();
     double* fsum = c->d_flux + (size_t)NS * NV * P.ncells;
-    if (c->timing) cudaEventRecord(c->ev[0], c->stream);
+    cudaEvent_t* E = c->timing ? step_events(c, P.ncells) : nullptr;
+    if (E) cudaEventRecord(E[0], c->stream);
     int nprim = P.ncells + P.nextra_prim;
     k_prim<NDIM><<<grid_for(c, nprim, 256), 256, 0, c->stream>>>(T, V, c->d_uold, c->d_prim, K.gamma, K.smalle);
-    if (c->timing) cudaEventRecord(c->ev[1], c->stream);
+    if (E) cudaEventRecord(E[1], c->stream);
     if (int rc = launch_face_tiles(c, P, K, c->d_uold, c->d_prim, c->d_flux, fsum)) return rc;
-    if (c->timing) cudaEventRecord(c->ev[2], c->stream);
+    if (E) cudaEventRecord(E[2], c->stream);
     k_fold<NDIM, false, true><<<grid_for(c, P.ntarg, 256), 256, 0, c->stream>>>(T, V, c->d_flux, c->d_unew,
                                                                                c->d_status, K.gamma, nullptr, fsum);
     launch_fold_long<NDIM, false, true>(c, P, T, V, c->d_flux, c->d_unew, K.gamma, nullptr, fsum);
-    if (c->timing) cudaEventRecord(c->ev[3], c->stream);
+    if (E) cudaEventRecord(E[3], c->stream);
     return check_cuda(c, cudaGetLastError(), "godunov kernels");
 }
 
@@ -611,6 +612,18 @@ int launch_godunov_ext_t(rg_ctx* c, const Plan& P, const double* uold, double* u
 }
 
 }  // namespace
+
+cudaEvent_t* step_events(rg_ctx* c, long long ncells) {
+    if (!c->timing_acc) return c->ev;
+    if (c->acc_n == c->acc_ev.size()) {
+        std::array<cudaEvent_t, 4> e{};
+        for (auto& x : e) cudaEventCreate(&x);
+        c->acc_ev.push_back(e);
+        c->acc_cells.push_back(0);
+    }
+    c->acc_cells[c->acc_n] = ncells;
+    return c->acc_ev[c->acc_n++].data();
+}
 
 int launch_godunov(rg_ctx* c, const Plan& P) {
     if (c->params.ndim == 1) return launch_godunov_t<1>(c, P);

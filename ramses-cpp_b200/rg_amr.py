@@ -23,7 +23,103 @@ makes the blast unstable at these resolutions.
 """
 
 
+import numpy as np
+
+import rg_tree
 import rgpu
+
+
+def sedov_primitives(ndim, base_level, gamma=1.4, rho0=1.0, p0=1e-5, e_blast=1.0, nx=1):
+    """The Sedov blast initial condition as a function of cell centres: density
+    rho0 and pressure p0 everywhere at rest, except the central 2^ndim cells of
+    ``base_level`` (|x - 0.5| < dx_base on every axis), which share the energy
+    e_blast as pressure (gamma-1) e_blast / (2 dx_base)^ndim."""
+    dxb = 1.0 / (nx * 2 ** (base_level - 1))
+    p_blast = (gamma - 1.0) * e_blast / (2 * dxb) ** ndim
+
+    def fn(xc):
+        inside = np.all(np.abs(xc[:, :ndim] - 0.5) < dxb, axis=1)
+        n = len(xc)
+        return np.full(n, rho0), [np.zeros(n)] * ndim, np.where(inside, p_blast, p0)
+    return fn
+
+
+def _cell_centres(a, ncoarse, ngridmax, nx, ndim, level, octs):
+    """AmrGrid::get_cell_center (AmrGrid.cpp:331-365) of the cells of level
+    list ``level`` (oct ids ``octs``), or of the coarse cells for level 0;
+    boxlen 1."""
+    if level == 0:
+        idx = np.arange(ncoarse)
+        out = np.full((ncoarse, 3), 0.5)
+        dxc = 1.0 / nx
+        xyz = [idx % nx, (idx % (nx * nx)) // nx, idx // (nx * nx)]
+        for d in range(ndim):
+            out[:, d] = (xyz[d] + 0.5) * dxc
+        return out
+    ttd = 1 << ndim
+    dx = 1.0 / (nx * (2.0 ** (level - 1)))
+    scale = 1.0 / nx
+    out = np.full((len(octs), ttd, 3), 0.5)
+    for ic in range(ttd):
+        for d in range(ndim):
+            bit = (ic >> d) & 1
+            out[:, ic, d] = a["xg"][d * ngridmax + octs - 1] * scale + (bit - 0.5) * dx
+    return out.reshape(-1, 3)
+
+
+def init_flow(ctx, like, ndim, nx, nlevelmax, ic_fn, gamma):
+    """Simulation::init_flow on the resident tree: the primitive initial
+    condition ic_fn(centres) -> (rho, [v], p) written as conservative
+    variables into uold of the coarse cells and of every level's cells, unew
+    made a copy of uold, then restrict_fine from nlevelmax-1 down to 0."""
+    a = ctx.tree_fetch(like)
+    ngm, ncell = ctx.tree_sizes()
+    ncoarse = nx ** ndim if ndim == 3 else nx
+    nvar = ndim + 2
+    u = a["uold"].reshape(nvar, ncell)
+    ttd = 1 << ndim
+    for L in range(0, nlevelmax + 1):
+        if L == 0:
+            ids = np.arange(1, ncoarse + 1)
+            octs = None
+        else:
+            octs = ctx.level_octs(L).astype(np.int64) if ctx.count_grids(L) > 0 else np.zeros(0, np.int64)
+            if len(octs) == 0:
+                continue
+            ic = np.arange(1, ttd + 1)
+            ids = (ncoarse + (ic[None, :] - 1) * ngm + octs[:, None]).reshape(-1)
+        xc = _cell_centres(a, ncoarse, ngm, nx, ndim, L, octs)
+        rho, vel, p = ic_fn(xc)
+        u[0, ids - 1] = rho
+        for d in range(ndim):
+            u[1 + d, ids - 1] = rho * vel[d]
+        u[ndim + 1, ids - 1] = p / (gamma - 1.0) + 0.5 * rho * sum(vel[d] ** 2 for d in range(ndim))
+    uold = np.ascontiguousarray(u.reshape(-1))
+    ctx.upload_state(uold, uold.copy())
+    for il in range(nlevelmax - 1, -1, -1):
+        ctx.restrict_fine(il)
+
+
+def initialize(ctx, ndim, levelmin, nlevelmax, ngridmax, ic_fn, gamma, ed=-1.0, ep=-1.0, ev=-1.0, nexpand=1):
+    """Simulation::initialize (src/core/Simulation.cpp:226-296) with the tree
+    on the device: the uniform grid to ``levelmin`` built on the host
+    (rg_tree.build_uniform, the arrays the reference's uniform refinement
+    leaves), attached to the context, then for each finer level the
+    reference's rounds -- initial condition, flag_fine and make_grid_fine of
+    every level -- until a level stays empty, and the initial condition once
+    more; all tree work by the device kernels.  nx = 1."""
+    g = rg_tree.build_uniform(ndim, levelmin, ngridmax=ngridmax, nlevelmax=nlevelmax)
+    arrays = rg_tree.tree_arrays(g)
+    ctx.tree_attach(g, arrays, levelmin)
+    like = {"headl": arrays["headl"], "taill": arrays["taill"], "numbl": arrays["numbl"]}
+    for il_ref in range(levelmin + 1, nlevelmax + 1):
+        init_flow(ctx, like, ndim, 1, nlevelmax, ic_fn, gamma)
+        for il in range(1, nlevelmax + 1):
+            ctx.flag_fine(il, ed, ep, ev, -1.0, nexpand, 1)
+            ctx.make_grid_fine(il)
+        if ctx.count_grids(il_ref) == 0:
+            break
+    init_flow(ctx, like, ndim, 1, nlevelmax, ic_fn, gamma)
 
 
 class DeviceAmrRun:

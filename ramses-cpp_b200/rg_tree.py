@@ -156,6 +156,43 @@ def build_uniform(ndim, levelmin, nx=1, ny=1, nz=1, ngridmax=None, nlevelmax=Non
     return g
 
 
+def tree_arrays(g):
+    """Every array and scalar of the AmrGrid tree (AmrGrid.hpp:26-31) as the
+    reference's uniform refinement leaves it, for ``rg_tree_attach``: the
+    arrays of ``build_uniform`` plus
+    - flag1 = 1 on the refined cells (the ones flag_fine marked before
+      make_grid_fine split them), 0 elsewhere;
+    - flag2 = cpu_map = 1 on every cell (one process owns the whole domain);
+    - prev = each oct's predecessor in its level list, and in the free list
+      (AmrGrid.cpp:259-302 keep both lists doubly linked);
+    - the level lists' tails and counts, and the free list: the octs after the
+      last used one, in id order (headf, tailf, numbf);
+    - uold = unew = 0 (the initial conditions come after).
+    The level-list arrays are indexed like headl: ilevel * (ncpu + nboundary)."""
+    ngm, ncell = g.ngridmax, g.ncell
+    nh = len(g.headl)
+    prev = np.zeros(ngm, np.int32)
+    taill = np.zeros(nh, np.int32)
+    numbl = np.zeros(nh, np.int32)
+    used = 0
+    for L, ids in g.level_octs.items():
+        if len(ids) == 0:
+            continue
+        prev[ids[1:] - 1] = ids[:-1]
+        taill[L] = ids[-1]
+        numbl[L] = len(ids)
+        used = max(used, int(ids[-1]))
+    free = np.arange(used + 1, ngm + 1)
+    if len(free):
+        prev[free[1:] - 1] = free[:-1]
+    return {"son": g.son, "father": g.father, "nbor": g.nbor, "next": g.next, "prev": prev, "headl": g.headl,
+            "taill": taill, "numbl": numbl, "flag1": (g.son > 0).astype(np.int32),
+            "flag2": np.ones(ncell, np.int32), "cpu_map": np.ones(ncell, np.int32), "xg": g.xg,
+            "uold": np.zeros(g.nvar * ncell), "unew": np.zeros(g.nvar * ncell),
+            "headf": int(free[0]) if len(free) else 0, "tailf": int(free[-1]) if len(free) else 0,
+            "numbf": int(len(free))}
+
+
 # ------------------------------------------------------------------ workloads
 
 def sedov_state(g, level, gamma=1.4, rho0=1.0, p0=1e-5, e_blast=1.0, base_level=None):

@@ -140,6 +140,8 @@ def lib():
     L.rg_level_cell_updates.argtypes = [C.c_void_p, C.c_int]
     L.rg_last_kernel_ms.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_int]
     L.rg_pool_usage.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    L.rg_kernel_ms_totals.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64),
+                                      C.POINTER(C.c_int64), C.c_int]
     L.rg_set_stream.argtypes = [C.c_void_p, C.c_void_p]
     L.rg_set_timing.argtypes = [C.c_void_p, C.c_int]
     L.rg_exact_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_int]
@@ -255,7 +257,7 @@ class Context:
         nv = self.nvar
         per = {"son": ncell, "father": ngm, "nbor": 6 * ngm, "next": ngm, "prev": ngm, "flag1": ncell,
                "flag2": ncell, "cpu_map": ncell, "xg": 3 * ngm, "uold": nv * ncell, "unew": nv * ncell}
-        d = {k: np.zeros(per.get(k, len(like[k])), dtype=np.int32) for k in TREE_INT_ARRAYS}
+        d = {k: np.zeros(per[k] if k in per else len(like[k]), dtype=np.int32) for k in TREE_INT_ARRAYS}
         d.update({k: np.zeros(per[k], dtype=np.float64) for k in TREE_F64_ARRAYS})
         d.update(headf=0, tailf=0, numbf=0)
         t = tree_arrays(d)
@@ -471,7 +473,15 @@ class Context:
         return g, loss.value
 
     def set_timing(self, on):
-        self._chk(self.L.rg_set_timing(self.h, 1 if on else 0))
+        """True/False: events of the last level step; "accumulate": every level step's events."""
+        self._chk(self.L.rg_set_timing(self.h, 2 if on == "accumulate" else (1 if on else 0)))
+
+    def kernel_ms_totals(self, reset=True):
+        """Accumulated (prim, face, fold) device ms, face-kernel cells and level steps."""
+        ms = (C.c_double * 3)()
+        cells, steps = C.c_int64(0), C.c_int64(0)
+        self._chk(self.L.rg_kernel_ms_totals(self.h, ms, C.byref(cells), C.byref(steps), 1 if reset else 0))
+        return list(ms), cells.value, steps.value
 
     def pool_usage(self):
         """(reserved, used) bytes of the context's device memory pool."""

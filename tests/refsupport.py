@@ -312,6 +312,16 @@ class Oracle:
     def slope(self, ql, qc, qr, t, theta=1.5, nu=0.0):
         return self.lib.orc_compute_slope(ql, qc, qr, t, theta, nu)
 
+    def exact_pstar(self, ql, qr, gamma, ndim, niter, tol, p0=-1.0):
+        """The exact solver's flux (nvar entries) and converged p*."""
+        ql = np.ascontiguousarray(ql, dtype=np.float64)
+        qr = np.ascontiguousarray(qr, dtype=np.float64)
+        f = np.zeros(20)
+        it, ps = C.c_int(0), C.c_double(0)
+        self.lib.orc_solve_exact(_ptr(ql, F64P), _ptr(qr, F64P), _ptr(f, F64P), gamma, ndim, niter, tol, p0,
+                                 C.byref(it), C.byref(ps))
+        return f[:ndim + 2].copy(), ps.value
+
 
 # ------------------------------------------------------------------ AMR replay
 

@@ -138,18 +138,44 @@ def test_training_is_reproducible(ctx):
     assert np.array_equal(ws[0].view(np.int32), ws[1].view(np.int32))
 
 
+def test_converged_mode_matches_oracle(ctx, oracle):
+    """Converged mode (100 updates, 1e-14) against the C oracle's same
+    bracketed iteration and polish: same root to 1e-13 on every pair, no pair
+    at the cap; fluxes within 3e-12 (the cube and pow() differ by ulps
+    between libm and CUDA)."""
+    n = 4096
+    ql, qr, g = stress(ctx, n, 77)
+    f, ps, it = solve(ctx, n, ql, qr, g, False, 100, 1e-14)
+    a, b, gam = ql.cpu().numpy().reshape(5, n), qr.cpu().numpy().reshape(5, n), g.cpu().numpy()
+    want_p = np.empty(n)
+    want_f = np.empty((5, n))
+    for i in range(n):
+        want_f[:, i], want_p[i] = oracle.exact_pstar(a[:, i], b[:, i], gam[i], 3, 100, 1e-14)
+    assert it.max() < 100, "a pair reached the iteration cap"
+    rel = np.abs(ps - want_p) / np.maximum(np.abs(want_p), 1e-300)
+    assert rel.max() <= 1e-13, rel.max()
+    scale = np.maximum(np.abs(want_f), 1e-300)
+    frel = np.abs(f - want_f) / scale
+    assert np.mean(frel <= 3e-12) > 0.9999, np.count_nonzero(frel > 3e-12)
+
+
 def test_learned_start_same_root_fewer_iterations(ctx):
+    """Converged mode: from the plain and from the learned start every pair
+    converges inside the cap, to the same p* bits and the same flux bits (the
+    polish from the root's 30 leading bits takes the start out of the
+    result), with fewer Newton updates from the learned start."""
     loss = ctx.mlp_train(seed=3)
     assert np.isfinite(loss) and loss < 0.02
     n = 1 << 20
     ql, qr, g = stress(ctx, n, 2026)  # held out: another seed than training
     f0, p0, i0 = solve(ctx, n, ql, qr, g, False, 100, 1e-14)
     f1, p1, i1 = solve(ctx, n, ql, qr, g, True, 100, 1e-14)
-    assert i1.mean() < 0.85 * i0.mean(), (i0.mean(), i1.mean())
+    assert i0.max() < 100 and i1.max() < 100, "a pair reached the iteration cap"
+    assert i1.mean() < 0.8 * i0.mean(), (i0.mean(), i1.mean())
     rel = np.abs(p1 - p0) / np.maximum(np.abs(p0), 1e-300)
-    assert np.mean(rel > 1e-13) < 1e-3 and rel.max() < 1e-9
+    assert np.count_nonzero(rel > 1e-13) == 0, rel.max()
     frel = np.abs(f1 - f0) / np.maximum(np.abs(f0), 1e-300)
-    assert np.mean(frel > 1e-12) < 1e-3
+    assert np.count_nonzero(frel > 1e-12) == 0, frel.max()
 
 
 def test_level_step_with_learned_start(ctx):

@@ -177,3 +177,32 @@ def test_free_list_growth_matches_reference(rgpu_lib):
     finally:
         ctx.close()
         h.close()
+
+
+@pytest.mark.parametrize("lmin,lmax,ngm", [(LMIN, LMAX, 30000), (5, 8, 60000)])
+def test_device_initialisation_matches_reference(rgpu_lib, lmin, lmax, ngm):
+    """rg_amr.initialize: the uniform grid built on the host (rg_tree), then
+    Simulation::initialize's rounds (initial condition, flag_fine and
+    make_grid_fine of every level, until a level stays empty) by the device
+    kernels, against the reference's own initialisation of the same Sedov run:
+    every tree array, the free list and the state equal; then two coarse steps
+    from each stay equal, time and cell-update counts included."""
+    import rg_amr
+    nml = namelist(slope_type=2, riemann="hllc", levelmin=lmin, levelmax=lmax, err_grad_d=ED, err_grad_p=EP)
+    h = RefHarness(3).create(nml, ngridmax=ngm, levelmin=lmin, nlevelmax=lmax, gamma=GAMMA)
+    r = AmrRun(h, lmin, lmax, GAMMA, ed=ED, ep=EP)
+    r.initialize(sedov_ic(3, lmin))
+    ctx = rgpu.Context(rgpu.make_params(3, slope_type=2, riemann="hllc", interpol_type=1, gamma=GAMMA), 0)
+    try:
+        rg_amr.initialize(ctx, 3, lmin, lmax, ngm, rg_amr.sedov_primitives(3, lmin, GAMMA), GAMMA, ed=ED, ep=EP)
+        assert ctx.tree_sizes() == (h.get("ngridmax"), h.get("ncell"))
+        assert_same_tree(h, ctx, "after initialisation")
+        d = DeviceAmrRun(ctx, nx=1, levelmin=lmin, nlevelmax=lmax, ed=ED, ep=EP)
+        for step in range(2):
+            r.coarse_step()
+            d.coarse_step()
+            assert_same_tree(h, ctx, f"coarse step {step}")
+            assert d.t == r.t and d.cell_updates == r.cell_updates
+    finally:
+        ctx.close()
+        h.close()

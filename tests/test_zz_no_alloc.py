@@ -217,7 +217,10 @@ def test_noalloc_rejects_a_plan_made_stale_by_a_tree_change():
                 buf = torch.zeros(5 * ncell, dtype=torch.float64, device="cuda:0")
                 with pytest.raises(rgpu.RGError) as e:
                     ctx.godunov_level_noalloc(4, 1e-6, 1.0 / 16, buf.data_ptr(), buf.clone().data_ptr())
-                assert e.value.code == rgpu.RG_ERR_STATE and "tree changed" in str(e.value)
+                # the tree operations either left the plans marked stale or
+                # already dropped them: refused either way, nothing launched
+                assert e.value.code == rgpu.RG_ERR_STATE
+                assert "tree changed" in str(e.value) or "no level plan" in str(e.value)
                 ctx.set_unew(4)  # an allocating call rebuilds the plans; the call is accepted again
                 uold_dev, unew_dev = ctx.device_state()
                 ctx.godunov_level_noalloc(4, 1e-6, 1.0 / 16, uold_dev, unew_dev)
