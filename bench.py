@@ -1,44 +1,53 @@
 #!/usr/bin/env python
-"""Throughput of the B200 Godunov level step (RAMSES-CPP HydroSolver::godunov_fine).
+"""Throughput of the B200 Godunov level step (RAMSES-CPP HydroSolver::godunov_fine)
+on the metric's own configuration: the 3D Sedov blast with octree AMR.
 
-Workload: 3D Sedov blast on a uniform 128^3 grid (the reference's
-levelmin=levelmax=8), MonCen slopes, HLLC, gamma 1.4, FP64, periodic.  One
-step = one level substep through the C ABI: on-device CFL (the reference
-formula without its p <= 100 rho cap), set_unew, godunov_fine, set_uold.
-Steps past the configured 200 continue the same run.
+Workload (the headline `value`): reference levelmin 7, levelmax 10 (a 64^3
+base grid refined to 512^3 effective; the Fortran numbering's levelmin 6 /
+levelmax 9), refinement on relative density and pressure gradients > 0.1,
+nexpand 1, sub-cycling 2, MonCen slopes, HLLC, gamma 1.4, Courant factor
+0.25, FP64, periodic.  The tree and the state are resident on the GPU: the
+run is initialised on the device (rg_amr.initialize: the reference's
+Simulation::initialize rounds with the device tree kernels) and every coarse
+step is one rg_amr_coarse_step call (Simulation::amr_step with flag_fine,
+make_grid_fine, remove_grid_fine, restrict_fine, the CFL step, set_unew,
+godunov_fine and set_uold all on the device).  One bench step = one coarse
+step; W warm-up coarse steps, then K timed ones (the window is coarse steps
+W+1..W+K of the run).  Cell updates = son == 0 cells processed by every
+godunov_fine call of the window, sub-cycled ones included.
+
+The reference's own scheme collapses on this run after about 40 coarse steps
+at Courant 0.25 (6 at the 0.8 of the other configs): refluxes that reach a
+cell after its own clamp drive coarse cells next to the refined region to
+negative density, the density floor then gives sound speeds of 1e4 and dt
+falls to 1e-13.  The default window (W=5, K=20) lies before that; the line
+reports the window's time span and its last finest-level dt.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Prints one JSON line (rank 0).  N > 1 runs one independent replica per GPU
-(weak scaling): the single-grid step of this workload is not partitioned, so
-the ranks exchange nothing but the final timing maximum.
+Prints one JSON line (rank 0).  N > 1 runs one independent replica of the
+AMR run per GPU (replicas only: the single grid is not partitioned), so the
+ranks exchange nothing but the final timing maximum.
 
-`e2e.bound` puts the end-to-end step against this box's own link: the level's
-cells up and down at the pinned copy bandwidth measured in the same run, plus
-the device step (the two cannot overlap: a step's input is the previous
-step's output).
-
-Besides the HBM `roofline` of the face kernel (the contract's), the line
-carries `roofline_fp64`: the same kernel against the FP64 pipe, its actual
-bound (executed FP64 FLOPs per cell update from the committed ncu summary,
-over its CUDA-event time, against the FP64 throughput measured on this GPU
-by rg_measure_fp64_peak).
-
-The line also carries the other workloads of the path, each measured on the
-same box:
-- "newton": the exact Riemann solver on the stress workload (256^3
-  independent interface pairs), plain two-shock Newton start against the
-  learned start (network trained on the GPU first), the Sedov step run with
-  the exact solver under both starts, and (N = 1) the sub-cycled Sedov AMR
-  run with the exact solver under both starts;
-- "ensemble": 512 independent uneven boxes stepped together (sharded over
-  the ranks when N > 1);
-- "amr": the sub-cycled Sedov AMR run through the reference's own
-  AmrGrid/TreeUpdater step, CPU reference against the GPU drop-in, and the
-  same run with the tree resident on the GPU (N = 1);
-- "sod1d": the 1D Sod run to t = 0.245, CPU reference against the GPU (N = 1).
+Keys besides the contract's:
+- `roofline`: the dominant kernel of the AMR step (the face kernel, summed
+  over every level step of two coarse steps with CUDA events) against the
+  measured HBM copy bandwidth; `traffic` and the FP64 counts come from the
+  machine-readable ncu record profiles/roofline_inputs.json, checked against
+  the hash of the kernel sources it was captured at (`stale` if they moved);
+- `e2e`: the same coarse steps with the state in page-locked host memory,
+  uploaded before and downloaded after every coarse step;
+- `cpu_baseline`: the reference compiled here, one core, on coarse steps of
+  the same window;
+- `parity`: the GPU run's uold and son after W+2 coarse steps against the
+  reference's (SHA-1 digest, computed in the CPU baseline's process);
+- `sedov128` (config 2: the uniform 128^3 level, brick face kernel, its own
+  rooflines), `newton` (config 5), `ensemble` (config 4), `amr_dropin`
+  (the reference's own AmrGrid/TreeUpdater step with the GPU hydro drop-in),
+  `sod1d` (config 1).
 """
 import argparse
+import hashlib
 import json
 import os
 import statistics
@@ -53,13 +62,13 @@ sys.path.insert(0, str(ROOT / "ramses-cpp_b200"))
 
 METRIC = "cell-updates/s 3D Sedov AMR FP64, %HBM roofline; Newton iters learned vs plain"
 UNIT = "cell-updates/s"
-WORKLOAD = "3D Sedov blast, uniform 128^3 (reference levelmin=levelmax=8), MonCen + HLLC, gamma 1.4, FP64"
-LEVEL = 8
+AMR = dict(lmin=7, lmax=10, ngridmax=400000, cfl=0.25, ed=0.1, ep=0.1, gamma=1.4)
+WORKLOAD = ("3D Sedov blast with octree AMR, reference levelmin 7 / levelmax 10 (64^3 base, 512^3 effective), "
+            "err_grad_d = err_grad_p = 0.1, nexpand 1, sub-cycled, MonCen + HLLC, gamma 1.4, courant 0.25, FP64, "
+            "tree and state resident on the GPU")
 BYTES_PER_CELL_UPDATE = 80  # uold read once + unew written once, 5 FP64 variables each
-# kernels per substep of the timed loop (a uniform level after its first
-# substep): dt finalize, face, fold (set_unew/set_uold and the next substep's
-# CFL candidates and primitives fused into the fold)
-GPU_KERNELS_PER_STEP = 3
+FACE_SOURCES = ("rg_face.cuh", "rg_face_brick.cuh", "rg_face_pipe.cuh", "rg_physics.cuh", "rg_face.cu",
+                "rg_face_1d.cu", "rg_face_3d.cu", "rg_internal.cuh", "rg_nav.cuh")
 
 
 def peaks():
@@ -70,23 +79,29 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def profile_value(kernel, key):
-    """A `key: value` figure of the face kernel's committed ncu summary."""
-    f = ROOT / "profiles" / f"{kernel}_sedov128.md"
+def face_source_sha():
+    """SHA-256 (16 hex digits) of the face kernels' sources, the key of the
+    ncu record in profiles/roofline_inputs.json."""
+    h = hashlib.sha256()
+    for name in FACE_SOURCES:
+        h.update((ROOT / "ramses-cpp_b200" / "csrc" / name).read_bytes())
+    return h.hexdigest()[:16]
+
+
+def roofline_inputs(key):
+    """The ncu record of a face kernel (profiles/roofline_inputs.json): DRAM
+    bytes, FP64 FLOPs and FP64 instructions per cell update, and whether the
+    sources have changed since the capture."""
+    f = ROOT / "profiles" / "roofline_inputs.json"
     if not f.exists():
         return None
-    for line in f.read_text().splitlines():
-        if line.startswith(key + ":"):
-            try:
-                return int(float(line.split(":", 1)[1].strip()))
-            except ValueError:
-                return None
-    return None
-
-
-def profile_traffic(kernel):
-    """dram bytes per launch of the face kernel from the committed ncu summary."""
-    return profile_value(kernel, "traffic_bytes_per_launch")
+    d = json.loads(f.read_text()).get(key)
+    if not d:
+        return None
+    d = dict(d)
+    d["current_source_sha"] = face_source_sha()
+    d["stale"] = d.get("source_sha") != d["current_source_sha"]
+    return d
 
 
 # ---------------------------------------------------------------- clocks
@@ -143,161 +158,332 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- CPU side
-def cpu_sample(level, steps, kind_pref="reference"):
-    """Time the reference CPU path (or the oracle port) on ``steps`` substeps of
-    the Sedov workload at ``level``; runs in its own process (no CUDA)."""
+def amr_cpu_window(warmup, steps, parity_after=None):
+    """The reference on the headline's AMR window, single-threaded: its own
+    initialisation and coarse steps (AmrGrid / TreeUpdater / HydroSolver
+    compiled here from its sources, driven through refsupport.AmrRun, which
+    replays Simulation::initialize and Simulation::amr_step with the CFL step
+    of the reference formula), `warmup` untimed coarse steps, then `steps`
+    timed ones.  Runs in its own process (the reference prints a line per
+    flagged cell).  parity_after = k: also the SHA-1 of uold and son after
+    coarse step k (1-based)."""
     sys.path.insert(0, str(ROOT / "tests"))
-    import numpy as np
-    import rg_tree
-    import refsupport as rs
-    gamma, cfl = 1.4, 0.8
-    g = rg_tree.build_uniform(3, level)
-    dx = 1.0 / 2 ** level
-    orc = rs.Oracle()
-    ga = rs.GridArrays(ncoarse=g.ncoarse, ngridmax=g.ngridmax, ncell=g.ncell, nvar=g.nvar, nx=1, ny=1, nz=1, ncpu=1,
-                       nboundary=0, nlevelmax=g.nlevelmax, son=g.son, father=g.father, nbor=g.nbor, next=g.next,
-                       headl=g.headl)
-    u0 = rg_tree.sedov_state(g, level, gamma)
-    kind = "port"
-    ref_lib = rs.ORACLE_DIR / "_ref" / "libref_harness3d.so"
-    if kind_pref == "reference" and ref_lib.exists():
-        kind = "reference"
-        h = rs.RefHarness(3).create(rs.namelist(slope_type=2, riemann="hllc", levelmin=level, levelmax=level),
-                                    ngridmax=g.ngridmax, levelmin=level, nlevelmax=level, gamma=gamma)
-        h.refine_uniform(level)
-        a = h.arrays()
-        a["uold"][:] = u0
-        a["unew"][:] = u0
-        el = 0.0
-        for _ in range(steps):
-            dt = orc.courant(ga, 3, 5, level, dx, gamma, cfl, a["uold"], pressure_cap=False)
-            t = time.perf_counter()
-            h.courant(level, dx, gamma, cfl)  # the reference's own CFL pass (value unused: its cap is unstable)
-            h.set_unew(level)
-            h.godunov_fine(level, dt, dx)
-            h.set_uold(level)
-            el += time.perf_counter() - t
-        h.close()
-    else:
-        params = rs.make_params(3, slope_type=2, riemann="hllc")
-        uold, unew = u0.copy(), u0.copy()
-        el = 0.0
-        for _ in range(steps):
-            t = time.perf_counter()
-            dt = orc.courant(ga, 3, 5, level, dx, gamma, cfl, uold, pressure_cap=False)
-            orc.set_unew(ga, 3, 5, level, uold, unew)
-            orc.godunov_fine(ga, params, level, dt, dx, uold, unew)
-            orc.set_uold(ga, 3, 5, level, uold, unew)
-            el += time.perf_counter() - t
-    cells = 8 ** (level - 1) * steps
-    return {"kind": kind, "seconds": el, "cells": cells, "level": level, "steps": steps}
+    from refsupport import AmrRun, RefHarness, namelist, sedov_ic
+    # the reference's flag_fine prints a line per flagged cell: to /dev/null,
+    # at the descriptor level (it writes through the C++ runtime)
+    sys.stdout.flush()
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    try:
+        return _amr_cpu_window(warmup, steps, parity_after, AmrRun, RefHarness, namelist, sedov_ic)
+    finally:
+        import ctypes
+        ctypes.CDLL(None).fflush(None)  # printf's buffer still belongs to /dev/null
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(devnull)
 
 
-def run_cpu_subprocess(level, steps):
-    cmd = [sys.executable, str(Path(__file__).resolve()), "--cpu-sample", str(level), str(steps)]
-    r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+def _amr_cpu_window(warmup, steps, parity_after, AmrRun, RefHarness, namelist, sedov_ic):
+    A = AMR
+    nml = namelist(slope_type=2, riemann="hllc", levelmin=A["lmin"], levelmax=A["lmax"], err_grad_d=A["ed"],
+                   err_grad_p=A["ep"])
+    h = RefHarness(3).create(nml, ngridmax=A["ngridmax"], levelmin=A["lmin"], nlevelmax=A["lmax"], gamma=A["gamma"])
+    r = AmrRun(h, A["lmin"], A["lmax"], A["gamma"], cfl=A["cfl"], ed=A["ed"], ep=A["ep"])
+    t0 = time.perf_counter()
+    r.initialize(sedov_ic(3, A["lmin"]))
+    init_s = time.perf_counter() - t0
+    digest = None
+    done = 0
+    for _ in range(warmup):
+        r.coarse_step()
+        done += 1
+        if parity_after == done:
+            a = h.arrays()
+            digest = hashlib.sha1(a["uold"].tobytes() + a["son"].tobytes()).hexdigest()
+    cu0 = r.cell_updates
+    el = 0.0
+    for _ in range(steps):
+        t = time.perf_counter()
+        r.coarse_step()
+        el += time.perf_counter() - t
+        done += 1
+        if parity_after == done:
+            a = h.arrays()
+            digest = hashlib.sha1(a["uold"].tobytes() + a["son"].tobytes()).hexdigest()
+    out = {"kind": "reference", "seconds": el, "cells": r.cell_updates - cu0, "steps": steps, "warmup": warmup,
+           "init_s": init_s, "t_end": r.t, "digest": digest,
+           "octs_per_level": [h.count_grids(il) for il in range(A["lmin"], A["lmax"] + 1)]}
+    h.close()
+    return out
+
+
+def run_cpu_window(warmup, steps, parity_after=None, timeout=1800):
+    cmd = [sys.executable, str(Path(__file__).resolve()), "--amr-cpu-window", str(warmup), str(steps),
+           str(parity_after or 0)]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
     for line in reversed(r.stdout.splitlines()):
         if line.startswith("{"):
             return json.loads(line)
-    raise RuntimeError("cpu sample failed: " + r.stderr[-2000:])
+    raise RuntimeError("CPU window failed: " + r.stderr[-2000:])
 
 
 def reference_arm(args, rank, world):
-    """Times the reference's own CPU implementation of the path on all host cores."""
+    """The reference's own CPU implementation on the same AMR window, on all
+    host cores: one independent process per core, each running the reference's
+    initialisation, W untimed and K timed coarse steps (the reference is
+    single-threaded); value = all processes' cell updates over the slowest
+    process's timed seconds."""
     if rank != 0:
         return None
     import multiprocessing as mp
     cores = os.cpu_count() or 1
-    # each step: every core runs one substep of the Sedov workload on a bounded
-    # sample grid, sized so that warmup+steps end within a few minutes
-    total = args.steps + args.warmup
-    level = 6 if total <= 300 else 5  # 32^3 (~0.25 s/step/core) or 16^3
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(cores) as pool:
-        res = pool.map(_ref_worker, [(level, args.steps, args.warmup)] * cores)
+        res = pool.starmap(amr_cpu_window, [(args.warmup, args.steps)] * cores)
     wall = time.perf_counter() - t0
     el = max(r["seconds"] for r in res)
     cells = sum(r["cells"] for r in res)
     value = cells / el
-    ms = 1e3 * el / args.steps
-    sample = (f"{cores} processes x one substep of the Sedov workload on a {2 ** (level - 1)}^3 grid per step "
-              f"(reference levelmin=levelmax={level}), {args.steps} timed steps after {args.warmup} warm-up")
+    sample = (f"{cores} processes (one per host core, no shared-memory parallelism in the reference), each the "
+              f"whole window: the reference's initialisation, {args.warmup} untimed and {args.steps} timed coarse "
+              f"steps of the Sedov AMR run")
     return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "sample_grid": f"{2 ** (level - 1)}^3", "parallelism": "processes"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": res[0]["kind"], "sample": sample},
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD.replace(", tree and state resident on the GPU", ""),
+                       "window": f"coarse steps {args.warmup + 1}..{args.warmup + args.steps}",
+                       "cells_per_step": res[0]["cells"] / args.steps, "parallelism": f"{cores} processes"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "wall_s": wall}
-
-
-def _ref_worker(a):
-    level, steps, warm = a
-    if warm:
-        cpu_sample(level, min(warm, 2))
-    return cpu_sample(level, steps)
+            "t_end": res[0]["t_end"], "octs_per_level": res[0]["octs_per_level"], "wall_s": wall}
 
 
 # ---------------------------------------------------------------- GPU arm
-def gpu_arm(args, rank, world, local_rank):
+def amr_params(rgpu):
+    return rgpu.make_params(3, slope_type=2, riemann="hllc", interpol_type=1, interpol_var=0, gamma=AMR["gamma"],
+                            courant_factor=AMR["cfl"])
+
+
+def amr_run(ctx):
+    """A fresh Sedov AMR run resident on ctx, initialised on the device."""
+    import rg_amr
+    A = AMR
+    rg_amr.initialize(ctx, 3, A["lmin"], A["lmax"], A["ngridmax"], rg_amr.sedov_primitives(3, A["lmin"], A["gamma"]),
+                      A["gamma"], ed=A["ed"], ep=A["ep"])
+    return rg_amr.DeviceAmrRun(ctx, nx=1, levelmin=A["lmin"], nlevelmax=A["lmax"], cfl=A["cfl"], ed=A["ed"],
+                               ep=A["ep"])
+
+
+def count_launches(torch, run, steps=2):
+    """This library's kernels launched per coarse step, counted by the CUDA
+    profiler interface (torch.profiler / CUPTI) over `steps` coarse steps."""
+    try:
+        from torch.profiler import ProfilerActivity, profile
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            for _ in range(steps):
+                run.coarse_step()
+            torch.cuda.synchronize()
+        n = sum(1 for e in prof.events() if e.device_type.name == "CUDA" and "rg::" in e.name)
+        return n / steps
+    except Exception:  # no profiler on this build: the count stays unreported
+        return None
+
+
+def amr_headline(args, rank, world, local_rank):
+    """The headline: K coarse steps of the resident Sedov AMR run after W
+    warm-up steps, CUDA events on the library's stream around each coarse step,
+    a 256 MB write between steps (outside the events) so every step starts
+    with a cold L2; max over ranks."""
     import numpy as np
     import torch
-    import rg_tree
     import rgpu
 
     torch.cuda.set_device(local_rank)
     dist = None
     if world > 1:
         import torch.distributed as dist
-    L = LEVEL
-    g = rg_tree.build_uniform(3, L)
-    u0 = rg_tree.sedov_state(g, L)
-    params = rgpu.make_params(3, slope_type=2, riemann="hllc", interpol_type=1, gamma=1.4, courant_factor=0.8)
-    ctx = rgpu.Context(params, local_rank)
+    dev = torch.device("cuda", local_rank)
     stream = torch.cuda.Stream()
+    ctx = rgpu.Context(amr_params(rgpu), local_rank)
     ctx.set_stream(stream.cuda_stream)
-    ctx.sync_topology(g)
-    ctx.upload_state(u0, u0)
-    if args.face_variant is not None:  # a fixed face-kernel shape instead of the autotuner's pick
-        ctx.set_face_config(L, args.face_variant, 1)
-    dx = 1.0 / 2 ** L
-    for _ in range(args.warmup):
-        ctx.level_substep(L, dx, pressure_cap=False, use_graph=True)
+    t0 = time.perf_counter()
+    run = amr_run(ctx)
     ctx.synchronize()
-    cells = ctx.cell_updates(L)
-
+    init_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        run.coarse_step()
+    ctx.synchronize()
+    t_start, cu0 = run.t, run.cell_updates
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB of L2
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     sampler = ClockSampler(local_rank) if rank == 0 else None
     time.sleep(0.3)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     tw0 = time.time()
-    e0.record(stream)
-    for _ in range(args.steps):
-        ctx.level_substep(L, dx, pressure_cap=False, use_graph=True)
-    e1.record(stream)
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))
+        ev[k][0].record(stream)
+        run.coarse_step()
+        ev[k][1].record(stream)
     torch.cuda.synchronize()
     tw1 = time.time()
-    ms = e0.elapsed_time(e1)
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
+    cells = run.cell_updates - cu0
     if dist:
         dist.barrier()
-        t = torch.tensor([ms], device="cuda")
+        t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     clocks = sampler.summary(tw0, tw1) if sampler else None
     if sampler:
         sampler.stop()
-    value = world * cells * args.steps / (ms / 1e3)
+    value = world * cells / (ms / 1e3)
+    window = {"coarse_steps": f"{args.warmup + 1}..{args.warmup + args.steps}", "t_start": t_start, "t_end": run.t,
+              "finest_dt_end": run.clock.dtnew[AMR["lmax"]], "init_s": init_s,
+              "octs_per_level": [ctx.count_grids(il) for il in range(AMR["lmin"], AMR["lmax"] + 1)],
+              "cells_per_step": cells / args.steps}
 
-    # the face-kernel shape the autotuner kept for this level
+    # the dominant kernel: the face kernel of every level step, two coarse steps
+    ctx.set_timing("accumulate")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(2):
+        run.coarse_step()
+    e1.record(stream)
+    kms, face_cells, level_steps = ctx.kernel_ms_totals()
+    step2_ms = e0.elapsed_time(e1)
+    ctx.set_timing(False)
+    launches = count_launches(torch, run)
+
+    # end to end: the state in page-locked host memory, uploaded before and
+    # downloaded after every coarse step (uold, nvar x ncell FP64 each way)
+    ngm, ncell = ctx.tree_sizes()
+    host = torch.empty(5 * ncell, dtype=torch.float64, pin_memory=True)
+    ctx.download_state_ptr(uold_ptr=host.data_ptr())
+    ne = min(args.steps, 10)
+    ee = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(ne)]
+    cu1 = run.cell_updates
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for k in range(ne):
+        ee[k][0].record(stream)
+        ctx.upload_state_ptr(uold_ptr=host.data_ptr())
+        run.coarse_step()
+        ctx.download_state_ptr(uold_ptr=host.data_ptr())
+        ee[k][1].record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = sum(a.elapsed_time(b) for a, b in ee)
+    cells_e2e = run.cell_updates - cu1
+    if dist:
+        t = torch.tensor([ms_e2e], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e_value = world * cells_e2e / (ms_e2e / 1e3)
+    fp64_peak = ctx.measure_fp64_peak() if rank == 0 else None
+    ctx.close()
+    del flush
+    torch.cuda.empty_cache()
+    if rank != 0:
+        return None
+
+    # a fresh run to coarse step W+2 for the parity digest against the reference
+    pctx = rgpu.Context(amr_params(rgpu), local_rank)
+    prun = amr_run(pctx)
+    for _ in range(args.warmup + 2):
+        prun.coarse_step()
+    got = pctx.tree_fetch({k: np.zeros(AMR["lmax"] + 1, np.int32) for k in ("headl", "taill", "numbl")})
+    digest = hashlib.sha1(got["uold"].tobytes() + got["son"].tobytes()).hexdigest()
+    pctx.close()
+
+    peak, peak_kind = peaks()
+    face_s = kms[1] / 1e3
+    achieved = BYTES_PER_CELL_UPDATE * face_cells / face_s / 1e9
+    rin = roofline_inputs("k_face_tiles_amr")
+    per_launch_cells = face_cells / max(level_steps, 1)
+    traffic = rin["dram_bytes_per_cell_update"] * per_launch_cells if rin else None
+    fp64 = None
+    if rin and fp64_peak:
+        fl = rin["fp64_flops_per_cell_update"] * face_cells / face_s / 1e12
+        ops = rin["fp64_ops_per_cell_update"] * face_cells / face_s / 1e12
+        fp64 = {"bound": "fp64", "achieved": fl, "peak": fp64_peak, "unit": "TFLOP/s", "frac": fl / fp64_peak,
+                "op_frac": ops / (fp64_peak / 2), "kernel": "k_face_tiles",
+                "flops_per_cell_update": rin["fp64_flops_per_cell_update"],
+                "peak_source": "rg_measure_fp64_peak: independent DFMA chains on every SM (measured here)",
+                "flops_source": "profiles/roofline_inputs.json k_face_tiles_amr (ncu)", "stale": rin["stale"]}
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "window": window, "riemann": "hllc", "slope_type": 2,
+                   "cfl": "reference compute_courant_step formula without its p <= 100 rho cap, courant_factor 0.25",
+                   "l2": "flushed between timed coarse steps (a 256 MB write outside the timed events)",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "k_face_tiles (every level step of the coarse step)",
+                     "algorithmic_bytes_per_launch": BYTES_PER_CELL_UPDATE * per_launch_cells,
+                     "launches": level_steps, "face_share_of_step": kms[1] / step2_ms,
+                     "kernel_ms_per_coarse_step": {"prim": kms[0] / 2, "face": kms[1] / 2, "fold": kms[2] / 2,
+                                                   "whole_step": step2_ms / 2},
+                     "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
+                     "traffic_source": ("profiles/roofline_inputs.json k_face_tiles_amr (ncu), scaled to the average "
+                                        "launch" if rin else None),
+                     "traffic_stale": rin["stale"] if rin else None,
+                     "step_hbm_frac": (BYTES_PER_CELL_UPDATE * value / world / 1e9) / peak},
+        "roofline_fp64": fp64,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * 5 * ncell, "d2h_bytes_per_step": 8 * 5 * ncell,
+                "ms_per_step": ms_e2e / ne, "steps": ne,
+                "path": "rg_upload_state (page-locked uold) + rg_amr_coarse_step + rg_download_state per coarse step"},
+        "gpu_launches": round(launches * args.steps) if launches else None,
+        "gpu_launches_per_step": launches,
+        "clocks": clocks,
+        "parity_digest": {"after_coarse_step": args.warmup + 2, "sha1_uold_son": digest},
+    }
+
+
+def uniform_report(local_rank, steps, warmup, face_variant=None):
+    """Config 2: the uniform 128^3 Sedov level (reference levelmin = levelmax
+    = 8), MonCen + HLLC, courant 0.8, one substep per step in a CUDA graph
+    (dt finalize, brick face kernel, fold that prepares the next substep);
+    inputs larger than L2 (state, primitives and flux scratch 0.8 GB)."""
+    import numpy as np
+    import torch
+    import rg_tree
+    import rgpu
+    L = 8
+    g = rg_tree.build_uniform(3, L)
+    u0 = rg_tree.sedov_state(g, L)
+    ctx = rgpu.Context(rgpu.make_params(3, slope_type=2, riemann="hllc", interpol_type=1, gamma=1.4,
+                                        courant_factor=0.8), local_rank)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    ctx.sync_topology(g)
+    ctx.upload_state(u0, u0)
+    if face_variant is not None:  # a fixed face-kernel shape instead of the autotuner's pick
+        ctx.set_face_config(L, face_variant, 1)
+    dx = 1.0 / 2 ** L
+    for _ in range(warmup):
+        ctx.level_substep(L, dx, pressure_cap=False, use_graph=True)
+    ctx.synchronize()
+    cells = ctx.cell_updates(L)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        ctx.level_substep(L, dx, pressure_cap=False, use_graph=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
     variant = ctx.face_config(L)[0]
     face_kernel = "k_face_brick" if variant >= 9 else ("k_face_pipe" if variant >= 7 else "k_face_tiles")
-
-    # per-kernel device time (events around prim / face / fold, same stream)
     ctx.set_timing(True)
-    nk = min(args.steps, 40)
+    nk = min(steps, 40)
     acc = np.zeros(3)
     for _ in range(nk):
         ctx.level_substep(L, dx, pressure_cap=False, use_graph=False)
@@ -305,16 +491,10 @@ def gpu_arm(args, rank, world, local_rank):
         acc += np.array(ctx.kernel_ms())
     ctx.set_timing(False)
     kms = acc / nk
-
-    # end to end through the C ABI with the state in (pinned) host memory: each
-    # step uploads the cells the substep reads, runs it, and downloads the
-    # cells it updated (rg_level_substep_host)
     n = g.nvar * g.ncell
     host = torch.empty(n, dtype=torch.float64, pin_memory=True)
     ctx.download_state_ptr(uold_ptr=host.data_ptr())
-    ne = min(args.steps, 40)
-    if dist:
-        dist.barrier()
+    ne = min(steps, 40)
     torch.cuda.synchronize()
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e2.record(stream)
@@ -323,43 +503,26 @@ def gpu_arm(args, rank, world, local_rank):
     e3.record(stream)
     torch.cuda.synchronize()
     ms_e2e = e2.elapsed_time(e3)
-    if dist:
-        t = torch.tensor([ms_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
-    e2e_value = world * cells * ne / (ms_e2e / 1e3)
-    fp64_peak = ctx.measure_fp64_peak() if rank == 0 else None
-    link = pinned_copy_gbs(torch, stream, 8 * g.nvar * cells) if rank == 0 else None
+    fp64_peak = ctx.measure_fp64_peak()
+    link = pinned_copy_gbs(torch, stream, 8 * g.nvar * cells)
     ctx.close()
-    if rank != 0:
-        return None
-
     peak, peak_kind = peaks()
     face_s = kms[1] / 1e3
-    alg_bytes = BYTES_PER_CELL_UPDATE * cells
-    achieved = alg_bytes / face_s / 1e9
-    out = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "cells_per_step": cells, "riemann": "hllc", "slope_type": 2,
-                   "cfl": "reference compute_courant_step formula, courant_factor 0.8, without the p<=100rho cap",
-                   "l2": "inputs larger than L2: uold+unew 192 MB, primitives 96 MB, flux scratch 503 MB per step",
-                   "parallelism": "replicas" if world > 1 else "single GPU", "cuda_graph": True},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": profile_traffic(face_kernel), "kernel": face_kernel, "variant": variant,
-                     "algorithmic_bytes_per_launch": alg_bytes, "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
-                     "step_hbm_frac": (BYTES_PER_CELL_UPDATE * value / world / 1e9) / peak},
-        "roofline_fp64": fp64_roofline(face_kernel, cells, face_s, fp64_peak),
-        "kernel_ms": {"prim": kms[0], "face": kms[1], "fold": kms[2]},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * g.nvar * cells,
-                "d2h_bytes_per_step": 8 * g.nvar * cells, "ms_per_step": ms_e2e / ne,
-                "path": "rg_level_substep_host on pinned host memory: the level's cells up, substep, its cells down",
-                "bound": e2e_bound(link, 8 * g.nvar * cells, ms / args.steps, ms_e2e / ne)},
-        "gpu_launches": GPU_KERNELS_PER_STEP * args.steps,
-        "clocks": clocks,
-    }
-    return out
+    achieved = BYTES_PER_CELL_UPDATE * cells / face_s / 1e9
+    rin = roofline_inputs(f"{face_kernel}_sedov128")
+    return {"workload": "3D Sedov blast, uniform 128^3 (reference levelmin=levelmax=8), MonCen + HLLC, gamma 1.4, "
+                        "courant 0.8 without the p <= 100 rho cap, FP64",
+            "value": cells * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
+            "cells_per_step": cells, "kernel_ms": {"prim": kms[0], "face": kms[1], "fold": kms[2]},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": rin["dram_bytes_per_cell_update"] * cells if rin else None,
+                         "traffic_stale": rin["stale"] if rin else None, "kernel": face_kernel, "variant": variant,
+                         "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})"},
+            "roofline_fp64": fp64_roofline(rin, face_kernel, cells, face_s, fp64_peak),
+            "e2e": {"value": cells * ne / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": 8 * g.nvar * cells,
+                    "d2h_bytes_per_step": 8 * g.nvar * cells, "ms_per_step": ms_e2e / ne,
+                    "path": "rg_level_substep_host on pinned host memory: the level's cells up, substep, its cells down",
+                    "bound": e2e_bound(link, 8 * g.nvar * cells, ms / steps, ms_e2e / ne)}}
 
 
 def pinned_copy_gbs(torch, stream, nbytes, reps=5):
@@ -396,23 +559,23 @@ def e2e_bound(link, nbytes, ms_device, ms_e2e):
                     "previous step's output)"}
 
 
-def fp64_roofline(face_kernel, cells, face_s, peak_tflops):
+def fp64_roofline(rin, face_kernel, cells, face_s, peak_tflops):
     """The face kernel against the FP64 pipe, its real bound: executed FP64
-    FLOPs per cell update (ncu instruction counts, a DFMA counted as 2) over
-    its CUDA-event time, against the FP64 throughput measured on this GPU."""
-    fpc = profile_value(face_kernel, "fp64_flops_per_cell_update")
-    if fpc is None or not peak_tflops:
+    FLOPs per cell update (ncu instruction counts, a DFMA counted as 2, from
+    profiles/roofline_inputs.json) over its CUDA-event time, against the FP64
+    throughput measured on this GPU."""
+    if not rin or not peak_tflops:
         return None
-    achieved = fpc * cells / face_s / 1e12
-    opc = profile_value(face_kernel, "fp64_ops_per_cell_update")
+    achieved = rin["fp64_flops_per_cell_update"] * cells / face_s / 1e12
+    ops = rin["fp64_ops_per_cell_update"] * cells / face_s / 1e12
     # instruction throughput: DMUL and DADD take an issue slot of the FP64 pipe
     # like a DFMA but carry one FLOP, so the FLOP fraction understates it
-    op_frac = (opc * cells / face_s / 1e12) / (peak_tflops / 2) if opc else None
     return {"bound": "fp64", "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
-            "frac": achieved / peak_tflops, "op_frac": op_frac, "flops_per_cell_update": fpc,
-            "ops_per_cell_update": opc, "kernel": face_kernel,
+            "frac": achieved / peak_tflops, "op_frac": ops / (peak_tflops / 2),
+            "flops_per_cell_update": rin["fp64_flops_per_cell_update"],
+            "ops_per_cell_update": rin["fp64_ops_per_cell_update"], "kernel": face_kernel, "stale": rin["stale"],
             "peak_source": "rg_measure_fp64_peak: independent DFMA chains on every SM, best of 5 (measured here)",
-            "flops_source": f"profiles/{face_kernel}_sedov128.md (ncu executed DFMA/DMUL/DADD per cell update)"}
+            "flops_source": f"profiles/roofline_inputs.json {face_kernel}_sedov128 (ncu)"}
 
 
 def newton_report(local_rank, stream, steps):
@@ -456,7 +619,8 @@ def newton_report(local_rank, stream, steps):
         cdf = np.cumsum(hist) / n
         res[learned] = (f, ps, {"mean_iters": float((hist * np.arange(len(hist))).sum() / n),
                                 "p99_iters": int(np.searchsorted(cdf, 0.99)),
-                                "at_cap_frac": float(hist[100:].sum() / n), "ms": ms,
+                                "at_cap_count": int(hist[100:].sum()), "max_iters": int(np.flatnonzero(hist).max()),
+                                "ms": ms,
                                 "interfaces_per_s": n / (ms / 1e3)})
     (f0, p0, a), (f1, p1, b) = res[False], res[True]
     rel = ((p1 - p0).abs() / p0.abs().clamp_min(1e-300))
@@ -465,13 +629,18 @@ def newton_report(local_rank, stream, steps):
                                  "30% strong double rarefactions, gamma 5/3 or 1.4, seed 20261203",
                      "interfaces": n, "plain": a, "learned": b,
                      "iteration_ratio": a["mean_iters"] / b["mean_iters"],
-                     "pstar_rel_max": float(rel.max()), "pstar_rel_gt_1e-13_frac": float((rel > 1e-13).double().mean()),
-                     "flux_rel_gt_1e-12_frac": float((frel > 1e-12).double().mean())}
+                     "polish_updates_per_interface": 2,
+                     "iteration_ratio_with_polish": (a["mean_iters"] + 2) / (b["mean_iters"] + 2),
+                     "pstar_rel_max": float(rel.max()), "pstar_rel_gt_1e-13_count": int((rel > 1e-13).sum().item()),
+                     "pstar_bits_differ_count": int((p1 != p0).sum().item()),
+                     "flux_rel_gt_1e-12_count": int((frel > 1e-12).sum().item()),
+                     "note": "converged mode: bracketed Newton-bisection to |dp|/p < 1e-14, then 2 polish updates "
+                             "from the root's 30 leading bits (counted apart: the same for both starts)"}
     del ql, qr, gam, f0, f1, p0, p1, res, rel, frel
     ctx.close()
     torch.cuda.empty_cache()
 
-    L = LEVEL
+    L = 8
     g = rg_tree.build_uniform(3, L)
     u0 = rg_tree.sedov_state(g, L)
     dx = 1.0 / 2 ** L
@@ -502,7 +671,8 @@ def newton_report(local_rank, stream, steps):
         sed["learned" if learned else "plain"] = {"cell_updates_per_s": cells / (ms / 1e3), "ms_per_step": ms,
                                                    "iters_per_interface": iters / max(calls, 1)}
         c.close()
-    sed["workload"] = WORKLOAD.replace("HLLC", "exact solver (converged mode)") + f", {steps} substeps after 3"
+    sed["workload"] = ("3D Sedov blast, uniform 128^3, MonCen + exact solver (converged mode), gamma 1.4, courant "
+                       f"0.8, {steps} substeps after 3")
     out["sedov_exact"] = sed
     return out
 
@@ -580,7 +750,7 @@ def amr_sample(variant, steps, lmin=7, lmax=10, ngridmax=400000):
         run.h.godunov_fine(il, dt, dx)
         hyd[0] += time.perf_counter() - t
 
-    r = AmrRun(h, lmin, lmax, 1.4, ed=0.1, ep=0.1, on_godunov=on_g)
+    r = AmrRun(h, lmin, lmax, 1.4, cfl=AMR["cfl"], ed=0.1, ep=0.1, on_godunov=on_g)
     r.initialize(sedov_ic(3, lmin))
     r.coarse_step()  # warm-up step (first-call costs)
     hyd[0] = 0.0
@@ -594,44 +764,6 @@ def amr_sample(variant, steps, lmin=7, lmax=10, ngridmax=400000):
            "cell_updates": r.cell_updates - cu0, "t": r.t,
            "octs_per_level": [h.count_grids(il) for il in range(lmin, lmax + 1)],
            "digest": hashlib.sha1(a["uold"].tobytes() + a["son"].tobytes()).hexdigest()}
-    h.close()
-    return out
-
-
-def amr_device_sample(steps, lmin=7, lmax=10, ngridmax=400000):
-    """Config 3 with the tree resident on the GPU: initialisation by the
-    reference on the host (as in the other arms), then rg_tree_attach and every
-    coarse step (tree maintenance, CFL, hydro) on the device through
-    rg_amr.DeviceAmrRun; the digest covers the same arrays as amr_sample's."""
-    import hashlib
-    sys.path.insert(0, str(ROOT / "tests"))
-    import rgpu
-    from rg_amr import DeviceAmrRun
-    from refsupport import AmrRun, RefHarness, namelist, sedov_ic
-    nml = namelist(slope_type=2, riemann="hllc", levelmin=lmin, levelmax=lmax, err_grad_d=0.1, err_grad_p=0.1)
-    h = RefHarness(3).create(nml, ngridmax=ngridmax, levelmin=lmin, nlevelmax=lmax, gamma=1.4)
-    r = AmrRun(h, lmin, lmax, 1.4, ed=0.1, ep=0.1)
-    r.initialize(sedov_ic(3, lmin))
-    ctx = rgpu.Context(rgpu.make_params(3, slope_type=2, riemann="hllc", interpol_type=1, interpol_var=0, gamma=1.4),
-                       0)
-    t0 = time.perf_counter()
-    ctx.tree_attach(h.grid(), h.tree_arrays(), lmin)
-    attach_s = time.perf_counter() - t0
-    d = DeviceAmrRun(ctx, nx=1, levelmin=lmin, nlevelmax=lmax, ed=0.1, ep=0.1)
-    d.coarse_step()  # warm-up step (plans, autotuner), as in the other arms
-    ctx.synchronize()
-    cu0 = d.cell_updates
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        d.coarse_step()
-    ctx.synchronize()
-    wall = time.perf_counter() - t0
-    got = ctx.tree_fetch(h.tree_arrays())
-    out = {"variant": "gpu_resident", "coarse_steps": steps, "wall_s": wall, "attach_s": attach_s,
-           "cell_updates": d.cell_updates - cu0, "t": d.t,
-           "octs_per_level": [ctx.count_grids(il) for il in range(lmin, lmax + 1)],
-           "digest": hashlib.sha1(got["uold"].tobytes() + got["son"].tobytes()).hexdigest()}
-    ctx.close()
     h.close()
     return out
 
@@ -768,6 +900,57 @@ def profile_case_learned():
     ctx.close()
 
 
+def profile_case_amr():
+    """A small run for ncu captures of the AMR step: the headline's run
+    initialised on the device and 5 coarse steps, two coarse steps inside the
+    NVTX range "steps" (the launch list), then one level step each of
+    level 7 (the 64^3 base level, 261,504 leaf cells) and level 10 (the finest)
+    inside the NVTX range "capture" (ncu --nvtx --nvtx-include capture/)."""
+    import torch
+    import rgpu
+    ctx = rgpu.Context(amr_params(rgpu), 0)
+    run = amr_run(ctx)
+    for _ in range(5):
+        run.coarse_step()
+    ctx.synchronize()
+    torch.cuda.nvtx.range_push("steps")  # two whole coarse steps: the launch list
+    for _ in range(2):
+        run.coarse_step()
+    ctx.synchronize()
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.nvtx.range_push("capture")
+    for il in (7, 10):
+        ctx.godunov_level(il, 1e-7, 1.0 / 2 ** il)
+    ctx.synchronize()
+    torch.cuda.nvtx.range_pop()
+    ctx.close()
+
+
+def profile_case_uniform():
+    """A small run for ncu captures of the brick face kernel: the uniform
+    128^3 Sedov level, two warm-up substeps, then one eager substep inside the
+    NVTX range "capture"."""
+    import torch
+    import rg_tree
+    import rgpu
+    L = 8
+    g = rg_tree.build_uniform(3, L)
+    u0 = rg_tree.sedov_state(g, L)
+    ctx = rgpu.Context(rgpu.make_params(3, slope_type=2, riemann="hllc", interpol_type=1, gamma=1.4,
+                                        courant_factor=0.8), 0)
+    ctx.sync_topology(g)
+    ctx.upload_state(u0, u0)
+    ctx.set_face_config(L, 10, 1)
+    for _ in range(2):
+        ctx.level_substep(L, 1.0 / 2 ** L, pressure_cap=False, use_graph=False)
+    ctx.synchronize()
+    torch.cuda.nvtx.range_push("capture")
+    ctx.level_substep(L, 1.0 / 2 ** L, pressure_cap=False, use_graph=False)
+    ctx.synchronize()
+    torch.cuda.nvtx.range_pop()
+    ctx.close()
+
+
 def run_sample(flag, *args, timeout=900):
     cmd = [sys.executable, str(Path(__file__).resolve()), flag, *[str(a) for a in args]]
     # load every kernel when the context is created (in the sample's untimed
@@ -781,23 +964,19 @@ def run_sample(flag, *args, timeout=900):
 
 
 def amr_report(steps):
+    """The AMR run through the reference's own AmrGrid / TreeUpdater /
+    Simulation step, CPU hydro against the GPU drop-in (the reference-facing
+    plugin: GpuHydroSolver through create_hydro_solver), coarse steps 2..1+steps."""
     ref = run_sample("--amr-sample", "cpu", steps)
     gpu = run_sample("--amr-sample", "gpu", steps)
-    res = run_sample("--amr-device-sample", steps)
-    return {"workload": "3D Sedov AMR, reference levelmin 7, levelmax 10 (64^3 base, 512^3 effective), "
-                        "err_grad_d = err_grad_p = 0.1, sub-cycled, MonCen + HLLC, through the reference's own "
-                        "AmrGrid/TreeUpdater/Simulation step with the hydro solver swapped by create_hydro_solver",
+    return {"workload": "the headline's Sedov AMR run through the reference's own AmrGrid/TreeUpdater/Simulation "
+                        "step with the hydro solver swapped by create_hydro_solver",
             "coarse_steps": steps, "after": "initialisation and one warm-up coarse step",
             "reference_cpu": ref, "gpu_dropin": gpu, "bit_identical": ref["digest"] == gpu["digest"],
             "wall_speedup": ref["wall_s"] / gpu["wall_s"], "hydro_speedup": ref["hydro_s"] / gpu["hydro_s"],
             "gpu_hydro_cell_updates_per_s": gpu["cell_updates"] / gpu["hydro_s"],
-            "gpu_resident": res, "resident_bit_identical": ref["digest"] == res["digest"],
-            "resident_wall_speedup": ref["wall_s"] / res["wall_s"],
-            "resident_cell_updates_per_s": res["cell_updates"] / res["wall_s"],
-            "note": "gpu_dropin: tree maintenance (flag/refine/restrict) on the host as in the reference, GPU hydro "
-                    "time includes the level-sparse host<->device copies of every godunov_fine call; "
-                    "gpu_resident: the tree on the device too (rg_tree_attach + DeviceAmrRun), the host reads "
-                    "back level counts and one dt per level step"}
+            "note": "tree maintenance (flag/refine/restrict) on the host as in the reference; the GPU hydro time "
+                    "includes the level-sparse host<->device copies of every godunov_fine call"}
 
 
 def amr_exact_report(steps):
@@ -825,24 +1004,26 @@ def sod_report():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--face-variant", type=int, default=None,
-                    help="face-kernel shape for the headline level (0-10) instead of the autotuner's pick; "
+                    help="face-kernel shape of the uniform 128^3 report (0-10) instead of the autotuner's pick; "
                          "for profiler runs, whose serialised launches would skew the autotuner's timings")
     ap.add_argument("--no-newton", action="store_true", help="skip the exact-solver plain/learned report")
-    ap.add_argument("--no-extra", action="store_true", help="skip the ensemble, AMR and Sod reports")
-    ap.add_argument("--cpu-sample", nargs=2, type=int, metavar=("LEVEL", "STEPS"), help=argparse.SUPPRESS)
+    ap.add_argument("--no-extra", action="store_true", help="skip the uniform, ensemble, drop-in and Sod reports")
+    ap.add_argument("--amr-cpu-window", nargs=3, type=int, metavar=("WARMUP", "STEPS", "PARITY"),
+                    help=argparse.SUPPRESS)
     ap.add_argument("--amr-sample", nargs=2, metavar=("VARIANT", "STEPS"), help=argparse.SUPPRESS)
     ap.add_argument("--sod-sample", metavar="VARIANT", help=argparse.SUPPRESS)
     ap.add_argument("--amr-exact-sample", nargs=2, metavar=("GUESS", "STEPS"), help=argparse.SUPPRESS)
-    ap.add_argument("--amr-device-sample", type=int, metavar="STEPS", help=argparse.SUPPRESS)
-    ap.add_argument("--profile-case", choices=["learned"], help="small run for ncu captures (no timing output)")
+    ap.add_argument("--profile-case", choices=["learned", "amr", "uniform"],
+                    help="small run for ncu captures (no timing output)")
     args = ap.parse_args()
-    if args.cpu_sample:
-        print(json.dumps(cpu_sample(*args.cpu_sample)))
+    if args.amr_cpu_window:
+        w, k, par = args.amr_cpu_window
+        print(json.dumps(amr_cpu_window(w, k, par or None)))
         return
     if args.amr_sample:
         print(json.dumps(amr_sample(args.amr_sample[0], int(args.amr_sample[1]))))
@@ -850,14 +1031,11 @@ def main():
     if args.sod_sample:
         print(json.dumps(sod_sample(args.sod_sample)))
         return
-    if args.amr_device_sample:
-        print(json.dumps(amr_device_sample(args.amr_device_sample)))
-        return
     if args.amr_exact_sample:
         print(json.dumps(amr_exact_sample(args.amr_exact_sample[0], int(args.amr_exact_sample[1]))))
         return
-    if args.profile_case == "learned":
-        profile_case_learned()
+    if args.profile_case:
+        {"learned": profile_case_learned, "amr": profile_case_amr, "uniform": profile_case_uniform}[args.profile_case]()
         return
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -875,23 +1053,31 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    cpu = None
+    cpu = cpu_run = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        # one full 128^3 substep of the reference on one core (~15-20 s), before any CUDA work
-        c = run_cpu_subprocess(LEVEL, 1)
-        cpu = {"value": c["cells"] / c["seconds"], "unit": UNIT, "cores": 1, "kind": c["kind"],
-               "sample": f"one substep (CFL, set_unew, godunov_fine, set_uold) of the 128^3 Sedov workload, "
-                         f"single-threaded, {c['seconds']:.1f} s"}
-    out = gpu_arm(args, rank, world, local_rank)
+        # the reference on one core, before any CUDA work: its initialisation,
+        # the W warm-up coarse steps and the first 2 coarse steps of the window
+        cpu_run = run_cpu_window(args.warmup, 2, parity_after=args.warmup + 2)
+        cpu = {"value": cpu_run["cells"] / cpu_run["seconds"], "unit": UNIT, "cores": 1, "kind": "reference",
+               "sample": f"coarse steps {args.warmup + 1}..{args.warmup + 2} of the same AMR run (the first two of "
+                         f"the window, {cpu_run['cells']} cell updates, {cpu_run['seconds']:.1f} s) after the "
+                         f"reference's own initialisation and {args.warmup} coarse steps, single-threaded"}
+    out = amr_headline(args, rank, world, local_rank)
+    if rank == 0:
+        if cpu_run:
+            out["parity_digest"]["reference_sha1_uold_son"] = cpu_run["digest"]
+            out["parity_digest"]["bit_identical"] = cpu_run["digest"] == out["parity_digest"]["sha1_uold_son"]
+        if not args.no_extra:
+            out["sedov128"] = uniform_report(local_rank, 20, 3, args.face_variant)
     if rank == 0 and not args.no_newton:
         import torch
-        out["newton"] = newton_report(local_rank, torch.cuda.Stream(), min(max(args.steps // 20, 5), 40))
+        out["newton"] = newton_report(local_rank, torch.cuda.Stream(), 10)
     if not args.no_extra:
         ens_out = ensemble_report(rank, world, local_rank, 100)
         if rank == 0:
             out["ensemble"] = ens_out
             if world == 1:
-                out["amr"] = amr_report(3)
+                out["amr_dropin"] = amr_report(3)
                 if "newton" in out:
                     out["newton"]["amr_exact"] = amr_exact_report(3)
                 out["sod1d"] = sod_report()
