@@ -67,15 +67,23 @@ int amr_step(rg_ctx* c, const rg_amr_config& cfg, AmrRunState& S, int il, int ic
     if (il > lmax) return RG_OK;
     if (count_grids(c, il) == 0 && il > 0) return RG_OK;
     if (lmin < lmax && (il == lmin || icount > 1)) {
-        for (int i = il; i <= lmax; ++i)
-            if (int rc = tree_make_grid_fine(c, i + 1)) return rc;
-        for (int i = lmax; i >= il; --i)
-            if (int rc = tree_remove_grid_fine(c, i + 1)) return rc;
+        // the refinements and removals below change nothing when no cell of
+        // those levels is flagged for refinement and no oct for removal:
+        // one probe instead of a scan and a read-back per call
+        bool pending = true;
+        if (int rc = tree_changes_pending(c, il + 1, lmax, &pending)) return rc;
+        if (pending) {
+            for (int i = il; i <= lmax; ++i)
+                if (int rc = tree_make_grid_fine(c, i + 1)) return rc;
+            for (int i = lmax; i >= il; --i)
+                if (int rc = tree_remove_grid_fine(c, i + 1)) return rc;
+        }
     }
     const double dx = cfg.boxlen / (double)(c->nx * (1 << il));
-    if (int rc = courant_step_device(c, il, dx, cfg.courant_factor, cfg.pressure_cap)) return rc;
+    // the CFL pass also does set_unew (both read the level's uold, nothing
+    // between them writes it; k_amr_dt only reads the CFL word)
+    if (int rc = courant_step_device(c, il, dx, cfg.courant_factor, cfg.pressure_cap, true)) return rc;
     k_amr_dt<<<1, 1, 0, c->stream>>>(S.ck, c->d_status, il, il > lmin ? nsubcycle(cfg, il - 1) : 0);
-    if (int rc = rg_set_unew(c, il)) return rc;
     const int nsub = nsubcycle(cfg, il);
     if (il < lmax) {
         if (count_grids(c, il + 1) > 0) {
@@ -91,9 +99,12 @@ int amr_step(rg_ctx* c, const rg_amr_config& cfg, AmrRunState& S, int il, int ic
     }
     // this level's dtnew is still the one set above: the finer steps only
     // change the finer levels' entries
-    if (int rc = godunov_level_device_dt(c, il, S.ck + il, dx)) return rc;
+    // set_uold folded into the fold kernels: a level target's result goes to
+    // uold as well (the fold reads only unew and the flux scratch)
+    if (int rc = godunov_level_device_dt(c, il, S.ck + il, dx, true)) return rc;
     S.cell_updates += rg_level_cell_updates(c, il);
-    if (int rc = rg_set_uold(c, il)) return rc;
+    if (rg::existing_plan(c, il) == nullptr || rg::existing_plan(c, il)->ncells == 0)
+        if (int rc = rg_set_uold(c, il)) return rc;
     if (il < lmax)
         if (int rc = tree_restrict_fine(c, il)) return rc;
     return tree_flag_fine(c, il + 1, cfg.err_grad_d, cfg.err_grad_p, cfg.err_grad_u, -1.0, cfg.nexpand, icount,

@@ -304,6 +304,7 @@ void rg_destroy(rg_ctx* c) {
     int* tp[] = {c->d_prev, c->d_flag1, c->d_flag2, c->d_cpu_map, c->d_fq, c->d_tscr};
     for (int* p : tp) dev_free(c, p);
     dev_free(c, c->d_xg);
+    for (int* p : c->lvl_octs) dev_free(c, p);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->pool) cudaMemPoolDestroy(c->pool);
     if (c->h_status) cudaFreeHost(c->h_status);
@@ -546,17 +547,17 @@ int rg_courant_step(rg_ctx* c, int ilevel, double dx, double courant_factor, int
 }  // extern "C"
 
 namespace rg {
-int courant_step_device(rg_ctx* c, int ilevel, double dx, double courant_factor, int pressure_cap) {
+int courant_step_device(rg_ctx* c, int ilevel, double dx, double courant_factor, int pressure_cap, bool set_unew) {
     CTX_GUARD(c);
     c->next_level = -1;  // the state or the CFL word may change
     if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state uploaded");
     Plan* P;
     if (int rc = get_plan(c, ilevel, &P)) return rc;
     if (P->nbox > 0) return set_error(c, RG_ERR_STATE, "ensemble level: read the per-box steps with rg_level_box_dt");
-    return launch_courant(c, *P, dx, pressure_cap, courant_factor);
+    return launch_courant(c, *P, dx, pressure_cap, courant_factor, set_unew);
 }
 
-int godunov_level_device_dt(rg_ctx* c, int ilevel, const double* dt_dev, double dx) {
+int godunov_level_device_dt(rg_ctx* c, int ilevel, const double* dt_dev, double dx, bool set_uold) {
     CTX_GUARD(c);
     c->next_level = -1;  // the state or the CFL word may change
     if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state uploaded");
@@ -568,7 +569,7 @@ int godunov_level_device_dt(rg_ctx* c, int ilevel, const double* dt_dev, double 
     if (P->ncells == 0) return RG_OK;
     if (int rc = ensure_flux(c, *P)) return rc;
     if (int rc = launch_set_dt_device(c, dt_dev, dx)) return rc;
-    if (int rc = launch_godunov(c, *P)) return rc;
+    if (int rc = launch_godunov(c, *P, set_uold)) return rc;
     if (P->face_variant < 0 && ++P->substeps_run >= 1) return autotune_face(c, *P, step_consts(c));
     return RG_OK;
 }

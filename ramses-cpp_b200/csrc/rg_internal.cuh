@@ -236,6 +236,13 @@ struct rg_ctx {
     std::vector<int> h_taill, h_numbl, h_fq;
     int fq_head = 0, numbf = 0, levelmin = 1;
     bool tree_resident = false;
+    // each level's oct list in list order for the tree operations, kept while
+    // the topology version it was built at is current (rg_plan.cu
+    // level_octs_cached): a coarse step calls the tree operations about 35
+    // times on unchanged lists
+    std::vector<int*> lvl_octs;
+    std::vector<int> lvl_cap, lvl_n;
+    std::vector<long long> lvl_ver;
     bool tree_dirty = false;  // links changed on the device: ranks, cell levels and plans are stale
     // authorize_fine (flag2 = cpu_map == myid over every cell) has an effect:
     // false while flag2 == (cpu_map == 1) holds everywhere, which only
@@ -270,6 +277,10 @@ int exclusive_scan(rg_ctx* c, const int* in, int* out, int n, int* total);
 // Octs of level list `ilevel` in linked-list order, from the list ranks, into the
 // device array out[cap]; *noct gets the count (synchronises).
 int level_oct_list(rg_ctx* c, int ilevel, int* out, int cap, int* noct);
+// The same list of a device-resident tree from a per-level cache, rebuilt
+// only when the topology changed since it was built; *octs stays valid until
+// the next tree change.
+int level_octs_cached(rg_ctx* c, int ilevel, const int** octs, int* noct);
 // after device tree operations changed links: drop plans, re-rank the lists,
 // recompute cell levels (no-op when nothing changed)
 int refresh_tree(rg_ctx* c);
@@ -284,21 +295,31 @@ int tree_flag_fine(rg_ctx* c, int ilevel, double ed, double ep, double ev, doubl
 int tree_make_grid_fine(rg_ctx* c, int ilevel);
 int tree_remove_grid_fine(rg_ctx* c, int ilevel);
 int tree_restrict_fine(rg_ctx* c, int ilevel);
+// Would make_grid_fine(L) for L = lo..hi followed by remove_grid_fine(L) for
+// L = hi..lo change the resident tree?  One pass over those levels (after the
+// authorisation the first make_grid_fine would run): false when no cell is a
+// refinement candidate and no oct a removal candidate, in which case every one
+// of those calls leaves the tree as it is.
+int tree_changes_pending(rg_ctx* c, int lo, int hi, bool* pending);
 Plan* existing_plan(rg_ctx* c, int ilevel);  // built plan or nullptr; never builds
 int compute_cell_levels(rg_ctx* c);
 // step launchers (enqueue only)
 int launch_set_unew(rg_ctx* c, const Plan& p);
 int launch_set_uold(rg_ctx* c, const Plan& p);
-int launch_courant(rg_ctx* c, const Plan& p, double dx, int pressure_cap, double courant_factor);
+// set_unew: also HydroSolver::set_unew of the level in the same pass
+int launch_courant(rg_ctx* c, const Plan& p, double dx, int pressure_cap, double courant_factor,
+                   bool set_unew = false);
 // the step values (dt, dt/dx, 1/dx) from a dt in device memory
 int launch_set_dt_device(rg_ctx* c, const double* dt, double dx);
 // rg_courant_step without reading the step back: the CFL word holds it
-int courant_step_device(rg_ctx* c, int ilevel, double dx, double courant_factor, int pressure_cap);
+int courant_step_device(rg_ctx* c, int ilevel, double dx, double courant_factor, int pressure_cap,
+                        bool set_unew = false);
 // rg_godunov_level with its dt read by the device from dt_dev
-int godunov_level_device_dt(rg_ctx* c, int ilevel, const double* dt_dev, double dx);
+// set_uold: HydroSolver::set_uold of the level folded into the fold kernels
+int godunov_level_device_dt(rg_ctx* c, int ilevel, const double* dt_dev, double dx, bool set_uold = false);
 int launch_set_dt_host(rg_ctx* c, double dt, double dx);
 int launch_finalize_dt(rg_ctx* c, double dx);
-int launch_godunov(rg_ctx* c, const Plan& p);
+int launch_godunov(rg_ctx* c, const Plan& p, bool set_uold = false);
 // the four events a level step records its kernel boundaries into: the
 // context's last-call set, or in accumulating mode the next set of the pool
 cudaEvent_t* step_events(rg_ctx* c, long long ncells);

@@ -633,4 +633,40 @@ int level_oct_list(rg_ctx* c, int ilevel, int* out, int cap, int* noct) {
     return RG_OK;
 }
 
+int level_octs_cached(rg_ctx* c, int ilevel, const int** octs, int* noct) {
+    *octs = nullptr;
+    *noct = 0;
+    if (ilevel < 1 || ilevel > c->nlevelmax) return set_error(c, RG_ERR_ARG, "level outside 1..nlevelmax");
+    if (!c->tree_resident) return set_error(c, RG_ERR_STATE, "oct-list cache needs the device-resident tree");
+    if (c->lvl_octs.size() < (size_t)c->nlevelmax + 1) {
+        c->lvl_octs.resize((size_t)c->nlevelmax + 1, nullptr);
+        c->lvl_cap.resize((size_t)c->nlevelmax + 1, 0);
+        c->lvl_n.resize((size_t)c->nlevelmax + 1, 0);
+        c->lvl_ver.resize((size_t)c->nlevelmax + 1, -1);
+    }
+    const size_t L = (size_t)ilevel;
+    if (c->lvl_ver[L] == c->topo_version && !c->tree_dirty) {
+        *octs = c->lvl_octs[L];
+        *noct = c->lvl_n[L];
+        return RG_OK;
+    }
+    const int n = c->h_numbl[L * (c->ncpu + c->nboundary)];
+    if (n > c->lvl_cap[L]) {
+        dev_free(c, c->lvl_octs[L]);
+        c->lvl_octs[L] = nullptr;
+        c->lvl_cap[L] = 0;
+        const int cap = (n + 1023) / 1024 * 1024;
+        if (int rc = check_cuda(c, dev_alloc(c, &c->lvl_octs[L], sizeof(int) * (size_t)cap), "level oct list"))
+            return rc;
+        c->lvl_cap[L] = cap;
+    }
+    int got = 0;
+    if (int rc = level_oct_list(c, ilevel, c->lvl_octs[L], c->lvl_cap[L], &got)) return rc;
+    c->lvl_n[L] = got;
+    c->lvl_ver[L] = c->topo_version;
+    *octs = c->lvl_octs[L];
+    *noct = got;
+    return RG_OK;
+}
+
 }  // namespace rg

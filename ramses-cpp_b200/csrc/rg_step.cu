@@ -118,10 +118,13 @@ __device__ __forceinline__ double box_dtdx(const PlanView& P, int a) {
 // set_uold (uold <- unew) of its cells are folded in: a level target starts
 // from uold and its result is written to both arrays.  Coarser targets start
 // from unew as always.
+// uold_out != nullptr (a level with refined cells in an AMR step): set_uold
+// folded in -- every level target (all of the level's son == 0 cells, each
+// with at least its own update) also writes its result to uold_out.
 template <int NDIM, bool LEAF = false, bool FSUM = false>
 __global__ void k_fold(TreeView T, PlanView P, const double* __restrict__ flux, double* __restrict__ unew,
                        const DevStatus* __restrict__ st, double gamma, double* __restrict__ uold = nullptr,
-                       const double* __restrict__ fsum = nullptr) {
+                       const double* __restrict__ fsum = nullptr, double* __restrict__ uold_out = nullptr) {
     constexpr int NV = Dims<NDIM>::NV;
     const size_t ncell = (size_t)T.ncell;
     const int nc = P.ncells;
@@ -143,6 +146,9 @@ __global__ void k_fold(TreeView T, PlanView P, const double* __restrict__ flux, 
         if (from_old) {
 #pragma unroll
             for (int iv = 0; iv < NV; ++iv) uold[(size_t)iv * ncell + cell - 1] = u[iv];
+        } else if (uold_out && t < nc) {
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) uold_out[(size_t)iv * ncell + cell - 1] = u[iv];
         }
     }
 }
@@ -168,7 +174,8 @@ template <int NDIM, bool LEAF = false, bool FSUM = false>
 __global__ void __launch_bounds__(kLongThreads)
     k_fold_long(TreeView T, PlanView P, const int* __restrict__ tlong, int nlong, const double* __restrict__ flux,
                 double* __restrict__ unew, const DevStatus* __restrict__ st, double gamma,
-                double* __restrict__ uold = nullptr, const double* __restrict__ fsum = nullptr) {
+                double* __restrict__ uold = nullptr, const double* __restrict__ fsum = nullptr,
+                double* __restrict__ uold_out = nullptr) {
     constexpr int NV = Dims<NDIM>::NV, NS = Dims<NDIM>::NS, TTD = Dims<NDIM>::TTD;
     // per warp: the terms of one chunk, variable-major, rows padded so the
     // NV walking lanes read from different banks
@@ -264,6 +271,9 @@ __global__ void __launch_bounds__(kLongThreads)
             if (from_old) {
 #pragma unroll
                 for (int iv = 0; iv < NV; ++iv) uold[(size_t)iv * ncell + cell - 1] = u[iv];
+            } else if (uold_out) {
+#pragma unroll
+                for (int iv = 0; iv < NV; ++iv) uold_out[(size_t)iv * ncell + cell - 1] = u[iv];
             }
         }
     }
@@ -272,11 +282,12 @@ __global__ void __launch_bounds__(kLongThreads)
 // k_fold_long over a plan's long targets (nothing when it has none)
 template <int NDIM, bool LEAF = false, bool FSUM = false>
 void launch_fold_long(rg_ctx* c, const Plan& P, const TreeView& T, const PlanView& V, const double* flux,
-                      double* unew, double gamma, double* uold = nullptr, const double* fsum = nullptr) {
+                      double* unew, double gamma, double* uold = nullptr, const double* fsum = nullptr,
+                      double* uold_out = nullptr) {
     if (P.nlong == 0) return;
     const int blocks = (int)std::min<long long>(((long long)P.nlong * 32 + kLongThreads - 1) / kLongThreads, 65535);
     k_fold_long<NDIM, LEAF, FSUM><<<blocks, kLongThreads, 0, c->stream>>>(T, V, P.tlong, P.nlong, flux, unew,
-                                                                          c->d_status, gamma, uold, fsum);
+                                                                          c->d_status, gamma, uold, fsum, uold_out);
 }
 
 // Leaf-level fold that also prepares the next substep: on a level whose
@@ -359,13 +370,20 @@ __global__ void k_copy_level(TreeView T, PlanView P, int nvar, const double* __r
     }
 }
 
+// unew_copy != nullptr: set_unew of the level in the same pass (every level
+// cell's uold copied into unew_copy, refined cells included, as
+// HydroSolver::set_unew does).
 template <int NDIM>
 __global__ void k_courant(TreeView T, PlanView P, const double* __restrict__ uold, DevStatus* st, double dx,
-                          double gamma, double cfl, int pressure_cap) {
+                          double gamma, double cfl, int pressure_cap, double* __restrict__ unew_copy) {
     const size_t ncell = (size_t)T.ncell;
     unsigned long long best = ~0ULL;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P.ncells; p += gridDim.x * blockDim.x) {
         int id = cell_of(T, P, p);
+        if (unew_copy) {
+#pragma unroll
+            for (int iv = 0; iv < NDIM + 2; ++iv) unew_copy[(size_t)iv * ncell + id - 1] = uold[(size_t)iv * ncell + id - 1];
+        }
         if (T.son[id - 1] > 0) continue;
         const double* u = uold + (id - 1);
         double d = smax(u[0], 1e-10), v2 = 0.0;
@@ -557,7 +575,7 @@ void launch_face_n(rg_ctx* c, const Plan& P, const StepK& K) {
 }
 
 template <int NDIM>
-int launch_godunov_t(rg_ctx* c, const Plan& P) {
+int launch_godunov_t(rg_ctx* c, const Plan& P, bool set_uold) {
     constexpr int NV = NDIM + 2, NS = 2 * NDIM;
     if (P.ncells == 0) return RG_OK;
     // the caller sized the shared flux scratch (ensure_flux) outside any capture:
@@ -574,9 +592,11 @@ int launch_godunov_t(rg_ctx* c, const Plan& P) {
     if (E) cudaEventRecord(E[1], c->stream);
     if (int rc = launch_face_tiles(c, P, K, c->d_uold, c->d_prim, c->d_flux, fsum)) return rc;
     if (E) cudaEventRecord(E[2], c->stream);
+    double* uold_out = set_uold ? c->d_uold : nullptr;
     k_fold<NDIM, false, true><<<grid_for(c, P.ntarg, 256), 256, 0, c->stream>>>(T, V, c->d_flux, c->d_unew,
-                                                                               c->d_status, K.gamma, nullptr, fsum);
-    launch_fold_long<NDIM, false, true>(c, P, T, V, c->d_flux, c->d_unew, K.gamma, nullptr, fsum);
+                                                                               c->d_status, K.gamma, nullptr, fsum,
+                                                                               uold_out);
+    launch_fold_long<NDIM, false, true>(c, P, T, V, c->d_flux, c->d_unew, K.gamma, nullptr, fsum, uold_out);
     if (E) cudaEventRecord(E[3], c->stream);
     return check_cuda(c, cudaGetLastError(), "godunov kernels");
 }
@@ -625,9 +645,9 @@ cudaEvent_t* step_events(rg_ctx* c, long long ncells) {
     return c->acc_ev[c->acc_n++].data();
 }
 
-int launch_godunov(rg_ctx* c, const Plan& P) {
-    if (c->params.ndim == 1) return launch_godunov_t<1>(c, P);
-    return launch_godunov_t<3>(c, P);
+int launch_godunov(rg_ctx* c, const Plan& P, bool set_uold) {
+    if (c->params.ndim == 1) return launch_godunov_t<1>(c, P, set_uold);
+    return launch_godunov_t<3>(c, P, set_uold);
 }
 
 int launch_godunov_ext(rg_ctx* c, const Plan& P, const double* uold, double* unew, double* prim, double* flux) {
@@ -727,18 +747,19 @@ int launch_set_uold(rg_ctx* c, const Plan& P) {
     return check_cuda(c, cudaGetLastError(), "set_uold");
 }
 
-int launch_courant(rg_ctx* c, const Plan& P, double dx, int pressure_cap, double cfl) {
+int launch_courant(rg_ctx* c, const Plan& P, double dx, int pressure_cap, double cfl, bool set_unew) {
     double start = c->params.boxlen / 1e-10;
     k_courant_init<<<1, 1, 0, c->stream>>>(c->d_status, start);
     if (P.ncells > 0) {
+        double* copy = set_unew ? c->d_unew : nullptr;
         if (c->params.ndim == 1)
             k_courant<1><<<grid_for(c, P.ncells, 256), 256, 0, c->stream>>>(tree_view(c), P.view(), c->d_uold,
                                                                              c->d_status, dx, c->params.gamma, cfl,
-                                                                             pressure_cap);
+                                                                             pressure_cap, copy);
         else
             k_courant<3><<<grid_for(c, P.ncells, 256), 256, 0, c->stream>>>(tree_view(c), P.view(), c->d_uold,
                                                                              c->d_status, dx, c->params.gamma, cfl,
-                                                                             pressure_cap);
+                                                                             pressure_cap, copy);
     }
     return check_cuda(c, cudaGetLastError(), "courant");
 }

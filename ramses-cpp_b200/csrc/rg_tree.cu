@@ -524,6 +524,23 @@ __global__ void k_kill_mark(TreeMut M, const int* __restrict__ octs, int noct, i
     }
 }
 
+// any make_grid_fine or remove_grid_fine candidate among a level's octs:
+// k_refine_mark's and k_kill_mark's tests, without writing marks
+__global__ void k_change_probe(TreeMut M, const int* __restrict__ octs, int noct, int* any) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < noct; k += gridDim.x * blockDim.x) {
+        const int ig = octs[k];
+        bool hit = false, refined_child = false;
+        for (int s = 0; s < 8; ++s) {
+            const int idc = M.ncoarse + s * M.ngridmax + ig - 1;
+            if (M.son[idc] > 0) refined_child = true;
+            else if (M.flag1[idc] == 1 && M.flag2[idc] == 1) hit = true;
+        }
+        const int fc = M.father[ig - 1];
+        if (fc > 0 && M.flag1[fc - 1] == 0 && !refined_child) hit = true;
+        if (hit) atomicExch(any, 1);
+    }
+}
+
 // unlink and free the marked octs (TreeUpdater.cpp:164-181, free_grid
 // AmrGrid.cpp:270-287): compacted kept list, freed ids in list order, the
 // freed ids appended to the free-list ring
@@ -799,8 +816,10 @@ int tree_flag_fine(rg_ctx* c, int ilevel, double ed, double ep, double ev, doubl
     TreeScratch S;
     if (int rc = tree_scratch(c, &S)) return rc;
     int noct = 0;
-    if (int rc = level_oct_list(c, ilevel, S.octs, c->ngridmax, &noct)) return rc;
+    const int* octs = nullptr;
+    if (int rc = level_octs_cached(c, ilevel, &octs, &noct)) return rc;
     if (noct == 0) return RG_OK;
+    S.octs = const_cast<int*>(octs);  // read only below
     const int n = 8 * noct;
     auto smooth = [&]() {
         k_smooth_mark<<<nblk(n), TPB, 0, s>>>(M, S.octs, noct, S.mark);
@@ -841,8 +860,10 @@ int tree_make_grid_fine(rg_ctx* c, int ilevel) {
         return RG_OK;
     }
     int noct = 0;
-    if (int rc = level_oct_list(c, ilevel, S.octs, c->ngridmax, &noct)) return rc;
+    const int* octs = nullptr;
+    if (int rc = level_octs_cached(c, ilevel, &octs, &noct)) return rc;
     if (noct == 0) return check_cuda(c, cudaStreamSynchronize(s), "authorize");
+    S.octs = const_cast<int*>(octs);  // read only below
     const int n8 = 8 * noct;
     k_refine_mark<<<nblk(n8), TPB, 0, s>>>(M, S.octs, noct, S.mark);
     int n = 0;
@@ -882,8 +903,10 @@ int tree_remove_grid_fine(rg_ctx* c, int ilevel) {
     TreeScratch S;
     if (int rc = tree_scratch(c, &S)) return rc;
     int noct = 0;
-    if (int rc = level_oct_list(c, ilevel, S.octs, c->ngridmax, &noct)) return rc;
+    const int* octs = nullptr;
+    if (int rc = level_octs_cached(c, ilevel, &octs, &noct)) return rc;
     if (noct == 0) return RG_OK;
+    S.octs = const_cast<int*>(octs);  // read only below
     TreeMut M = tree_mut(c);
     cudaStream_t s = c->stream;
     k_kill_mark<<<nblk(noct), TPB, 0, s>>>(M, S.octs, noct, S.mark);
@@ -915,6 +938,40 @@ int tree_remove_grid_fine(rg_ctx* c, int ilevel) {
     return check_device_status(c);
 }
 
+int tree_changes_pending(rg_ctx* c, int lo, int hi, bool* pending) {
+    *pending = true;
+    if (!c->tree_resident) return set_error(c, RG_ERR_STATE, "no device-resident tree: call rg_tree_attach first");
+    hi = std::min(hi, c->nlevelmax - 1);  // both operations are no-ops at and above nlevelmax
+    if (lo < 2 || lo > hi) {              // level 1 (coarse cells) keeps its own path
+        *pending = lo <= hi;
+        return RG_OK;
+    }
+    c->next_level = -1;
+    if (int rc = refresh_tree(c)) return rc;
+    TreeScratch S;
+    if (int rc = tree_scratch(c, &S)) return rc;
+    cudaStream_t s = c->stream;
+    TreeMut M = tree_mut(c);
+    if (c->auth_dirty) {  // what the first make_grid_fine of the range does first
+        k_authorize<<<nblk(c->ncell), TPB, 0, s>>>(M);
+        c->auth_dirty = false;
+    }
+    int* d_any = S.list;
+    cudaMemsetAsync(d_any, 0, sizeof(int), s);
+    for (int L = lo; L <= hi; ++L) {
+        const int* octs = nullptr;
+        int noct = 0;
+        if (int rc = level_octs_cached(c, L, &octs, &noct)) return rc;
+        if (noct > 0) k_change_probe<<<nblk(noct), TPB, 0, s>>>(M, octs, noct, d_any);
+    }
+    int any = 1;
+    if (int rc = check_cuda(c, cudaMemcpyAsync(&any, d_any, sizeof(int), cudaMemcpyDeviceToHost, s), "change probe"))
+        return rc;
+    if (int rc = check_cuda(c, cudaStreamSynchronize(s), "change probe")) return rc;
+    *pending = any != 0;
+    return RG_OK;
+}
+
 int tree_restrict_fine(rg_ctx* c, int ilevel) {
     // restrict_fine(ilevel) reads level ilevel + 1; the reference walks an
     // empty list when ilevel + 1 > nlevelmax
@@ -926,8 +983,10 @@ int tree_restrict_fine(rg_ctx* c, int ilevel) {
     TreeScratch S;
     if (int rc = tree_scratch(c, &S)) return rc;
     int noct = 0;
-    if (int rc = level_oct_list(c, ilevel + 1, S.octs, c->ngridmax, &noct)) return rc;
+    const int* octs = nullptr;
+    if (int rc = level_octs_cached(c, ilevel + 1, &octs, &noct)) return rc;
     if (noct == 0) return RG_OK;
+    S.octs = const_cast<int*>(octs);  // read only below
     k_restrict<<<nblk(noct), TPB, 0, c->stream>>>(tree_mut(c), S.octs, noct);
     return check_cuda(c, cudaGetLastError(), "restrict_fine kernel");
 }
