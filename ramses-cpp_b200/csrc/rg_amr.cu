@@ -62,6 +62,79 @@ int count_grids(const rg_ctx* c, int il) {
 
 int nsubcycle(const rg_amr_config& cfg, int il) { return il >= cfg.levelmin ? 2 : 1; }
 
+// Segments of a level step as CUDA graphs.  Between tree changes a level
+// step issues the same kernels with the same arguments every time: the CFL
+// pass with set_unew and the clock update before the finer sub-steps, and
+// after them the level step proper (dt, primitives, face, fold with
+// set_uold), restrict_fine and flag_fine; on a level without finer octs both
+// halves and the time update form one segment.  A segment runs eagerly the
+// first time at a topology version (which warms every cache it touches: the
+// plan, the autotuned face shape, the flux scratch size, the level oct
+// lists), is captured the second time, and is replayed from then on until the
+// tree changes (the topology version moves) or a scratch buffer it names is
+// reallocated.  Captured segments call nothing that waits or allocates; if a
+// capture fails anyway the segment stays eager for that topology version.
+bool segment_ok(rg_ctx* c, int il) {
+    if (!c->amr_graphs_on || c->timing || c->tree_dirty || !c->d_tscr) return false;
+    Plan* P = existing_plan(c, il);
+    if (!P || P->face_variant < 0) return false;
+    const size_t need = (size_t)(2 * c->params.ndim + 1) * (c->params.ndim + 2) * (size_t)P->ncells;
+    if (P->ncells > 0 && (c->cap_flux < need || !c->d_flux)) return false;
+    // the finer level's oct list, which restrict_fine and flag_fine read
+    const int L = il + 1;
+    if (L <= c->nlevelmax && count_grids(c, L) > 0)
+        if ((int)c->lvl_ver.size() <= L || c->lvl_ver[(size_t)L] != c->topo_version) return false;
+    return true;
+}
+
+template <class F>
+int run_segment(rg_ctx* c, int key, bool ok, F&& body) {
+    SegGraph& g = c->amr_graphs[key];
+    const long long v = c->topo_version;
+    if (ok && g.exec && g.topo == v && g.flux == c->d_flux && g.tscr == c->d_tscr) {
+        ++c->amr_replayed;
+        return check_cuda(c, cudaGraphLaunch(g.exec, c->stream), "level-step graph");
+    }
+    if (!ok || g.warm != v || g.failed == v) {
+        const int rc = body();
+        if (rc == RG_OK && ok) g.warm = v;
+        return rc;
+    }
+    if (g.exec) {
+        cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+    }
+    const void* flux = c->d_flux;
+    const void* tscr = c->d_tscr;
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        g.failed = v;
+        return body();
+    }
+    const int rc = body();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    cudaGraphExec_t exec = nullptr;
+    bool good = rc == RG_OK && e == cudaSuccess && graph != nullptr &&
+                cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    if (!good || flux != c->d_flux || tscr != c->d_tscr) {
+        // nothing of the captured work ran: run it eagerly
+        cudaGetLastError();
+        if (exec) cudaGraphExecDestroy(exec);
+        g.failed = v;
+        return body();
+    }
+    g.exec = exec;
+    g.topo = v;
+    g.flux = flux;
+    g.tscr = tscr;
+    ++c->amr_captured;
+    return check_cuda(c, cudaGraphLaunch(exec, c->stream), "level-step graph");
+}
+
+int seg_key(int il, int kind, int icount) { return (il * 4 + kind) * 4 + (icount & 3); }
+
 int amr_step(rg_ctx* c, const rg_amr_config& cfg, AmrRunState& S, int il, int icount) {
     const int lmin = cfg.levelmin, lmax = c->nlevelmax;
     if (il > lmax) return RG_OK;
@@ -80,35 +153,50 @@ int amr_step(rg_ctx* c, const rg_amr_config& cfg, AmrRunState& S, int il, int ic
         }
     }
     const double dx = cfg.boxlen / (double)(c->nx * (1 << il));
-    // the CFL pass also does set_unew (both read the level's uold, nothing
-    // between them writes it; k_amr_dt only reads the CFL word)
-    if (int rc = courant_step_device(c, il, dx, cfg.courant_factor, cfg.pressure_cap, true)) return rc;
-    k_amr_dt<<<1, 1, 0, c->stream>>>(S.ck, c->d_status, il, il > lmin ? nsubcycle(cfg, il - 1) : 0);
     const int nsub = nsubcycle(cfg, il);
-    if (il < lmax) {
-        if (count_grids(c, il + 1) > 0) {
-            for (int i = 1; i <= nsub; ++i)
-                if (int rc = amr_step(c, cfg, S, il + 1, i)) return rc;
-        } else {
-            k_amr_no_finer<<<1, 1, 0, c->stream>>>(S.ck, il, nsub);
-            S.nstep++;
+    const bool finer = il < lmax && count_grids(c, il + 1) > 0;
+    double* ck = S.ck;
+    // before the finer sub-steps: the CFL pass, which also does set_unew (both
+    // read the level's uold, nothing between them writes it; k_amr_dt only
+    // reads the CFL word), and the level's new dt
+    auto pre = [&]() -> int {
+        if (int rc = courant_step_device(c, il, dx, cfg.courant_factor, cfg.pressure_cap, true)) return rc;
+        k_amr_dt<<<1, 1, 0, c->stream>>>(ck, c->d_status, il, il > lmin ? nsubcycle(cfg, il - 1) : 0);
+        if (!finer) {
+            if (il < lmax) k_amr_no_finer<<<1, 1, 0, c->stream>>>(ck, il, nsub);
+            else k_amr_advance<<<1, 1, 0, c->stream>>>(ck, il);
         }
-    } else {
-        k_amr_advance<<<1, 1, 0, c->stream>>>(S.ck, il);
+        return check_cuda(c, cudaGetLastError(), "clock kernels");
+    };
+    // after them: the level step with set_uold folded into the fold kernels (a
+    // level target's result goes to uold as well; the fold reads only unew and
+    // the flux scratch), restrict_fine, flag_fine of the next finer level.
+    // This level's dtnew is still the one set above: the finer steps only
+    // change the finer levels' entries.
+    auto post = [&]() -> int {
+        if (int rc = godunov_level_device_dt(c, il, ck + il, dx, true)) return rc;
+        if (Plan* P = existing_plan(c, il); P == nullptr || P->ncells == 0)
+            if (int rc = rg_set_uold(c, il)) return rc;
+        if (il < lmax)
+            if (int rc = tree_restrict_fine(c, il)) return rc;
+        return tree_flag_fine(c, il + 1, cfg.err_grad_d, cfg.err_grad_p, cfg.err_grad_u, -1.0, cfg.nexpand, icount,
+                              il > 0 ? nsubcycle(cfg, il - 1) : 1);
+    };
+    if (!finer) {
+        if (int rc = run_segment(c, seg_key(il, 2, icount), segment_ok(c, il), [&]() -> int {
+                if (int rc = pre()) return rc;
+                return post();
+            }))
+            return rc;
         S.nstep++;
+    } else {
+        if (int rc = run_segment(c, seg_key(il, 0, icount), segment_ok(c, il), pre)) return rc;
+        for (int i = 1; i <= nsub; ++i)
+            if (int rc = amr_step(c, cfg, S, il + 1, i)) return rc;
+        if (int rc = run_segment(c, seg_key(il, 1, icount), segment_ok(c, il), post)) return rc;
     }
-    // this level's dtnew is still the one set above: the finer steps only
-    // change the finer levels' entries
-    // set_uold folded into the fold kernels: a level target's result goes to
-    // uold as well (the fold reads only unew and the flux scratch)
-    if (int rc = godunov_level_device_dt(c, il, S.ck + il, dx, true)) return rc;
     S.cell_updates += rg_level_cell_updates(c, il);
-    if (rg::existing_plan(c, il) == nullptr || rg::existing_plan(c, il)->ncells == 0)
-        if (int rc = rg_set_uold(c, il)) return rc;
-    if (il < lmax)
-        if (int rc = tree_restrict_fine(c, il)) return rc;
-    return tree_flag_fine(c, il + 1, cfg.err_grad_d, cfg.err_grad_p, cfg.err_grad_u, -1.0, cfg.nexpand, icount,
-                          il > 0 ? nsubcycle(cfg, il - 1) : 1);
+    return RG_OK;
 }
 
 int coarse_step(rg_ctx* c, const rg_amr_config& cfgr, AmrRunState& S) {
@@ -132,6 +220,14 @@ int coarse_step(rg_ctx* c, const rg_amr_config& cfgr, AmrRunState& S) {
 
 using namespace rg;
 
+extern "C" int rg_amr_graphs(rg_ctx* c, int on, int64_t* captured, int64_t* replayed) {
+    if (!c) return RG_ERR_ARG;
+    if (on >= 0) c->amr_graphs_on = on != 0;
+    if (captured) *captured = c->amr_captured;
+    if (replayed) *replayed = c->amr_replayed;
+    return RG_OK;
+}
+
 extern "C" int rg_amr_coarse_step(rg_ctx* c, const rg_amr_config* cfg, rg_amr_clock* clock) {
     if (!c) return RG_ERR_ARG;
     if (c->broken) return set_error(c, RG_ERR_CUDA, c->err.empty() ? "context unusable after a device fault" : c->err);
@@ -141,16 +237,17 @@ extern "C" int rg_amr_coarse_step(rg_ctx* c, const rg_amr_config* cfg, rg_amr_cl
     if (cfg->levelmin < 1 || cfg->levelmin > c->nlevelmax) return set_error(c, RG_ERR_ARG, "levelmin outside 1..nlevelmax");
     if (!(cfg->boxlen > 0.0)) return set_error(c, RG_ERR_ARG, "boxlen must be positive");
     cudaSetDevice(c->device);
+    c->next_level = -1;  // replayed level steps skip that host bookkeeping
     AmrRunState S;
     double h[kClockN];
     std::copy(clock->dtnew, clock->dtnew + kMaxLevel + 1, h);
     std::copy(clock->dtold, clock->dtold + kMaxLevel + 1, h + kDtOld);
     h[kClockT] = clock->t;
-    if (int rc = check_cuda(c, dev_alloc(c, &S.ck, sizeof(h)), "coarse-step clock")) return rc;
-    if (int rc = check_cuda(c, cudaMemcpyAsync(S.ck, h, sizeof(h), cudaMemcpyHostToDevice, c->stream), "clock upload")) {
-        dev_free(c, S.ck);
+    if (!c->d_clock)  // kept for the context's lifetime: captured level steps name it
+        if (int rc = check_cuda(c, dev_alloc(c, &c->d_clock, sizeof(h)), "coarse-step clock")) return rc;
+    S.ck = c->d_clock;
+    if (int rc = check_cuda(c, cudaMemcpyAsync(S.ck, h, sizeof(h), cudaMemcpyHostToDevice, c->stream), "clock upload"))
         return rc;
-    }
     S.nstep = clock->nstep;
     S.cell_updates = clock->cell_updates;
     const int rc_step = coarse_step(c, *cfg, S);
@@ -158,7 +255,6 @@ extern "C" int rg_amr_coarse_step(rg_ctx* c, const rg_amr_config* cfg, rg_amr_cl
     // the caller's clock is left as it was
     const int rc_copy = check_cuda(c, cudaMemcpyAsync(h, S.ck, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "clock");
     const int rc_sync = check_cuda(c, cudaStreamSynchronize(c->stream), "coarse step");
-    dev_free(c, S.ck);
     if (rc_step) return rc_step;
     if (rc_copy) return rc_copy;
     if (rc_sync) return rc_sync;

@@ -279,6 +279,8 @@ rg_ctx* rg_create(const rg_params* params, int device) {
     for (auto& e : c->ev) cudaEventCreate(&e);
     const char* t = getenv("RG_TIMING");
     c->timing = t && t[0] == '1';
+    const char* g = getenv("RG_AMR_GRAPHS");
+    c->amr_graphs_on = !(g && g[0] == '0');
     return c;
 }
 
@@ -305,6 +307,9 @@ void rg_destroy(rg_ctx* c) {
     for (int* p : tp) dev_free(c, p);
     dev_free(c, c->d_xg);
     for (int* p : c->lvl_octs) dev_free(c, p);
+    for (auto& kv : c->amr_graphs)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    dev_free(c, c->d_clock);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->pool) cudaMemPoolDestroy(c->pool);
     if (c->h_status) cudaFreeHost(c->h_status);

@@ -26,6 +26,7 @@
 #include <stdint.h>
 
 #include <array>
+#include <map>
 #include <string>
 #include <utility>
 #include <vector>
@@ -154,6 +155,15 @@ struct TunedShape {
     float ms = 0.f;
 };
 
+// A captured segment of a level step of the resident AMR step (rg_amr.cu),
+// valid for the topology version and scratch buffers it was captured with.
+struct SegGraph {
+    cudaGraphExec_t exec = nullptr;
+    long long topo = -1, warm = -1, failed = -1;
+    const void* flux = nullptr;
+    const void* tscr = nullptr;
+};
+
 struct Tuning {
     int face_block = 128;
     int face_blocks_per_sm = 0;  // 0 = plain grid covering all work
@@ -243,6 +253,12 @@ struct rg_ctx {
     std::vector<int*> lvl_octs;
     std::vector<int> lvl_cap, lvl_n;
     std::vector<long long> lvl_ver;
+    // rg_amr_coarse_step: the clock buffer (kept so captured graphs can name
+    // it) and the level-step graphs, replayed while the topology is unchanged
+    double* d_clock = nullptr;
+    std::map<int, rg::SegGraph> amr_graphs;
+    bool amr_graphs_on = true;
+    long long amr_captured = 0, amr_replayed = 0;
     bool tree_dirty = false;  // links changed on the device: ranks, cell levels and plans are stale
     // authorize_fine (flag2 = cpu_map == myid over every cell) has an effect:
     // false while flag2 == (cpu_map == 1) holds everywhere, which only

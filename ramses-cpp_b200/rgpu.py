@@ -177,6 +177,7 @@ def lib():
     L.rg_tree_sizes.argtypes = [VP, IP, IP]
     L.rg_level_plan_info.argtypes = [VP, C.c_int, C.POINTER(rg_plan_info)]
     L.rg_amr_coarse_step.argtypes = [VP, C.POINTER(rg_amr_config), C.POINTER(rg_amr_clock)]
+    L.rg_amr_graphs.argtypes = [VP, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.rg_measure_fp64_peak.argtypes = [VP, C.POINTER(C.c_double)]
     L.rg_level_run.argtypes = [VP, C.c_int, C.c_double, C.c_int, C.c_double, C.c_double, C.c_int64,
                                C.POINTER(C.c_double), C.POINTER(C.c_int64)]
@@ -280,6 +281,13 @@ class Context:
     def amr_coarse_step(self, cfg, clock):
         """rg_amr_coarse_step: one coarse step of the resident run (clock updated in place)."""
         self._chk(self.L.rg_amr_coarse_step(self.h, C.byref(cfg), C.byref(clock)))
+
+    def amr_graphs(self, on=None):
+        """Switch the coarse step's level-step graphs (on=True/False) and return
+        (captured, replayed) segment counts."""
+        cap, rep = C.c_int64(0), C.c_int64(0)
+        self._chk(self.L.rg_amr_graphs(self.h, -1 if on is None else (1 if on else 0), C.byref(cap), C.byref(rep)))
+        return cap.value, rep.value
 
     def level_run(self, il, dx, t_end, t_start=0.0, pressure_cap=False, max_steps=10**7):
         """rg_level_run: substeps until t >= t_end in one graph launch; returns (t, steps)."""

@@ -3,7 +3,8 @@
 CPU: the merge keeps every box closed (ids point inside the box) and the
 oracle's level step over the forest's leaf list, with one dt for all boxes,
 equals bit for bit the oracle's step of each box alone; the sharding over
-ranks covers every box once (gloo, world size 2).
+ranks covers every box once, and two gloo ranks stepping their shards after a
+min-reduction of the CFL step give the one-rank forest's bits (world size 2).
 GPU: one substep sequence over a mixed ensemble (edges 16, 24, 32; nx = 1
 and 3) through rg_set_level_boxes equals, per box, the oracle run of that box
 alone with its own CFL step: same dt bits, same state bits.
@@ -144,6 +145,77 @@ def test_sharding_covers_every_box_once_gloo(tmp_path):
     assert np.all(cover == 1)
     assert abs(int(loads[0]) - int(loads[1])) <= 64 ** 3
     assert loads.sum() == sum(s.cells for s in ens.box_specs(512))
+
+
+def _step_forest(f, dt, steps):
+    """`steps` oracle level steps of a same-dx forest with one dt; the level
+    state of each box (box index -> array) afterwards."""
+    orc = Oracle()
+    params = make_params(3, slope_type=2, riemann="hllc", gamma=f.gamma)
+    ga = ga_of(f.grid)
+    dx = float(f.dx[0])
+    uold = f.initial_state()
+    unew = uold.copy()
+    for _ in range(steps):
+        orc.set_unew(ga, 3, 5, f.level, uold, unew)
+        orc.godunov_fine(ga, params, f.level, dt, dx, uold, unew)
+        orc.set_uold(ga, 3, 5, f.level, uold, unew)
+    return {s.index: f.extract(uold, i) for i, s in enumerate(f.specs)}
+
+
+def _forest_dt(f):
+    orc = Oracle()
+    dx = float(f.dx[0])
+    return min(orc.courant(ga_of(b), 3, 5, s.level, dx, f.gamma, 0.8, f.box_state(i), pressure_cap=False)
+               for i, (s, b) in enumerate(zip(f.specs, f.boxes)))
+
+
+def _sharded_step_worker(rank, world, port, out_dir, idx):
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    specs = [s for s in ens.box_specs(64, seed=7) if s.index in idx]
+    mine = ens.Forest(ens.shard_boxes(specs, world)[rank])
+    # the one exchange of the step: the CFL step, min over every rank's boxes
+    dt = torch.tensor([_forest_dt(mine)], dtype=torch.float64)
+    dist.all_reduce(dt, op=dist.ReduceOp.MIN)
+    res = _step_forest(mine, float(dt.item()), 2)
+    gathered = [None] * world
+    dist.all_gather_object(gathered, res)
+    if rank == 0:
+        merged = {}
+        for part in gathered:
+            assert not set(part) & set(merged), "a box was stepped on two ranks"
+            merged.update(part)
+        np.savez(os.path.join(out_dir, "sharded.npz"), dt=float(dt.item()),
+                 **{f"b{k}": v for k, v in merged.items()})
+    dist.destroy_process_group()
+
+
+def test_sharded_forest_steps_equal_the_one_rank_forest_gloo(tmp_path):
+    """Boxes partitioned over two gloo ranks: each rank steps its shard with the
+    oracle after a min-reduction of the CFL step over the ranks; the boxes
+    gathered on rank 0 equal, bit for bit, the same boxes stepped as one forest
+    on one rank, and the reduced dt equals the one-rank forest's."""
+    import socket
+
+    import torch.multiprocessing as mp
+    pool = ens.box_specs(64, seed=7)
+    idx = [s.index for s in pool if s.edge == 16][:6]  # same dx: the oracle takes one dx per level step
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    mp.start_processes(_sharded_step_worker, args=(2, port, str(tmp_path), idx), nprocs=2, join=True,
+                       start_method="spawn")
+    got = np.load(tmp_path / "sharded.npz")
+    whole = ens.Forest([s for s in pool if s.index in idx])
+    dt = _forest_dt(whole)
+    assert float(got["dt"]) == dt
+    want = _step_forest(whole, dt, 2)
+    assert sorted(int(k[1:]) for k in got.files if k.startswith("b")) == sorted(want)
+    for k, v in want.items():
+        assert bits_equal(got[f"b{k}"], v), k
 
 
 @pytest.mark.gpu

@@ -206,3 +206,31 @@ def test_device_initialisation_matches_reference(rgpu_lib, lmin, lmax, ngm):
     finally:
         ctx.close()
         h.close()
+
+
+@pytest.mark.parametrize("graphs", [True, False])
+def test_replayed_level_steps_match_reference(rgpu_lib, graphs):
+    """Twelve coarse steps at Courant 0.25 (the tree settles, so the native
+    step captures its level steps as graphs and replays them between tree
+    changes) against the reference after every step; and the same with the
+    graphs switched off."""
+    nml = namelist(slope_type=2, riemann="hllc", levelmin=LMIN, levelmax=LMAX, err_grad_d=ED, err_grad_p=EP)
+    h = RefHarness(3).create(nml, ngridmax=30000, levelmin=LMIN, nlevelmax=LMAX, gamma=GAMMA)
+    r = AmrRun(h, LMIN, LMAX, GAMMA, cfl=0.25, ed=ED, ep=EP)
+    r.initialize(sedov_ic(3, LMIN))
+    ctx = device_ctx(h)
+    try:
+        ctx.amr_graphs(graphs)
+        d = DeviceAmrRun(ctx, nx=1, levelmin=LMIN, nlevelmax=LMAX, cfl=0.25, ed=ED, ep=EP)
+        for step in range(12):
+            r.coarse_step()
+            d.coarse_step()
+            assert_same_tree(h, ctx, f"coarse step {step}")
+            assert d.t == r.t and d.cell_updates == r.cell_updates
+        captured, replayed = ctx.amr_graphs()
+        if graphs:
+            assert captured > 0 and replayed > captured, (captured, replayed)
+        else:
+            assert captured == 0 and replayed == 0
+    finally:
+        ctx.close()
