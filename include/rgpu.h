@@ -221,6 +221,19 @@ int rg_mlp_grad(rg_ctx* ctx, int n, const float* x, const float* t, float* grad,
  * the reference leaves it.  uold/unew: host arrays of nvar*ncell doubles in
  * AmrGrid's layout.  Synchronises the context stream before returning. */
 int rg_godunov_level_host(rg_ctx* ctx, int ilevel, double dt, double dx, const double* uold, double* unew);
+/* Level-wise transfers for a host application that keeps the state resident
+ * on the device between its hydro calls and touches it on the host in between
+ * (the reference's TreeUpdater reads uold, restrict_fine writes the refined
+ * cells' uold, make_grid_fine writes the new cells' uold and unew; none reads
+ * unew).  rg_upload_level: the cells a level step of ilevel reads -- the
+ * level's cells, refined ones included, and the coarser cells of its ghost
+ * stencils -- from host uold (nvar*ncell doubles, AmrGrid's layout).
+ * rg_download_level: every cell of the level from the device uold and unew
+ * into host arrays (either may be null); synchronises.  No reference
+ * counterpart: they replace the host-resident vectors of AmrGrid.hpp:104-107
+ * around HydroSolver::set_unew / set_uold (HydroSolver.cpp:575-611). */
+int rg_upload_level(rg_ctx* ctx, int ilevel, const double* uold);
+int rg_download_level(rg_ctx* ctx, int ilevel, double* uold, double* unew);
 
 /* Snapshot records of level ilevel from the device state, as
  * RamsesWriter::write_hydro (src/io/RamsesWriter.cpp:145-226) writes them:

@@ -1123,6 +1123,26 @@ int rg_last_kernel_ms(rg_ctx* c, float* out, int n) {
     return c->timing ? RG_OK : set_error(c, RG_ERR_STATE, "timing disabled (set RG_TIMING=1)");
 }
 
+int rg_upload_level(rg_ctx* c, int ilevel, const double* uold) {
+    CTX_GUARD(c);
+    c->next_level = -1;  // the state changes
+    if (!uold) return set_error(c, RG_ERR_ARG, "uold must be a host array of nvar*ncell doubles");
+    if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state uploaded (rg_upload_state first)");
+    Plan* P;
+    if (int rc = get_plan(c, ilevel, &P)) return rc;
+    if (P->ncells == 0) return RG_OK;
+    return upload_level_host(c, *P, uold, nullptr);
+}
+
+int rg_download_level(rg_ctx* c, int ilevel, double* uold, double* unew) {
+    CTX_GUARD(c);
+    if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state uploaded (rg_upload_state first)");
+    Plan* P;
+    if (int rc = get_plan(c, ilevel, &P)) return rc;
+    if (int rc = download_level_cells(c, *P, uold, unew)) return rc;
+    return check_device_status(c);
+}
+
 int rg_pool_usage(rg_ctx* c, uint64_t* reserved, uint64_t* used) {
     CTX_GUARD(c);
     if (!reserved || !used) return set_error(c, RG_ERR_ARG, "reserved and used must be non-null");

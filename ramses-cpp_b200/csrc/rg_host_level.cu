@@ -64,6 +64,18 @@ __global__ void k_scatter_level(const int* __restrict__ read_ids, int nread, con
     }
 }
 
+// ids[0..n) of two state arrays (b may be null) into stage [2][nvar][n]
+__global__ void k_gather_ids2(const int* __restrict__ ids, int n, int nvar, size_t ncell, const double* __restrict__ a,
+                              const double* __restrict__ b, double* stage) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const size_t id = (size_t)ids[t] - 1;
+        for (int iv = 0; iv < nvar; ++iv) {
+            if (a) stage[(size_t)iv * n + t] = a[iv * ncell + id];
+            if (b) stage[((size_t)nvar + iv) * n + t] = b[iv * ncell + id];
+        }
+    }
+}
+
 __global__ void k_gather_targets(const int* __restrict__ targ_ids, int ntarg, int nvar, size_t ncell,
                                   const double* __restrict__ unew, double* stage) {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntarg; t += gridDim.x * blockDim.x) {
@@ -132,6 +144,8 @@ int level_ids(rg_ctx* c, Plan& P) {
     };
     P.read_runs = runs(P.h_read);
     P.targ_runs = runs(P.h_targ);
+    P.h_cells.assign(P.h_read.begin(), P.h_read.begin() + P.ncells);
+    P.cell_runs = runs(P.h_cells);
     P.ids_ready = true;
     return RG_OK;
 }
@@ -255,6 +269,32 @@ int download_level_host(rg_ctx* c, Plan& P, double* unew, const double* src_dev)
         return rc;
     if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "level download sync")) return rc;
     scatter_host(P.h_targ, P.targ_runs, c->h_stage, ncell, nv, unew);
+    return RG_OK;
+}
+
+int download_level_cells(rg_ctx* c, Plan& P, double* uold, double* unew) {
+    if (int rc = level_ids(c, P)) return rc;
+    const int n = P.ncells;
+    if (n == 0 || (!uold && !unew)) return check_cuda(c, cudaStreamSynchronize(c->stream), "level download sync");
+    if (P.cell_runs.size() <= kMaxRuns && (!uold || state_pinned(c, uold)) && (!unew || state_pinned(c, unew))) {
+        if (uold)
+            if (int rc = copy_runs(c, P.cell_runs, uold, c->d_uold, cudaMemcpyDeviceToHost)) return rc;
+        if (unew)
+            if (int rc = copy_runs(c, P.cell_runs, unew, c->d_unew, cudaMemcpyDeviceToHost)) return rc;
+        return check_cuda(c, cudaStreamSynchronize(c->stream), "level download sync");
+    }
+    const int nv = c->nvar;
+    const size_t ncell = (size_t)c->ncell, m = (size_t)nv * n;
+    if (int rc = grow_stage(c, 2 * m)) return rc;
+    k_gather_ids2<<<blocks(c, n), 256, 0, c->stream>>>(P.read_ids, n, nv, ncell, uold ? c->d_uold : nullptr,
+                                                       unew ? c->d_unew : nullptr, c->d_stage);
+    if (int rc = check_cuda(c, cudaMemcpyAsync(c->h_stage, c->d_stage, 2 * m * sizeof(double), cudaMemcpyDeviceToHost,
+                                               c->stream),
+                            "level download"))
+        return rc;
+    if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "level download sync")) return rc;
+    if (uold) scatter_host(P.h_cells, P.cell_runs, c->h_stage, ncell, nv, uold);
+    if (unew) scatter_host(P.h_cells, P.cell_runs, c->h_stage + m, ncell, nv, unew);
     return RG_OK;
 }
 

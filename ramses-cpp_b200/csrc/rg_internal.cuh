@@ -130,9 +130,10 @@ struct Plan {
     int* read_ids = nullptr;   // [ncells + nextra_prim] then targ_ids [ntarg] (one allocation)
     int* targ_ids = nullptr;
     std::vector<int> h_read, h_targ;
+    std::vector<int> h_cells;  // the level's own cells (the first ncells read ids)
     // the same cells as runs of consecutive cell ids (first id, count): few on
     // a uniform level (one per child slot), so transfers are plain copies
-    std::vector<std::pair<int, int>> read_runs, targ_runs;
+    std::vector<std::pair<int, int>> read_runs, targ_runs, cell_runs;
     // targets with more than kLongEvents updates (coarse cells taking the
     // refluxes of many finer faces), folded one warp each by k_fold_long and
     // skipped by k_fold
@@ -354,6 +355,9 @@ int set_box_lattices(rg_ctx* c, Plan& P, const int* ext, const int* lat_id, cons
 int upload_level_host(rg_ctx* c, Plan& P, const double* uold, const double* unew);
 // the level's targets of src_dev (default: the device unew) into host array dst
 int download_level_host(rg_ctx* c, Plan& P, double* dst, const double* src_dev = nullptr);
+// every cell of the level (refined ones too) of the device uold / unew into
+// host arrays (either may be null); synchronises
+int download_level_cells(rg_ctx* c, Plan& P, double* uold, double* unew);
 int mlp_ensure(rg_ctx* c);
 int mlp_train(rg_ctx* c, int nsamples, int epochs, int batch, float lr, unsigned long long seed, float* loss_out);
 int mlp_grad(rg_ctx* c, int n, const float* x_host, const float* t_host, float* grad_host, float* loss_host);

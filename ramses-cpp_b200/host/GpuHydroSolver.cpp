@@ -5,19 +5,27 @@
 // (include/ramses/core/SolverFactory.hpp:23, default at
 // src/core/SolverFactory.cpp:5-9), so Simulation gets this class instead of
 // HydroSolver and nothing else in the reference changes.  It overrides the
-// virtual hot-path entry points of HydroSolver (HydroSolver.hpp:19-22) and
-// forwards them to librgpu.so through the C ABI of include/rgpu.h.
+// virtual hot-path entry points of HydroSolver (HydroSolver.hpp:19-22:
+// godunov_fine, set_unew, set_uold, compute_courant_step) and forwards them
+// to librgpu.so through the C ABI of include/rgpu.h.
 //
-// State ownership: AmrGrid keeps owning the host vectors.  The tree
-// maintenance (TreeUpdater) and the rest of Simulation read and write
-// grid_.uold/unew between hydro calls, so godunov_fine uploads the state it
-// reads -- only the level's cells, the stencil cells around it and the update
-// targets (rg_godunov_level_host) -- runs the step on the device and writes
-// the updated targets back; the tree arrays are re-sent only when they
-// changed (compared with the copy sent last time).  set_unew/set_uold stay plain host copies here: they are memory
-// copies the host has to see anyway.  Unsupported configurations (non-thermal
-// energies, passive scalars, barotropic EOS, boundary patches) throw: there is
-// no silent CPU fallback.
+// State: the device keeps uold and unew of the whole grid between calls.
+// AmrGrid still owns the host vectors, and the reference's TreeUpdater works
+// on them between hydro calls: it reads uold (flag_fine, restrict_fine,
+// make_grid_fine's interpolation), writes the refined cells' uold
+// (restrict_fine) and the new cells' uold and unew (make_grid_fine), and
+// never reads unew.  So a level step moves only its own cells: set_unew (or
+// compute_courant_step, whichever comes first in the step) uploads the cells
+// the step reads -- the level's cells and the coarser cells of its ghost
+// stencils -- from the host uold, and set_uold downloads the level's cells of
+// both arrays once the step is done; godunov_fine moves nothing.  The tree
+// arrays are re-sent when the tree changed, detected from next[] and the
+// level heads alone: every refinement or removal allocates or frees octs, and
+// moving an oct between the free list and a level list rewrites a next[]
+// entry (the predecessor's or the oct's own) or a head.  The state is sent
+// whole at the start and whenever ngridmax changes (resize_grids relabels the
+// cells).  Unsupported configurations (non-thermal energies, passive scalars,
+// barotropic EOS, boundary patches) throw: there is no silent CPU fallback.
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -38,18 +46,48 @@ public:
         if (ctx_) rg_destroy(ctx_);
     }
 
+    real_t compute_courant_step(int ilevel, real_t dx, real_t gamma, real_t courant_factor) override {
+        ensure_context();
+        sync_topology();
+        if (gamma != params_.gamma)
+            throw std::runtime_error("GpuHydroSolver: compute_courant_step with a gamma other than the grid's");
+        check(rg_upload_level(ctx_, ilevel, grid_.uold_vec.data()), "rg_upload_level");
+        uploaded_level_ = ilevel;
+        double dt = 0.0;
+        check(rg_courant_step(ctx_, ilevel, dx, courant_factor, 1, &dt), "rg_courant_step");
+        return dt;
+    }
+
+    void set_unew(int ilevel) override {
+        ensure_context();
+        sync_topology();
+        if (uploaded_level_ != ilevel)  // compute_courant_step of this step already sent the level
+            check(rg_upload_level(ctx_, ilevel, grid_.uold_vec.data()), "rg_upload_level");
+        uploaded_level_ = -1;
+        check(rg_set_unew(ctx_, ilevel), "rg_set_unew");
+    }
+
     void godunov_fine(int ilevel, real_t dt, real_t dx) override {
         ensure_context();
         sync_topology();
-        check(rg_godunov_level_host(ctx_, ilevel, dt, dx, grid_.uold_vec.data(), grid_.unew_vec.data()),
-              "rg_godunov_level_host");
+        uploaded_level_ = -1;
+        check(rg_godunov_level(ctx_, ilevel, dt, dx), "rg_godunov_level");
+    }
+
+    void set_uold(int ilevel) override {
+        ensure_context();
+        sync_topology();
+        uploaded_level_ = -1;
+        check(rg_set_uold(ctx_, ilevel), "rg_set_uold");
+        check(rg_download_level(ctx_, ilevel, grid_.uold_vec.data(), grid_.unew_vec.data()), "rg_download_level");
     }
 
 private:
     rg_ctx* ctx_ = nullptr;
     rg_params params_{};
-    std::vector<int> sent_son_, sent_father_, sent_nbor_, sent_next_, sent_headl_;
+    std::vector<int> sent_next_, sent_headl_;
     int sent_ngridmax_ = -1;
+    int uploaded_level_ = -1;
 
     void check(int rc, const char* what) {
         if (rc != RG_OK)
@@ -97,9 +135,8 @@ private:
     }
 
     void sync_topology() {
-        bool changed = sent_ngridmax_ != grid_.ngridmax || !same(sent_son_, grid_.son) ||
-                       !same(sent_father_, grid_.father) || !same(sent_nbor_, grid_.nbor) ||
-                       !same(sent_next_, grid_.next) || !same(sent_headl_, grid_.headl_vec);
+        const bool resized = sent_ngridmax_ != grid_.ngridmax;
+        const bool changed = resized || !same(sent_next_, grid_.next) || !same(sent_headl_, grid_.headl_vec);
         if (!changed) return;
         rg_grid_view v{};
         v.ncoarse = grid_.ncoarse;
@@ -120,9 +157,9 @@ private:
         v.bound_type = grid_.bound_type.empty() ? nullptr : grid_.bound_type.data();
         v.nbound_type = (int)grid_.bound_type.size();
         check(rg_sync_topology(ctx_, &v), "rg_sync_topology");
-        sent_son_ = grid_.son;
-        sent_father_ = grid_.father;
-        sent_nbor_ = grid_.nbor;
+        if (resized)  // the first call, or resize_grids relabelled every cell
+            check(rg_upload_state(ctx_, grid_.uold_vec.data(), grid_.unew_vec.data()), "rg_upload_state");
+        uploaded_level_ = -1;
         sent_next_ = grid_.next;
         sent_headl_ = grid_.headl_vec;
         sent_ngridmax_ = grid_.ngridmax;
