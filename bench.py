@@ -734,6 +734,84 @@ def ensemble_report(rank, world, local_rank, steps):
             "face_variant": list(variant), "host_build_s": build_s}
 
 
+def _ensemble_box_oracle(index, steps):
+    """One ensemble box alone, `steps` substeps with its own CFL step, by the C
+    oracle (the CPU side of the ensemble parity check)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import numpy as np
+    import rg_ensemble as ens
+    from refsupport import GridArrays, Oracle, make_params
+    spec = next(s for s in ens.box_specs(512) if s.index == index)
+    f = ens.Forest([spec])
+    b, g = f.boxes[0], f.gamma
+    ga = GridArrays(ncoarse=b.ncoarse, ngridmax=b.ngridmax, ncell=b.ncell, nvar=b.nvar, nx=b.nx, ny=b.ny, nz=b.nz,
+                    ncpu=1, nboundary=0, nlevelmax=b.nlevelmax, son=b.son, father=b.father, nbor=b.nbor, next=b.next,
+                    headl=b.headl)
+    orc = Oracle()
+    params = make_params(3, slope_type=2, riemann="hllc", gamma=g)
+    uold = f.box_state(0)
+    unew = uold.copy()
+    dts = []
+    for _ in range(steps):
+        dt = orc.courant(ga, 3, 5, spec.level, spec.dx, g, 0.8, uold, pressure_cap=False)
+        dts.append(dt)
+        orc.set_unew(ga, 3, 5, spec.level, uold, unew)
+        orc.godunov_fine(ga, params, spec.level, dt, spec.dx, uold, unew)
+        orc.set_uold(ga, 3, 5, spec.level, uold, unew)
+    want = np.ascontiguousarray(uold.reshape(5, b.ncell)[:, b.cell_ids(spec.level) - 1])
+    return index, hashlib.sha1(want.tobytes()).hexdigest(), dts
+
+
+def ensemble_parity(local_rank, nbox=32, steps=3):
+    """Config 4's parity check on a seeded, edge-stratified subset of the 512
+    boxes (about the same number of boxes of every edge): the subset stepped
+    together on the GPU (per-box CFL, brick face kernel over the boxes'
+    lattices) against each box stepped alone by the C oracle, per-box state
+    digests and dt bits compared."""
+    import multiprocessing as mp
+
+    import numpy as np
+    import rg_ensemble as ens
+    import rgpu
+    specs = ens.box_specs(512)
+    edges = sorted({s.edge for s in specs})
+    per = {e: [s for s in specs if s.edge == e] for e in edges}
+    subset = []
+    k = 0
+    while len(subset) < nbox:
+        for e in edges:
+            if len(subset) < nbox and k < len(per[e]):
+                subset.append(per[e][k])
+        k += 1
+    f = ens.Forest(subset)
+    ctx = rgpu.Context(rgpu.make_params(3, slope_type=2, riemann="hllc", gamma=f.gamma, courant_factor=0.8), local_rank)
+    try:
+        ctx.sync_topology(f.grid)
+        u0 = f.initial_state()
+        ctx.upload_state(u0, u0)
+        ctx.set_level_boxes(f.level, f.first_oct, f.dx)
+        ctx.set_level_lattices(f.level, *f.lattices())
+        dts = []
+        for k in range(steps):
+            ctx.level_substep(f.level, 0.0, pressure_cap=False, use_graph=k > 0)
+            dts.append(ctx.level_box_dt(f.level, f.nbox))
+        got = np.empty_like(u0)
+        ctx.download_state(uold=got)
+    finally:
+        ctx.close()
+    with mp.get_context("spawn").Pool(os.cpu_count() or 1) as pool:
+        res = pool.starmap(_ensemble_box_oracle, [(s.index, steps) for s in subset])
+    want = {i: (d, t) for i, d, t in res}
+    same_state = same_dt = 0
+    for i, s in enumerate(f.specs):
+        d = hashlib.sha1(np.ascontiguousarray(f.extract(got, i)).tobytes()).hexdigest()
+        same_state += d == want[s.index][0]
+        same_dt += all(float(dts[k][i]) == want[s.index][1][k] for k in range(steps))
+    return {"boxes": nbox, "edges": {str(e): sum(1 for s in subset if s.edge == e) for e in edges},
+            "substeps": steps, "cells": int(f.cells), "bit_identical_boxes": same_state, "same_dt_boxes": same_dt,
+            "check": "GPU forest of the subset (brick face kernel, per-box CFL) against each box alone by the C oracle"}
+
+
 def amr_sample(variant, steps, lmin=7, lmax=10, ngridmax=400000):
     """Config 3 through the reference's own AmrGrid / TreeUpdater / HydroSolver
     (the CPU reference, or the reference with the GPU drop-in); runs in its own
@@ -1086,6 +1164,7 @@ def main():
         ens_out = ensemble_report(rank, world, local_rank, 100)
         if rank == 0:
             out["ensemble"] = ens_out
+            out["ensemble"]["parity"] = ensemble_parity(local_rank)
             if world == 1:
                 out["amr_dropin"] = amr_report(3)
                 if "newton" in out:
