@@ -33,27 +33,32 @@ struct AmrRunState {
 
 // Simulation.cpp:552-554: dtold = dtnew; dtnew = the CFL step (the CFL
 // word), capped by the coarser level's dtnew over its sub-cycles
-// (nsub_coarser > 0 above levelmin)
-__global__ void k_amr_dt(double* ck, const DevStatus* st, int il, int nsub_coarser) {
+// (nsub_coarser > 0 above levelmin).  The word is re-armed at dt_start for
+// the next level's CFL pass (the coarse step arms it once at its start).  On a
+// level without finer octs the time update follows (Simulation.cpp:600-607):
+// finer = 1, no finer octs below nlevelmax (the finer level's steps become
+// this one's over its sub-cycles, nsub), finer = 2 at nlevelmax.
+__global__ void k_amr_dt(double* ck, DevStatus* st, int il, int nsub_coarser, double dt_start, int finer, int nsub) {
     ck[kDtOld + il] = ck[il];
     double d = __longlong_as_double((long long)st->dtmin_bits);
+    st->dtmin_bits = (unsigned long long)__double_as_longlong(dt_start);
     if (nsub_coarser > 0) {
         const double cand = ck[il - 1] / (double)nsub_coarser;
         d = cand < d ? cand : d;  // std::min(d, cand)
     }
     ck[il] = d;
+    if (finer == 1) {
+        const double v = ck[il] / (double)nsub;
+        ck[kDtOld + il + 1] = v;
+        ck[il + 1] = v;
+    }
+    if (finer) ck[kClockT] += ck[il];
 }
 
-// a level without finer octs (Simulation.cpp:600-603): the finer level's
-// steps are this one's over its sub-cycles, and the time advances
-__global__ void k_amr_no_finer(double* ck, int il, int nsub) {
-    const double v = ck[il] / (double)nsub;
-    ck[kDtOld + il + 1] = v;
-    ck[il + 1] = v;
-    ck[kClockT] += ck[il];
+__global__ void k_arm_cfl(DevStatus* st, double dt_start) {
+    st->dtmin_bits = (unsigned long long)__double_as_longlong(dt_start);
 }
 
-__global__ void k_amr_advance(double* ck, int il) { ck[kClockT] += ck[il]; }
 
 int count_grids(const rg_ctx* c, int il) {
     if (il < 0 || il > c->nlevelmax) return 0;
@@ -160,12 +165,9 @@ int amr_step(rg_ctx* c, const rg_amr_config& cfg, AmrRunState& S, int il, int ic
     // read the level's uold, nothing between them writes it; k_amr_dt only
     // reads the CFL word), and the level's new dt
     auto pre = [&]() -> int {
-        if (int rc = courant_step_device(c, il, dx, cfg.courant_factor, cfg.pressure_cap, true)) return rc;
-        k_amr_dt<<<1, 1, 0, c->stream>>>(ck, c->d_status, il, il > lmin ? nsubcycle(cfg, il - 1) : 0);
-        if (!finer) {
-            if (il < lmax) k_amr_no_finer<<<1, 1, 0, c->stream>>>(ck, il, nsub);
-            else k_amr_advance<<<1, 1, 0, c->stream>>>(ck, il);
-        }
+        if (int rc = courant_step_device(c, il, dx, cfg.courant_factor, cfg.pressure_cap, true, true)) return rc;
+        k_amr_dt<<<1, 1, 0, c->stream>>>(ck, c->d_status, il, il > lmin ? nsubcycle(cfg, il - 1) : 0,
+                                         c->params.boxlen / 1e-10, finer ? 0 : (il < lmax ? 1 : 2), nsub);
         return check_cuda(c, cudaGetLastError(), "clock kernels");
     };
     // after them: the level step with set_uold folded into the fold kernels (a
@@ -250,6 +252,9 @@ extern "C" int rg_amr_coarse_step(rg_ctx* c, const rg_amr_config* cfg, rg_amr_cl
         return rc;
     S.nstep = clock->nstep;
     S.cell_updates = clock->cell_updates;
+    // the CFL word's start value, as every CFL pass arms it (launch_courant);
+    // each level's k_amr_dt re-arms it after reading
+    k_arm_cfl<<<1, 1, 0, c->stream>>>(c->d_status, c->params.boxlen / 1e-10);
     const int rc_step = coarse_step(c, *cfg, S);
     // the clock comes back with the step (the copy waits for it); on an error
     // the caller's clock is left as it was

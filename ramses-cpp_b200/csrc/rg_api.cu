@@ -552,14 +552,15 @@ int rg_courant_step(rg_ctx* c, int ilevel, double dx, double courant_factor, int
 }  // extern "C"
 
 namespace rg {
-int courant_step_device(rg_ctx* c, int ilevel, double dx, double courant_factor, int pressure_cap, bool set_unew) {
+int courant_step_device(rg_ctx* c, int ilevel, double dx, double courant_factor, int pressure_cap, bool set_unew,
+                        bool armed) {
     CTX_GUARD(c);
     c->next_level = -1;  // the state or the CFL word may change
     if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state uploaded");
     Plan* P;
     if (int rc = get_plan(c, ilevel, &P)) return rc;
     if (P->nbox > 0) return set_error(c, RG_ERR_STATE, "ensemble level: read the per-box steps with rg_level_box_dt");
-    return launch_courant(c, *P, dx, pressure_cap, courant_factor, set_unew);
+    return launch_courant(c, *P, dx, pressure_cap, courant_factor, set_unew, armed);
 }
 
 int godunov_level_device_dt(rg_ctx* c, int ilevel, const double* dt_dev, double dx, bool set_uold) {
@@ -573,8 +574,7 @@ int godunov_level_device_dt(rg_ctx* c, int ilevel, const double* dt_dev, double 
     record_updates(c, ilevel, *P);
     if (P->ncells == 0) return RG_OK;
     if (int rc = ensure_flux(c, *P)) return rc;
-    if (int rc = launch_set_dt_device(c, dt_dev, dx)) return rc;
-    if (int rc = launch_godunov(c, *P, set_uold)) return rc;
+    if (int rc = launch_godunov(c, *P, set_uold, dt_dev, dx)) return rc;  // the primitive pass sets dt
     if (P->face_variant < 0 && ++P->substeps_run >= 1) return autotune_face(c, *P, step_consts(c));
     return RG_OK;
 }

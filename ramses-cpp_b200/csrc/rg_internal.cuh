@@ -323,20 +323,23 @@ int compute_cell_levels(rg_ctx* c);
 // step launchers (enqueue only)
 int launch_set_unew(rg_ctx* c, const Plan& p);
 int launch_set_uold(rg_ctx* c, const Plan& p);
-// set_unew: also HydroSolver::set_unew of the level in the same pass
+// set_unew: also HydroSolver::set_unew of the level in the same pass;
+// armed: the CFL word already holds its start value (no arming launch)
 int launch_courant(rg_ctx* c, const Plan& p, double dx, int pressure_cap, double courant_factor,
-                   bool set_unew = false);
+                   bool set_unew = false, bool armed = false);
 // the step values (dt, dt/dx, 1/dx) from a dt in device memory
 int launch_set_dt_device(rg_ctx* c, const double* dt, double dx);
 // rg_courant_step without reading the step back: the CFL word holds it
 int courant_step_device(rg_ctx* c, int ilevel, double dx, double courant_factor, int pressure_cap,
-                        bool set_unew = false);
+                        bool set_unew = false, bool armed = false);
 // rg_godunov_level with its dt read by the device from dt_dev
 // set_uold: HydroSolver::set_uold of the level folded into the fold kernels
 int godunov_level_device_dt(rg_ctx* c, int ilevel, const double* dt_dev, double dx, bool set_uold = false);
 int launch_set_dt_host(rg_ctx* c, double dt, double dx);
 int launch_finalize_dt(rg_ctx* c, double dx);
-int launch_godunov(rg_ctx* c, const Plan& p, bool set_uold = false);
+// dt_dev != nullptr: the primitive pass also sets the step values from it
+int launch_godunov(rg_ctx* c, const Plan& p, bool set_uold = false, const double* dt_dev = nullptr,
+                   double dx = 0.0);
 // the four events a level step records its kernel boundaries into: the
 // context's last-call set, or in accumulating mode the next set of the pool
 cudaEvent_t* step_events(rg_ctx* c, long long ncells);

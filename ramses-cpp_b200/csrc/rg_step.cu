@@ -88,11 +88,18 @@ __global__ void __launch_bounds__(128) k_face(TreeView T, PlanView P, const doub
     if (RS == RG_RIEMANN_EXACT && exact_iters && iters) atomicAdd(exact_iters, iters);
 }
 
+__device__ __forceinline__ void set_step_values(DevStatus* st, double dt, double dx);
+
+// dt_dev != nullptr: also the step values (dt, dt/dx, 1/dx) from the dt in
+// device memory, by one thread (nothing in this kernel reads them; the face
+// and fold kernels after it do).
 template <int NDIM>
 __global__ void k_prim(TreeView T, PlanView P, const double* __restrict__ uold, double* __restrict__ prim,
-                       double gamma, double smalle) {
+                       double gamma, double smalle, DevStatus* st = nullptr, const double* dt_dev = nullptr,
+                       double dx = 0.0) {
     constexpr int NV = Dims<NDIM>::NV;
     const size_t ncell = (size_t)T.ncell;
+    if (dt_dev && blockIdx.x == 0 && threadIdx.x == 0) set_step_values(st, *dt_dev, dx);
     const int total = P.ncells + P.nextra_prim;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
         int c = (t < P.ncells) ? cell_of(T, P, t) : P.xprim[t - P.ncells];
@@ -575,7 +582,7 @@ void launch_face_n(rg_ctx* c, const Plan& P, const StepK& K) {
 }
 
 template <int NDIM>
-int launch_godunov_t(rg_ctx* c, const Plan& P, bool set_uold) {
+int launch_godunov_t(rg_ctx* c, const Plan& P, bool set_uold, const double* dt_dev, double dx) {
     constexpr int NV = NDIM + 2, NS = 2 * NDIM;
     if (P.ncells == 0) return RG_OK;
     // the caller sized the shared flux scratch (ensure_flux) outside any capture:
@@ -588,7 +595,8 @@ int launch_godunov_t(rg_ctx* c, const Plan& P, bool set_uold) {
     cudaEvent_t* E = c->timing ? step_events(c, P.ncells) : nullptr;
     if (E) cudaEventRecord(E[0], c->stream);
     int nprim = P.ncells + P.nextra_prim;
-    k_prim<NDIM><<<grid_for(c, nprim, 256), 256, 0, c->stream>>>(T, V, c->d_uold, c->d_prim, K.gamma, K.smalle);
+    k_prim<NDIM><<<grid_for(c, nprim, 256), 256, 0, c->stream>>>(T, V, c->d_uold, c->d_prim, K.gamma, K.smalle,
+                                                                 c->d_status, dt_dev, dx);
     if (E) cudaEventRecord(E[1], c->stream);
     if (int rc = launch_face_tiles(c, P, K, c->d_uold, c->d_prim, c->d_flux, fsum)) return rc;
     if (E) cudaEventRecord(E[2], c->stream);
@@ -645,9 +653,9 @@ cudaEvent_t* step_events(rg_ctx* c, long long ncells) {
     return c->acc_ev[c->acc_n++].data();
 }
 
-int launch_godunov(rg_ctx* c, const Plan& P, bool set_uold) {
-    if (c->params.ndim == 1) return launch_godunov_t<1>(c, P, set_uold);
-    return launch_godunov_t<3>(c, P, set_uold);
+int launch_godunov(rg_ctx* c, const Plan& P, bool set_uold, const double* dt_dev, double dx) {
+    if (c->params.ndim == 1) return launch_godunov_t<1>(c, P, set_uold, dt_dev, dx);
+    return launch_godunov_t<3>(c, P, set_uold, dt_dev, dx);
 }
 
 int launch_godunov_ext(rg_ctx* c, const Plan& P, const double* uold, double* unew, double* prim, double* flux) {
@@ -747,9 +755,9 @@ int launch_set_uold(rg_ctx* c, const Plan& P) {
     return check_cuda(c, cudaGetLastError(), "set_uold");
 }
 
-int launch_courant(rg_ctx* c, const Plan& P, double dx, int pressure_cap, double cfl, bool set_unew) {
+int launch_courant(rg_ctx* c, const Plan& P, double dx, int pressure_cap, double cfl, bool set_unew, bool armed) {
     double start = c->params.boxlen / 1e-10;
-    k_courant_init<<<1, 1, 0, c->stream>>>(c->d_status, start);
+    if (!armed) k_courant_init<<<1, 1, 0, c->stream>>>(c->d_status, start);
     if (P.ncells > 0) {
         double* copy = set_unew ? c->d_unew : nullptr;
         if (c->params.ndim == 1)
