@@ -62,7 +62,7 @@ sys.path.insert(0, str(ROOT / "ramses-cpp_b200"))
 
 METRIC = "cell-updates/s 3D Sedov AMR FP64, %HBM roofline; Newton iters learned vs plain"
 UNIT = "cell-updates/s"
-AMR = dict(lmin=7, lmax=10, ngridmax=400000, cfl=0.25, ed=0.1, ep=0.1, gamma=1.4)
+AMR = dict(lmin=7, lmax=10, ngridmax=48000, cfl=0.25, ed=0.1, ep=0.1, gamma=1.4)
 WORKLOAD = ("3D Sedov blast with octree AMR, reference levelmin 7 / levelmax 10 (64^3 base, 512^3 effective), "
             "err_grad_d = err_grad_p = 0.1, nexpand 1, sub-cycled, MonCen + HLLC, gamma 1.4, courant 0.25, FP64, "
             "tree and state resident on the GPU")
