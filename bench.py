@@ -636,9 +636,25 @@ def newton_report(local_rank, stream, steps):
                      "flux_rel_gt_1e-12_count": int((frel > 1e-12).sum().item()),
                      "note": "converged mode: bracketed Newton-bisection to |dp|/p < 1e-14, then 2 polish updates "
                              "from the root's 30 leading bits (counted apart: the same for both starts)"}
-    del ql, qr, gam, f0, f1, p0, p1, res, rel, frel
+    # reference mode (10 updates, 1e-6: RiemannSolver.cpp:220-235) on a strided
+    # sample of the same pairs against the reference's own solve_godunov_nr
+    m = 65536
+    idx = torch.arange(0, n, n // m, device=dev)[:m]
+    fr = torch.empty(5 * n, dtype=torch.float64, device=dev)
+    ctx.exact_batch(n, ql.data_ptr(), qr.data_ptr(), gam.data_ptr(), fr.data_ptr(), 0, 0, learned=False, niter=10,
+                    tol=1e-6)
+    torch.cuda.synchronize()
+    import tempfile
+    tmp = Path(tempfile.mkdtemp()) / "stress_sample.npz"
+    np.savez(tmp, ql=ql.view(5, n)[:, idx].cpu().numpy(), qr=qr.view(5, n)[:, idx].cpu().numpy(),
+             gam=gam[idx].cpu().numpy(), flux=fr.view(5, n)[:, idx].cpu().numpy())
+    del ql, qr, gam, f0, f1, p0, p1, res, rel, frel, fr
     ctx.close()
     torch.cuda.empty_cache()
+    try:
+        out["stress"]["reference_mode_vs_reference"] = run_sample("--stress-ref", str(tmp))
+    finally:
+        tmp.unlink(missing_ok=True)
 
     L = 8
     g = rg_tree.build_uniform(3, L)
@@ -732,6 +748,34 @@ def ensemble_report(rank, world, local_rank, steps):
             "value": cells * steps / (ms / 1e3), "unit": UNIT, "n_gpus": world,
             "sharding": "boxes partitioned over ranks by cell count, no exchange" if world > 1 else "one GPU",
             "face_variant": list(variant), "host_build_s": build_s}
+
+
+def stress_ref(path):
+    """The exact solver in reference mode on GPU against the reference's own
+    RiemannSolver::solve_godunov_nr (compiled here) on a sample of the stress
+    pairs: per flux entry, relative differences (3e-12 is the tolerance the
+    ulp-level pow() differences between CUDA and glibc stay inside)."""
+    import numpy as np
+    sys.path.insert(0, str(ROOT / "tests"))
+    from refsupport import RefHarness
+    d = np.load(path)
+    ql, qr, gam, got = d["ql"], d["qr"], d["gam"], d["flux"]
+    h = RefHarness(3)
+    sys.stdout.flush()
+    saved, devnull = os.dup(1), os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)  # the reference prints its first solves
+    try:
+        want = np.array([h.riemann("exact", ql[:, i], qr[:, i], float(gam[i]))[:5] for i in range(ql.shape[1])]).T
+    finally:
+        import ctypes
+        ctypes.CDLL(None).fflush(None)
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(devnull)
+    rel = np.abs(got - want) / np.maximum(np.abs(want), 1e-300)
+    return {"pairs": int(ql.shape[1]), "flux_entries": int(rel.size), "identical_frac": float(np.mean(got == want)),
+            "within_3e-12_frac": float(np.mean(rel <= 3e-12)), "rel_max": float(rel.max()),
+            "check": "GPU reference mode (10 updates, 1e-6) against the reference's solve_godunov_nr, compiled here"}
 
 
 def _ensemble_box_oracle(index, steps):
@@ -1106,6 +1150,7 @@ def main():
     ap.add_argument("--amr-sample", nargs=2, metavar=("VARIANT", "STEPS"), help=argparse.SUPPRESS)
     ap.add_argument("--sod-sample", metavar="VARIANT", help=argparse.SUPPRESS)
     ap.add_argument("--amr-exact-sample", nargs=2, metavar=("GUESS", "STEPS"), help=argparse.SUPPRESS)
+    ap.add_argument("--stress-ref", metavar="NPZ", help=argparse.SUPPRESS)
     ap.add_argument("--profile-case", choices=["learned", "amr", "uniform"],
                     help="small run for ncu captures (no timing output)")
     args = ap.parse_args()
@@ -1118,6 +1163,9 @@ def main():
         return
     if args.sod_sample:
         print(json.dumps(sod_sample(args.sod_sample)))
+        return
+    if args.stress_ref:
+        print(json.dumps(stress_ref(args.stress_ref)))
         return
     if args.amr_exact_sample:
         print(json.dumps(amr_exact_sample(args.amr_exact_sample[0], int(args.amr_exact_sample[1]))))
