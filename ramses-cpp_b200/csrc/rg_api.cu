@@ -498,7 +498,9 @@ int rg_godunov_level(rg_ctx* c, int ilevel, double dt, double dx) {
     if (int rc = get_plan(c, ilevel, &P)) return rc;
     if (P->nbox > 0) return set_error(c, RG_ERR_STATE, "ensemble level: every box has its own dt, use rg_level_substep");
     record_updates(c, ilevel, *P);
-    if (P->ncells == 0) return RG_OK;
+    // no son == 0 cell (a fully refined level): godunov_fine computes nothing
+    // (HydroSolver.cpp:119), so neither is anything launched or moved
+    if (P->ncells == 0 || P->nactive == 0) return RG_OK;
     if (int rc = ensure_flux(c, *P)) return rc;
     if (int rc = launch_set_dt_host(c, dt, dx)) return rc;
     if (int rc = launch_godunov(c, *P)) return rc;
@@ -517,7 +519,9 @@ int rg_godunov_level_host(rg_ctx* c, int ilevel, double dt, double dx, const dou
     if (int rc = get_plan(c, ilevel, &P)) return rc;
     if (P->nbox > 0) return set_error(c, RG_ERR_STATE, "ensemble level: every box has its own dt, use rg_level_substep");
     record_updates(c, ilevel, *P);
-    if (P->ncells == 0) return RG_OK;
+    // no son == 0 cell (a fully refined level): godunov_fine computes nothing
+    // (HydroSolver.cpp:119), so neither is anything launched or moved
+    if (P->ncells == 0 || P->nactive == 0) return RG_OK;
     if (int rc = ensure_flux(c, *P)) return rc;
     if (int rc = upload_level_host(c, *P, uold, unew)) return rc;
     if (int rc = launch_set_dt_host(c, dt, dx)) return rc;
@@ -572,7 +576,9 @@ int godunov_level_device_dt(rg_ctx* c, int ilevel, const double* dt_dev, double 
     if (int rc = get_plan(c, ilevel, &P)) return rc;
     if (P->nbox > 0) return set_error(c, RG_ERR_STATE, "ensemble level: every box has its own dt, use rg_level_substep");
     record_updates(c, ilevel, *P);
-    if (P->ncells == 0) return RG_OK;
+    // no son == 0 cell (a fully refined level): godunov_fine computes nothing
+    // (HydroSolver.cpp:119), so neither is anything launched or moved
+    if (P->ncells == 0 || P->nactive == 0) return RG_OK;
     if (int rc = ensure_flux(c, *P)) return rc;
     if (int rc = launch_godunov(c, *P, set_uold, dt_dev, dx)) return rc;  // the primitive pass sets dt
     if (P->face_variant < 0 && ++P->substeps_run >= 1) return autotune_face(c, *P, step_consts(c));
