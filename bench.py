@@ -1188,7 +1188,7 @@ def main():
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     cpu = cpu_run = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         # the reference on one core, before any CUDA work: its initialisation,
@@ -1199,21 +1199,25 @@ def main():
                          f"the window, {cpu_run['cells']} cell updates, {cpu_run['seconds']:.1f} s) after the "
                          f"reference's own initialisation and {args.warmup} coarse steps, single-threaded"}
     out = amr_headline(args, rank, world, local_rank)
+    # the other configs' reports run on one GPU only: with N > 1 the other
+    # ranks would wait for rank 0's single-GPU work at the final barrier; the
+    # ensemble, whose boxes shard over the ranks, runs at every N
+    single = world == 1
     if rank == 0:
         if cpu_run:
             out["parity_digest"]["reference_sha1_uold_son"] = cpu_run["digest"]
             out["parity_digest"]["bit_identical"] = cpu_run["digest"] == out["parity_digest"]["sha1_uold_son"]
-        if not args.no_extra:
+        if single and not args.no_extra:
             out["sedov128"] = uniform_report(local_rank, 20, 3, args.face_variant)
-    if rank == 0 and not args.no_newton:
+    if rank == 0 and single and not args.no_newton:
         import torch
         out["newton"] = newton_report(local_rank, torch.cuda.Stream(), 10)
     if not args.no_extra:
         ens_out = ensemble_report(rank, world, local_rank, 100)
         if rank == 0:
             out["ensemble"] = ens_out
-            out["ensemble"]["parity"] = ensemble_parity(local_rank)
-            if world == 1:
+            if single:
+                out["ensemble"]["parity"] = ensemble_parity(local_rank)
                 out["amr_dropin"] = amr_report(3)
                 if "newton" in out:
                     out["newton"]["amr_exact"] = amr_exact_report(3)
