@@ -27,15 +27,24 @@ int launch_face_tiles(rg_ctx* c, const Plan& P, const StepK& K, const double* uo
 
 // Times every (variant, batch) on the level's current data (the face kernel
 // only writes the flux scratch, so repeating it changes no state) and keeps
-// the fastest.  Levels below 2^17 cells keep the default.  Must run outside a
+// the fastest.  Levels below 2^17 cells are not timed.  Must run outside a
 // capture.
 int autotune_face(rg_ctx* c, Plan& P, const StepK& K) {
     if (P.face_variant >= 0) return RG_OK;
     P.face_variant = kDefaultFaceVariant;
     P.face_batch = 1;
-    // small levels keep the default: timing 75 launches would cost more than
-    // any shape can save, and AMR rebuilds its small levels every coarse step
-    if (P.ncells < (1 << 17) || c->no_autotune) return RG_OK;
+    // small levels are not timed (75 launches would cost more than any shape
+    // can save, and AMR rebuilds its small levels whenever the tree changes).
+    // They keep the default shape (8 resident blocks per SM, one tile a block)
+    // unless their tiles outnumber its resident blocks; then the shape with 10
+    // resident blocks per SM (variant 2) -- on the finest level of the Sedov
+    // AMR run (1,280 tiles) face 0.373 instead of 0.409 ms per coarse step
+    if (c->no_autotune) return RG_OK;
+    if (P.ncells < (1 << 17)) {
+        const int ntiles = (P.ncells + TILE - 1) / TILE;
+        if (c->params.ndim == 3 && P.nbox == 0 && !P.lattice && ntiles > 8 * c->sm_count) P.face_variant = 2;
+        return RG_OK;
+    }
     const int ns = 2 * c->params.ndim, nv = c->params.ndim + 2;
     double* fsum = c->d_flux + (size_t)ns * nv * P.ncells;
     cudaEvent_t e0, e1;

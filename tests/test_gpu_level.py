@@ -300,7 +300,7 @@ def test_every_face_kernel_shape_is_bit_identical(ctx_factory, oracle, variant):
 
 
 def test_autotuner_picks_a_shape_and_exact_stats_count(ctx_factory):
-    L = 7  # 64^3: levels below 2^17 cells keep the default shape untimed
+    L = 7  # 64^3 = 2^18 cells: timed (levels below 2^17 cells are not)
     g = rg_tree.build_uniform(3, L)
     ctx = ctx_factory(make_params(3, slope_type=2, riemann="exact"))
     ctx.sync_topology(g)
