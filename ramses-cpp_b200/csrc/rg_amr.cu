@@ -105,10 +105,6 @@ int run_segment(rg_ctx* c, int key, bool ok, F&& body) {
         if (rc == RG_OK && ok) g.warm = v;
         return rc;
     }
-    if (g.exec) {
-        cudaGraphExecDestroy(g.exec);
-        g.exec = nullptr;
-    }
     const void* flux = c->d_flux;
     const void* tscr = c->d_tscr;
     if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
@@ -120,8 +116,25 @@ int run_segment(rg_ctx* c, int key, bool ok, F&& body) {
     cudaGraph_t graph = nullptr;
     const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
     cudaGraphExec_t exec = nullptr;
-    bool good = rc == RG_OK && e == cudaSuccess && graph != nullptr &&
-                cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    bool good = rc == RG_OK && e == cudaSuccess && graph != nullptr;
+    if (good && g.exec) {
+        // after a tree change a segment usually issues the same kernels with
+        // new sizes and pointers: updating the old executable graph in place
+        // costs a fraction of instantiating a new one (launches already
+        // queued keep the old parameters)
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(g.exec, graph, &info) == cudaSuccess) {
+            exec = g.exec;
+        } else {
+            cudaGetLastError();
+            cudaGraphExecDestroy(g.exec);
+        }
+        g.exec = nullptr;
+    } else if (g.exec) {
+        cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+    }
+    if (good && !exec) good = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
     if (graph) cudaGraphDestroy(graph);
     if (!good || flux != c->d_flux || tscr != c->d_tscr) {
         // nothing of the captured work ran: run it eagerly
@@ -139,17 +152,20 @@ int run_segment(rg_ctx* c, int key, bool ok, F&& body) {
 }
 
 int seg_key(int il, int kind, int icount) { return (il * 4 + kind) * 4 + (icount & 3); }
+constexpr int kTailKey = 3;  // below every level step's key (levels >= 1)
 
-int amr_step(rg_ctx* c, const rg_amr_config& cfg, AmrRunState& S, int il, int icount) {
+// probed_clean: the caller's probe covered this step's refinement levels and
+// found nothing to do
+int amr_step(rg_ctx* c, const rg_amr_config& cfg, AmrRunState& S, int il, int icount, bool probed_clean = false) {
     const int lmin = cfg.levelmin, lmax = c->nlevelmax;
     if (il > lmax) return RG_OK;
     if (count_grids(c, il) == 0 && il > 0) return RG_OK;
-    if (lmin < lmax && (il == lmin || icount > 1)) {
+    if (lmin < lmax && (il == lmin || icount > 1) && !probed_clean) {
         // the refinements and removals below change nothing when no cell of
         // those levels is flagged for refinement and no oct for removal:
         // one probe instead of a scan and a read-back per call
         bool pending = true;
-        if (int rc = tree_changes_pending(c, il + 1, lmax, &pending)) return rc;
+        if (int rc = tree_changes_pending(c, level_bits(il + 1, lmax), &pending)) return rc;
         if (pending) {
             for (int i = il; i <= lmax; ++i)
                 if (int rc = tree_make_grid_fine(c, i + 1)) return rc;
@@ -204,16 +220,38 @@ int amr_step(rg_ctx* c, const rg_amr_config& cfg, AmrRunState& S, int il, int ic
 int coarse_step(rg_ctx* c, const rg_amr_config& cfgr, AmrRunState& S) {
     const rg_amr_config* cfg = &cfgr;
     const int lmin = cfg->levelmin, lmax = c->nlevelmax;
-    if (lmin < lmax)
-        for (int il = 1; il <= lmin - 1; ++il)
-            if (int rc = tree_make_grid_fine(c, il)) return rc;
-    if (int rc = amr_step(c, *cfg, S, lmin, 1)) return rc;
-    for (int il = lmin; il >= 1; --il)
-        if (int rc = tree_flag_fine(c, il, cfg->err_grad_d, cfg->err_grad_p, cfg->err_grad_u, -1.0, cfg->nexpand, 2, 2))
+    bool pending = false;
+    if (lmin < lmax) {
+        // one probe for the refinements of the levels below levelmin (complete
+        // after the initialisation, so normally nothing) and for those that
+        // open amr_step(levelmin, 1), which follows them directly
+        if (int rc = tree_changes_pending(c, level_bits(1, lmin - 1) | level_bits(lmin + 1, lmax), &pending))
             return rc;
-    if (lmin < lmax)
-        for (int il = lmin - 1; il >= 0; --il)
-            if (int rc = tree_restrict_fine(c, il)) return rc;
+        if (pending)
+            for (int il = 1; il <= lmin - 1; ++il)
+                if (int rc = tree_make_grid_fine(c, il)) return rc;
+    }
+    if (int rc = amr_step(c, *cfg, S, lmin, 1, lmin < lmax && !pending)) return rc;
+    // the step's tail: flag_fine from levelmin down and the restrictions below
+    // levelmin, one segment like the level steps' (it reads the oct lists of
+    // levels 1..levelmin, which must be current for a capture)
+    auto tail = [&]() -> int {
+        for (int il = lmin; il >= 1; --il)
+            if (int rc = tree_flag_fine(c, il, cfg->err_grad_d, cfg->err_grad_p, cfg->err_grad_u, -1.0, cfg->nexpand,
+                                        2, 2))
+                return rc;
+        if (lmin < lmax)
+            for (int il = lmin - 1; il >= 0; --il)
+                if (int rc = tree_restrict_fine(c, il)) return rc;
+        return RG_OK;
+    };
+    bool tail_ok = c->amr_graphs_on && !c->timing && !c->tree_dirty && c->d_tscr;
+    for (int L = 1; tail_ok && L <= lmin && L <= lmax; ++L)
+        if (count_grids(c, L) > 0 && ((int)c->lvl_ver.size() <= L || c->lvl_ver[(size_t)L] != c->topo_version))
+            tail_ok = false;
+    if (int rc = run_segment(c, kTailKey, tail_ok, tail)) return rc;
+    // what flag_fine(1) leaves on the host, which a replay does not
+    if (lmin > 1 && lmax > 1) c->auth_dirty = true;
     return check_cuda(c, cudaGetLastError(), "coarse-step clock kernels");
 }
 

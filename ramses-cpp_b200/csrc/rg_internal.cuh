@@ -312,12 +312,18 @@ int tree_flag_fine(rg_ctx* c, int ilevel, double ed, double ep, double ev, doubl
 int tree_make_grid_fine(rg_ctx* c, int ilevel);
 int tree_remove_grid_fine(rg_ctx* c, int ilevel);
 int tree_restrict_fine(rg_ctx* c, int ilevel);
-// Would make_grid_fine(L) for L = lo..hi followed by remove_grid_fine(L) for
-// L = hi..lo change the resident tree?  One pass over those levels (after the
-// authorisation the first make_grid_fine would run): false when no cell is a
-// refinement candidate and no oct a removal candidate, in which case every one
-// of those calls leaves the tree as it is.
-int tree_changes_pending(rg_ctx* c, int lo, int hi, bool* pending);
+// Would make_grid_fine(L) and remove_grid_fine(L) for the levels L whose bit
+// is set in `levels` (bit L; L = 1 is the coarse cells, which only
+// make_grid_fine looks at) change the resident tree?  One pass over those
+// levels (after the authorisation the first make_grid_fine would run) and one
+// read-back: false when no cell is a refinement candidate and no oct a removal
+// candidate, in which case every one of those calls leaves the tree as it is.
+int tree_changes_pending(rg_ctx* c, uint64_t levels, bool* pending);
+inline uint64_t level_bits(int lo, int hi) {  // bits lo..hi, 1 <= lo, hi <= 63
+    uint64_t m = 0;
+    for (int L = lo < 1 ? 1 : lo; L <= hi && L <= 63; ++L) m |= 1ull << L;
+    return m;
+}
 Plan* existing_plan(rg_ctx* c, int ilevel);  // built plan or nullptr; never builds
 int compute_cell_levels(rg_ctx* c);
 // step launchers (enqueue only)

@@ -938,12 +938,12 @@ int tree_remove_grid_fine(rg_ctx* c, int ilevel) {
     return check_device_status(c);
 }
 
-int tree_changes_pending(rg_ctx* c, int lo, int hi, bool* pending) {
+int tree_changes_pending(rg_ctx* c, uint64_t levels, bool* pending) {
     *pending = true;
     if (!c->tree_resident) return set_error(c, RG_ERR_STATE, "no device-resident tree: call rg_tree_attach first");
-    hi = std::min(hi, c->nlevelmax - 1);  // both operations are no-ops at and above nlevelmax
-    if (lo < 2 || lo > hi) {              // level 1 (coarse cells) keeps its own path
-        *pending = lo <= hi;
+    levels &= level_bits(1, c->nlevelmax - 1);  // both operations are no-ops at and above nlevelmax
+    if (levels == 0) {
+        *pending = false;
         return RG_OK;
     }
     c->next_level = -1;
@@ -958,7 +958,10 @@ int tree_changes_pending(rg_ctx* c, int lo, int hi, bool* pending) {
     }
     int* d_any = S.list;
     cudaMemsetAsync(d_any, 0, sizeof(int), s);
-    for (int L = lo; L <= hi; ++L) {
+    // make_grid_fine(1)'s test: a coarse cell flagged and authorised without a son
+    if (levels & 2ull) k_coarse_candidates<<<nblk(c->ncoarse), TPB, 0, s>>>(M, d_any);
+    for (int L = 2; L <= 63; ++L) {
+        if (!(levels & (1ull << L))) continue;
         const int* octs = nullptr;
         int noct = 0;
         if (int rc = level_octs_cached(c, L, &octs, &noct)) return rc;
