@@ -154,24 +154,47 @@ int run_segment(rg_ctx* c, int key, bool ok, F&& body) {
 int seg_key(int il, int kind, int icount) { return (il * 4 + kind) * 4 + (icount & 3); }
 constexpr int kTailKey = 3;  // below every level step's key (levels >= 1)
 
-// probed_clean: the caller's probe covered this step's refinement levels and
-// found nothing to do
-int amr_step(rg_ctx* c, const rg_amr_config& cfg, AmrRunState& S, int il, int icount, bool probed_clean = false) {
+// The refinements and removals that open a level step, make_grid_fine(L)
+// for L = lo..hi then remove_grid_fine(L) for L = hi..lo, skipping the calls
+// that cannot change the tree by the probe `ch` and by what the calls before
+// them changed: make_grid_fine(L) runs when list L has refinement candidates
+// or make_grid_fine(L - 1) created octs, remove_grid_fine(L) when list L has
+// removal candidates or remove_grid_fine(L + 1) freed octs.  Every call that
+// is skipped would have found no candidate, so the tree ends as the full
+// sequence leaves it.
+int refine_and_remove(rg_ctx* c, int lo, int hi, const TreeChanges& ch, int* made_total = nullptr) {
+    int made = 0, freed = 0, total = 0;
+    for (int L = lo; L <= hi; ++L) {
+        const bool run = (L < 64 && (ch.refine >> L) & 1ull) || made > 0;
+        made = 0;
+        if (run)
+            if (int rc = tree_make_grid_fine(c, L, &made)) return rc;
+        total += made;
+    }
+    for (int L = hi; L >= lo; --L) {
+        const bool run = (L < 64 && (ch.kill >> L) & 1ull) || freed > 0;
+        freed = 0;
+        if (run)
+            if (int rc = tree_remove_grid_fine(c, L, &freed)) return rc;
+    }
+    if (made_total) *made_total = total;
+    return RG_OK;
+}
+
+// probed: the caller's probe of this step's refinement levels, taken with
+// nothing changing the tree since (nullptr: probe here)
+int amr_step(rg_ctx* c, const rg_amr_config& cfg, AmrRunState& S, int il, int icount,
+             const TreeChanges* probed = nullptr) {
     const int lmin = cfg.levelmin, lmax = c->nlevelmax;
     if (il > lmax) return RG_OK;
     if (count_grids(c, il) == 0 && il > 0) return RG_OK;
-    if (lmin < lmax && (il == lmin || icount > 1) && !probed_clean) {
-        // the refinements and removals below change nothing when no cell of
-        // those levels is flagged for refinement and no oct for removal:
+    if (lmin < lmax && (il == lmin || icount > 1)) {
         // one probe instead of a scan and a read-back per call
-        bool pending = true;
-        if (int rc = tree_changes_pending(c, level_bits(il + 1, lmax), &pending)) return rc;
-        if (pending) {
-            for (int i = il; i <= lmax; ++i)
-                if (int rc = tree_make_grid_fine(c, i + 1)) return rc;
-            for (int i = lmax; i >= il; --i)
-                if (int rc = tree_remove_grid_fine(c, i + 1)) return rc;
-        }
+        TreeChanges ch;
+        if (probed) ch = *probed;
+        else if (int rc = tree_changes_pending(c, level_bits(il + 1, lmax), &ch)) return rc;
+        if (ch.any(level_bits(il + 1, lmax)))
+            if (int rc = refine_and_remove(c, il + 1, lmax + 1, ch)) return rc;
     }
     const double dx = cfg.boxlen / (double)(c->nx * (1 << il));
     const int nsub = nsubcycle(cfg, il);
@@ -220,18 +243,27 @@ int amr_step(rg_ctx* c, const rg_amr_config& cfg, AmrRunState& S, int il, int ic
 int coarse_step(rg_ctx* c, const rg_amr_config& cfgr, AmrRunState& S) {
     const rg_amr_config* cfg = &cfgr;
     const int lmin = cfg->levelmin, lmax = c->nlevelmax;
-    bool pending = false;
+    TreeChanges ch;
+    bool created = false;
     if (lmin < lmax) {
         // one probe for the refinements of the levels below levelmin (complete
-        // after the initialisation, so normally nothing) and for those that
-        // open amr_step(levelmin, 1), which follows them directly
-        if (int rc = tree_changes_pending(c, level_bits(1, lmin - 1) | level_bits(lmin + 1, lmax), &pending))
-            return rc;
-        if (pending)
-            for (int il = 1; il <= lmin - 1; ++il)
-                if (int rc = tree_make_grid_fine(c, il)) return rc;
+        // after the initialisation, so normally nothing) and for the
+        // refinements and removals that open amr_step(levelmin, 1), which
+        // follows them directly; make_grid_fine of a level below levelmin runs
+        // when the probe or the refinement of the level before asks for it
+        if (int rc = tree_changes_pending(c, level_bits(1, lmin - 1) | level_bits(lmin + 1, lmax), &ch)) return rc;
+        int made = 0;
+        for (int il = 1; il <= lmin - 1; ++il) {
+            const bool run = (il < 64 && (ch.refine >> il) & 1ull) || made > 0;
+            made = 0;
+            if (run)
+                if (int rc = tree_make_grid_fine(c, il, &made)) return rc;
+            created = created || made > 0;
+        }
     }
-    if (int rc = amr_step(c, *cfg, S, lmin, 1, lmin < lmax && !pending)) return rc;
+    // when nothing was created below levelmin the probe still holds for the
+    // levelmin step's refinements
+    if (int rc = amr_step(c, *cfg, S, lmin, 1, lmin < lmax && !created ? &ch : nullptr)) return rc;
     // the step's tail: flag_fine from levelmin down and the restrictions below
     // levelmin, one segment like the level steps' (it reads the oct lists of
     // levels 1..levelmin, which must be current for a capture)

@@ -309,16 +309,25 @@ int launch_run_block(rg_ctx* c, const Plan& P, double dx, int pressure_cap, doub
 // TreeUpdater operations on the device-resident tree (rg_tree.cu)
 int tree_flag_fine(rg_ctx* c, int ilevel, double ed, double ep, double ev, double eb2, int nexp, int icount,
                    int nsub);
-int tree_make_grid_fine(rg_ctx* c, int ilevel);
-int tree_remove_grid_fine(rg_ctx* c, int ilevel);
+// `changed` (optional): the number of octs created / freed
+int tree_make_grid_fine(rg_ctx* c, int ilevel, int* changed = nullptr);
+int tree_remove_grid_fine(rg_ctx* c, int ilevel, int* changed = nullptr);
 int tree_restrict_fine(rg_ctx* c, int ilevel);
-// Would make_grid_fine(L) and remove_grid_fine(L) for the levels L whose bit
-// is set in `levels` (bit L; L = 1 is the coarse cells, which only
-// make_grid_fine looks at) change the resident tree?  One pass over those
+// Which of make_grid_fine(L) and remove_grid_fine(L), for the levels L whose
+// bit is set in `levels` (bit L; L = 1 is the coarse cells, which only
+// make_grid_fine looks at), can change the resident tree?  One pass over those
 // levels (after the authorisation the first make_grid_fine would run) and one
-// read-back: false when no cell is a refinement candidate and no oct a removal
-// candidate, in which case every one of those calls leaves the tree as it is.
-int tree_changes_pending(rg_ctx* c, uint64_t levels, bool* pending);
+// read-back.  Bit L of `refine` is clear when no cell of level list L is a
+// refinement candidate, bit L of `kill` when no oct of it is a removal
+// candidate; bits of levels not probed stay set.  A clear bit holds until a
+// call changes the tree: make_grid_fine(L) can make cells of list L + 1
+// candidates (the new octs' cells keep the flags their slots held), and
+// remove_grid_fine(L + 1) octs of list L.
+struct TreeChanges {
+    uint64_t refine = ~0ull, kill = ~0ull;
+    bool any(uint64_t levels) const { return ((refine | kill) & levels) != 0; }
+};
+int tree_changes_pending(rg_ctx* c, uint64_t levels, TreeChanges* out);
 inline uint64_t level_bits(int lo, int hi) {  // bits lo..hi, 1 <= lo, hi <= 63
     uint64_t m = 0;
     for (int L = lo < 1 ? 1 : lo; L <= hi && L <= 63; ++L) m |= 1ull << L;

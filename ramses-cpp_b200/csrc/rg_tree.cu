@@ -524,20 +524,21 @@ __global__ void k_kill_mark(TreeMut M, const int* __restrict__ octs, int noct, i
     }
 }
 
-// any make_grid_fine or remove_grid_fine candidate among a level's octs:
-// k_refine_mark's and k_kill_mark's tests, without writing marks
-__global__ void k_change_probe(TreeMut M, const int* __restrict__ octs, int noct, int* any) {
+// make_grid_fine and remove_grid_fine candidates among a level's octs:
+// k_refine_mark's and k_kill_mark's tests, without writing marks; `bit` (the
+// level's) is or-ed into bits[0] for a refinement, bits[1] for a removal
+__global__ void k_change_probe(TreeMut M, const int* __restrict__ octs, int noct, unsigned* bits, unsigned bit) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < noct; k += gridDim.x * blockDim.x) {
         const int ig = octs[k];
-        bool hit = false, refined_child = false;
+        bool refine = false, refined_child = false;
         for (int s = 0; s < 8; ++s) {
             const int idc = M.ncoarse + s * M.ngridmax + ig - 1;
             if (M.son[idc] > 0) refined_child = true;
-            else if (M.flag1[idc] == 1 && M.flag2[idc] == 1) hit = true;
+            else if (M.flag1[idc] == 1 && M.flag2[idc] == 1) refine = true;
         }
         const int fc = M.father[ig - 1];
-        if (fc > 0 && M.flag1[fc - 1] == 0 && !refined_child) hit = true;
-        if (hit) atomicExch(any, 1);
+        if (refine) atomicOr(bits, bit);
+        if (fc > 0 && M.flag1[fc - 1] == 0 && !refined_child) atomicOr(bits + 1, bit);
     }
 }
 
@@ -839,7 +840,8 @@ int tree_flag_fine(rg_ctx* c, int ilevel, double ed, double ep, double ev, doubl
     return check_cuda(c, cudaGetLastError(), "flag_fine kernels");
 }
 
-int tree_make_grid_fine(rg_ctx* c, int ilevel) {
+int tree_make_grid_fine(rg_ctx* c, int ilevel, int* changed) {
+    if (changed) *changed = 0;
     if (int rc = check_tree(c, ilevel)) return rc == kNoOp ? RG_OK : rc;  // no-op at and above nlevelmax (TreeUpdater.cpp:28)
     TreeScratch S;
     if (int rc = tree_scratch(c, &S)) return rc;
@@ -873,7 +875,7 @@ int tree_make_grid_fine(rg_ctx* c, int ilevel) {
         // the free list is too short: grow the arrays as the reference does,
         // then start over on the relabelled tree (authorisation is idempotent)
         if (int rc = tree_grow(c, n)) return rc;
-        return tree_make_grid_fine(c, ilevel);
+        return tree_make_grid_fine(c, ilevel, changed);
     }
     const StepK K = step_consts(c);
     k_refine<<<nblk(n8), TPB, 0, s>>>(M, tree_view(c), Geo{c->nx, c->ny, c->nz, c->params.boxlen}, S.octs, noct,
@@ -894,11 +896,13 @@ int tree_make_grid_fine(rg_ctx* c, int ilevel) {
     if (c->numbf > 0)
         if (int rc = set_dev_int(c, c->d_prev + c->h_fq[(size_t)c->fq_head] - 1, 0)) return rc;
     c->tree_dirty = true;
+    if (changed) *changed = n;
     if (int rc = check_cuda(c, cudaGetLastError(), "make_grid_fine kernels")) return rc;
     return check_device_status(c);
 }
 
-int tree_remove_grid_fine(rg_ctx* c, int ilevel) {
+int tree_remove_grid_fine(rg_ctx* c, int ilevel, int* changed) {
+    if (changed) *changed = 0;
     if (int rc = check_tree(c, ilevel)) return rc == kNoOp ? RG_OK : rc;  // no-op at and above nlevelmax (TreeUpdater.cpp:152)
     TreeScratch S;
     if (int rc = tree_scratch(c, &S)) return rc;
@@ -934,16 +938,20 @@ int tree_remove_grid_fine(rg_ctx* c, int ilevel) {
     c->h_taill[(size_t)hidx(c, ilevel)] = ends[1];
     c->h_numbl[(size_t)hidx(c, ilevel)] -= nkill;
     c->tree_dirty = true;
+    if (changed) *changed = nkill;
     if (int rc = check_cuda(c, cudaGetLastError(), "remove_grid_fine kernels")) return rc;
     return check_device_status(c);
 }
 
-int tree_changes_pending(rg_ctx* c, uint64_t levels, bool* pending) {
-    *pending = true;
+int tree_changes_pending(rg_ctx* c, uint64_t levels, TreeChanges* out) {
+    *out = TreeChanges{};
     if (!c->tree_resident) return set_error(c, RG_ERR_STATE, "no device-resident tree: call rg_tree_attach first");
     levels &= level_bits(1, c->nlevelmax - 1);  // both operations are no-ops at and above nlevelmax
-    if (levels == 0) {
-        *pending = false;
+    // the results are 32-bit masks: levels from 32 on stay "may change"
+    const uint64_t probed = levels & level_bits(1, 31);
+    if (probed == 0) {
+        out->refine &= ~levels;
+        out->kill &= ~levels;
         return RG_OK;
     }
     c->next_level = -1;
@@ -956,22 +964,27 @@ int tree_changes_pending(rg_ctx* c, uint64_t levels, bool* pending) {
         k_authorize<<<nblk(c->ncell), TPB, 0, s>>>(M);
         c->auth_dirty = false;
     }
-    int* d_any = S.list;
-    cudaMemsetAsync(d_any, 0, sizeof(int), s);
+    // [refine bits, kill bits, coarse candidates]
+    unsigned* d_bits = reinterpret_cast<unsigned*>(S.list);
+    cudaMemsetAsync(d_bits, 0, 3 * sizeof(unsigned), s);
     // make_grid_fine(1)'s test: a coarse cell flagged and authorised without a son
-    if (levels & 2ull) k_coarse_candidates<<<nblk(c->ncoarse), TPB, 0, s>>>(M, d_any);
-    for (int L = 2; L <= 63; ++L) {
-        if (!(levels & (1ull << L))) continue;
+    if (probed & 2ull) k_coarse_candidates<<<nblk(c->ncoarse), TPB, 0, s>>>(M, reinterpret_cast<int*>(d_bits + 2));
+    for (int L = 2; L <= 31; ++L) {
+        if (!(probed & (1ull << L))) continue;
         const int* octs = nullptr;
         int noct = 0;
         if (int rc = level_octs_cached(c, L, &octs, &noct)) return rc;
-        if (noct > 0) k_change_probe<<<nblk(noct), TPB, 0, s>>>(M, octs, noct, d_any);
+        if (noct > 0) k_change_probe<<<nblk(noct), TPB, 0, s>>>(M, octs, noct, d_bits, 1u << L);
     }
-    int any = 1;
-    if (int rc = check_cuda(c, cudaMemcpyAsync(&any, d_any, sizeof(int), cudaMemcpyDeviceToHost, s), "change probe"))
+    unsigned h[3] = {~0u, ~0u, 1u};
+    if (int rc = check_cuda(c, cudaMemcpyAsync(h, d_bits, sizeof(h), cudaMemcpyDeviceToHost, s), "change probe"))
         return rc;
     if (int rc = check_cuda(c, cudaStreamSynchronize(s), "change probe")) return rc;
-    *pending = any != 0;
+    uint64_t refine = h[0], kill = h[1];
+    if (h[2] != 0) refine |= 2ull;
+    kill |= 2ull;  // remove_grid_fine(1) is not probed
+    out->refine = (out->refine & ~probed) | (refine & probed);
+    out->kill = (out->kill & ~probed) | (kill & probed);
     return RG_OK;
 }
 
