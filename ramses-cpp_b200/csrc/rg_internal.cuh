@@ -98,7 +98,7 @@ struct PlanView {
 // Box of level cell p (ensemble levels only).
 __device__ __forceinline__ int box_of(const PlanView& P, int p) { return P.obox[p % P.noct]; }
 
-// A target with more updates than this is folded by a whole warp (k_fold_long).
+// A target with more updates than this is folded by a whole warp (fold_long).
 constexpr int kLongEvents = 16;
 
 struct Plan {

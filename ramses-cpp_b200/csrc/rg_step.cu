@@ -128,17 +128,19 @@ __device__ __forceinline__ double box_dtdx(const PlanView& P, int a) {
 // uold_out != nullptr (a level with refined cells in an AMR step): set_uold
 // folded in -- every level target (all of the level's son == 0 cells, each
 // with at least its own update) also writes its result to uold_out.
-template <int NDIM, bool LEAF = false, bool FSUM = false>
-__global__ void k_fold(TreeView T, PlanView P, const double* __restrict__ flux, double* __restrict__ unew,
-                       const DevStatus* __restrict__ st, double gamma, double* __restrict__ uold = nullptr,
-                       const double* __restrict__ fsum = nullptr, double* __restrict__ uold_out = nullptr) {
+// (blocks bid of nb; a thread a target)
+template <int NDIM, bool LEAF, bool FSUM>
+__device__ __forceinline__ void fold_short(int bid, int nb, const TreeView& T, const PlanView& P,
+                                           const double* __restrict__ flux, double* __restrict__ unew,
+                                           const DevStatus* __restrict__ st, double gamma, double* __restrict__ uold,
+                                           const double* __restrict__ fsum, double* __restrict__ uold_out) {
     constexpr int NV = Dims<NDIM>::NV;
     const size_t ncell = (size_t)T.ncell;
     const int nc = P.ncells;
     const double dtdx0 = st->dtdx;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < P.ntarg; t += gridDim.x * blockDim.x) {
+    for (int t = bid * blockDim.x + threadIdx.x; t < P.ntarg; t += nb * blockDim.x) {
         int a = P.toff[t], b = P.toff[t + 1];
-        if (a == b || b - a > kLongEvents) continue;  // long targets: k_fold_long
+        if (a == b || b - a > kLongEvents) continue;  // long targets: fold_long
         const double dtdx = P.obox ? box_dtdx<NDIM>(P, a) : dtdx0;
         int cell = (t < nc) ? cell_of(T, P, t) : P.textra[t - nc];
         const bool from_old = LEAF && t < nc;
@@ -160,9 +162,9 @@ __global__ void k_fold(TreeView T, PlanView P, const double* __restrict__ flux, 
     }
 }
 
-// The targets k_fold skips, those with more than kLongEvents updates (in AMR
-// runs, coarse cells that take the refluxes of many finer faces: 192 at the
-// edge of the finest level of the 64^3-base Sedov run), one warp each.  A
+// The targets fold_short skips, those with more than kLongEvents updates (in
+// AMR runs, coarse cells that take the refluxes of many finer faces: 192 at
+// the edge of the finest level of the 64^3-base Sedov run), one warp each.  A
 // thread walking such a chain waits on its loads event after event, and the
 // few long chains set the whole fold's duration.  Here the lanes fetch 32
 // events at a time and form each one's term -- dtdx * sign * flux * factor
@@ -177,12 +179,12 @@ __global__ void k_fold(TreeView T, PlanView P, const double* __restrict__ flux, 
 // Either way the result is the sequential fold's arithmetic, bit for bit.
 constexpr int kLongThreads = 256, kLongChunk = 32, kLongPad = kLongChunk + 1;
 
-template <int NDIM, bool LEAF = false, bool FSUM = false>
-__global__ void __launch_bounds__(kLongThreads)
-    k_fold_long(TreeView T, PlanView P, const int* __restrict__ tlong, int nlong, const double* __restrict__ flux,
-                double* __restrict__ unew, const DevStatus* __restrict__ st, double gamma,
-                double* __restrict__ uold = nullptr, const double* __restrict__ fsum = nullptr,
-                double* __restrict__ uold_out = nullptr) {
+template <int NDIM, bool LEAF, bool FSUM>
+__device__ __forceinline__ void fold_long(int bid, int nb, const TreeView& T, const PlanView& P,
+                                          const int* __restrict__ tlong, int nlong, const double* __restrict__ flux,
+                                          double* __restrict__ unew, const DevStatus* __restrict__ st, double gamma,
+                                          double* __restrict__ uold, const double* __restrict__ fsum,
+                                          double* __restrict__ uold_out) {
     constexpr int NV = Dims<NDIM>::NV, NS = Dims<NDIM>::NS, TTD = Dims<NDIM>::TTD;
     // per warp: the terms of one chunk, variable-major, rows padded so the
     // NV walking lanes read from different banks
@@ -190,9 +192,9 @@ __global__ void __launch_bounds__(kLongThreads)
     double* my = terms[threadIdx.x >> 5];
     const size_t ncell = (size_t)T.ncell;
     const int nc = P.ncells, lane = threadIdx.x & 31;
-    const int nwarp = (int)(((size_t)gridDim.x * blockDim.x) >> 5);
+    const int nwarp = (int)(((size_t)nb * blockDim.x) >> 5);
     const double factor = 1.0 / (1 << NDIM);
-    for (int w = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5); w < nlong; w += nwarp) {
+    for (int w = (int)(((size_t)bid * blockDim.x + threadIdx.x) >> 5); w < nlong; w += nwarp) {
         const int t = tlong[w];
         const int a = P.toff[t], b = P.toff[t + 1];
         const double dtdx = P.obox ? box_dtdx<NDIM>(P, a) : st->dtdx;
@@ -286,15 +288,39 @@ __global__ void __launch_bounds__(kLongThreads)
     }
 }
 
-// k_fold_long over a plan's long targets (nothing when it has none)
+inline int grid_for(rg_ctx* c, long long work, int block) {
+    long long b = (work + block - 1) / block;
+    long long cap = (long long)c->sm_count * 32;
+    if (b > cap) b = cap;
+    return (int)std::max(1LL, b);
+}
+
+// One launch for a level's targets: its first long_blocks blocks walk the
+// long targets a warp each, the others the rest a thread each.  The two sets
+// are disjoint and each target is folded by one thread or warp, so the split
+// changes no result; scheduled first, the long chains overlap the short ones.
 template <int NDIM, bool LEAF = false, bool FSUM = false>
-void launch_fold_long(rg_ctx* c, const Plan& P, const TreeView& T, const PlanView& V, const double* flux,
-                      double* unew, double gamma, double* uold = nullptr, const double* fsum = nullptr,
-                      double* uold_out = nullptr) {
-    if (P.nlong == 0) return;
-    const int blocks = (int)std::min<long long>(((long long)P.nlong * 32 + kLongThreads - 1) / kLongThreads, 65535);
-    k_fold_long<NDIM, LEAF, FSUM><<<blocks, kLongThreads, 0, c->stream>>>(T, V, P.tlong, P.nlong, flux, unew,
-                                                                          c->d_status, gamma, uold, fsum, uold_out);
+__global__ void __launch_bounds__(kLongThreads)
+    k_fold(TreeView T, PlanView P, const int* __restrict__ tlong, int nlong, int long_blocks,
+           const double* __restrict__ flux, double* __restrict__ unew, const DevStatus* __restrict__ st, double gamma,
+           double* __restrict__ uold = nullptr, const double* __restrict__ fsum = nullptr,
+           double* __restrict__ uold_out = nullptr) {
+    const int b = (int)blockIdx.x;
+    if (b < long_blocks)
+        fold_long<NDIM, LEAF, FSUM>(b, long_blocks, T, P, tlong, nlong, flux, unew, st, gamma, uold, fsum, uold_out);
+    else
+        fold_short<NDIM, LEAF, FSUM>(b - long_blocks, (int)gridDim.x - long_blocks, T, P, flux, unew, st, gamma, uold,
+                                     fsum, uold_out);
+}
+
+template <int NDIM, bool LEAF = false, bool FSUM = false>
+void launch_fold(rg_ctx* c, const Plan& P, const TreeView& T, const PlanView& V, const double* flux, double* unew,
+                 double gamma, double* uold = nullptr, const double* fsum = nullptr, double* uold_out = nullptr) {
+    const int long_blocks =
+        P.nlong > 0 ? (int)std::min<long long>(((long long)P.nlong * 32 + kLongThreads - 1) / kLongThreads, 4096) : 0;
+    const int grid = long_blocks + grid_for(c, P.ntarg, kLongThreads);
+    k_fold<NDIM, LEAF, FSUM><<<grid, kLongThreads, 0, c->stream>>>(T, V, P.tlong, P.nlong, long_blocks, flux, unew,
+                                                                   c->d_status, gamma, uold, fsum, uold_out);
 }
 
 // Leaf-level fold that also prepares the next substep: on a level whose
@@ -555,12 +581,6 @@ StepK step_consts(const rg_ctx* c) {
 
 namespace {
 
-inline int grid_for(rg_ctx* c, long long work, int block) {
-    long long b = (work + block - 1) / block;
-    long long cap = (long long)c->sm_count * 32;
-    if (b > cap) b = cap;
-    return (int)std::max(1LL, b);
-}
 
 template <int NDIM, int RS>
 void launch_face_t(rg_ctx* c, const Plan& P, const StepK& K) {
@@ -601,10 +621,7 @@ int launch_godunov_t(rg_ctx* c, const Plan& P, bool set_uold, const double* dt_d
     if (int rc = launch_face_tiles(c, P, K, c->d_uold, c->d_prim, c->d_flux, fsum)) return rc;
     if (E) cudaEventRecord(E[2], c->stream);
     double* uold_out = set_uold ? c->d_uold : nullptr;
-    k_fold<NDIM, false, true><<<grid_for(c, P.ntarg, 256), 256, 0, c->stream>>>(T, V, c->d_flux, c->d_unew,
-                                                                               c->d_status, K.gamma, nullptr, fsum,
-                                                                               uold_out);
-    launch_fold_long<NDIM, false, true>(c, P, T, V, c->d_flux, c->d_unew, K.gamma, nullptr, fsum, uold_out);
+    launch_fold<NDIM, false, true>(c, P, T, V, c->d_flux, c->d_unew, K.gamma, nullptr, fsum, uold_out);
     if (E) cudaEventRecord(E[3], c->stream);
     return check_cuda(c, cudaGetLastError(), "godunov kernels");
 }
@@ -634,8 +651,7 @@ int launch_godunov_ext_t(rg_ctx* c, const Plan& P, const double* uold, double* u
         case RG_RIEMANN_ACOUSTIC: launch_face_ext_t<NDIM, RG_RIEMANN_ACOUSTIC>(c, P, K, uold, prim, flux); break;
         default: launch_face_ext_t<NDIM, RG_RIEMANN_LLF>(c, P, K, uold, prim, flux); break;
     }
-    k_fold<NDIM><<<grid_for(c, P.ntarg, 256), 256, 0, c->stream>>>(T, V, flux, unew, c->d_status, K.gamma);
-    launch_fold_long<NDIM>(c, P, T, V, flux, unew, K.gamma);
+    launch_fold<NDIM>(c, P, T, V, flux, unew, K.gamma);
     return check_cuda(c, cudaGetLastError(), "godunov kernels (caller buffers)");
 }
 
@@ -712,9 +728,7 @@ int launch_leaf_core_t(rg_ctx* c, const Plan& P, double dx, int pressure_cap, do
                                                                K.smalle, c->d_uold, fsum, c->d_prim, dx, cfl,
                                                                pressure_cap);
     } else {
-        k_fold<NDIM, true, true><<<g, 256, 0, c->stream>>>(T, V, c->d_flux, c->d_unew, c->d_status, K.gamma,
-                                                           c->d_uold, fsum);
-        launch_fold_long<NDIM, true, true>(c, P, T, V, c->d_flux, c->d_unew, K.gamma, c->d_uold, fsum);
+        launch_fold<NDIM, true, true>(c, P, T, V, c->d_flux, c->d_unew, K.gamma, c->d_uold, fsum);
     }
     if (c->timing) cudaEventRecord(c->ev[3], c->stream);
     return check_cuda(c, cudaGetLastError(), "leaf substep kernels");
