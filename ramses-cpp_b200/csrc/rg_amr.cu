@@ -26,9 +26,19 @@ constexpr int kMaxLevel = 32;
 // device clock: dtnew[0..32], dtold[0..32], t
 constexpr int kDtOld = kMaxLevel + 1, kClockT = 2 * (kMaxLevel + 1), kClockN = kClockT + 1;
 
+enum RunMode { RUN_EAGER, RUN_CAPTURE, RUN_REPLAY };
+
 struct AmrRunState {
     double* ck = nullptr;  // device clock
     long long nstep = 0, cell_updates = 0;
+    const rg_amr_config* cfg = nullptr;
+    // the current run (the level-step segments between two of the host's
+    // waits): its index in the coarse step, how it is issued, and whether an
+    // eager visit may count as the warm-up of a capture
+    int run = 0;
+    RunMode mode = RUN_EAGER;
+    bool open = false, warm_ok = false;
+    long long topo = -1;
 };
 
 // Simulation.cpp:552-554: dtold = dtnew; dtnew = the CFL step (the CFL
@@ -67,24 +77,33 @@ int count_grids(const rg_ctx* c, int il) {
 
 int nsubcycle(const rg_amr_config& cfg, int il) { return il >= cfg.levelmin ? 2 : 1; }
 
-// Segments of a level step as CUDA graphs.  Between tree changes a level
-// step issues the same kernels with the same arguments every time: the CFL
-// pass with set_unew and the clock update before the finer sub-steps, and
-// after them the level step proper (dt, primitives, face, fold with
-// set_uold), restrict_fine and flag_fine; on a level without finer octs both
-// halves and the time update form one segment.  A segment runs eagerly the
-// first time at a topology version (which warms every cache it touches: the
-// plan, the autotuned face shape, the flux scratch size, the level oct
-// lists), is captured the second time, and is replayed from then on until the
-// tree changes (the topology version moves) or a scratch buffer it names is
-// reallocated.  Captured segments call nothing that waits or allocates; if a
-// capture fails anyway the segment stays eager for that topology version.
+// The coarse step as CUDA graphs.  Between tree changes a level step issues
+// the same kernels with the same arguments every time: the CFL pass with
+// set_unew and the clock update before the finer sub-steps, and after them
+// the level step proper (dt, primitives, face, fold with set_uold),
+// restrict_fine and flag_fine; on a level without finer octs both halves and
+// the time update form one segment.  The host waits only at the change
+// probes, so the segments between two probes -- a run -- form one graph: a
+// run is issued eagerly the first time at a topology version (which warms
+// every cache its segments touch: the plans, the autotuned face shapes, the
+// flux scratch size, the level oct lists), captured whole the second time,
+// and replayed from then on until the tree changes (the topology version
+// moves), a scratch buffer it names is reallocated or the configuration
+// differs.  The host still walks the step's recursion on a replay (the probes
+// and the counts depend on it), issuing nothing until the run's end.  A
+// captured run calls nothing that waits or allocates: a segment that is not
+// ready for capture ends the capture there, the part captured so far is
+// launched and the rest of the run goes eagerly.
 bool segment_ok(rg_ctx* c, int il) {
     if (!c->amr_graphs_on || c->timing || c->tree_dirty || !c->d_tscr) return false;
     Plan* P = existing_plan(c, il);
-    if (!P || P->face_variant < 0) return false;
-    const size_t need = (size_t)(2 * c->params.ndim + 1) * (c->params.ndim + 2) * (size_t)P->ncells;
-    if (P->ncells > 0 && (c->cap_flux < need || !c->d_flux)) return false;
+    if (!P) return false;
+    // a level without a leaf cell launches no face kernel (no shape, no scratch)
+    if (P->ncells > 0 && P->nactive > 0) {
+        if (P->face_variant < 0) return false;
+        const size_t need = (size_t)(2 * c->params.ndim + 1) * (c->params.ndim + 2) * (size_t)P->ncells;
+        if (c->cap_flux < need || !c->d_flux) return false;
+    }
     // the finer level's oct list, which restrict_fine and flag_fine read
     const int L = il + 1;
     if (L <= c->nlevelmax && count_grids(c, L) > 0)
@@ -92,36 +111,54 @@ bool segment_ok(rg_ctx* c, int il) {
     return true;
 }
 
-template <class F>
-int run_segment(rg_ctx* c, int key, bool ok, F&& body) {
-    SegGraph& g = c->amr_graphs[key];
+bool same_cfg(const rg_amr_config& a, const rg_amr_config& b) {
+    return a.levelmin == b.levelmin && a.nexpand == b.nexpand && a.courant_factor == b.courant_factor &&
+           a.err_grad_d == b.err_grad_d && a.err_grad_p == b.err_grad_p && a.err_grad_u == b.err_grad_u &&
+           a.pressure_cap == b.pressure_cap && a.boxlen == b.boxlen;
+}
+
+int run_begin(rg_ctx* c, AmrRunState& S) {
+    // settle the topology first: a run never changes it, so its version holds
+    // for every segment of the run
+    if (int rc = refresh_tree(c)) return rc;
+    RunGraph& g = c->amr_graphs[S.run];
     const long long v = c->topo_version;
-    if (ok && g.exec && g.topo == v && g.flux == c->d_flux && g.tscr == c->d_tscr) {
-        ++c->amr_replayed;
-        return check_cuda(c, cudaGraphLaunch(g.exec, c->stream), "level-step graph");
+    const bool base = c->amr_graphs_on && !c->timing && !c->tree_dirty && c->d_tscr;
+    S.open = true;
+    S.topo = v;
+    S.warm_ok = false;
+    if (base && g.exec && g.topo == v && g.flux == c->d_flux && g.tscr == c->d_tscr && same_cfg(g.cfg, *S.cfg)) {
+        S.mode = RUN_REPLAY;
+        return RG_OK;
     }
-    if (!ok || g.warm != v || g.failed == v) {
-        const int rc = body();
-        if (rc == RG_OK && ok) g.warm = v;
-        return rc;
-    }
-    const void* flux = c->d_flux;
-    const void* tscr = c->d_tscr;
-    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    if (base && g.warm == v && g.failed != v && same_cfg(g.cfg, *S.cfg)) {
+        if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            S.mode = RUN_CAPTURE;
+            g.flux = c->d_flux;
+            g.tscr = c->d_tscr;
+            return RG_OK;
+        }
         cudaGetLastError();
         g.failed = v;
-        return body();
     }
-    const int rc = body();
+    S.mode = RUN_EAGER;
+    S.warm_ok = base;
+    return RG_OK;
+}
+
+// end a capture and launch what it holds (the whole run, or the part before a
+// segment that could not be captured); keep it for replays when it is whole
+int run_launch_capture(rg_ctx* c, AmrRunState& S, bool whole) {
+    RunGraph& g = c->amr_graphs[S.run];
     cudaGraph_t graph = nullptr;
     const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
     cudaGraphExec_t exec = nullptr;
-    bool good = rc == RG_OK && e == cudaSuccess && graph != nullptr;
+    bool good = e == cudaSuccess && graph != nullptr;
     if (good && g.exec) {
-        // after a tree change a segment usually issues the same kernels with
-        // new sizes and pointers: updating the old executable graph in place
-        // costs a fraction of instantiating a new one (launches already
-        // queued keep the old parameters)
+        // after a tree change a run usually issues the same kernels with new
+        // sizes and pointers: updating the old executable graph in place costs
+        // a fraction of instantiating a new one (launches already queued keep
+        // the old parameters)
         cudaGraphExecUpdateResultInfo info;
         if (cudaGraphExecUpdate(g.exec, graph, &info) == cudaSuccess) {
             exec = g.exec;
@@ -136,23 +173,68 @@ int run_segment(rg_ctx* c, int key, bool ok, F&& body) {
     }
     if (good && !exec) good = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
     if (graph) cudaGraphDestroy(graph);
-    if (!good || flux != c->d_flux || tscr != c->d_tscr) {
-        // nothing of the captured work ran: run it eagerly
+    if (!good || g.flux != c->d_flux || g.tscr != c->d_tscr) {
+        // the captured work cannot be issued: the step is incomplete
         cudaGetLastError();
         if (exec) cudaGraphExecDestroy(exec);
-        g.failed = v;
-        return body();
+        g.failed = S.topo;
+        c->broken = true;
+        return set_error(c, RG_ERR_CUDA, "a captured run of the coarse step could not be instantiated");
     }
-    g.exec = exec;
-    g.topo = v;
-    g.flux = flux;
-    g.tscr = tscr;
-    ++c->amr_captured;
-    return check_cuda(c, cudaGraphLaunch(exec, c->stream), "level-step graph");
+    const cudaError_t le = cudaGraphLaunch(exec, c->stream);
+    if (whole) {
+        g.exec = exec;
+        g.topo = S.topo;
+        g.cfg = *S.cfg;
+        ++c->amr_captured;
+    } else {
+        cudaGraphExecDestroy(exec);  // the launch keeps what it needs
+        g.failed = S.topo;
+    }
+    return check_cuda(c, le, "coarse-step graph");
 }
 
-int seg_key(int il, int kind, int icount) { return (il * 4 + kind) * 4 + (icount & 3); }
-constexpr int kTailKey = 3;  // below every level step's key (levels >= 1)
+int run_end(rg_ctx* c, AmrRunState& S) {
+    if (!S.open) return RG_OK;
+    S.open = false;
+    RunGraph& g = c->amr_graphs[S.run];
+    int rc = RG_OK;
+    if (S.mode == RUN_REPLAY) {
+        ++c->amr_replayed;
+        rc = check_cuda(c, cudaGraphLaunch(g.exec, c->stream), "coarse-step graph");
+    } else if (S.mode == RUN_CAPTURE) {
+        rc = run_launch_capture(c, S, true);
+    } else if (S.warm_ok && c->topo_version == S.topo && !c->tree_dirty) {
+        g.warm = S.topo;
+        g.cfg = *S.cfg;
+    }
+    ++S.run;
+    return rc;
+}
+
+// an error inside a run: leave the stream out of capture
+void run_abort(rg_ctx* c, AmrRunState& S) {
+    if (S.open && S.mode == RUN_CAPTURE) {
+        cudaGraph_t graph = nullptr;
+        cudaStreamEndCapture(c->stream, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        c->amr_graphs[S.run].failed = S.topo;
+    }
+    S.open = false;
+}
+
+template <class F>
+int run_segment(rg_ctx* c, AmrRunState& S, bool ok, F&& body) {
+    if (S.mode == RUN_REPLAY) return RG_OK;
+    if (S.mode == RUN_CAPTURE && !ok) {
+        if (int rc = run_launch_capture(c, S, false)) return rc;
+        S.mode = RUN_EAGER;
+        S.warm_ok = false;
+    }
+    return body();
+}
+
 
 // The refinements and removals that open a level step, make_grid_fine(L)
 // for L = lo..hi then remove_grid_fine(L) for L = hi..lo, skipping the calls
@@ -181,20 +263,28 @@ int refine_and_remove(rg_ctx* c, int lo, int hi, const TreeChanges& ch, int* mad
     return RG_OK;
 }
 
-// probed: the caller's probe of this step's refinement levels, taken with
-// nothing changing the tree since (nullptr: probe here)
+// probed: what the caller's probe of this step's refinement levels leaves to
+// do, with nothing changing the tree since (nullptr: probe here)
 int amr_step(rg_ctx* c, const rg_amr_config& cfg, AmrRunState& S, int il, int icount,
              const TreeChanges* probed = nullptr) {
     const int lmin = cfg.levelmin, lmax = c->nlevelmax;
     if (il > lmax) return RG_OK;
     if (count_grids(c, il) == 0 && il > 0) return RG_OK;
     if (lmin < lmax && (il == lmin || icount > 1)) {
-        // one probe instead of a scan and a read-back per call
+        // one probe instead of a scan and a read-back per call; the host waits
+        // for it, so the run of segments before it ends here
+        const uint64_t m = level_bits(il + 1, std::min(lmax, c->nlevelmax - 1));
         TreeChanges ch;
-        if (probed) ch = *probed;
-        else if (int rc = tree_changes_pending(c, level_bits(il + 1, lmax), &ch)) return rc;
-        if (ch.any(level_bits(il + 1, lmax)))
+        if (probed) {
+            ch = *probed;
+        } else if (m) {
+            if (int rc = run_end(c, S)) return rc;
+            if (int rc = tree_changes_pending(c, m, &ch)) return rc;
+        }
+        if (ch.any(m))
             if (int rc = refine_and_remove(c, il + 1, lmax + 1, ch)) return rc;
+        if (!probed && m)
+            if (int rc = run_begin(c, S)) return rc;
     }
     const double dx = cfg.boxlen / (double)(c->nx * (1 << il));
     const int nsub = nsubcycle(cfg, il);
@@ -224,17 +314,17 @@ int amr_step(rg_ctx* c, const rg_amr_config& cfg, AmrRunState& S, int il, int ic
                               il > 0 ? nsubcycle(cfg, il - 1) : 1);
     };
     if (!finer) {
-        if (int rc = run_segment(c, seg_key(il, 2, icount), segment_ok(c, il), [&]() -> int {
+        if (int rc = run_segment(c, S, segment_ok(c, il), [&]() -> int {
                 if (int rc = pre()) return rc;
                 return post();
             }))
             return rc;
         S.nstep++;
     } else {
-        if (int rc = run_segment(c, seg_key(il, 0, icount), segment_ok(c, il), pre)) return rc;
+        if (int rc = run_segment(c, S, segment_ok(c, il), pre)) return rc;
         for (int i = 1; i <= nsub; ++i)
             if (int rc = amr_step(c, cfg, S, il + 1, i)) return rc;
-        if (int rc = run_segment(c, seg_key(il, 1, icount), segment_ok(c, il), post)) return rc;
+        if (int rc = run_segment(c, S, segment_ok(c, il), post)) return rc;
     }
     S.cell_updates += rg_level_cell_updates(c, il);
     return RG_OK;
@@ -261,9 +351,20 @@ int coarse_step(rg_ctx* c, const rg_amr_config& cfgr, AmrRunState& S) {
             created = created || made > 0;
         }
     }
-    // when nothing was created below levelmin the probe still holds for the
-    // levelmin step's refinements
-    if (int rc = amr_step(c, *cfg, S, lmin, 1, lmin < lmax && !created ? &ch : nullptr)) return rc;
+    // the refinements and removals that open amr_step(levelmin, 1), issued
+    // here so that the run of segments starts after them (when nothing was
+    // created below levelmin the probe still holds for them)
+    TreeChanges done;
+    done.refine = done.kill = 0;
+    if (lmin < lmax) {
+        const uint64_t m = level_bits(lmin + 1, std::min(lmax, c->nlevelmax - 1));
+        if (created && m)
+            if (int rc = tree_changes_pending(c, m, &ch)) return rc;
+        if (ch.any(m))
+            if (int rc = refine_and_remove(c, lmin + 1, lmax + 1, ch)) return rc;
+    }
+    if (int rc = run_begin(c, S)) return rc;
+    if (int rc = amr_step(c, *cfg, S, lmin, 1, lmin < lmax ? &done : nullptr)) return rc;
     // the step's tail: flag_fine from levelmin down and the restrictions below
     // levelmin, one segment like the level steps' (it reads the oct lists of
     // levels 1..levelmin, which must be current for a capture)
@@ -281,9 +382,10 @@ int coarse_step(rg_ctx* c, const rg_amr_config& cfgr, AmrRunState& S) {
     for (int L = 1; tail_ok && L <= lmin && L <= lmax; ++L)
         if (count_grids(c, L) > 0 && ((int)c->lvl_ver.size() <= L || c->lvl_ver[(size_t)L] != c->topo_version))
             tail_ok = false;
-    if (int rc = run_segment(c, kTailKey, tail_ok, tail)) return rc;
+    if (int rc = run_segment(c, S, tail_ok, tail)) return rc;
     // what flag_fine(1) leaves on the host, which a replay does not
     if (lmin > 1 && lmax > 1) c->auth_dirty = true;
+    if (int rc = run_end(c, S)) return rc;
     return check_cuda(c, cudaGetLastError(), "coarse-step clock kernels");
 }
 
@@ -322,10 +424,12 @@ extern "C" int rg_amr_coarse_step(rg_ctx* c, const rg_amr_config* cfg, rg_amr_cl
         return rc;
     S.nstep = clock->nstep;
     S.cell_updates = clock->cell_updates;
+    S.cfg = cfg;
     // the CFL word's start value, as every CFL pass arms it (launch_courant);
     // each level's k_amr_dt re-arms it after reading
     k_arm_cfl<<<1, 1, 0, c->stream>>>(c->d_status, c->params.boxlen / 1e-10);
     const int rc_step = coarse_step(c, *cfg, S);
+    if (rc_step) run_abort(c, S);
     // the clock comes back with the step (the copy waits for it); on an error
     // the caller's clock is left as it was
     const int rc_copy = check_cuda(c, cudaMemcpyAsync(h, S.ck, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "clock");

@@ -227,6 +227,12 @@ int refresh_tree(rg_ctx* c) {
     return check_device_status(c);
 }
 
+void drop_amr_graphs(rg_ctx* c) {
+    for (auto& kv : c->amr_graphs)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    c->amr_graphs.clear();
+}
+
 Plan* existing_plan(rg_ctx* c, int ilevel) {
     if (!c->have_topology || ilevel < 0 || ilevel >= (int)c->plans.size()) return nullptr;
     Plan& p = c->plans[ilevel];
@@ -307,8 +313,7 @@ void rg_destroy(rg_ctx* c) {
     for (int* p : tp) dev_free(c, p);
     dev_free(c, c->d_xg);
     for (int* p : c->lvl_octs) dev_free(c, p);
-    for (auto& kv : c->amr_graphs)
-        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    drop_amr_graphs(c);
     dev_free(c, c->d_clock);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->pool) cudaMemPoolDestroy(c->pool);
@@ -339,6 +344,7 @@ int rg_set_params(rg_ctx* c, const rg_params* params) {
             cudaGraphExecDestroy(p.graph);
             p.graph = nullptr;
         }
+    drop_amr_graphs(c);
     return RG_OK;
 }
 
@@ -1008,6 +1014,7 @@ int rg_exact_stats(rg_ctx* c, int64_t* iters, int64_t* calls, int reset) {
 int rg_set_autotune(rg_ctx* c, int on) {
     CTX_GUARD(c);
     c->no_autotune = (on == 0);
+    drop_amr_graphs(c);
     return RG_OK;
 }
 
@@ -1034,6 +1041,7 @@ int rg_set_face_config(rg_ctx* c, int ilevel, int variant, int batch) {
         cudaGraphExecDestroy(P->graph);
         P->graph = nullptr;
     }
+    drop_amr_graphs(c);
     return RG_OK;
 }
 
@@ -1061,6 +1069,7 @@ int rg_mlp_nparam(void) { return MLP_NPARAM; }
 
 int rg_mlp_train(rg_ctx* c, int nsamples, int epochs, int batch, float lr, uint64_t seed, float* loss_out) {
     CTX_GUARD(c);
+    drop_amr_graphs(c);  // captured steps name the network (or its absence)
     return mlp_train(c, nsamples, epochs, batch, lr, (unsigned long long)seed, loss_out);
 }
 
@@ -1078,6 +1087,7 @@ int rg_mlp_get(rg_ctx* c, float* params) {
 int rg_mlp_set(rg_ctx* c, const float* params) {
     CTX_GUARD(c);
     if (!params) return set_error(c, RG_ERR_ARG, "params is NULL");
+    drop_amr_graphs(c);  // captured steps name the network (or its absence)
     if (int rc = mlp_ensure(c)) return rc;
     if (int rc = check_cuda(c, cudaMemcpyAsync(c->d_mlp, params, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice,
                                                c->stream),

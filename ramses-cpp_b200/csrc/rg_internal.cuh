@@ -156,13 +156,15 @@ struct TunedShape {
     float ms = 0.f;
 };
 
-// A captured segment of a level step of the resident AMR step (rg_amr.cu),
-// valid for the topology version and scratch buffers it was captured with.
-struct SegGraph {
+// A captured run of the resident AMR coarse step (rg_amr.cu: the level-step
+// segments between two of the host's waits), valid for the topology version,
+// scratch buffers and configuration it was captured with.
+struct RunGraph {
     cudaGraphExec_t exec = nullptr;
     long long topo = -1, warm = -1, failed = -1;
     const void* flux = nullptr;
     const void* tscr = nullptr;
+    rg_amr_config cfg{};
 };
 
 struct Tuning {
@@ -255,9 +257,10 @@ struct rg_ctx {
     std::vector<int> lvl_cap, lvl_n;
     std::vector<long long> lvl_ver;
     // rg_amr_coarse_step: the clock buffer (kept so captured graphs can name
-    // it) and the level-step graphs, replayed while the topology is unchanged
+    // it) and the captured runs by their index in the coarse step, replayed
+    // while the topology is unchanged
     double* d_clock = nullptr;
-    std::map<int, rg::SegGraph> amr_graphs;
+    std::map<int, rg::RunGraph> amr_graphs;
     bool amr_graphs_on = true;
     long long amr_captured = 0, amr_replayed = 0;
     bool tree_dirty = false;  // links changed on the device: ranks, cell levels and plans are stale
@@ -334,6 +337,9 @@ inline uint64_t level_bits(int lo, int hi) {  // bits lo..hi, 1 <= lo, hi <= 63
     return m;
 }
 Plan* existing_plan(rg_ctx* c, int ilevel);  // built plan or nullptr; never builds
+// forget the captured AMR coarse-step runs (they bake in the solver constants,
+// face shapes and network pointer)
+void drop_amr_graphs(rg_ctx* c);
 int compute_cell_levels(rg_ctx* c);
 // step launchers (enqueue only)
 int launch_set_unew(rg_ctx* c, const Plan& p);

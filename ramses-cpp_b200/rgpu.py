@@ -283,8 +283,9 @@ class Context:
         self._chk(self.L.rg_amr_coarse_step(self.h, C.byref(cfg), C.byref(clock)))
 
     def amr_graphs(self, on=None):
-        """Switch the coarse step's level-step graphs (on=True/False) and return
-        (captured, replayed) segment counts."""
+        """Switch the coarse step's graphs (on=True/False) and return the
+        (captured, replayed) counts of runs (the level-step segments between two
+        of the host's waits)."""
         cap, rep = C.c_int64(0), C.c_int64(0)
         self._chk(self.L.rg_amr_graphs(self.h, -1 if on is None else (1 if on else 0), C.byref(cap), C.byref(rep)))
         return cap.value, rep.value
