@@ -369,7 +369,15 @@ int coarse_step(rg_ctx* c, const rg_amr_config& cfgr, AmrRunState& S) {
     // levelmin, one segment like the level steps' (it reads the oct lists of
     // levels 1..levelmin, which must be current for a capture)
     auto tail = [&]() -> int {
-        for (int il = lmin; il >= 1; --il)
+        if (int rc = tree_flag_fine(c, lmin, cfg->err_grad_d, cfg->err_grad_p, cfg->err_grad_u, -1.0, cfg->nexpand,
+                                    2, 2))
+            return rc;
+        // the levels below levelmin (all cells flagged, restrictions) in two
+        // launches when they are small, else call by call
+        bool fused = false;
+        if (int rc = tree_tail_below_min(c, lmin, lmin < lmax, &fused)) return rc;
+        if (fused) return RG_OK;
+        for (int il = lmin - 1; il >= 1; --il)
             if (int rc = tree_flag_fine(c, il, cfg->err_grad_d, cfg->err_grad_p, cfg->err_grad_u, -1.0, cfg->nexpand,
                                         2, 2))
                 return rc;

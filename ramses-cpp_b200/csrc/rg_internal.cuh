@@ -316,6 +316,9 @@ int tree_flag_fine(rg_ctx* c, int ilevel, double ed, double ep, double ev, doubl
 int tree_make_grid_fine(rg_ctx* c, int ilevel, int* changed = nullptr);
 int tree_remove_grid_fine(rg_ctx* c, int ilevel, int* changed = nullptr);
 int tree_restrict_fine(rg_ctx* c, int ilevel);
+// flag_fine(il) for il = lmin-1..1 and, with `restrictions`, restrict_fine(il)
+// for il = lmin-1..0 as two launches; *done false when not applicable
+int tree_tail_below_min(rg_ctx* c, int lmin, bool restrictions, bool* done);
 // Which of make_grid_fine(L) and remove_grid_fine(L), for the levels L whose
 // bit is set in `levels` (bit L; L = 1 is the coarse cells, which only
 // make_grid_fine looks at), can change the resident tree?  One pass over those

@@ -585,6 +585,47 @@ __global__ void k_restrict(TreeMut M, const int* __restrict__ octs, int noct) {
     }
 }
 
+// The coarse step's work below levelmin in one block: flag_fine(il) for il =
+// levelmin-1..2 (k_flag_init's below-levelmin case: every cell flagged) and
+// for the coarse cells (k_flag_coarse_below_min), then restrict_fine(il) for
+// il = levelmin-2..0 over the lists F.octs given coarsest last, with a barrier
+// between levels so that each restriction reads the one before it (the
+// threads of a block see each other's global writes after __syncthreads).
+// These levels are small (4,681 octs below a levelmin of 7): one block's
+// latency is below the launches it replaces.
+struct LevelLists {
+    const int* octs[32];
+    int noct[32];
+    int n;
+};
+
+__global__ void __launch_bounds__(1024) k_tail_below_min(TreeMut M, LevelLists F, LevelLists R) {
+    for (int j = 0; j < F.n; ++j) {
+        const int noct = F.noct[j], n = 8 * noct;
+        for (int p = threadIdx.x; p < n; p += blockDim.x) M.flag1[lvl_cell(M, F.octs[j], noct, p) - 1] = 1;
+    }
+    for (int i = threadIdx.x; i < M.ncoarse; i += blockDim.x) {
+        M.cpu_map[i] = 1;
+        M.flag1[i] = 1;
+    }
+    const size_t nc = (size_t)M.ncell;
+    for (int j = 0; j < R.n; ++j) {
+        __syncthreads();
+        const int* octs = R.octs[j];
+        for (int k = threadIdx.x; k < R.noct[j]; k += blockDim.x) {
+            const int ig = octs[k];
+            const int fc = M.father[ig - 1];
+            if (fc <= 0) continue;
+            for (int iv = 0; iv < 5; ++iv) {
+                double sum = 0;
+                for (int s = 0; s < 8; ++s)
+                    sum += M.uold[(size_t)iv * nc + M.ncoarse + (size_t)s * M.ngridmax + ig - 1];
+                M.uold[(size_t)iv * nc + fc - 1] = sum / 8;
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------- host side
 int hidx(const rg_ctx* c, int ilevel) { return ilevel * (c->ncpu + c->nboundary); }
 
@@ -827,11 +868,15 @@ int tree_flag_fine(rg_ctx* c, int ilevel, double ed, double ep, double ev, doubl
         k_smooth_apply<<<nblk(n), TPB, 0, s>>>(M, S.octs, noct, S.mark);
     };
     k_flag_init<<<nblk(n), TPB, 0, s>>>(M, S.octs, noct, ilevel < lmin ? 1 : 0);
+    // below levelmin every cell of the level is now flagged, and smoothing a
+    // fully flagged level flags nothing more: the smoothing passes run from
+    // levelmin on only
     if (ilevel >= lmin) smooth();
     if (ilevel >= lmin && (ed > 0.0 || ep > 0.0 || ev > 0.0))
         k_flag_grad<<<nblk(n), TPB, 0, s>>>(M, S.octs, noct, ed, ep, ev, c->params.gamma);
     if (ilevel > lmin && icount < nsub) k_test_flag<<<nblk(n), TPB, 0, s>>>(M, S.octs, noct);
-    for (int i = 0; i < nexp; ++i) smooth();
+    if (ilevel >= lmin)
+        for (int i = 0; i < nexp; ++i) smooth();
     if (ilevel > lmin && icount < nsub)
         k_ensure_ref_rules<<<nblk(27LL * noct), TPB, 0, s>>>(M, Geo{c->nx, c->ny, c->nz, c->params.boxlen}, S.octs,
                                                               noct);
@@ -1005,6 +1050,54 @@ int tree_restrict_fine(rg_ctx* c, int ilevel) {
     S.octs = const_cast<int*>(octs);  // read only below
     k_restrict<<<nblk(noct), TPB, 0, c->stream>>>(tree_mut(c), S.octs, noct);
     return check_cuda(c, cudaGetLastError(), "restrict_fine kernel");
+}
+
+// The tail of the coarse step below levelmin: flag_fine(il) for il =
+// levelmin-1..1 and restrict_fine(il) for il = levelmin-1..0 (the
+// restrictions when `restrictions` is set), as the calls one by one leave the
+// tree and the state, in two launches: restrict_fine(levelmin-1) over the
+// levelmin list, then k_tail_below_min.  *done stays false (nothing issued)
+// when the lists below levelmin are not small or not cached, and the caller
+// makes the calls one by one.  Enqueue only.
+int tree_tail_below_min(rg_ctx* c, int lmin, bool restrictions, bool* done) {
+    *done = false;
+    if (!c->tree_resident || c->tree_dirty || lmin < 2 || lmin > c->nlevelmax || lmin > 32 || c->levelmin != lmin)
+        return RG_OK;
+    LevelLists F{}, R{};
+    long long total = 0;
+    for (int L = 1; L <= lmin; ++L) {
+        if ((int)c->lvl_ver.size() <= L || (c->lvl_ver[(size_t)L] != c->topo_version && c->h_numbl[(size_t)hidx(c, L)] > 0))
+            return RG_OK;
+        if (L < lmin) total += c->h_numbl[(size_t)hidx(c, L)];
+    }
+    if (total > 16384) return RG_OK;
+    for (int L = lmin - 1; L >= 2; --L) {
+        const int* octs = nullptr;
+        int noct = 0;
+        if (int rc = level_octs_cached(c, L, &octs, &noct)) return rc;
+        F.octs[F.n] = octs;
+        F.noct[F.n++] = noct;
+    }
+    if (restrictions)
+        for (int L = lmin - 1; L >= 1; --L) {
+            const int* octs = nullptr;
+            int noct = 0;
+            if (int rc = level_octs_cached(c, L, &octs, &noct)) return rc;
+            R.octs[R.n] = octs;
+            R.noct[R.n++] = noct;
+        }
+    c->next_level = -1;
+    TreeMut M = tree_mut(c);
+    if (restrictions) {
+        const int* octs = nullptr;
+        int noct = 0;
+        if (int rc = level_octs_cached(c, lmin, &octs, &noct)) return rc;
+        if (noct > 0) k_restrict<<<nblk(noct), TPB, 0, c->stream>>>(M, octs, noct);
+    }
+    k_tail_below_min<<<1, 1024, 0, c->stream>>>(M, F, R);
+    c->auth_dirty = true;  // k_flag_coarse_below_min's part: the coarse cells' cpu_map
+    *done = true;
+    return check_cuda(c, cudaGetLastError(), "tail below levelmin");
 }
 
 }  // namespace rg
