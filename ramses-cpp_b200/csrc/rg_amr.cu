@@ -16,6 +16,7 @@
 // Simulation's nsubcycle_ default.  Physics modules the hydro configs switch
 // off (turbulence, sinks, stars, cooling, RT) are not called.
 #include <algorithm>
+#include <cstring>
 
 #include "rg_internal.cuh"
 
@@ -89,8 +90,8 @@ int nsubcycle(const rg_amr_config& cfg, int il) { return il >= cfg.levelmin ? 2 
 // flux scratch size, the level oct lists), captured whole the second time,
 // and replayed from then on until the tree changes (the topology version
 // moves), a scratch buffer it names is reallocated or the configuration
-// differs.  The host still walks the step's recursion on a replay (the probes
-// and the counts depend on it), issuing nothing until the run's end.  A
+// differs.  A replay is launched at the run's start; the host still walks the
+// step's recursion (the probes and the counts depend on it), issuing nothing.  A
 // captured run calls nothing that waits or allocates: a segment that is not
 // ready for capture ends the capture there, the part captured so far is
 // launched and the rest of the run goes eagerly.
@@ -128,8 +129,11 @@ int run_begin(rg_ctx* c, AmrRunState& S) {
     S.topo = v;
     S.warm_ok = false;
     if (base && g.exec && g.topo == v && g.flux == c->d_flux && g.tscr == c->d_tscr && same_cfg(g.cfg, *S.cfg)) {
+        // issued at once: the device works through the run while the host
+        // walks the same recursion to the run's end, issuing nothing
         S.mode = RUN_REPLAY;
-        return RG_OK;
+        ++c->amr_replayed;
+        return check_cuda(c, cudaGraphLaunch(g.exec, c->stream), "coarse-step graph");
     }
     if (base && g.warm == v && g.failed != v && same_cfg(g.cfg, *S.cfg)) {
         if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
@@ -199,10 +203,7 @@ int run_end(rg_ctx* c, AmrRunState& S) {
     S.open = false;
     RunGraph& g = c->amr_graphs[S.run];
     int rc = RG_OK;
-    if (S.mode == RUN_REPLAY) {
-        ++c->amr_replayed;
-        rc = check_cuda(c, cudaGraphLaunch(g.exec, c->stream), "coarse-step graph");
-    } else if (S.mode == RUN_CAPTURE) {
+    if (S.mode == RUN_CAPTURE) {
         rc = run_launch_capture(c, S, true);
     } else if (S.warm_ok && c->topo_version == S.topo && !c->tree_dirty) {
         g.warm = S.topo;
@@ -427,9 +428,21 @@ extern "C" int rg_amr_coarse_step(rg_ctx* c, const rg_amr_config* cfg, rg_amr_cl
     h[kClockT] = clock->t;
     if (!c->d_clock)  // kept for the context's lifetime: captured level steps name it
         if (int rc = check_cuda(c, dev_alloc(c, &c->d_clock, sizeof(h)), "coarse-step clock")) return rc;
+    if (!c->h_clock) {
+        if (int rc = check_cuda(c, cudaMallocHost((void**)&c->h_clock, sizeof(h)), "coarse-step clock (host)"))
+            return rc;
+        c->clock_known = false;
+    }
     S.ck = c->d_clock;
-    if (int rc = check_cuda(c, cudaMemcpyAsync(S.ck, h, sizeof(h), cudaMemcpyHostToDevice, c->stream), "clock upload"))
-        return rc;
+    // the device keeps the clock of the last step: send it only when the
+    // caller's differs
+    if (!c->clock_known || std::memcmp(c->h_clock, h, sizeof(h)) != 0) {
+        c->clock_known = false;
+        std::memcpy(c->h_clock, h, sizeof(h));
+        if (int rc = check_cuda(c, cudaMemcpyAsync(S.ck, c->h_clock, sizeof(h), cudaMemcpyHostToDevice, c->stream),
+                                "clock upload"))
+            return rc;
+    }
     S.nstep = clock->nstep;
     S.cell_updates = clock->cell_updates;
     S.cfg = cfg;
@@ -440,11 +453,15 @@ extern "C" int rg_amr_coarse_step(rg_ctx* c, const rg_amr_config* cfg, rg_amr_cl
     if (rc_step) run_abort(c, S);
     // the clock comes back with the step (the copy waits for it); on an error
     // the caller's clock is left as it was
-    const int rc_copy = check_cuda(c, cudaMemcpyAsync(h, S.ck, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "clock");
+    c->clock_known = false;
+    const int rc_copy =
+        check_cuda(c, cudaMemcpyAsync(c->h_clock, S.ck, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "clock");
     const int rc_sync = check_cuda(c, cudaStreamSynchronize(c->stream), "coarse step");
     if (rc_step) return rc_step;
     if (rc_copy) return rc_copy;
     if (rc_sync) return rc_sync;
+    std::memcpy(h, c->h_clock, sizeof(h));
+    c->clock_known = true;
     std::copy(h, h + kMaxLevel + 1, clock->dtnew);
     std::copy(h + kDtOld, h + kDtOld + kMaxLevel + 1, clock->dtold);
     clock->t = h[kClockT];

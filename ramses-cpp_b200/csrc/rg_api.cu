@@ -315,6 +315,7 @@ void rg_destroy(rg_ctx* c) {
     for (int* p : c->lvl_octs) dev_free(c, p);
     drop_amr_graphs(c);
     dev_free(c, c->d_clock);
+    if (c->h_clock) cudaFreeHost(c->h_clock);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->pool) cudaMemPoolDestroy(c->pool);
     if (c->h_status) cudaFreeHost(c->h_status);

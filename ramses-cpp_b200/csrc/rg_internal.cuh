@@ -260,6 +260,10 @@ struct rg_ctx {
     // it) and the captured runs by their index in the coarse step, replayed
     // while the topology is unchanged
     double* d_clock = nullptr;
+    // page-locked copy of the clock the device holds (valid when clock_known):
+    // a coarse step called with that clock uploads nothing
+    double* h_clock = nullptr;
+    bool clock_known = false;
     std::map<int, rg::RunGraph> amr_graphs;
     bool amr_graphs_on = true;
     long long amr_captured = 0, amr_replayed = 0;

@@ -994,9 +994,22 @@ int tree_changes_pending(rg_ctx* c, uint64_t levels, TreeChanges* out) {
     levels &= level_bits(1, c->nlevelmax - 1);  // both operations are no-ops at and above nlevelmax
     // the results are 32-bit masks: levels from 32 on stay "may change"
     const uint64_t probed = levels & level_bits(1, 31);
-    if (probed == 0) {
-        out->refine &= ~levels;
-        out->kill &= ~levels;
+    // a level whose every cell has a son has no candidate of either kind (a
+    // refinement needs a cell without a son, a removal an oct without a
+    // refined cell); the host's counts show it, since every oct has one father
+    // cell: list L + 1 holds 8 octs per oct of list L (per coarse cell for
+    // L = 1, whose cells are the coarse cells)
+    uint64_t scan = 0;
+    for (int L = 1; L <= 31; ++L) {
+        if (!(probed & (1ull << L))) continue;
+        const long long cells = L == 1 ? c->ncoarse : 8LL * c->h_numbl[(size_t)hidx(c, L)];
+        const bool full = L + 1 <= c->nlevelmax && c->h_numbl[(size_t)hidx(c, L + 1)] == cells;
+        if (!full) scan |= 1ull << L;
+    }
+    if (scan == 0) {
+        out->refine &= ~probed;
+        out->kill &= ~probed;
+        out->kill |= probed & 2ull;  // remove_grid_fine(1) is not probed
         return RG_OK;
     }
     c->next_level = -1;
@@ -1013,9 +1026,9 @@ int tree_changes_pending(rg_ctx* c, uint64_t levels, TreeChanges* out) {
     unsigned* d_bits = reinterpret_cast<unsigned*>(S.list);
     cudaMemsetAsync(d_bits, 0, 3 * sizeof(unsigned), s);
     // make_grid_fine(1)'s test: a coarse cell flagged and authorised without a son
-    if (probed & 2ull) k_coarse_candidates<<<nblk(c->ncoarse), TPB, 0, s>>>(M, reinterpret_cast<int*>(d_bits + 2));
+    if (scan & 2ull) k_coarse_candidates<<<nblk(c->ncoarse), TPB, 0, s>>>(M, reinterpret_cast<int*>(d_bits + 2));
     for (int L = 2; L <= 31; ++L) {
-        if (!(probed & (1ull << L))) continue;
+        if (!(scan & (1ull << L))) continue;
         const int* octs = nullptr;
         int noct = 0;
         if (int rc = level_octs_cached(c, L, &octs, &noct)) return rc;
