@@ -298,6 +298,9 @@ void dev_free(rg_ctx* c, void* p);
 int rank_lists(rg_ctx* c);
 // Exclusive scan of n ints on the context stream; *total gets the sum (synchronises).
 int exclusive_scan(rg_ctx* c, const int* in, int* out, int n, int* total);
+// the same, enqueue only: the total stays in device memory (*total_dev, or
+// the scan scratch when total_dev is null; *total_at gets where)
+int exclusive_scan_dev(rg_ctx* c, const int* in, int* out, int n, int* total_dev, int** total_at = nullptr);
 // Octs of level list `ilevel` in linked-list order, from the list ranks, into the
 // device array out[cap]; *noct gets the count (synchronises).
 int level_oct_list(rg_ctx* c, int ilevel, int* out, int cap, int* noct);

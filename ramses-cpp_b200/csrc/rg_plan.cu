@@ -239,8 +239,11 @@ __global__ void k_ev_fill(int ncells, int level0, int noct, const int* __restric
     }
 }
 
-// targets whose event count exceeds `limit`, appended to out (count in *n)
-__global__ void k_long_targets(int ntarg, const int* __restrict__ off, int limit, int* out, int* n) {
+// targets whose event count exceeds `limit`, appended to out (count in *n);
+// the targets are the level's nc cells and the *nextra extra ones
+__global__ void k_long_targets(int nc, const int* __restrict__ nextra, const int* __restrict__ off, int limit, int* out,
+                               int* n) {
+    const int ntarg = nc + *nextra;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntarg; t += gridDim.x * blockDim.x)
         if (off[t + 1] - off[t] > limit) out[atomicAdd(n, 1)] = t;
 }
@@ -248,7 +251,9 @@ __global__ void k_long_targets(int ntarg, const int* __restrict__ off, int limit
 // each target's events into ascending key order (the CPU order), one thread
 // per target; targets with more than `skip_above` events are left to
 // k_ev_sort_long
-__global__ void k_ev_sort(int ntarg, const int* __restrict__ off, int* ev, int skip_above) {
+__global__ void k_ev_sort(int nc, const int* __restrict__ nextra, const int* __restrict__ off, int* ev,
+                          int skip_above) {
+    const int ntarg = nc + *nextra;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntarg; t += gridDim.x * blockDim.x) {
         int a = off[t], b = off[t + 1];
         if (b - a > skip_above) continue;
@@ -471,12 +476,16 @@ int build_plan_t(rg_ctx* c, int ilevel, Plan& P) {
             c->cap_scan = 1024;
             d_count = c->d_scan;
         }
-        cudaMemsetAsync(d_count, 0, sizeof(int), s);
+        cudaMemsetAsync(d_count, 0, 2 * sizeof(int), s);
+        // with the tree resident the count is the host's: the chain is checked
+        // on the device and reported with the plan's read-back below
         k_level_octs<<<nblk(c->ngridmax), TPB, 0, s>>>(c->ngridmax, c->d_jump, c->d_dist, head - 1, P.noct, P.octs,
-                                                       d_count, c->d_status, false);
-        cudaMemcpyAsync(&hv[0], d_count, sizeof(int), cudaMemcpyDeviceToHost, s);
-        if (int rc = check_cuda(c, cudaStreamSynchronize(s), "level octs")) return rc;
-        if (hv[0] != P.noct) return set_error(c, RG_ERR_TOPOLOGY, "level linked list merges with another chain");
+                                                       d_count, c->d_status, c->tree_resident);
+        if (!c->tree_resident) {
+            cudaMemcpyAsync(&hv[0], d_count, sizeof(int), cudaMemcpyDeviceToHost, s);
+            if (int rc = check_cuda(c, cudaStreamSynchronize(s), "level octs")) return rc;
+            if (hv[0] != P.noct) return set_error(c, RG_ERR_TOPOLOGY, "level linked list merges with another chain");
+        }
         P.ncells = P.noct * TTD;
     } else {
         P.ncells = c->ncoarse;
@@ -497,63 +506,56 @@ int build_plan_t(rg_ctx* c, int ilevel, Plan& P) {
                                                 P.kind, d_nact, c->d_status);
     if (int rc = check_cuda(c, cudaGetLastError(), "plan cells")) return rc;
 
-    // ---- extra primitives (coarser cells read by ghost stencils) and extra
-    //      targets (coarser cells receiving reflux); both lists are bounded by ncell
-    int* d_nx = nullptr;  // [0] extra-prim count, [1] extra-target count
-    int* d_xp = nullptr;
-    int* d_textra = nullptr;
-    auto cleanup = [&]() { dev_free(c, d_nx); dev_free(c, d_xp); dev_free(c, d_textra); };
+    // The rest runs without a read-back: the arrays whose lengths the device
+    // counts are sized by bounds, and the counts come back once at the end.
+    //   extra primitives (coarser cells read by ghost stencils) and extra
+    //   targets (coarser cells receiving reflux): distinct cells, <= ncell;
+    //   targets: the level's cells and the extra ones, distinct, <= ncell;
+    //   events: an own update and at most one reflux per face of each cell.
+    const size_t ncell1 = (size_t)c->ncell + 1;
+    const size_t tbound = std::min(ncell1, (size_t)nc * (NS + 1) + 1);  // targets + 1
+    const size_t ebound = (size_t)nc * (NS + 1);
+    int* d_nx = nullptr;  // [0] extra primitives, [1] extra targets, [2] long targets, [3] events
+    int* cnt = nullptr;
+    auto cleanup = [&]() { dev_free(c, d_nx); dev_free(c, cnt); };
     if (int rc = dalloc(c, &d_nx, 8, "plan counters")) return rc;
-    if (int rc = dalloc(c, &d_xp, (size_t)c->ncell + 1, "xprim")) { cleanup(); return rc; }
-    if (int rc = dalloc(c, &d_textra, (size_t)c->ncell + 1, "textra")) { cleanup(); return rc; }
+    if (int rc = dalloc(c, &cnt, tbound, "event counts")) { cleanup(); return rc; }
+    if (int rc = dalloc(c, &P.xprim, ncell1, "xprim")) { cleanup(); return rc; }
+    if (int rc = dalloc(c, &P.textra, ncell1, "textra")) { cleanup(); return rc; }
+    if (int rc = dalloc(c, &P.toff, tbound, "toff")) { cleanup(); return rc; }
+    if (int rc = dalloc(c, &P.tev, ebound, "events")) { cleanup(); return rc; }
+    if (int rc = dalloc(c, &P.tlong, tbound, "long targets")) { cleanup(); return rc; }
     cudaMemsetAsync(d_nx, 0, sizeof(int) * 8, s);
-    k_plan_xprim<NDIM><<<nblk(nc), TPB, 0, s>>>(nc, c->d_cpos, P.icn, P.stc, P.kind, c->d_pmark, d_xp, d_nx);
-    k_ev_claim<NDIM><<<nblk(nc), TPB, 0, s>>>(nc, c->d_cpos, P.icn, P.kind, c->d_tmap, d_textra, d_nx + 1);
-    cudaMemcpyAsync(hv, d_nx, 2 * sizeof(int), cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(&P.nactive, d_nact, sizeof(long long), cudaMemcpyDeviceToHost, s);
-    if (int rc = check_cuda(c, cudaStreamSynchronize(s), "plan extras")) { cleanup(); return rc; }
-    P.nextra_prim = hv[0];
-    int nextra = hv[1];
-    P.ntarg = nc + nextra;
-    if (int rc = dalloc(c, &P.xprim, (size_t)P.nextra_prim, "xprim")) { cleanup(); return rc; }
-    if (int rc = dalloc(c, &P.textra, (size_t)nextra, "textra")) { cleanup(); return rc; }
-    if (P.nextra_prim) cudaMemcpyAsync(P.xprim, d_xp, sizeof(int) * P.nextra_prim, cudaMemcpyDeviceToDevice, s);
-    if (nextra) cudaMemcpyAsync(P.textra, d_textra, sizeof(int) * nextra, cudaMemcpyDeviceToDevice, s);
+    k_plan_xprim<NDIM><<<nblk(nc), TPB, 0, s>>>(nc, c->d_cpos, P.icn, P.stc, P.kind, c->d_pmark, P.xprim, d_nx);
+    k_ev_claim<NDIM><<<nblk(nc), TPB, 0, s>>>(nc, c->d_cpos, P.icn, P.kind, c->d_tmap, P.textra, d_nx + 1);
 
-    // ---- ordered event lists (CSR over targets)
-    // targets are distinct cells, so ntarg + 1 <= ncell + 1 and d_xp can hold the counts
-    int* cnt = d_xp;
-    if ((size_t)P.ntarg + 1 > (size_t)c->ncell + 1) { cleanup(); return set_error(c, RG_ERR_TOPOLOGY, "too many targets"); }
-    cudaMemsetAsync(cnt, 0, sizeof(int) * ((size_t)P.ntarg + 1), s);
+    // ---- ordered event lists (CSR over targets): counts beyond the last
+    //      target stay 0, so the offsets there hold the total
+    cudaMemsetAsync(cnt, 0, sizeof(int) * tbound, s);
     k_ev_count<NDIM><<<nblk(nc), TPB, 0, s>>>(nc, c->d_cpos, c->d_tmap, P.icn, P.kind, cnt);
-    if (int rc = dalloc(c, &P.toff, (size_t)P.ntarg + 1, "toff")) { cleanup(); return rc; }
-    int total = 0;
-    if (int rc = exclusive_scan(c, cnt, P.toff, P.ntarg + 1, &total)) { cleanup(); return rc; }
-    P.nevents = total;
-    if (int rc = dalloc(c, &P.tev, (size_t)total, "events")) { cleanup(); return rc; }
-    cudaMemsetAsync(cnt, 0, sizeof(int) * ((size_t)P.ntarg + 1), s);
+    if (int rc = exclusive_scan_dev(c, cnt, P.toff, (int)tbound, d_nx + 3)) { cleanup(); return rc; }
+    cudaMemsetAsync(cnt, 0, sizeof(int) * tbound, s);
     k_ev_fill<NDIM><<<nblk(nc), TPB, 0, s>>>(nc, P.level0, P.noct, c->d_cpos, c->d_tmap, P.icn, P.kind, P.toff, cnt,
                                              P.tev);
-    // long targets, compacted into d_textra's space (its content was copied
-    // out above); their events are sorted a block each, the rest a thread each
-    int* d_nlong = d_nx + 2;
-    k_long_targets<<<nblk(P.ntarg), TPB, 0, s>>>(P.ntarg, P.toff, kLongEvents, d_textra, d_nlong);
-    k_ev_sort<<<nblk(P.ntarg), TPB, 0, s>>>(P.ntarg, P.toff, P.tev, kLongEvents);
-    k_ev_sort_long<<<2 * c->sm_count, kSortThreads, 0, s>>>(d_textra, d_nlong, P.toff, P.tev);
-    cudaMemcpyAsync(&hv[2], d_nlong, sizeof(int), cudaMemcpyDeviceToHost, s);
-    int rc_ev = check_cuda(c, cudaStreamSynchronize(s), "plan events");
-    if (!rc_ev && hv[2] > 0) {
-        P.nlong = hv[2];
-        rc_ev = dalloc(c, &P.tlong, (size_t)P.nlong, "long targets");
-        if (!rc_ev) {
-            // in atomic order: targets are independent, so the order changes no result
-            cudaMemcpyAsync(P.tlong, d_textra, sizeof(int) * P.nlong, cudaMemcpyDeviceToDevice, s);
-            rc_ev = check_cuda(c, cudaStreamSynchronize(s), "long targets");
-        }
-    }
+    // long targets (more than kLongEvents events): their events are sorted a
+    // block each, the rest a thread each
+    k_long_targets<<<nblk((long long)tbound), TPB, 0, s>>>(nc, d_nx + 1, P.toff, kLongEvents, P.tlong, d_nx + 2);
+    k_ev_sort<<<nblk((long long)tbound), TPB, 0, s>>>(nc, d_nx + 1, P.toff, P.tev, kLongEvents);
+    k_ev_sort_long<<<2 * c->sm_count, kSortThreads, 0, s>>>(P.tlong, d_nx + 2, P.toff, P.tev);
+    if (int rc = check_cuda(c, cudaGetLastError(), "plan events")) { cleanup(); return rc; }
+    long long nact = 0;
+    cudaMemcpyAsync(hv, d_nx, 4 * sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&nact, d_nact, sizeof(long long), cudaMemcpyDeviceToHost, s);
     cleanup();
-    if (rc_ev) return rc_ev;
+    // one wait: the counts, and the device's checks (the list, the cells)
     if (int rc = check_device_status(c)) return rc;
+    P.nextra_prim = hv[0];
+    P.ntarg = nc + hv[1];
+    P.nlong = hv[2];
+    P.nevents = hv[3];
+    P.nactive = nact;
+    if ((size_t)P.ntarg + 1 > tbound || (size_t)P.nevents > ebound)
+        return set_error(c, RG_ERR_TOPOLOGY, "plan counts above their bounds");
     P.valid = true;
     return RG_OK;
 }
@@ -568,8 +570,9 @@ int build_plan(rg_ctx* c, int ilevel, Plan& plan) {
     }
 }
 
-// Exclusive scan of n ints on the context stream; returns the grand total.
-int exclusive_scan(rg_ctx* c, const int* in, int* out, int n, int* total) {
+// Exclusive scan of n ints on the context stream, the grand total left in
+// device memory (*total_dev; nullptr: the scan scratch).  Enqueue only.
+int exclusive_scan_dev(rg_ctx* c, const int* in, int* out, int n, int* total_dev, int** total_at) {
     int nb = (n + SCAN_ITEMS - 1) / SCAN_ITEMS;
     if (nb < 1) nb = 1;
     size_t need = (size_t)nb + 1;
@@ -579,11 +582,19 @@ int exclusive_scan(rg_ctx* c, const int* in, int* out, int n, int* total) {
         if (dev_alloc(c, &c->d_scan, sizeof(int) * need) != cudaSuccess) return set_error(c, RG_ERR_NOMEM, "scan scratch");
         c->cap_scan = need;
     }
+    int* grand = total_dev ? total_dev : c->d_scan + nb;
     k_scan_blocks<<<nb, SCAN_TPB, 0, c->stream>>>(in, out, n, c->d_scan);
-    k_scan_sums<<<1, SCAN_TPB, 0, c->stream>>>(c->d_scan, nb, c->d_scan + nb);
+    k_scan_sums<<<1, SCAN_TPB, 0, c->stream>>>(c->d_scan, nb, grand);
     k_scan_add<<<nb, SCAN_TPB, 0, c->stream>>>(out, n, c->d_scan);
-    if (int rc = check_cuda(c, cudaGetLastError(), "scan")) return rc;
-    if (int rc = check_cuda(c, cudaMemcpyAsync(total, c->d_scan + nb, sizeof(int), cudaMemcpyDeviceToHost, c->stream),
+    if (total_at) *total_at = grand;
+    return check_cuda(c, cudaGetLastError(), "scan");
+}
+
+// Exclusive scan of n ints on the context stream; returns the grand total.
+int exclusive_scan(rg_ctx* c, const int* in, int* out, int n, int* total) {
+    int* grand = nullptr;
+    if (int rc = exclusive_scan_dev(c, in, out, n, nullptr, &grand)) return rc;
+    if (int rc = check_cuda(c, cudaMemcpyAsync(total, grand, sizeof(int), cudaMemcpyDeviceToHost, c->stream),
                             "scan total"))
         return rc;
     return check_cuda(c, cudaStreamSynchronize(c->stream), "scan sync");
