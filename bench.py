@@ -1033,15 +1033,16 @@ def profile_case_learned():
 
 def profile_case_amr():
     """A small run for ncu captures of the AMR step: the headline's run
-    initialised on the device and 5 coarse steps, two coarse steps inside the
-    NVTX range "steps" (the launch list), then one level step each of
-    level 7 (the 64^3 base level, 261,504 leaf cells) and level 10 (the finest)
-    inside the NVTX range "capture" (ncu --nvtx --nvtx-include capture/)."""
+    initialised on the device and 10 coarse steps, two coarse steps without a
+    tree change (coarse steps 11 and 12, replayed graphs) inside the NVTX range
+    "steps" (the launch list), then one level step each of level 7 (the 64^3
+    base level) and level 10 (the finest) inside the NVTX range "capture"
+    (ncu --nvtx --nvtx-include capture/)."""
     import torch
     import rgpu
     ctx = rgpu.Context(amr_params(rgpu), 0)
     run = amr_run(ctx)
-    for _ in range(5):
+    for _ in range(10):
         run.coarse_step()
     ctx.synchronize()
     torch.cuda.nvtx.range_push("steps")  # two whole coarse steps: the launch list

@@ -23,9 +23,9 @@
 namespace rg {
 namespace {
 
-constexpr int kMaxLevel = 32;
-// device clock: dtnew[0..32], dtold[0..32], t
-constexpr int kDtOld = kMaxLevel + 1, kClockT = 2 * (kMaxLevel + 1), kClockN = kClockT + 1;
+constexpr int kMaxLevel = kClockLevels - 1;
+// device clock: dtnew[0..32], dtold[0..32], t (ClockStep's layout)
+constexpr int kDtOld = kClockDtOld, kClockT = kClockTime, kClockN = kClockT + 1;
 
 enum RunMode { RUN_EAGER, RUN_CAPTURE, RUN_REPLAY };
 
@@ -41,30 +41,6 @@ struct AmrRunState {
     bool open = false, warm_ok = false;
     long long topo = -1;
 };
-
-// Simulation.cpp:552-554: dtold = dtnew; dtnew = the CFL step (the CFL
-// word), capped by the coarser level's dtnew over its sub-cycles
-// (nsub_coarser > 0 above levelmin).  The word is re-armed at dt_start for
-// the next level's CFL pass (the coarse step arms it once at its start).  On a
-// level without finer octs the time update follows (Simulation.cpp:600-607):
-// finer = 1, no finer octs below nlevelmax (the finer level's steps become
-// this one's over its sub-cycles, nsub), finer = 2 at nlevelmax.
-__global__ void k_amr_dt(double* ck, DevStatus* st, int il, int nsub_coarser, double dt_start, int finer, int nsub) {
-    ck[kDtOld + il] = ck[il];
-    double d = __longlong_as_double((long long)st->dtmin_bits);
-    st->dtmin_bits = (unsigned long long)__double_as_longlong(dt_start);
-    if (nsub_coarser > 0) {
-        const double cand = ck[il - 1] / (double)nsub_coarser;
-        d = cand < d ? cand : d;  // std::min(d, cand)
-    }
-    ck[il] = d;
-    if (finer == 1) {
-        const double v = ck[il] / (double)nsub;
-        ck[kDtOld + il + 1] = v;
-        ck[il + 1] = v;
-    }
-    if (finer) ck[kClockT] += ck[il];
-}
 
 __global__ void k_arm_cfl(DevStatus* st, double dt_start) {
     st->dtmin_bits = (unsigned long long)__double_as_longlong(dt_start);
@@ -292,13 +268,17 @@ int amr_step(rg_ctx* c, const rg_amr_config& cfg, AmrRunState& S, int il, int ic
     const bool finer = il < lmax && count_grids(c, il + 1) > 0;
     double* ck = S.ck;
     // before the finer sub-steps: the CFL pass, which also does set_unew (both
-    // read the level's uold, nothing between them writes it; k_amr_dt only
+    // read the level's uold, nothing between them writes it; the clock update only
     // reads the CFL word), and the level's new dt
     auto pre = [&]() -> int {
-        if (int rc = courant_step_device(c, il, dx, cfg.courant_factor, cfg.pressure_cap, true, true)) return rc;
-        k_amr_dt<<<1, 1, 0, c->stream>>>(ck, c->d_status, il, il > lmin ? nsubcycle(cfg, il - 1) : 0,
-                                         c->params.boxlen / 1e-10, finer ? 0 : (il < lmax ? 1 : 2), nsub);
-        return check_cuda(c, cudaGetLastError(), "clock kernels");
+        ClockStep cs;
+        cs.ck = ck;
+        cs.il = il;
+        cs.nsub_coarser = il > lmin ? nsubcycle(cfg, il - 1) : 0;
+        cs.finer = finer ? 0 : (il < lmax ? 1 : 2);
+        cs.nsub = nsub;
+        cs.dt_start = c->params.boxlen / 1e-10;
+        return courant_step_device(c, il, dx, cfg.courant_factor, cfg.pressure_cap, true, true, &cs);
     };
     // after them: the level step with set_uold folded into the fold kernels (a
     // level target's result goes to uold as well; the fold reads only unew and
@@ -447,7 +427,7 @@ extern "C" int rg_amr_coarse_step(rg_ctx* c, const rg_amr_config* cfg, rg_amr_cl
     S.cell_updates = clock->cell_updates;
     S.cfg = cfg;
     // the CFL word's start value, as every CFL pass arms it (launch_courant);
-    // each level's k_amr_dt re-arms it after reading
+    // each level's clock update (the CFL pass's last block) re-arms it after reading
     k_arm_cfl<<<1, 1, 0, c->stream>>>(c->d_status, c->params.boxlen / 1e-10);
     const int rc_step = coarse_step(c, *cfg, S);
     if (rc_step) run_abort(c, S);

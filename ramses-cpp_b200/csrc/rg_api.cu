@@ -564,14 +564,14 @@ int rg_courant_step(rg_ctx* c, int ilevel, double dx, double courant_factor, int
 
 namespace rg {
 int courant_step_device(rg_ctx* c, int ilevel, double dx, double courant_factor, int pressure_cap, bool set_unew,
-                        bool armed) {
+                        bool armed, const ClockStep* clock) {
     CTX_GUARD(c);
     c->next_level = -1;  // the state or the CFL word may change
     if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state uploaded");
     Plan* P;
     if (int rc = get_plan(c, ilevel, &P)) return rc;
     if (P->nbox > 0) return set_error(c, RG_ERR_STATE, "ensemble level: read the per-box steps with rg_level_box_dt");
-    return launch_courant(c, *P, dx, pressure_cap, courant_factor, set_unew, armed);
+    return launch_courant(c, *P, dx, pressure_cap, courant_factor, set_unew, armed, clock);
 }
 
 int godunov_level_device_dt(rg_ctx* c, int ilevel, const double* dt_dev, double dx, bool set_uold) {

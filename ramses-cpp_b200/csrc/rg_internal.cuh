@@ -58,7 +58,43 @@ struct DevStatus {
     double run_t;                                 // rg_level_run: the level's time and
     long long run_steps;                          // substeps, advanced on the device,
     long long run_limit;                          // and the step count this launch stops at
+    unsigned int cfl_done, cfl_pad;               // blocks of a CFL pass done (its clock update)
 };
+
+// The resident AMR step's clock update after a level's CFL pass
+// (Simulation.cpp:552-554, 600-607): on the device clock ck (dtnew[0..32],
+// dtold[0..32], t), dtold = dtnew; dtnew = the CFL word, capped by the
+// coarser level's dtnew over its sub-cycles (nsub_coarser > 0 above
+// levelmin); the word re-armed at dt_start for the next pass; on a level
+// without finer octs the time update follows (finer = 1: no finer octs below
+// nlevelmax, the finer level's steps become this one's over its nsub
+// sub-cycles; finer = 2 at nlevelmax).  ck == nullptr: no update.
+constexpr int kClockLevels = 33, kClockDtOld = kClockLevels, kClockTime = 2 * kClockLevels;
+struct ClockStep {
+    double* ck = nullptr;
+    int il = 0, nsub_coarser = 0, finer = 0, nsub = 1;
+    double dt_start = 0.0;
+};
+
+// word: the CFL word as the pass left it
+__device__ __forceinline__ void clock_step_apply(const ClockStep& cs, DevStatus* st, unsigned long long word) {
+    double* ck = cs.ck;
+    const int il = cs.il;
+    ck[kClockDtOld + il] = ck[il];
+    double d = __longlong_as_double((long long)word);
+    st->dtmin_bits = (unsigned long long)__double_as_longlong(cs.dt_start);
+    if (cs.nsub_coarser > 0) {
+        const double cand = ck[il - 1] / (double)cs.nsub_coarser;
+        d = cand < d ? cand : d;  // std::min(d, cand)
+    }
+    ck[il] = d;
+    if (cs.finer == 1) {
+        const double v = ck[il] / (double)cs.nsub;
+        ck[kClockDtOld + il + 1] = v;
+        ck[il + 1] = v;
+    }
+    if (cs.finer) ck[kClockTime] += ck[il];
+}
 
 // Step values of one box of an ensemble level (independent periodic boxes
 // whose leaf octs share one level list, each with its own dx and CFL step):
@@ -356,13 +392,14 @@ int launch_set_unew(rg_ctx* c, const Plan& p);
 int launch_set_uold(rg_ctx* c, const Plan& p);
 // set_unew: also HydroSolver::set_unew of the level in the same pass;
 // armed: the CFL word already holds its start value (no arming launch)
+// clock (optional): the AMR clock update, done by the pass's last block
 int launch_courant(rg_ctx* c, const Plan& p, double dx, int pressure_cap, double courant_factor,
-                   bool set_unew = false, bool armed = false);
+                   bool set_unew = false, bool armed = false, const ClockStep* clock = nullptr);
 // the step values (dt, dt/dx, 1/dx) from a dt in device memory
 int launch_set_dt_device(rg_ctx* c, const double* dt, double dx);
 // rg_courant_step without reading the step back: the CFL word holds it
 int courant_step_device(rg_ctx* c, int ilevel, double dx, double courant_factor, int pressure_cap,
-                        bool set_unew = false, bool armed = false);
+                        bool set_unew = false, bool armed = false, const ClockStep* clock = nullptr);
 // rg_godunov_level with its dt read by the device from dt_dev
 // set_uold: HydroSolver::set_uold of the level folded into the fold kernels
 int godunov_level_device_dt(rg_ctx* c, int ilevel, const double* dt_dev, double dx, bool set_uold = false);

@@ -408,7 +408,8 @@ __global__ void k_copy_level(TreeView T, PlanView P, int nvar, const double* __r
 // HydroSolver::set_unew does).
 template <int NDIM>
 __global__ void k_courant(TreeView T, PlanView P, const double* __restrict__ uold, DevStatus* st, double dx,
-                          double gamma, double cfl, int pressure_cap, double* __restrict__ unew_copy) {
+                          double gamma, double cfl, int pressure_cap, double* __restrict__ unew_copy,
+                          ClockStep clock) {
     const size_t ncell = (size_t)T.ncell;
     unsigned long long best = ~0ULL;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P.ncells; p += gridDim.x * blockDim.x) {
@@ -451,7 +452,23 @@ __global__ void k_courant(TreeView T, PlanView P, const double* __restrict__ uol
         best = other < best ? other : best;
     }
     if ((threadIdx.x & 31) == 0 && best != ~0ULL) atomicMin(&st->dtmin_bits, best);
+    if (!clock.ck) return;
+    // the last block to finish (every other block's minimum is in the word by
+    // then: each block's warps reduce before its thread 0 fences and counts)
+    // does the clock update and resets the count for the next pass
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&st->cfl_done, 1u) == gridDim.x - 1) {
+            __threadfence();
+            st->cfl_done = 0;
+            clock_step_apply(clock, st, atomicOr(&st->dtmin_bits, 0ULL));  // the word read at L2
+        }
+    }
 }
+
+// The clock update alone (a level without cells in its plan).
+__global__ void k_clock_step(DevStatus* st, ClockStep clock) { clock_step_apply(clock, st, st->dtmin_bits); }
 
 // CFL candidate and primitives in one pass over uold (leaf-level substep).
 template <int NDIM>
@@ -769,19 +786,23 @@ int launch_set_uold(rg_ctx* c, const Plan& P) {
     return check_cuda(c, cudaGetLastError(), "set_uold");
 }
 
-int launch_courant(rg_ctx* c, const Plan& P, double dx, int pressure_cap, double cfl, bool set_unew, bool armed) {
+int launch_courant(rg_ctx* c, const Plan& P, double dx, int pressure_cap, double cfl, bool set_unew, bool armed,
+                   const ClockStep* clock) {
     double start = c->params.boxlen / 1e-10;
     if (!armed) k_courant_init<<<1, 1, 0, c->stream>>>(c->d_status, start);
+    const ClockStep cs = clock ? *clock : ClockStep{};
     if (P.ncells > 0) {
         double* copy = set_unew ? c->d_unew : nullptr;
         if (c->params.ndim == 1)
             k_courant<1><<<grid_for(c, P.ncells, 256), 256, 0, c->stream>>>(tree_view(c), P.view(), c->d_uold,
                                                                              c->d_status, dx, c->params.gamma, cfl,
-                                                                             pressure_cap, copy);
+                                                                             pressure_cap, copy, cs);
         else
             k_courant<3><<<grid_for(c, P.ncells, 256), 256, 0, c->stream>>>(tree_view(c), P.view(), c->d_uold,
                                                                              c->d_status, dx, c->params.gamma, cfl,
-                                                                             pressure_cap, copy);
+                                                                             pressure_cap, copy, cs);
+    } else if (cs.ck) {
+        k_clock_step<<<1, 1, 0, c->stream>>>(c->d_status, cs);
     }
     return check_cuda(c, cudaGetLastError(), "courant");
 }

@@ -570,19 +570,29 @@ __global__ void k_kill(TreeMut M, const int* __restrict__ octs, int noct, const 
 }
 
 // ---------------------------------------------------------------- restrict_fine
-// father = mean of its 8 children, summed in child order (TreeUpdater.cpp:188-207)
-__global__ void k_restrict(TreeMut M, const int* __restrict__ octs, int noct) {
+// father = mean of its 8 children, summed in child order (TreeUpdater.cpp:188-207).
+// The 40 child values are loaded before any store, so they are in flight
+// together (a store to the father could alias a later load otherwise).
+__device__ __forceinline__ void restrict_oct(const TreeMut& M, int ig) {
     const size_t nc = (size_t)M.ncell;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < noct; k += gridDim.x * blockDim.x) {
-        const int ig = octs[k];
-        const int fc = M.father[ig - 1];
-        if (fc <= 0) continue;
-        for (int iv = 0; iv < 5; ++iv) {
-            double sum = 0;
-            for (int s = 0; s < 8; ++s) sum += M.uold[(size_t)iv * nc + M.ncoarse + (size_t)s * M.ngridmax + ig - 1];
-            M.uold[(size_t)iv * nc + fc - 1] = sum / 8;
-        }
+    const int fc = M.father[ig - 1];
+    if (fc <= 0) return;
+    double v[5][8];
+#pragma unroll
+    for (int iv = 0; iv < 5; ++iv)
+#pragma unroll
+        for (int s = 0; s < 8; ++s) v[iv][s] = M.uold[(size_t)iv * nc + M.ncoarse + (size_t)s * M.ngridmax + ig - 1];
+#pragma unroll
+    for (int iv = 0; iv < 5; ++iv) {
+        double sum = 0;
+#pragma unroll
+        for (int s = 0; s < 8; ++s) sum += v[iv][s];
+        M.uold[(size_t)iv * nc + fc - 1] = sum / 8;
     }
+}
+
+__global__ void k_restrict(TreeMut M, const int* __restrict__ octs, int noct) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < noct; k += gridDim.x * blockDim.x) restrict_oct(M, octs[k]);
 }
 
 // The coarse step's work below levelmin in one block: flag_fine(il) for il =
@@ -608,21 +618,10 @@ __global__ void __launch_bounds__(1024) k_tail_below_min(TreeMut M, LevelLists F
         M.cpu_map[i] = 1;
         M.flag1[i] = 1;
     }
-    const size_t nc = (size_t)M.ncell;
     for (int j = 0; j < R.n; ++j) {
         __syncthreads();
         const int* octs = R.octs[j];
-        for (int k = threadIdx.x; k < R.noct[j]; k += blockDim.x) {
-            const int ig = octs[k];
-            const int fc = M.father[ig - 1];
-            if (fc <= 0) continue;
-            for (int iv = 0; iv < 5; ++iv) {
-                double sum = 0;
-                for (int s = 0; s < 8; ++s)
-                    sum += M.uold[(size_t)iv * nc + M.ncoarse + (size_t)s * M.ngridmax + ig - 1];
-                M.uold[(size_t)iv * nc + fc - 1] = sum / 8;
-            }
-        }
+        for (int k = threadIdx.x; k < R.noct[j]; k += blockDim.x) restrict_oct(M, octs[k]);
     }
 }
 
