@@ -119,11 +119,14 @@ __global__ void k_smooth_mark(TreeMut M, const int* __restrict__ octs, int noct,
         const int idc = M.ncoarse + icx * M.ngridmax + ig - 1;
         int o = 0;
         if (M.flag1[idc] == 0) {
+            // the six lookups first, so that their loads are in flight together
+            int nc[6];
+#pragma unroll
+            for (int s = 0; s < 6; ++s) nc[s] = nbor_exact_dir(M, ig, ic, s >> 1, s & 1);
             int nf = 0;
-            for (int s = 0; s < 6; ++s) {
-                const int nc = nbor_exact_dir(M, ig, ic, s >> 1, s & 1);
-                if (nc > 0 && nc <= M.ncell && M.flag1[nc - 1] == 1) ++nf;
-            }
+#pragma unroll
+            for (int s = 0; s < 6; ++s)
+                if (nc[s] > 0 && nc[s] <= M.ncell && M.flag1[nc[s] - 1] == 1) ++nf;
             o = nf > 0;
         }
         ok[p] = o;
@@ -182,13 +185,24 @@ __global__ void k_flag_grad(TreeMut M, const int* __restrict__ octs, int noct, d
         const int icx = p / noct, k = p - icx * noct, ig = octs[k], ic = icx + 1;
         const int idc = M.ncoarse + icx * M.ngridmax + ig - 1;
         if (M.flag1[idc] != 0) continue;
+        // every direction's neighbour ids first (independent lookups, their
+        // loads in flight together); the directions are then tested in order
+        // up to the first that flags the cell, as in the reference
+        int nl[3], nr[3];
+#pragma unroll
+        for (int idim = 0; idim < 3; ++idim) {
+            nl[idim] = nbor_exact_dir(M, ig, ic, idim, 0);
+            nr[idim] = nbor_exact_dir(M, ig, ic, idim, 1);
+        }
+#pragma unroll
+        for (int idim = 0; idim < 3; ++idim) {
+            if (nl[idim] == 0) nl[idim] = M.nbor[(size_t)(2 * idim) * M.ngridmax + ig - 1];
+            if (nr[idim] == 0) nr[idim] = M.nbor[(size_t)(2 * idim + 1) * M.ngridmax + ig - 1];
+        }
         const CellState sc = cell_state(M, idc + 1, gamma);
         bool ok = false;
         for (int idim = 0; idim < 3 && !ok; ++idim) {
-            int id_l = nbor_exact_dir(M, ig, ic, idim, 0);
-            if (id_l == 0) id_l = M.nbor[(size_t)(2 * idim) * M.ngridmax + ig - 1];
-            int id_r = nbor_exact_dir(M, ig, ic, idim, 1);
-            if (id_r == 0) id_r = M.nbor[(size_t)(2 * idim + 1) * M.ngridmax + ig - 1];
+            const int id_l = nl[idim], id_r = nr[idim];
             const CellState sl = (id_l > 0 && id_l <= M.ncell) ? cell_state(M, id_l, gamma) : sc;
             const CellState sr = (id_r > 0 && id_r <= M.ncell) ? cell_state(M, id_r, gamma) : sc;
             if (ed > 0.0 && err_grad(sl.d, sc.d, sr.d, 1e-10) > ed) ok = true;
@@ -595,31 +609,45 @@ __global__ void k_restrict(TreeMut M, const int* __restrict__ octs, int noct) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < noct; k += gridDim.x * blockDim.x) restrict_oct(M, octs[k]);
 }
 
-// The coarse step's work below levelmin in one block: flag_fine(il) for il =
-// levelmin-1..2 (k_flag_init's below-levelmin case: every cell flagged) and
-// for the coarse cells (k_flag_coarse_below_min), then restrict_fine(il) for
-// il = levelmin-2..0 over the lists F.octs given coarsest last, with a barrier
-// between levels so that each restriction reads the one before it (the
-// threads of a block see each other's global writes after __syncthreads).
-// These levels are small (4,681 octs below a levelmin of 7): one block's
-// latency is below the launches it replaces.
+// The coarse step's work below levelmin in two launches.  k_tail_flags_restrict:
+// its first nb_r blocks do restrict_fine(levelmin-1) over the levelmin list
+// (octs, noct), the others flag_fine(il) for il = levelmin-1..2 over the
+// lists F (k_flag_init's below-levelmin case: every cell flagged) and for the
+// coarse cells (k_flag_coarse_below_min) -- independent writes (uold of the
+// levelmin-1 cells, flags).  k_tail_cascade: restrict_fine(il) for il =
+// levelmin-2..0 over the lists R given coarsest last, in one block with a
+// barrier between levels so that each restriction reads the one before it
+// (the threads of a block see each other's global writes after
+// __syncthreads); these levels are small (585 octs in the lists below
+// levelmin-1 for a levelmin of 7), so one block's latency is below the
+// launches it replaces.
 struct LevelLists {
     const int* octs[32];
     int noct[32];
     int n;
 };
 
-__global__ void __launch_bounds__(1024) k_tail_below_min(TreeMut M, LevelLists F, LevelLists R) {
-    for (int j = 0; j < F.n; ++j) {
-        const int noct = F.noct[j], n = 8 * noct;
-        for (int p = threadIdx.x; p < n; p += blockDim.x) M.flag1[lvl_cell(M, F.octs[j], noct, p) - 1] = 1;
+__global__ void k_tail_flags_restrict(TreeMut M, const int* __restrict__ octs, int noct, int nb_r, LevelLists F) {
+    const int b = (int)blockIdx.x;
+    if (b < nb_r) {
+        for (int k = b * blockDim.x + threadIdx.x; k < noct; k += nb_r * blockDim.x) restrict_oct(M, octs[k]);
+        return;
     }
-    for (int i = threadIdx.x; i < M.ncoarse; i += blockDim.x) {
+    const int fb = b - nb_r, nfb = (int)gridDim.x - nb_r;
+    const int stride = nfb * blockDim.x;
+    for (int j = 0; j < F.n; ++j) {
+        const int nj = F.noct[j], n = 8 * nj;
+        for (int p = fb * blockDim.x + threadIdx.x; p < n; p += stride) M.flag1[lvl_cell(M, F.octs[j], nj, p) - 1] = 1;
+    }
+    for (int i = fb * blockDim.x + threadIdx.x; i < M.ncoarse; i += stride) {
         M.cpu_map[i] = 1;
         M.flag1[i] = 1;
     }
+}
+
+__global__ void __launch_bounds__(1024) k_tail_cascade(TreeMut M, LevelLists R) {
     for (int j = 0; j < R.n; ++j) {
-        __syncthreads();
+        if (j > 0) __syncthreads();
         const int* octs = R.octs[j];
         for (int k = threadIdx.x; k < R.noct[j]; k += blockDim.x) restrict_oct(M, octs[k]);
     }
@@ -1067,22 +1095,23 @@ int tree_restrict_fine(rg_ctx* c, int ilevel) {
 // The tail of the coarse step below levelmin: flag_fine(il) for il =
 // levelmin-1..1 and restrict_fine(il) for il = levelmin-1..0 (the
 // restrictions when `restrictions` is set), as the calls one by one leave the
-// tree and the state, in two launches: restrict_fine(levelmin-1) over the
-// levelmin list, then k_tail_below_min.  *done stays false (nothing issued)
-// when the lists below levelmin are not small or not cached, and the caller
-// makes the calls one by one.  Enqueue only.
+// tree and the state, in a few launches (k_tail_flags_restrict, k_restrict
+// for the larger lists, k_tail_cascade for the small ones).
+// *done stays false (nothing issued) when the lists below levelmin are not
+// small or not cached, and the caller makes the calls one by one.  Enqueue
+// only.
 int tree_tail_below_min(rg_ctx* c, int lmin, bool restrictions, bool* done) {
     *done = false;
     if (!c->tree_resident || c->tree_dirty || lmin < 2 || lmin > c->nlevelmax || lmin > 32 || c->levelmin != lmin)
         return RG_OK;
-    LevelLists F{}, R{};
-    long long total = 0;
-    for (int L = 1; L <= lmin; ++L) {
+    for (int L = 1; L <= lmin; ++L)
         if ((int)c->lvl_ver.size() <= L || (c->lvl_ver[(size_t)L] != c->topo_version && c->h_numbl[(size_t)hidx(c, L)] > 0))
             return RG_OK;
-        if (L < lmin) total += c->h_numbl[(size_t)hidx(c, L)];
-    }
-    if (total > 16384) return RG_OK;
+    // lists below levelmin beyond a few thousand octs: call by call
+    long long below = 0;
+    for (int L = 1; L <= lmin - 1; ++L) below += c->h_numbl[(size_t)hidx(c, L)];
+    if (below > 65536) return RG_OK;
+    LevelLists F{}, R{};
     for (int L = lmin - 1; L >= 2; --L) {
         const int* octs = nullptr;
         int noct = 0;
@@ -1090,23 +1119,35 @@ int tree_tail_below_min(rg_ctx* c, int lmin, bool restrictions, bool* done) {
         F.octs[F.n] = octs;
         F.noct[F.n++] = noct;
     }
+    // lists with more octs than the cascade's block takes in a few rounds get
+    // their own launch (those come first: the lists grow with the level)
+    const int* big[32];
+    int nbig[32], nb = 0;
     if (restrictions)
         for (int L = lmin - 1; L >= 1; --L) {
             const int* octs = nullptr;
             int noct = 0;
             if (int rc = level_octs_cached(c, L, &octs, &noct)) return rc;
+            if (R.n == 0 && noct > 2048) {
+                big[nb] = octs;
+                nbig[nb++] = noct;
+                continue;
+            }
             R.octs[R.n] = octs;
             R.noct[R.n++] = noct;
         }
+    const int* top = nullptr;
+    int ntop = 0;
+    if (restrictions)
+        if (int rc = level_octs_cached(c, lmin, &top, &ntop)) return rc;
+    long long nflag = c->ncoarse;
+    for (int j = 0; j < F.n; ++j) nflag += 8LL * F.noct[j];
     c->next_level = -1;
     TreeMut M = tree_mut(c);
-    if (restrictions) {
-        const int* octs = nullptr;
-        int noct = 0;
-        if (int rc = level_octs_cached(c, lmin, &octs, &noct)) return rc;
-        if (noct > 0) k_restrict<<<nblk(noct), TPB, 0, c->stream>>>(M, octs, noct);
-    }
-    k_tail_below_min<<<1, 1024, 0, c->stream>>>(M, F, R);
+    const int nb_r = ntop > 0 ? nblk(ntop) : 0;
+    k_tail_flags_restrict<<<nb_r + nblk(nflag), TPB, 0, c->stream>>>(M, top, ntop, nb_r, F);
+    for (int i = 0; i < nb; ++i) k_restrict<<<nblk(nbig[i]), TPB, 0, c->stream>>>(M, big[i], nbig[i]);
+    if (R.n > 0) k_tail_cascade<<<1, 1024, 0, c->stream>>>(M, R);
     c->auth_dirty = true;  // k_flag_coarse_below_min's part: the coarse cells' cpu_map
     *done = true;
     return check_cuda(c, cudaGetLastError(), "tail below levelmin");
