@@ -1051,10 +1051,14 @@ def profile_case_amr():
     ctx.synchronize()
     torch.cuda.nvtx.range_pop()
     torch.cuda.nvtx.range_push("capture")
+    cells = {}
     for il in (7, 10):
         ctx.godunov_level(il, 1e-7, 1.0 / 2 ** il)
+        cells[il] = ctx.cell_updates(il)
     ctx.synchronize()
     torch.cuda.nvtx.range_pop()
+    print(json.dumps({"profile_case": "amr", "cell_updates_per_launch": cells,
+                      "face_variants": {il: ctx.face_config(il)[0] for il in (7, 10)}}))
     ctx.close()
 
 
