@@ -220,8 +220,16 @@ int refresh_tree(rg_ctx* c) {
     if (!c->tree_dirty) return RG_OK;
     c->tree_dirty = false;
     if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "tree refresh")) return rc;
-    invalidate_plans(c);
+    // the plans and oct lists of the levels the changes cannot reach stay
+    // (make_grid_fine and remove_grid_fine mark the levels they reach)
+    auto dirty = [](uint64_t m, size_t L) { return L > 63 || ((m >> L) & 1ull); };
+    for (size_t L = 0; L < c->plans.size(); ++L)
+        if (dirty(c->plans_dirty, L)) free_plan(c, c->plans[L]);
+    const long long old = c->topo_version;
     c->topo_version++;
+    for (size_t L = 0; L < c->lvl_ver.size(); ++L)
+        if (c->lvl_ver[L] == old && !dirty(c->lists_dirty, L)) c->lvl_ver[L] = c->topo_version;
+    c->plans_dirty = c->lists_dirty = 0;
     if (int rc = rank_lists(c)) return rc;
     if (int rc = compute_cell_levels(c)) return rc;
     return check_device_status(c);
@@ -367,6 +375,7 @@ int rg_sync_topology(rg_ctx* c, const rg_grid_view* g) {
     if (g->ncpu != 1) return set_error(c, RG_ERR_UNSUPPORTED, "ncpu must be 1 (the hydro path has no halo exchange)");
     cudaStreamSynchronize(c->stream);
     invalidate_plans(c);
+    c->plans_dirty = c->lists_dirty = ~0ull;
     bool resized = g->ncell != c->ncell;
     c->ncoarse = g->ncoarse;
     c->ngridmax = g->ngridmax;

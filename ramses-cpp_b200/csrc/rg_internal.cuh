@@ -304,6 +304,10 @@ struct rg_ctx {
     bool amr_graphs_on = true;
     long long amr_captured = 0, amr_replayed = 0;
     bool tree_dirty = false;  // links changed on the device: ranks, cell levels and plans are stale
+    // the levels whose plans (bit L) and oct lists a tree change since the
+    // last refresh may have changed: the next refresh drops only those (bits
+    // above 63 stand for themselves: such levels always count as changed)
+    uint64_t plans_dirty = ~0ull, lists_dirty = ~0ull;
     // authorize_fine (flag2 = cpu_map == myid over every cell) has an effect:
     // false while flag2 == (cpu_map == 1) holds everywhere, which only
     // attaching, refining (new cells' cpu_map), removing (freed cells' flag2)

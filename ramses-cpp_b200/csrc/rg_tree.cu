@@ -656,6 +656,13 @@ __global__ void __launch_bounds__(1024) k_tail_cascade(TreeMut M, LevelLists R) 
 // ---------------------------------------------------------------- host side
 int hidx(const rg_ctx* c, int ilevel) { return ilevel * (c->ncpu + c->nboundary); }
 
+// A change of the tree's links reaches the plans of levels lo..hi (bits of
+// levels above 63 are implied) and the oct list of level `list`.
+void mark_changed(rg_ctx* c, int lo, int hi, int list) {
+    for (int L = lo < 0 ? 0 : lo; L <= hi && L <= 63; ++L) c->plans_dirty |= 1ull << L;
+    if (list >= 0 && list <= 63) c->lists_dirty |= 1ull << list;
+}
+
 // RG_OK to go on, kNoOp when the call does nothing (ilevel >= nlevelmax, where
 // the reference returns at once), else an error code (error codes are negative)
 constexpr int kNoOp = 1;
@@ -858,6 +865,7 @@ int tree_grow_arrays(rg_ctx* c, int need) {
     c->ncell = n1;
     c->next_level = -1;
     c->tree_dirty = true;  // cell ids moved: plans, ranks and cell levels are stale
+    c->plans_dirty = c->lists_dirty = ~0ull;
     if (int rc = check_cuda(c, cudaGetLastError(), "tree growth kernels")) return rc;
     // the upload above reads the host ring: keep it alive until the copy is done
     return check_cuda(c, cudaStreamSynchronize(c->stream), "tree growth");
@@ -968,6 +976,11 @@ int tree_make_grid_fine(rg_ctx* c, int ilevel, int* changed) {
     if (c->numbf > 0)
         if (int rc = set_dev_int(c, c->d_prev + c->h_fq[(size_t)c->fq_head] - 1, 0)) return rc;
     c->tree_dirty = true;
+    // refining level-L cells changes their son links (the plan of level L),
+    // adds octs to list L + 1 (its plan and list), and changes which cells
+    // exist at level L + 1, hence the neighbour and ghost-stencil cells of
+    // levels L + 1 and L + 2; level L - 1 is included as a margin
+    mark_changed(c, ilevel - 1, ilevel + 2, ilevel + 1);
     if (changed) *changed = n;
     if (int rc = check_cuda(c, cudaGetLastError(), "make_grid_fine kernels")) return rc;
     return check_device_status(c);
@@ -1010,6 +1023,10 @@ int tree_remove_grid_fine(rg_ctx* c, int ilevel, int* changed) {
     c->h_taill[(size_t)hidx(c, ilevel)] = ends[1];
     c->h_numbl[(size_t)hidx(c, ilevel)] -= nkill;
     c->tree_dirty = true;
+    // removing level-L octs changes list L (its plan and list), the son links
+    // of their fathers (the plan of level L - 1) and the ghost-stencil cells of
+    // level L + 1; level L - 2 is included as a margin
+    mark_changed(c, ilevel - 2, ilevel + 1, ilevel);
     if (changed) *changed = nkill;
     if (int rc = check_cuda(c, cudaGetLastError(), "remove_grid_fine kernels")) return rc;
     return check_device_status(c);
