@@ -94,6 +94,29 @@ bool same_cfg(const rg_amr_config& a, const rg_amr_config& b) {
            a.pressure_cap == b.pressure_cap && a.boxlen == b.boxlen;
 }
 
+// Everything a run can touch made ready ahead of a capture: every stepped
+// level's plan, flux scratch and face shape, every level's oct list.  A run
+// warmed this way is captured at its first visit; false (nothing captured)
+// when a level waits for its shape to be timed, or the tree scratch is not
+// there yet.
+int prepare_run(rg_ctx* c, const rg_amr_config& cfg, bool* ready) {
+    *ready = false;
+    if (!c->d_tscr) return RG_OK;
+    bool ok = true;
+    for (int L = cfg.levelmin; L <= c->nlevelmax && ok; ++L)
+        if (count_grids(c, L) > 0)
+            if (int rc = prepare_level_step(c, L, &ok)) return rc;
+    if (!ok) return RG_OK;
+    for (int L = 1; L <= c->nlevelmax; ++L) {
+        if (count_grids(c, L) == 0) continue;
+        const int* octs = nullptr;
+        int noct = 0;
+        if (int rc = level_octs_cached(c, L, &octs, &noct)) return rc;
+    }
+    *ready = !c->tree_dirty;
+    return RG_OK;
+}
+
 int run_begin(rg_ctx* c, AmrRunState& S) {
     // settle the topology first: a run never changes it, so its version holds
     // for every segment of the run
@@ -111,7 +134,13 @@ int run_begin(rg_ctx* c, AmrRunState& S) {
         ++c->amr_replayed;
         return check_cuda(c, cudaGraphLaunch(g.exec, c->stream), "coarse-step graph");
     }
-    if (base && g.warm == v && g.failed != v && same_cfg(g.cfg, *S.cfg)) {
+    bool warm = base && g.failed != v && g.warm == v && same_cfg(g.cfg, *S.cfg);
+    if (base && g.failed != v && !warm) {
+        // first visit at this topology: warm the caches here and capture now
+        if (int rc = prepare_run(c, *S.cfg, &warm)) return rc;
+        warm = warm && c->topo_version == v;
+    }
+    if (warm) {
         if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
             S.mode = RUN_CAPTURE;
             g.flux = c->d_flux;

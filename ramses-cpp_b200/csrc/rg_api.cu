@@ -583,6 +583,26 @@ int courant_step_device(rg_ctx* c, int ilevel, double dx, double courant_factor,
     return launch_courant(c, *P, dx, pressure_cap, courant_factor, set_unew, armed, clock);
 }
 
+int prepare_level_step(rg_ctx* c, int ilevel, bool* ready) {
+    Plan* P;
+    if (int rc = get_plan(c, ilevel, &P)) return rc;
+    if (P->nbox > 0) {
+        *ready = false;
+        return RG_OK;
+    }
+    if (P->ncells == 0 || P->nactive == 0) return RG_OK;
+    if (int rc = ensure_flux(c, *P)) return rc;
+    if (P->face_variant < 0) {
+        // a level the tuner would time waits for its first eager substep
+        if (P->ncells >= (1 << 17) && !c->no_autotune) {
+            *ready = false;
+            return RG_OK;
+        }
+        if (int rc = autotune_face(c, *P, step_consts(c))) return rc;
+    }
+    return RG_OK;
+}
+
 int godunov_level_device_dt(rg_ctx* c, int ilevel, const double* dt_dev, double dx, bool set_uold) {
     CTX_GUARD(c);
     c->next_level = -1;  // the state or the CFL word may change

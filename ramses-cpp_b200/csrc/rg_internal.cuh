@@ -348,6 +348,11 @@ int level_oct_list(rg_ctx* c, int ilevel, int* out, int cap, int* noct);
 // only when the topology changed since it was built; *octs stays valid until
 // the next tree change.
 int level_octs_cached(rg_ctx* c, int ilevel, const int** octs, int* noct);
+// what a level step needs before it can be captured: the plan, the flux
+// scratch, the face shape of a level too small to be timed (*ready becomes
+// false, nothing else done, for a level whose shape waits for timing or an
+// ensemble level)
+int prepare_level_step(rg_ctx* c, int ilevel, bool* ready);
 // after device tree operations changed links: drop plans, re-rank the lists,
 // recompute cell levels (no-op when nothing changed)
 int refresh_tree(rg_ctx* c);
