@@ -322,8 +322,9 @@ int rg_exact_stats(rg_ctx* ctx, int64_t* iters, int64_t* calls, int reset);
 /* The face kernel's launch shape (tiles per block, register cap, batch of
  * tiles per queue grab) is timed on the first substep of each level of 2^17
  * cells or more and the fastest kept; a smaller 3-D level takes the default
- * shape, or the one with 10 resident blocks per SM when its tiles of 32 cells
- * outnumber the default's 8 per SM.  on == 0 keeps the default shape. */
+ * shape, or, when its tiles of 32 cells outnumber the default's 8 resident
+ * blocks per SM, the one with 9 or 10 that holds them in one wave.  on == 0
+ * keeps the default shape. */
 int rg_set_autotune(rg_ctx* ctx, int on);
 /* ---- ensembles of independent boxes (no reference counterpart) ----------
  * Many independent periodic boxes, each a uniform grid the reference would

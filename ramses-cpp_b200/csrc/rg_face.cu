@@ -35,14 +35,17 @@ int autotune_face(rg_ctx* c, Plan& P, const StepK& K) {
     P.face_batch = 1;
     // small levels are not timed (75 launches would cost more than any shape
     // can save, and AMR rebuilds its small levels whenever the tree changes).
-    // They keep the default shape (8 resident blocks per SM, one tile a block)
-    // unless their tiles outnumber its resident blocks; then the shape with 10
-    // resident blocks per SM (variant 2) -- on the finest level of the Sedov
-    // AMR run (1,280 tiles) face 0.373 instead of 0.409 ms per coarse step
+    // A level whose tiles (one block each) outnumber the default shape's
+    // resident blocks (8 per SM) takes the shape with the fewest resident
+    // blocks per SM that still holds them all in one wave -- 9 (variant 3)
+    // or 10 (variant 2), the fewer the more registers a thread keeps -- and
+    // variant 2 beyond that (on the finest level of the Sedov AMR run, 1,272
+    // tiles: face 0.373 instead of 0.409 ms per coarse step with variant 2)
     if (c->no_autotune) return RG_OK;
     if (P.ncells < (1 << 17)) {
         const int ntiles = (P.ncells + TILE - 1) / TILE;
-        if (c->params.ndim == 3 && P.nbox == 0 && !P.lattice && ntiles > 8 * c->sm_count) P.face_variant = 2;
+        if (c->params.ndim == 3 && P.nbox == 0 && !P.lattice && ntiles > 8 * c->sm_count)
+            P.face_variant = ntiles <= 9 * c->sm_count ? 3 : 2;
         return RG_OK;
     }
     const int ns = 2 * c->params.ndim, nv = c->params.ndim + 2;

@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(TILE * NDIM * R, MINB)
 // elsewhere they fall back to the default variant); ids 9 and 10 the brick
 // kernel (launch-bounds minimum 3 and 2) on levels that form one complete
 // periodic lattice, the default variant elsewhere.
-#define RG_FACE_VARIANTS(X) X(0, 1, 6) X(1, 1, 8) X(2, 1, 10) X(3, 1, 12) X(4, 2, 4) X(5, 2, 5) X(6, 2, 6)
+#define RG_FACE_VARIANTS(X) X(0, 1, 6) X(1, 1, 8) X(2, 1, 10) X(3, 1, 9) X(4, 2, 4) X(5, 2, 5) X(6, 2, 6)
 constexpr int kFirstPipeVariant = 7;
 constexpr int kFirstBrickVariant = 9;  // 9, 10: brick kernel (rg_face_brick.cuh), lattice levels only
 constexpr int kNumFaceVariants = 11;
