@@ -299,6 +299,9 @@ int amr_step(rg_ctx* c, const rg_amr_config& cfg, AmrRunState& S, int il, int ic
     // before the finer sub-steps: the CFL pass, which also does set_unew (both
     // read the level's uold, nothing between them writes it; the clock update only
     // reads the CFL word), and the level's new dt
+    // On a level without finer octs the level step follows at once: the CFL
+    // pass then also forms the primitives (uold changes in between for none
+    // of the cells they are read from) and sets the step values.
     auto pre = [&]() -> int {
         ClockStep cs;
         cs.ck = ck;
@@ -307,7 +310,9 @@ int amr_step(rg_ctx* c, const rg_amr_config& cfg, AmrRunState& S, int il, int ic
         cs.finer = finer ? 0 : (il < lmax ? 1 : 2);
         cs.nsub = nsub;
         cs.dt_start = c->params.boxlen / 1e-10;
-        return courant_step_device(c, il, dx, cfg.courant_factor, cfg.pressure_cap, true, true, &cs);
+        cs.set_step = finer ? 0 : 1;
+        cs.dx = dx;
+        return courant_step_device(c, il, dx, cfg.courant_factor, cfg.pressure_cap, true, true, &cs, !finer);
     };
     // after them: the level step with set_uold folded into the fold kernels (a
     // level target's result goes to uold as well; the fold reads only unew and
@@ -315,7 +320,7 @@ int amr_step(rg_ctx* c, const rg_amr_config& cfg, AmrRunState& S, int il, int ic
     // This level's dtnew is still the one set above: the finer steps only
     // change the finer levels' entries.
     auto post = [&]() -> int {
-        if (int rc = godunov_level_device_dt(c, il, ck + il, dx, true)) return rc;
+        if (int rc = godunov_level_device_dt(c, il, ck + il, dx, true, !finer)) return rc;
         if (Plan* P = existing_plan(c, il); P == nullptr || P->ncells == 0)
             if (int rc = rg_set_uold(c, il)) return rc;
         if (il < lmax)

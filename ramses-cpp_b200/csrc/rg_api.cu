@@ -573,14 +573,14 @@ int rg_courant_step(rg_ctx* c, int ilevel, double dx, double courant_factor, int
 
 namespace rg {
 int courant_step_device(rg_ctx* c, int ilevel, double dx, double courant_factor, int pressure_cap, bool set_unew,
-                        bool armed, const ClockStep* clock) {
+                        bool armed, const ClockStep* clock, bool with_prim) {
     CTX_GUARD(c);
     c->next_level = -1;  // the state or the CFL word may change
     if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state uploaded");
     Plan* P;
     if (int rc = get_plan(c, ilevel, &P)) return rc;
     if (P->nbox > 0) return set_error(c, RG_ERR_STATE, "ensemble level: read the per-box steps with rg_level_box_dt");
-    return launch_courant(c, *P, dx, pressure_cap, courant_factor, set_unew, armed, clock);
+    return launch_courant(c, *P, dx, pressure_cap, courant_factor, set_unew, armed, clock, with_prim);
 }
 
 int prepare_level_step(rg_ctx* c, int ilevel, bool* ready) {
@@ -603,7 +603,7 @@ int prepare_level_step(rg_ctx* c, int ilevel, bool* ready) {
     return RG_OK;
 }
 
-int godunov_level_device_dt(rg_ctx* c, int ilevel, const double* dt_dev, double dx, bool set_uold) {
+int godunov_level_device_dt(rg_ctx* c, int ilevel, const double* dt_dev, double dx, bool set_uold, bool prim_ready) {
     CTX_GUARD(c);
     c->next_level = -1;  // the state or the CFL word may change
     if (!c->have_state) return set_error(c, RG_ERR_STATE, "no state uploaded");
@@ -616,7 +616,7 @@ int godunov_level_device_dt(rg_ctx* c, int ilevel, const double* dt_dev, double 
     // (HydroSolver.cpp:119), so neither is anything launched or moved
     if (P->ncells == 0 || P->nactive == 0) return RG_OK;
     if (int rc = ensure_flux(c, *P)) return rc;
-    if (int rc = launch_godunov(c, *P, set_uold, dt_dev, dx)) return rc;  // the primitive pass sets dt
+    if (int rc = launch_godunov(c, *P, set_uold, dt_dev, dx, prim_ready)) return rc;  // the primitive pass sets dt
     if (P->face_variant < 0 && ++P->substeps_run >= 1) return autotune_face(c, *P, step_consts(c));
     return RG_OK;
 }

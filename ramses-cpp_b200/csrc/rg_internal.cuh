@@ -74,6 +74,10 @@ struct ClockStep {
     double* ck = nullptr;
     int il = 0, nsub_coarser = 0, finer = 0, nsub = 1;
     double dt_start = 0.0;
+    // set_step: the level's step values (dt, dx, dt/dx) are set from the new
+    // dtnew right away (a level whose godunov step follows its CFL pass)
+    int set_step = 0;
+    double dx = 0.0;
 };
 
 // word: the CFL word as the pass left it
@@ -402,21 +406,27 @@ int launch_set_uold(rg_ctx* c, const Plan& p);
 // set_unew: also HydroSolver::set_unew of the level in the same pass;
 // armed: the CFL word already holds its start value (no arming launch)
 // clock (optional): the AMR clock update, done by the pass's last block
+// with_prim: the pass also writes the primitives of the level's cells and its
+// extra (ghost-stencil) cells, the godunov step's first pass
 int launch_courant(rg_ctx* c, const Plan& p, double dx, int pressure_cap, double courant_factor,
-                   bool set_unew = false, bool armed = false, const ClockStep* clock = nullptr);
+                   bool set_unew = false, bool armed = false, const ClockStep* clock = nullptr, bool with_prim = false);
 // the step values (dt, dt/dx, 1/dx) from a dt in device memory
 int launch_set_dt_device(rg_ctx* c, const double* dt, double dx);
 // rg_courant_step without reading the step back: the CFL word holds it
 int courant_step_device(rg_ctx* c, int ilevel, double dx, double courant_factor, int pressure_cap,
-                        bool set_unew = false, bool armed = false, const ClockStep* clock = nullptr);
+                        bool set_unew = false, bool armed = false, const ClockStep* clock = nullptr,
+                        bool with_prim = false);
 // rg_godunov_level with its dt read by the device from dt_dev
 // set_uold: HydroSolver::set_uold of the level folded into the fold kernels
-int godunov_level_device_dt(rg_ctx* c, int ilevel, const double* dt_dev, double dx, bool set_uold = false);
+// prim_ready: the primitives and step values are in place (the CFL pass with
+// with_prim and set_step), so the primitive pass is not launched
+int godunov_level_device_dt(rg_ctx* c, int ilevel, const double* dt_dev, double dx, bool set_uold = false,
+                            bool prim_ready = false);
 int launch_set_dt_host(rg_ctx* c, double dt, double dx);
 int launch_finalize_dt(rg_ctx* c, double dx);
 // dt_dev != nullptr: the primitive pass also sets the step values from it
 int launch_godunov(rg_ctx* c, const Plan& p, bool set_uold = false, const double* dt_dev = nullptr,
-                   double dx = 0.0);
+                   double dx = 0.0, bool prim_ready = false);
 // the four events a level step records its kernel boundaries into: the
 // context's last-call set, or in accumulating mode the next set of the pool
 cudaEvent_t* step_events(rg_ctx* c, long long ncells);

@@ -409,11 +409,24 @@ __global__ void k_copy_level(TreeView T, PlanView P, int nvar, const double* __r
 template <int NDIM>
 __global__ void k_courant(TreeView T, PlanView P, const double* __restrict__ uold, DevStatus* st, double dx,
                           double gamma, double cfl, int pressure_cap, double* __restrict__ unew_copy,
-                          ClockStep clock) {
+                          ClockStep clock, double* __restrict__ prim, double smalle) {
+    constexpr int NV = NDIM + 2;
     const size_t ncell = (size_t)T.ncell;
     unsigned long long best = ~0ULL;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P.ncells; p += gridDim.x * blockDim.x) {
-        int id = cell_of(T, P, p);
+    // with prim: the extra (ghost-stencil) cells after the level's, primitives only
+    const int total = prim ? P.ncells + P.nextra_prim : P.ncells;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x) {
+        int id = (p < P.ncells) ? cell_of(T, P, p) : P.xprim[p - P.ncells];
+        if (prim) {
+            // k_prim's pass (ctoprim of uold), folded in
+            double u[NV], q[NV];
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) u[iv] = uold[(size_t)iv * ncell + id - 1];
+            ctoprim<NDIM>(u, q, gamma, smalle);
+#pragma unroll
+            for (int iv = 0; iv < NV; ++iv) prim[(size_t)iv * ncell + id - 1] = q[iv];
+            if (p >= P.ncells) continue;
+        }
         if (unew_copy) {
 #pragma unroll
             for (int iv = 0; iv < NDIM + 2; ++iv) unew_copy[(size_t)iv * ncell + id - 1] = uold[(size_t)iv * ncell + id - 1];
@@ -463,12 +476,16 @@ __global__ void k_courant(TreeView T, PlanView P, const double* __restrict__ uol
             __threadfence();
             st->cfl_done = 0;
             clock_step_apply(clock, st, atomicOr(&st->dtmin_bits, 0ULL));  // the word read at L2
+            if (clock.set_step) set_step_values(st, clock.ck[clock.il], clock.dx);
         }
     }
 }
 
 // The clock update alone (a level without cells in its plan).
-__global__ void k_clock_step(DevStatus* st, ClockStep clock) { clock_step_apply(clock, st, st->dtmin_bits); }
+__global__ void k_clock_step(DevStatus* st, ClockStep clock) {
+    clock_step_apply(clock, st, st->dtmin_bits);
+    if (clock.set_step) set_step_values(st, clock.ck[clock.il], clock.dx);
+}
 
 // CFL candidate and primitives in one pass over uold (leaf-level substep).
 template <int NDIM>
@@ -619,7 +636,7 @@ void launch_face_n(rg_ctx* c, const Plan& P, const StepK& K) {
 }
 
 template <int NDIM>
-int launch_godunov_t(rg_ctx* c, const Plan& P, bool set_uold, const double* dt_dev, double dx) {
+int launch_godunov_t(rg_ctx* c, const Plan& P, bool set_uold, const double* dt_dev, double dx, bool prim_ready) {
     constexpr int NV = NDIM + 2, NS = 2 * NDIM;
     if (P.ncells == 0) return RG_OK;
     // the caller sized the shared flux scratch (ensure_flux) outside any capture:
@@ -632,8 +649,9 @@ int launch_godunov_t(rg_ctx* c, const Plan& P, bool set_uold, const double* dt_d
     cudaEvent_t* E = c->timing ? step_events(c, P.ncells) : nullptr;
     if (E) cudaEventRecord(E[0], c->stream);
     int nprim = P.ncells + P.nextra_prim;
-    k_prim<NDIM><<<grid_for(c, nprim, 256), 256, 0, c->stream>>>(T, V, c->d_uold, c->d_prim, K.gamma, K.smalle,
-                                                                 c->d_status, dt_dev, dx);
+    if (!prim_ready)
+        k_prim<NDIM><<<grid_for(c, nprim, 256), 256, 0, c->stream>>>(T, V, c->d_uold, c->d_prim, K.gamma, K.smalle,
+                                                                     c->d_status, dt_dev, dx);
     if (E) cudaEventRecord(E[1], c->stream);
     if (int rc = launch_face_tiles(c, P, K, c->d_uold, c->d_prim, c->d_flux, fsum)) return rc;
     if (E) cudaEventRecord(E[2], c->stream);
@@ -686,9 +704,9 @@ cudaEvent_t* step_events(rg_ctx* c, long long ncells) {
     return c->acc_ev[c->acc_n++].data();
 }
 
-int launch_godunov(rg_ctx* c, const Plan& P, bool set_uold, const double* dt_dev, double dx) {
-    if (c->params.ndim == 1) return launch_godunov_t<1>(c, P, set_uold, dt_dev, dx);
-    return launch_godunov_t<3>(c, P, set_uold, dt_dev, dx);
+int launch_godunov(rg_ctx* c, const Plan& P, bool set_uold, const double* dt_dev, double dx, bool prim_ready) {
+    if (c->params.ndim == 1) return launch_godunov_t<1>(c, P, set_uold, dt_dev, dx, prim_ready);
+    return launch_godunov_t<3>(c, P, set_uold, dt_dev, dx, prim_ready);
 }
 
 int launch_godunov_ext(rg_ctx* c, const Plan& P, const double* uold, double* unew, double* prim, double* flux) {
@@ -787,20 +805,23 @@ int launch_set_uold(rg_ctx* c, const Plan& P) {
 }
 
 int launch_courant(rg_ctx* c, const Plan& P, double dx, int pressure_cap, double cfl, bool set_unew, bool armed,
-                   const ClockStep* clock) {
+                   const ClockStep* clock, bool with_prim) {
     double start = c->params.boxlen / 1e-10;
     if (!armed) k_courant_init<<<1, 1, 0, c->stream>>>(c->d_status, start);
     const ClockStep cs = clock ? *clock : ClockStep{};
     if (P.ncells > 0) {
         double* copy = set_unew ? c->d_unew : nullptr;
+        double* prim = with_prim ? c->d_prim : nullptr;
+        const long long work = with_prim ? (long long)P.ncells + P.nextra_prim : P.ncells;
+        const StepK K = step_consts(c);
         if (c->params.ndim == 1)
-            k_courant<1><<<grid_for(c, P.ncells, 256), 256, 0, c->stream>>>(tree_view(c), P.view(), c->d_uold,
-                                                                             c->d_status, dx, c->params.gamma, cfl,
-                                                                             pressure_cap, copy, cs);
+            k_courant<1><<<grid_for(c, work, 256), 256, 0, c->stream>>>(tree_view(c), P.view(), c->d_uold,
+                                                                        c->d_status, dx, c->params.gamma, cfl,
+                                                                        pressure_cap, copy, cs, prim, K.smalle);
         else
-            k_courant<3><<<grid_for(c, P.ncells, 256), 256, 0, c->stream>>>(tree_view(c), P.view(), c->d_uold,
-                                                                             c->d_status, dx, c->params.gamma, cfl,
-                                                                             pressure_cap, copy, cs);
+            k_courant<3><<<grid_for(c, work, 256), 256, 0, c->stream>>>(tree_view(c), P.view(), c->d_uold,
+                                                                        c->d_status, dx, c->params.gamma, cfl,
+                                                                        pressure_cap, copy, cs, prim, K.smalle);
     } else if (cs.ck) {
         k_clock_step<<<1, 1, 0, c->stream>>>(c->d_status, cs);
     }
