@@ -323,6 +323,24 @@ void launch_fold(rg_ctx* c, const Plan& P, const TreeView& T, const PlanView& V,
                                                                    c->d_status, gamma, uold, fsum, uold_out);
 }
 
+// The block's minimum of `best` (every thread of the block calls this, none
+// may have returned) min-ed into *dst with one global atomic per block: the
+// warps' minima meet in shared memory first, so thousands of warps do not
+// queue on the one word.  The minimum of bit patterns is the same in any
+// order.
+__device__ __forceinline__ void block_atomic_min(unsigned long long best, unsigned long long* dst) {
+    __shared__ unsigned long long s_min;
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
+        best = other < best ? other : best;
+    }
+    if (threadIdx.x == 0) s_min = ~0ULL;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0 && best != ~0ULL) atomicMin(&s_min, best);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_min != ~0ULL) atomicMin(dst, s_min);
+}
+
 // Leaf-level fold that also prepares the next substep: on a level whose
 // stencils and updates stay inside it (no extra primitive cells, no extra
 // targets), the new state of every level cell is in registers here, so its
@@ -384,13 +402,7 @@ __global__ void k_fold_next(TreeView T, PlanView P, const double* __restrict__ f
             best_all = best < best_all ? best : best_all;
         }
     }
-    if constexpr (!BOXED) {
-        for (int o = 16; o > 0; o >>= 1) {
-            const unsigned long long other = __shfl_xor_sync(0xffffffffu, best_all, o);
-            best_all = other < best_all ? other : best_all;
-        }
-        if (lane == 0 && best_all != ~0ULL) atomicMin(&st->dtmin_bits, best_all);
-    }
+    if constexpr (!BOXED) block_atomic_min(best_all, &st->dtmin_bits);
 }
 
 __global__ void k_copy_level(TreeView T, PlanView P, int nvar, const double* __restrict__ src, double* __restrict__ dst,
@@ -459,17 +471,11 @@ __global__ void k_courant(TreeView T, PlanView P, const double* __restrict__ uol
         unsigned long long b = (unsigned long long)__double_as_longlong(dtc);
         if (dtc >= 0.0 && b < best) best = b;
     }
-    // warp reduction then one atomic per warp
-    for (int o = 16; o > 0; o >>= 1) {
-        unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
-        best = other < best ? other : best;
-    }
-    if ((threadIdx.x & 31) == 0 && best != ~0ULL) atomicMin(&st->dtmin_bits, best);
+    block_atomic_min(best, &st->dtmin_bits);
     if (!clock.ck) return;
     // the last block to finish (every other block's minimum is in the word by
-    // then: each block's warps reduce before its thread 0 fences and counts)
+    // then: each block's thread 0 puts it there before it fences and counts)
     // does the clock update and resets the count for the next pass
-    __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
         if (atomicAdd(&st->cfl_done, 1u) == gridDim.x - 1) {
@@ -507,11 +513,7 @@ __global__ void k_courant_prim(TreeView T, PlanView P, const double* __restrict_
         unsigned long long b;
         if (cfl_candidate<NDIM>(u, dx, gamma, cfl, pressure_cap, &b) && b < best) best = b;
     }
-    for (int o = 16; o > 0; o >>= 1) {
-        unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
-        best = other < best ? other : best;
-    }
-    if ((threadIdx.x & 31) == 0 && best != ~0ULL) atomicMin(&st->dtmin_bits, best);
+    block_atomic_min(best, &st->dtmin_bits);
 }
 
 __global__ void k_courant_init(DevStatus* st, double dt_start) {
