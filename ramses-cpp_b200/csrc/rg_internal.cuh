@@ -175,8 +175,8 @@ struct Plan {
     // a uniform level (one per child slot), so transfers are plain copies
     std::vector<std::pair<int, int>> read_runs, targ_runs, cell_runs;
     // targets with more than kLongEvents updates (coarse cells taking the
-    // refluxes of many finer faces), folded one warp each by k_fold_long and
-    // skipped by k_fold
+    // refluxes of many finer faces), folded one warp each by k_fold's first
+    // blocks and skipped by its others
     int nlong = 0;
     int* tlong = nullptr;      // [nlong] target indices
     int nbox = 0;              // ensemble level: number of boxes (0: one grid)
