@@ -234,3 +234,45 @@ def test_replayed_level_steps_match_reference(rgpu_lib, graphs):
             assert captured == 0 and replayed == 0
     finally:
         ctx.close()
+
+
+def test_captured_runs_follow_parameter_changes(rgpu_lib):
+    """Runs captured as graphs bake in the solver constants and the step's
+    configuration: after rg_set_params (here the Riemann solver) and after a
+    new Courant factor in the coarse step's configuration, the replayed steps
+    must match steps issued eagerly (graphs off) bit for bit."""
+    import rg_amr
+    out = []
+    for graphs in (True, False):
+        ctx = rgpu.Context(rgpu.make_params(3, slope_type=2, riemann="hllc", gamma=GAMMA), 0)
+        try:
+            ctx.amr_graphs(graphs)
+            rg_amr.initialize(ctx, 3, LMIN, LMAX, 30000, rg_amr.sedov_primitives(3, LMIN, GAMMA), GAMMA, ed=ED, ep=EP)
+            d = DeviceAmrRun(ctx, nx=1, levelmin=LMIN, nlevelmax=LMAX, cfl=0.25, ed=ED, ep=EP)
+            for _ in range(6):
+                d.coarse_step()
+            before = ctx.amr_graphs()
+            ctx.set_params(rgpu.make_params(3, slope_type=2, riemann="llf", gamma=GAMMA))
+            for _ in range(3):
+                d.coarse_step()
+            d.cfg.courant_factor = 0.2
+            for _ in range(3):
+                d.coarse_step()
+            a = ctx.tree_fetch(level_list_like())
+            out.append((a["uold"].copy(), a["son"].copy(), d.t, d.cell_updates, before, ctx.amr_graphs()))
+        finally:
+            ctx.close()
+    (u1, s1, t1, n1, b1, e1), (u2, s2, t2, n2, _, e2) = out
+    assert b1[1] > 0, b1  # runs were replayed before the changes
+    assert e1[0] > b1[0], (b1, e1)  # and captured again after them
+    assert e2 == (0, 0)
+    assert t1 == t2 and n1 == n2
+    assert np.array_equal(s1, s2) and bits_equal(u1, u2)
+
+
+def level_list_like():
+    """Level-list arrays of the right lengths for Context.tree_fetch on a tree
+    that rg_amr.initialize built on the device."""
+    import rg_tree
+    arrays = rg_tree.tree_arrays(rg_tree.build_uniform(3, LMIN, ngridmax=30000, nlevelmax=LMAX))
+    return {k: arrays[k] for k in ("headl", "taill", "numbl")}
