@@ -210,7 +210,8 @@ __device__ __forceinline__ int riemann(const double* ql, const double* qr, doubl
 // side 0, its left-face state (qp) for side 1.  qside, if not null, is the
 // rotated primitive state of neighbour cell n already in registers (the own
 // trace's stencil cell on that side); otherwise it is loaded here.
-template <int NDIM>
+// LEVEL0: 1 the plan is level 0's, 0 it is not, -1 read P.level0
+template <int NDIM, int LEVEL0 = -1>
 __device__ __forceinline__ void neighbour_face(const TreeView& T, const PlanView& P, const double* __restrict__ prim,
                                                const double* __restrict__ uold, size_t ncell, int p, int c, int idim,
                                                int side, int kd, int n, const double* qc, const double* qside,
@@ -229,7 +230,7 @@ __device__ __forceinline__ void neighbour_face(const TreeView& T, const PlanView
         if (kd & KIND_REFLECT) qb[1] *= -1.0;
         trace<NDIM>(qb, dq0, dt, D.dx, qm, qp, K.gamma);
     } else {
-        if (P.level0) {
+        if (LEVEL0 == 1 || (LEVEL0 < 0 && P.level0)) {
             // level 0 traces are unrotated first-order states (HydroSolver.cpp:77-91)
             double qn[NV], dq0[NV], qmn[NV], qpn[NV];
             load_rot<NDIM>(prim, ncell, n, 0, qn);
@@ -298,7 +299,9 @@ __device__ __forceinline__ void neighbour_face(const TreeView& T, const PlanView
 // the next launch (nothing ever waits on another block).
 constexpr int TILE = 32;
 
-template <int NDIM, int RS, int R, int MINB, bool BOXED>
+// LEVEL0: instantiated for level 0 (the coarse cells, first-order traces) or
+// for the other levels, so neither instance carries the other's code
+template <int NDIM, int RS, int R, int MINB, bool BOXED, bool LEVEL0 = false>
 __global__ void __launch_bounds__(TILE * NDIM * R, MINB)
     k_face_tiles(TreeView T, PlanView P, const double* __restrict__ prim, const double* __restrict__ uold,
                  double* __restrict__ flux, double* __restrict__ fsum, DevStatus* st, StepK K, int batch) {
@@ -336,7 +339,7 @@ __global__ void __launch_bounds__(TILE * NDIM * R, MINB)
                     if constexpr (BOXED) step_of_box(P, p, dt, D);
                     double qc[NV], qmo[NV], qpo[NV];
                     load_rot<NDIM>(prim, ncell, c, idim, qc);
-                    if (P.level0) {
+                    if constexpr (LEVEL0) {
                         double qn[NV], dq0[NV];
                         load_rot<NDIM>(prim, ncell, c, 0, qn);
 #pragma unroll
@@ -362,7 +365,7 @@ __global__ void __launch_bounds__(TILE * NDIM * R, MINB)
                         } else {
                             const int n = P.icn[(size_t)s * nc + p];
                             double qf[NV];
-                            neighbour_face<NDIM>(T, P, prim, uold, ncell, p, c, idim, side, kd, n, qc, nullptr,
+                            neighbour_face<NDIM, LEVEL0 ? 1 : 0>(T, P, prim, uold, ncell, p, c, idim, side, kd, n, qc, nullptr,
                                                  dt, D, K, qf);
                             if (side == 0) iters += riemann<NDIM, RS>(qf, qpo, f, K);
                             else iters += riemann<NDIM, RS>(qmo, qf, f, K);
@@ -434,10 +437,10 @@ inline bool boxed_variant_distinct(int v) {
     return v == kDefaultFaceVariant || v == kBoxedAltVariant || v == kFirstPipeVariant || v == kFirstBrickVariant;
 }
 
-template <int NDIM, int RS, int R, int MINB, bool BOXED = false>
+template <int NDIM, int RS, int R, int MINB, bool BOXED = false, bool LEVEL0 = false>
 int launch_face_one(rg_ctx* c, const Plan& P, const StepK& K, int batch, const double* uold, const double* prim,
                     double* flux, double* fsum) {
-    auto kern = k_face_tiles<NDIM, RS, R, MINB, BOXED>;
+    auto kern = k_face_tiles<NDIM, RS, R, MINB, BOXED, LEVEL0>;
     const int block = TILE * NDIM * R;
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, 0);
@@ -454,6 +457,8 @@ int launch_face_one(rg_ctx* c, const Plan& P, const StepK& K, int batch, const d
 template <int NDIM, int RS>
 int launch_face_rs(rg_ctx* c, const Plan& P, const StepK& K, int variant, int batch, const double* uold,
                    const double* prim, double* flux, double* fsum) {
+    // level 0 (coarse cells): the default shape only
+    if (P.level0) return launch_face_one<NDIM, RS, 1, 8, false, true>(c, P, K, batch, uold, prim, flux, fsum);
     if (P.nbox > 0) {
         // ensemble levels (per-box dt and dx): two shapes are instantiated
         if (variant == kBoxedAltVariant) return launch_face_one<NDIM, RS, 2, 4, true>(c, P, K, batch, uold, prim, flux, fsum);
