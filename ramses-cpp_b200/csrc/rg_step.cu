@@ -402,7 +402,13 @@ __global__ void k_fold_next(TreeView T, PlanView P, const double* __restrict__ f
             best_all = best < best_all ? best : best_all;
         }
     }
-    if constexpr (!BOXED) block_atomic_min(best_all, &st->dtmin_bits);
+    if constexpr (!BOXED) {
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long other = __shfl_xor_sync(0xffffffffu, best_all, o);
+            best_all = other < best_all ? other : best_all;
+        }
+        if (lane == 0 && best_all != ~0ULL) atomicMin(&st->dtmin_bits, best_all);
+    }
 }
 
 __global__ void k_copy_level(TreeView T, PlanView P, int nvar, const double* __restrict__ src, double* __restrict__ dst,
