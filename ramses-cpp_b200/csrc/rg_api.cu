@@ -230,7 +230,10 @@ int refresh_tree(rg_ctx* c) {
     for (size_t L = 0; L < c->lvl_ver.size(); ++L)
         if (c->lvl_ver[L] == old && !dirty(c->lists_dirty, L)) c->lvl_ver[L] = c->topo_version;
     c->plans_dirty = c->lists_dirty = 0;
-    if (int rc = rank_lists(c)) return rc;
+    // list ranks (pointer jumping over every oct) only when a list must be
+    // walked again: make_grid_fine and remove_grid_fine keep the cached lists
+    // of the levels they change in order themselves
+    c->ranked = false;
     if (int rc = compute_cell_levels(c)) return rc;
     return check_device_status(c);
 }

@@ -469,6 +469,15 @@ int build_plan_t(rg_ctx* c, int ilevel, Plan& P) {
             return RG_OK;
         }
         if (int rc = dalloc(c, &P.octs, P.noct, "octs")) return rc;
+        if (c->tree_resident) {
+            // the resident tree's cached list (kept in order by the tree
+            // operations, walked again only when it must be)
+            const int* lo = nullptr;
+            int ln = 0;
+            if (int rc = level_octs_cached(c, ilevel, &lo, &ln)) return rc;
+            if (ln != P.noct) return set_error(c, RG_ERR_TOPOLOGY, "level count and cached list disagree");
+            cudaMemcpyAsync(P.octs, lo, sizeof(int) * (size_t)P.noct, cudaMemcpyDeviceToDevice, s);
+        }
         int* d_count = c->d_scan;  // reuse scan scratch as a counter
         if (c->cap_scan < 4) {
             dev_free(c, c->d_scan);
@@ -476,12 +485,12 @@ int build_plan_t(rg_ctx* c, int ilevel, Plan& P) {
             c->cap_scan = 1024;
             d_count = c->d_scan;
         }
-        cudaMemsetAsync(d_count, 0, 2 * sizeof(int), s);
-        // with the tree resident the count is the host's: the chain is checked
-        // on the device and reported with the plan's read-back below
-        k_level_octs<<<nblk(c->ngridmax), TPB, 0, s>>>(c->ngridmax, c->d_jump, c->d_dist, head - 1, P.noct, P.octs,
-                                                       d_count, c->d_status, c->tree_resident);
         if (!c->tree_resident) {
+            if (!c->ranked)
+                if (int rc = rank_lists(c)) return rc;
+            cudaMemsetAsync(d_count, 0, 2 * sizeof(int), s);
+            k_level_octs<<<nblk(c->ngridmax), TPB, 0, s>>>(c->ngridmax, c->d_jump, c->d_dist, head - 1, P.noct, P.octs,
+                                                           d_count, c->d_status, false);
             cudaMemcpyAsync(&hv[0], d_count, sizeof(int), cudaMemcpyDeviceToHost, s);
             if (int rc = check_cuda(c, cudaStreamSynchronize(s), "level octs")) return rc;
             if (hv[0] != P.noct) return set_error(c, RG_ERR_TOPOLOGY, "level linked list merges with another chain");
@@ -622,6 +631,8 @@ int level_oct_list(rg_ctx* c, int ilevel, int* out, int cap, int* noct) {
     }
     const int n = dh + 1;
     if (n > cap) return set_error(c, RG_ERR_TOPOLOGY, "level list longer than ngridmax");
+    if (!c->ranked)
+        if (int rc = rank_lists(c)) return rc;
     if (c->cap_scan < 4) {
         dev_free(c, c->d_scan);
         if (int rc = dalloc(c, &c->d_scan, 1024, "scan scratch")) return rc;

@@ -657,10 +657,33 @@ __global__ void __launch_bounds__(1024) k_tail_cascade(TreeMut M, LevelLists R) 
 int hidx(const rg_ctx* c, int ilevel) { return ilevel * (c->ncpu + c->nboundary); }
 
 // A change of the tree's links reaches the plans of levels lo..hi (bits of
-// levels above 63 are implied) and the oct list of level `list`.
+// levels above 63 are implied) and the oct list of level `list` (-1: none).
 void mark_changed(rg_ctx* c, int lo, int hi, int list) {
     for (int L = lo < 0 ? 0 : lo; L <= hi && L <= 63; ++L) c->plans_dirty |= 1ull << L;
     if (list >= 0 && list <= 63) c->lists_dirty |= 1ull << list;
+}
+
+// The cached oct list of level L (current before the change) made the
+// level's list after it: `keep` entries from the old list's start, then the
+// `add` octs (device, in list order) after them.  false (nothing done) when
+// the list is not cached; it is then walked again after the refresh.
+bool keep_cached_list(rg_ctx* c, int L, int keep, const int* add, int nadd) {
+    if (L < 0 || (int)c->lvl_ver.size() <= L || c->lvl_ver[(size_t)L] != c->topo_version) return false;
+    const size_t l = (size_t)L;
+    const int need = keep + nadd;
+    if (need > c->lvl_cap[l]) {
+        const int cap = (need + 1023) / 1024 * 1024;
+        int* grown = nullptr;
+        if (dev_alloc(c, &grown, sizeof(int) * (size_t)cap) != cudaSuccess) return false;
+        if (keep > 0) cudaMemcpyAsync(grown, c->lvl_octs[l], sizeof(int) * (size_t)keep, cudaMemcpyDeviceToDevice, c->stream);
+        dev_free(c, c->lvl_octs[l]);
+        c->lvl_octs[l] = grown;
+        c->lvl_cap[l] = cap;
+    }
+    if (nadd > 0)
+        cudaMemcpyAsync(c->lvl_octs[l] + keep, add, sizeof(int) * (size_t)nadd, cudaMemcpyDeviceToDevice, c->stream);
+    c->lvl_n[l] = need;
+    return true;
 }
 
 // RG_OK to go on, kNoOp when the call does nothing (ilevel >= nlevelmax, where
@@ -979,8 +1002,12 @@ int tree_make_grid_fine(rg_ctx* c, int ilevel, int* changed) {
     // refining level-L cells changes their son links (the plan of level L),
     // adds octs to list L + 1 (its plan and list), and changes which cells
     // exist at level L + 1, hence the neighbour and ghost-stencil cells of
-    // levels L + 1 and L + 2; level L - 1 is included as a margin
-    mark_changed(c, ilevel - 1, ilevel + 2, ilevel + 1);
+    // levels L + 1 and L + 2; level L - 1 is included as a margin.  The new
+    // octs follow list L + 1's old tail in rank order (k_link_chain), so its
+    // cached list stays in order with them appended.
+    const int L1 = ilevel + 1;
+    const int kept = ((int)c->lvl_n.size() > L1) ? c->lvl_n[(size_t)L1] : 0;
+    mark_changed(c, ilevel - 1, ilevel + 2, keep_cached_list(c, L1, kept, S.list, n) ? -1 : L1);
     if (changed) *changed = n;
     if (int rc = check_cuda(c, cudaGetLastError(), "make_grid_fine kernels")) return rc;
     return check_device_status(c);
@@ -1025,8 +1052,9 @@ int tree_remove_grid_fine(rg_ctx* c, int ilevel, int* changed) {
     c->tree_dirty = true;
     // removing level-L octs changes list L (its plan and list), the son links
     // of their fathers (the plan of level L - 1) and the ghost-stencil cells of
-    // level L + 1; level L - 2 is included as a margin
-    mark_changed(c, ilevel - 2, ilevel + 1, ilevel);
+    // level L + 1; level L - 2 is included as a margin.  The kept octs, in
+    // list order (k_kill), are the level's list now.
+    mark_changed(c, ilevel - 2, ilevel + 1, keep_cached_list(c, ilevel, 0, S.list, m) ? -1 : ilevel);
     if (changed) *changed = nkill;
     if (int rc = check_cuda(c, cudaGetLastError(), "remove_grid_fine kernels")) return rc;
     return check_device_status(c);
