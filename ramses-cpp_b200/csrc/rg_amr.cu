@@ -60,14 +60,16 @@ int nsubcycle(const rg_amr_config& cfg, int il) { return il >= cfg.levelmin ? 2 
 // the level step proper (dt, primitives, face, fold with set_uold),
 // restrict_fine and flag_fine; on a level without finer octs both halves and
 // the time update form one segment.  The host waits only at the change
-// probes, so the segments between two probes -- a run -- form one graph: a
-// run is issued eagerly the first time at a topology version (which warms
-// every cache its segments touch: the plans, the autotuned face shapes, the
-// flux scratch size, the level oct lists), captured whole the second time,
-// and replayed from then on until the tree changes (the topology version
-// moves), a scratch buffer it names is reallocated or the configuration
-// differs.  A replay is launched at the run's start; the host still walks the
-// step's recursion (the probes and the counts depend on it), issuing nothing.  A
+// probes, so the segments between two probes -- a run -- form one graph.  At
+// a run's first visit at a topology version every cache its segments touch is
+// prepared (the plans, the face shapes, the flux scratch size, the level oct
+// lists: prepare_run) and the run is captured whole; it is replayed from then
+// on until the tree changes (the topology version moves), a scratch buffer it
+// names is reallocated or the configuration differs.  When the preparation
+// cannot finish (a level whose face shape waits to be timed) the run goes
+// eagerly once, which warms the rest, and is captured at its next visit.  A
+// replay is launched at the run's start; the host still walks the step's
+// recursion (the probes and the counts depend on it), issuing nothing.  A
 // captured run calls nothing that waits or allocates: a segment that is not
 // ready for capture ends the capture there, the part captured so far is
 // launched and the rest of the run goes eagerly.
