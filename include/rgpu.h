@@ -458,8 +458,9 @@ typedef struct rg_amr_clock {
 int rg_amr_coarse_step(rg_ctx* ctx, const rg_amr_config* cfg, rg_amr_clock* clock);
 /* No reference counterpart.  Between tree changes rg_amr_coarse_step replays
  * its level steps as CUDA graphs: the segments between two of the host's
- * waits (the change probes) form a run, captured whole on the second visit at
- * a topology and replayed until the tree changes.  on > 0 / on == 0 switches
+ * waits (the change probes) form a run, captured whole at its first visit at
+ * a topology (after the plans and other caches it reads are prepared) and
+ * replayed until the tree changes.  on > 0 / on == 0 switches
  * that on or off (on < 0 leaves it; the RG_AMR_GRAPHS=0 environment variable
  * sets the initial value off); *captured and *replayed (either may be null)
  * get the context's counts of captured and replayed runs.  Changing the
